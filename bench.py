@@ -1,0 +1,417 @@
+#!/usr/bin/env python3
+"""Benchmark of the stwo commit path on B200 (one JSON line on rank 0).
+
+Workloads (seeded synthetic M31 data, values uniform in [0, P)):
+  commit_uneven  512 columns, log sizes U{12..22}, blowup 2, one lifted
+                 Blake2s tree (L = 24): interpolate -> evaluate -> leaves ->
+                 nodes.  Unit: committed trace cells / s.
+  commit_plain   32 columns of log 16, blowup 1: bit-reverse -> interpolate ->
+                 evaluate -> Merkle (L = 17).
+
+A step is one commit of the whole trace.  `value` is device-timed with inputs
+resident in HBM; `e2e` goes through the same public calls with the trace in
+pinned host memory (H2D copy of the trace + D2H of the root inside every
+step).  Multi-GPU runs are independent replicas (weak scaling, no collective).
+`--impl reference` times the CPU restatement of stwo's SimdBackend (the
+oracle port; Rust/SimdBackend itself cannot be built here) on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "stwo-metal_b200"))
+
+P = (1 << 31) - 1
+METRIC = "proved trace cells/s, batched vs per-column on B200 (bit-exact); p99 prove ms"
+
+
+def load_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# ------------------------------------------------------------ workloads ----
+def workload_spec(name: str):
+    if name == "commit_uneven":
+        r = np.random.default_rng(3)
+        logs = [int(x) for x in r.integers(12, 23, 512)]
+        return dict(name=name, logs=logs, blowup=2, bitrev=False, seed=3)
+    if name == "commit_plain":
+        return dict(name=name, logs=[16] * 32, blowup=1, bitrev=True, seed=1)
+    raise SystemExit(f"unknown workload {name}")
+
+
+def make_columns(spec):
+    r = np.random.default_rng(spec["seed"] + 1000)
+    return [r.integers(0, P, 1 << l, dtype=np.uint32) for l in spec["logs"]]
+
+
+# ---------------------------------------------------------- clock sampling --
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except FileNotFoundError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sms, maxes, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sms.append(float(parts[1]))
+                maxes.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sms) if sms else None, "sm_max_mhz": max(maxes) if maxes else None,
+                "reasons": sorted(reasons), "samples": len(sms)}
+
+
+# ------------------------------------------------------------ dist helpers --
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    return world, rank, local
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+# --------------------------------------------------------- CPU reference ----
+def cpu_commit_rate(spec, host_cols, budget_s=15.0, threads=None):
+    """Oracle commit of a bounded sample of the workload's columns; returns
+    (cells/s, sample description, threads)."""
+    from oracle import ffi as oracle
+    n_threads = oracle.set_threads(threads or os.cpu_count() or 1)
+    blowup = spec["blowup"]
+    maxlog = max(spec["logs"]) + blowup
+    init, lg = oracle.canonic_half_coset_root(maxlog + 1)
+    tw, itw = oracle.precompute_twiddles(init, lg)
+    # sample: columns in workload order until ~1/16 of the cells (bounded)
+    order = list(range(len(host_cols)))
+    total = sum(c.size for c in host_cols)
+    target = max(total // 16, host_cols[0].size)
+    take, cells = [], 0
+    for i in order:
+        if cells >= target:
+            break
+        take.append(i)
+        cells += host_cols[i].size
+    cols = [host_cols[i] for i in take]
+    L = max(spec["logs"][i] for i in take) + blowup
+    reps, elapsed = 0, 0.0
+    while elapsed < budget_s or reps == 0:
+        t0 = time.perf_counter()
+        src = [oracle.bit_reverse(c) for c in cols] if spec["bitrev"] else cols
+        coeffs = oracle.interpolate_columns(src, itw)
+        evals = oracle.evaluate_columns(coeffs, blowup, tw)
+        oracle.merkle_build_layers(evals, L)
+        elapsed += time.perf_counter() - t0
+        reps += 1
+        if elapsed > budget_s / 3 and reps >= 1:
+            break
+    rate = reps * cells / elapsed
+    return rate, f"{len(take)} of {len(host_cols)} columns ({cells} cells, lifted L={L}), {reps} rep(s)", n_threads
+
+
+def run_reference(args, spec, world, rank):
+    if rank != 0:
+        return
+    host_cols = make_columns(spec)
+    from oracle import ffi as oracle
+    n_threads = oracle.set_threads(os.cpu_count() or 1)
+    rates = []
+    for i in range(args.warmup + args.steps):
+        rate, sample, n_threads = cpu_commit_rate(spec, host_cols, budget_s=4.0)
+        if i >= args.warmup:
+            rates.append(rate)
+    value = statistics.median(rates)
+    cells = sum(c.size for c in host_cols)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "committed trace cells/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000.0 * cells / value, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u32 (M31)", "data": "synthetic (seeded numpy PCG64, uniform [0, 2^31-1))",
+        "config": {"workload": spec["name"], "n_columns": len(spec["logs"]), "log_sizes": "U{12..22}"
+                   if spec["name"] == "commit_uneven" else "16", "log_blowup": spec["blowup"],
+                   "parallelism": f"replicas x{args.gpus}"},
+        "cpu_baseline": {"value": value, "unit": "committed trace cells/s", "cores": n_threads, "kind": "port",
+                         "sample": "per step: " + sample + "; SimdBackend restatement (C++, OpenMP)"},
+        "e2e": {"value": value, "unit": "committed trace cells/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------- B200 ------
+def run_b200(args, spec, world, rank, local):
+    import torch
+    from stwo_b200 import B200Backend, DeviceBuffer, DeviceColumn, ffi, layer_to_host
+    from stwo_b200.backend import canonic_half_coset
+
+    torch.cuda.set_device(local)
+    ffi.init(local)
+    stream = torch.cuda.Stream()
+    be = B200Backend(stream.cuda_stream)
+    logs, blowup = spec["logs"], spec["blowup"]
+    host_cols = make_columns(spec)
+    order = sorted(range(len(logs)), key=lambda i: logs[i])  # stable by length
+    L = max(logs) + blowup
+    init, lg = canonic_half_coset(L + 1)
+    tree = be.precompute_twiddles(init, lg)
+    inputs = [DeviceColumn.from_host(c, stream.cuda_stream) for c in host_cols]
+    coeffs = [DeviceColumn(c.size, stream.cuda_stream) for c in host_cols]
+    evals = [DeviceColumn(c.size << blowup, stream.cuda_stream) for c in host_cols]
+    layers = [DeviceBuffer(32 << k, stream.cuda_stream) for k in range(L + 1)]
+    evals_sorted = [evals[i] for i in order]
+    cells = sum(c.size for c in host_cols)
+    eval_cells = cells << blowup
+    n_leaf_blocks = (len(logs) + 15) // 16
+    torch.cuda.synchronize()
+
+    phases = ["bitrev", "ifft", "rfft", "leaves", "nodes"]
+
+    def step(evs=None):
+        if spec["bitrev"]:
+            # bit-reverse the natural-order trace into the coefficient buffers,
+            # then interpolate in place.
+            for s_, d_ in zip(inputs, coeffs):
+                ffi.call("stwo_b200_memcpy_d2d", ffi_ptr(d_), ffi_ptr(s_), size_t(s_.nbytes), be.stream)
+                be.bit_reverse_column(d_)
+            rec(evs, 0)
+            be.interpolate_columns(coeffs, tree)
+        else:
+            rec(evs, 0)
+            be.interpolate_columns_into(inputs, coeffs, tree)
+        rec(evs, 1)
+        be.evaluate_polynomials_into(coeffs, blowup, tree, evals)
+        rec(evs, 2)
+        be.build_leaves_into(evals_sorted, L, layers[L])
+        rec(evs, 3)
+        be.build_nodes(layers)
+        rec(evs, 4)
+
+    import ctypes
+
+    def ffi_ptr(b):
+        return ctypes.c_void_p(b.ptr)
+
+    def size_t(n):
+        return ctypes.c_size_t(n)
+
+    def rec(evs, i):
+        if evs is not None:
+            evs[i].record(stream)
+
+    def new_events():
+        return [torch.cuda.Event(enable_timing=True) for _ in range(6)]
+
+    # correctness gate on the first step: the root must match the oracle for
+    # commit_plain (whole workload) -- commit_uneven is checked by the tests.
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            step()
+    torch.cuda.synchronize()
+    root = bytes(layer_to_host(layers[0])[0])
+
+    # ---- device-timed region ----
+    sampler = ClockSampler(local)
+    barrier(world)
+    torch.cuda.synchronize()
+    sampler.start()
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    all_evs = [new_events() for _ in range(args.steps)]
+    launches0 = ffi.launch_count()
+    with torch.cuda.stream(stream):
+        t_start.record(stream)
+        for k in range(args.steps):
+            evs = all_evs[k]
+            evs[5].record(stream)
+            step(evs)
+        t_end.record(stream)
+    torch.cuda.synchronize()
+    launches = ffi.launch_count() - launches0
+    ms = t_start.elapsed_time(t_end) / args.steps
+    clocks = sampler.stop()
+    barrier(world)
+    ms = max_over_ranks(ms, world)
+    phase_ms = {p: 0.0 for p in phases}
+    for evs in all_evs:
+        phase_ms["bitrev"] += evs[5].elapsed_time(evs[0])
+        phase_ms["ifft"] += evs[0].elapsed_time(evs[1])
+        phase_ms["rfft"] += evs[1].elapsed_time(evs[2])
+        phase_ms["leaves"] += evs[2].elapsed_time(evs[3])
+        phase_ms["nodes"] += evs[3].elapsed_time(evs[4])
+    for p in phase_ms:
+        phase_ms[p] /= args.steps
+
+    # ---- e2e: host trace -> device -> commit -> root to host ----
+    pinned = []
+    for c in host_cols:
+        t = torch.empty(c.size, dtype=torch.int32).pin_memory()
+        t.numpy().view(np.uint32)[:] = c
+        pinned.append(t)
+    root_host = torch.empty(32, dtype=torch.uint8).pin_memory()
+    h2d = sum(c.nbytes for c in host_cols)
+
+    def e2e_step():
+        for t, d in zip(pinned, inputs):
+            ffi.call("stwo_b200_memcpy_h2d", ffi_ptr(d), ctypes.c_void_p(t.data_ptr()), size_t(d.nbytes), be.stream)
+        step()
+        ffi.call("stwo_b200_memcpy_d2h", ctypes.c_void_p(root_host.data_ptr()), ffi_ptr(layers[0]), size_t(32),
+                 be.stream)
+        ffi.call("stwo_b200_stream_sync", be.stream)
+
+    with torch.cuda.stream(stream):
+        for _ in range(max(1, args.warmup // 2)):
+            e2e_step()
+    barrier(world)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        e0.record(stream)
+        for _ in range(args.steps):
+            e2e_step()
+        e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, world)
+    assert bytes(root_host.numpy()) == root, "e2e root differs from device-resident root"
+
+    if rank != 0:
+        return
+    hbm_peak, peak_kind = load_peaks()
+    # algorithmic bytes per phase (inputs + outputs once; twiddles excluded)
+    alg_bytes = {
+        "bitrev": 8 * cells if spec["bitrev"] else 0,
+        "ifft": 8 * cells,
+        "rfft": 4 * cells + 4 * eval_cells,
+        "leaves": 4 * eval_cells + 32 * (1 << L),
+        "nodes": 32 * (1 << L) + 32 * ((1 << L) - 1),
+    }
+    dominant = max(("ifft", "rfft", "leaves", "nodes"), key=lambda p: phase_ms[p])
+    achieved = alg_bytes[dominant] / (phase_ms[dominant] * 1e-3) / 1e9
+    compressions = (1 << L) * n_leaf_blocks
+    cpu_rate, cpu_sample, cpu_cores = cpu_commit_rate(spec, host_cols, budget_s=10.0)
+    line = {
+        "metric": METRIC,
+        "value": cells / (ms * 1e-3),
+        "unit": "committed trace cells/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "u32 (M31)",
+        "data": "synthetic (seeded numpy PCG64, uniform [0, 2^31-1))",
+        "config": {"workload": spec["name"], "n_columns": len(logs), "total_trace_cells": cells,
+                   "log_sizes": "U{12..22} seed 3" if spec["name"] == "commit_uneven" else "16",
+                   "log_blowup": blowup, "lifting_log_size": L, "merkle": "lifted Blake2s",
+                   "l2": "inputs larger than L2 (no flush)", "parallelism": f"replicas x{world}"},
+        "clocks": clocks,
+        "gpu_launches": launches,
+        "e2e": {"value": cells / (e2e_ms * 1e-3), "unit": "committed trace cells/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": 32, "ms_per_step": e2e_ms},
+        "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                     "frac": achieved / hbm_peak, "peak_kind": peak_kind, "traffic": None,
+                     "alg_bytes_per_step": alg_bytes[dominant]},
+        "phases_ms": phase_ms,
+        "blake2s_compressions_per_s": compressions / (phase_ms["leaves"] * 1e-3),
+        "cpu_baseline": {"value": cpu_rate, "unit": "committed trace cells/s", "cores": cpu_cores, "kind": "port",
+                         "sample": cpu_sample + "; SimdBackend restatement (C++ oracle, OpenMP)"},
+        "root": root.hex(),
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="commit_uneven", choices=["commit_uneven", "commit_plain"])
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    spec = workload_spec(args.workload)
+    world, rank, local = dist_setup()
+    try:
+        if args.impl == "reference":
+            run_reference(args, spec, world, rank)
+        else:
+            run_b200(args, spec, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

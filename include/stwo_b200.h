@@ -1,0 +1,181 @@
+/*
+ * stwo_b200 — B200-native (sm_100a) backend for stwo's Circle-STARK commit +
+ * FRI path.  Flat C ABI: plain pointers and sizes, no torch types.
+ *
+ * Conventions
+ *  - Every entry point returns 0 on success or a negative STWO_B200_E* code,
+ *    and writes a NUL-terminated message into (err, err_len) when err != NULL.
+ *    No entry point aborts the process.
+ *  - Pointers named d_* are device pointers on the context's device.  Arrays
+ *    of device pointers (e.g. `uint32_t* const* d_cols`) are HOST arrays whose
+ *    elements are device pointers.
+ *  - `stream` is a cudaStream_t passed as void* (NULL = legacy default
+ *    stream).  Work is enqueued; nothing synchronises unless documented.
+ *  - Field elements are u32 words: M31 in [0, 2^31-1); QM31 columns are four
+ *    M31 coordinate columns (SecureColumnByCoords layout).
+ *  - Columns are evaluations in bit-reversed circle-domain order, or
+ *    coefficients in natural order (CpuBackend order), exactly as stwo's
+ *    CircleEvaluation<_, _, BitReversedOrder> / CircleCoefficients.
+ *  - Twiddle trees use CpuBackend's layout with canonical values (SimdBackend
+ *    stores the same values doubled): 2^R words for a root coset of log size
+ *    R.  Every domain used with a tree must be a doubling of its root coset.
+ *
+ * Reference interfaces replaced (paths relative to the vendored stwo crate
+ * vendor/stwo-upstream-dev-62b228e/crates/stwo/src/ of teddyjfpender/stwo-metal,
+ * and to crates/stwo-metal-sys/src/raw.rs for the reference's CUDA ABI):
+ */
+#ifndef STWO_B200_H
+#define STWO_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  STWO_B200_OK = 0,
+  STWO_B200_EARG = -1,     /* invalid argument (size, alignment, null) */
+  STWO_B200_ECUDA = -2,    /* CUDA runtime error */
+  STWO_B200_ENOMEM = -3,   /* device allocation failed */
+  STWO_B200_ETIMEOUT = -4, /* a bounded device wait gave up */
+  STWO_B200_ESTATE = -5    /* call not valid in the current state */
+};
+
+/* ------------------------------------------------------------ runtime --- */
+/* Library version string. */
+const char* stwo_b200_version(void);
+
+/* Number of kernels launched by this library since load (all threads). */
+uint64_t stwo_b200_launch_count(void);
+
+/* Selects `device`, checks it is sm_100 and prepares the stream-ordered
+ * memory pool.  Replaces the reference's global runtime probe
+ * (crates/stwo-metal-sys/src/metal.rs:4424-4448 metal_runtime_support). */
+int stwo_b200_init(int device, char* err, size_t err_len);
+
+/* Device memory from the stream-ordered pool (cudaMallocAsync).  Replaces
+ * cuda_malloc_uint32_t / cuda_free_memory (raw.rs:57,71). */
+int stwo_b200_alloc(size_t bytes, void** d_out, void* stream, char* err, size_t err_len);
+int stwo_b200_free(void* d_ptr, void* stream, char* err, size_t err_len);
+/* Async copies; host buffers should be pinned for overlap.  Replace
+ * copy_uint32_t_vec_from_{host_to_device,device_to_host} (raw.rs:43-50). */
+int stwo_b200_memcpy_h2d(void* d_dst, const void* h_src, size_t bytes, void* stream, char* err, size_t err_len);
+int stwo_b200_memcpy_d2h(void* h_dst, const void* d_src, size_t bytes, void* stream, char* err, size_t err_len);
+int stwo_b200_memcpy_d2d(void* d_dst, const void* d_src, size_t bytes, void* stream, char* err, size_t err_len);
+int stwo_b200_memset(void* d_dst, int value, size_t bytes, void* stream, char* err, size_t err_len);
+int stwo_b200_stream_create(void** stream_out, char* err, size_t err_len);
+int stwo_b200_stream_destroy(void* stream, char* err, size_t err_len);
+int stwo_b200_stream_sync(void* stream, char* err, size_t err_len);
+/* Pinned host memory for the e2e copies. */
+int stwo_b200_host_alloc(size_t bytes, void** h_out, char* err, size_t err_len);
+int stwo_b200_host_free(void* h_ptr, char* err, size_t err_len);
+
+/* ------------------------------------------------------------ ColumnOps -- */
+/* ColumnOps<BaseField>::bit_reverse_column (prover/backend/mod.rs:37-39;
+ * SimdBackend prover/backend/simd/bit_reverse.rs:22-33), in place.  Replaces
+ * bit_reverse_base_field (raw.rs:77). */
+int stwo_b200_bit_reverse_column(uint32_t* d_col, uint32_t log_size, void* stream, char* err, size_t err_len);
+
+/* -------------------------------------------------------------- PolyOps -- */
+/* PolyOps::precompute_twiddles (prover/poly/circle/ops.rs:144; SimdBackend
+ * prover/backend/simd/circle.rs:449-486) for the coset
+ * (initial_index, log_size): writes 2^log_size twiddles and their inverses.
+ * Replaces precompute_twiddles (raw.rs:84-88). */
+int stwo_b200_precompute_twiddles(uint64_t initial_index, uint32_t log_size, uint32_t* d_twiddles,
+                                  uint32_t* d_itwiddles, void* stream, char* err, size_t err_len);
+
+/* PolyOps::interpolate_columns (prover/poly/circle/ops.rs:29-40 ->
+ * PolyOps::interpolate ops.rs:24, simd/circle.rs:138-166): in place, evaluation ->
+ * coefficients, for n_cols columns of sizes 2^log_sizes[i] on canonic
+ * circle domains.  `half_initial_indices` may be NULL (canonic domains) or
+ * give each domain's half-coset initial index (only read for log size <= 2).
+ * Replaces ntt_b2n_column (raw.rs:472-479). */
+int stwo_b200_interpolate_columns(uint32_t* const* d_cols, const uint32_t* log_sizes,
+                                  const uint64_t* half_initial_indices, uint32_t n_cols, const uint32_t* d_itwiddles,
+                                  uint32_t tree_log_size, void* stream, char* err, size_t err_len);
+
+/* Out-of-place form of stwo_b200_interpolate_columns: reads d_evals[i],
+ * writes d_coeffs[i] (stwo's interpolate consumes its evaluation; this form
+ * leaves it intact at no extra traffic). */
+int stwo_b200_interpolate_columns_into(const uint32_t* const* d_evals, uint32_t* const* d_coeffs,
+                                       const uint32_t* log_sizes, const uint64_t* half_initial_indices,
+                                       uint32_t n_cols, const uint32_t* d_itwiddles, uint32_t tree_log_size,
+                                       void* stream, char* err, size_t err_len);
+
+/* PolyOps::evaluate_polynomials (prover/poly/circle/ops.rs:110-211 ->
+ * evaluate_into, simd/circle.rs:388-443): coefficients (2^log_sizes[i]) ->
+ * evaluations on CanonicCoset(log_sizes[i] + log_blowup), bit-reversed.
+ * Replaces evaluate_columns (raw.rs:90-97). */
+int stwo_b200_evaluate_polynomials(const uint32_t* const* d_coeffs, const uint32_t* log_sizes, uint32_t n_cols,
+                                   uint32_t log_blowup, uint32_t* const* d_evals, const uint32_t* d_twiddles,
+                                   uint32_t tree_log_size, void* stream, char* err, size_t err_len);
+
+/* ------------------------------------------------------ MerkleOpsLifted -- */
+/* MerkleOpsLifted<Blake2sMerkleHasherGeneric<m31_output>>::build_leaves
+ * (prover/vcs_lifted/ops.rs:14-15; spec prover/backend/cpu/merkle_lifted.rs:
+ * 44-78).  Columns must already be sorted by non-decreasing log size.
+ * Writes 2^lifting_log_size 32-byte leaves (1 leaf when n_cols == 0).
+ * Replaces commit_on_first_layer_lifted (raw.rs:176-183). */
+int stwo_b200_merkle_build_leaves(const uint32_t* const* d_cols, const uint32_t* log_sizes, uint32_t n_cols,
+                                  uint32_t lifting_log_size, int m31_output, uint8_t* d_leaves, void* stream,
+                                  char* err, size_t err_len);
+
+/* MerkleOpsLifted::build_next_layer (prover/vcs_lifted/ops.rs:19;
+ * cpu/merkle_lifted.rs:80-85): 2^prev_log_size hashes -> half as many. */
+int stwo_b200_merkle_build_next_layer(const uint8_t* d_prev, uint32_t prev_log_size, int m31_output,
+                                      uint8_t* d_out, void* stream, char* err, size_t err_len);
+
+/* MerkleOpsLifted::build_merkle_layers (prover/vcs_lifted/ops.rs:29-45):
+ * stable-sorts the columns by length, builds leaves and all node layers.
+ * d_layers[k] (k = 0..lifting_log_size, root first) receives 2^k hashes. */
+int stwo_b200_merkle_build_layers(const uint32_t* const* d_cols, const uint32_t* log_sizes, uint32_t n_cols,
+                                  uint32_t lifting_log_size, int m31_output, uint8_t* const* d_layers,
+                                  void* stream, char* err, size_t err_len);
+
+/* Node layers of a lifted tree whose leaves are already in
+ * d_layers[lifting_log_size]: fills d_layers[lifting_log_size-1 .. 0]
+ * (the second half of build_merkle_layers, prover/vcs_lifted/ops.rs:39-43). */
+int stwo_b200_merkle_build_nodes(uint8_t* const* d_layers, uint32_t lifting_log_size, int m31_output,
+                                 void* stream, char* err, size_t err_len);
+
+/* ------------------------------------------------------------ MerkleOps -- */
+/* MerkleOps<Blake2sMerkleHasherGeneric<m31_output>>::commit_on_layer
+ * (prover/vcs/ops.rs:24-28; cpu/blake2s.rs:13-26): node i = Blake2s(
+ * prev[2i] || prev[2i+1] (when d_prev != NULL) || LE32(col[i]) for cols).
+ * Replaces commit_on_layer_with_previous / commit_on_first_layer
+ * (raw.rs:169-190). */
+int stwo_b200_commit_on_layer(uint32_t log_size, const uint8_t* d_prev, const uint32_t* const* d_cols,
+                              uint32_t n_cols, int m31_output, uint8_t* d_out, void* stream, char* err,
+                              size_t err_len);
+
+/* -------------------------------------------------------------- FriOps --- */
+/* FriOps::fold_line (prover/fri.rs:39-50; simd/fri.rs:32-122): 4 coordinate
+ * columns of a line evaluation of size 2^log_size on a domain in the tree's
+ * tower -> 2^(log_size - fold_step).  alpha = 4 M31 words.
+ * Replaces fold_line (raw.rs:142-149). */
+int stwo_b200_fold_line(const uint32_t* const* d_in4, uint32_t log_size, const uint32_t* alpha,
+                        uint32_t fold_step, const uint32_t* d_itwiddles, uint32_t tree_log_size,
+                        uint32_t* const* d_out4, void* stream, char* err, size_t err_len);
+
+/* FriOps::fold_circle_into_line (prover/fri.rs:61-69; simd/fri.rs:124-172):
+ * dst (2^(log_size-1)) <- dst * alpha^2 + fold(src (2^log_size)).
+ * `half_initial_index` is the source circle domain's half-coset initial
+ * index (read only for log_size <= 4).  Replaces fold_circle_into_line
+ * (raw.rs:151-158). */
+int stwo_b200_fold_circle_into_line(uint32_t* const* d_dst4, const uint32_t* const* d_src4, uint32_t log_size,
+                                    uint64_t half_initial_index, const uint32_t* alpha,
+                                    const uint32_t* d_itwiddles, uint32_t tree_log_size, void* stream, char* err,
+                                    size_t err_len);
+
+/* FriOps::decompose (prover/fri.rs:92-104; simd/fri.rs:174-195,265-296):
+ * g = f -/+ lambda; lambda (4 words) is written to host memory (the call
+ * synchronises `stream`). */
+int stwo_b200_decompose(const uint32_t* const* d_in4, uint32_t log_size, uint32_t* const* d_out4,
+                        uint32_t* lambda_out, void* stream, char* err, size_t err_len);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* STWO_B200_H */

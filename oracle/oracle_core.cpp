@@ -367,22 +367,21 @@ void fold_circle_into_line(uint32_t* const dst[4], const uint32_t* const src[4],
   }
 }
 
-// prover/backend/simd/fri.rs:174-195 decompose + :265-296 coefficient.  With
-// fewer than 16 elements the packed loop sums nothing, so lambda = 0.
+// prover/backend/simd/fri.rs:174-195 decompose + :265-296 coefficient, on
+// 16-lane packed vectors: the coefficient adds vectors [0, (n/16)/2) and
+// subtracts vectors [(n/16)/2, n/16) (so n < 16 gives lambda = 0 and n = 16
+// gives -sum/16); g subtracts lambda on vectors [0, ceil(n/16)/2) and adds it
+// on the rest.
 QM31 decompose(const uint32_t* const in[4], uint32_t log_n, uint32_t* const out[4]) {
   size_t n = (size_t)1 << log_n;
-  QM31 lambda = QM31::zero();
-  if (n >= 16) {
-    uint32_t s[4] = {0, 0, 0, 0};
-    for (int k = 0; k < 4; k++) {
-      for (size_t i = 0; i < n / 2; i++) s[k] = add(s[k], in[k][i]);
-      for (size_t i = n / 2; i < n; i++) s[k] = sub(s[k], in[k][i]);
-    }
-    lambda = qmul_m31(QM31::from(s[0], s[1], s[2], s[3]), inv((uint32_t)n));
+  size_t range = n / 16, half_a = range / 2;
+  uint32_t s[4] = {0, 0, 0, 0};
+  for (int k = 0; k < 4; k++) {
+    for (size_t i = 0; i < 16 * half_a; i++) s[k] = add(s[k], in[k][i]);
+    for (size_t i = 16 * half_a; i < 16 * range; i++) s[k] = sub(s[k], in[k][i]);
   }
-  // g: packed index range [0, half_range) subtracts, the rest adds; half_range
-  // = ceil(n/16)/2 packed vectors.
-  size_t range = (n + 15) / 16, half_range = range / 2;
+  QM31 lambda = qmul_m31(QM31::from(s[0], s[1], s[2], s[3]), inv((uint32_t)n));
+  size_t half_range = ((n + 15) / 16) / 2;
   for (size_t i = 0; i < n; i++) {
     QM31 v = QM31::from(in[0][i], in[1][i], in[2][i], in[3][i]);
     QM31 r = (i / 16 < half_range) ? v - lambda : v + lambda;

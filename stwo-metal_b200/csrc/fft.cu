@@ -1,0 +1,485 @@
+// Circle FFT (PolyOps::interpolate / evaluate) and bit reversal for sm_100a.
+//
+// A transform of n butterfly layers runs as 1-3 passes.  A pass covers the
+// consecutive layers [layer0, layer0 + T) on tiles of 2^T rows x 2^C columns
+// held in shared memory: row r, column c of tile (hi, lo) is element
+//   g = hi * 2^(layer0 + T) + r * 2^layer0 + lo * 2^C + c,
+// so a tile row is 2^C contiguous words (C = 3: one 32-byte sector) and every
+// butterfly of the pass stays inside the tile.  Inside the tile, layers run in
+// register stages of up to 4 (radix-16 per thread); stages exchange through
+// shared memory.  Butterflies and layer order follow
+// crates/stwo/src/prover/backend/cpu/circle.rs:28-80,199-250 (fft_layer_loop
+// :313-327): IFFT layer 0 (circle) upward, then x n^-1; RFFT top layer down to
+// the circle layer.  Twiddles are read from the tree tail exactly as
+// core/poly/utils.rs:98-114 slices it; circle-layer twiddles are derived from
+// line layer 1 as [y, -y, -x, x] (cpu/circle.rs:332-354).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "common.cuh"
+#include "field.cuh"
+
+namespace stwo_b200 {
+
+// A column table passed by value: up to kFftMaxCols (src, dst) pairs per launch.
+constexpr int kFftMaxCols = 256;
+struct FftCols {
+  const uint32_t* src[kFftMaxCols];
+  uint32_t* dst[kFftMaxCols];
+};
+
+struct FftPass {
+  const uint32_t* tree;  // twiddle (or inverse twiddle) tree
+  uint64_t tree_len;
+  uint64_t src_mask;   // element g reads src[g & src_mask] ...
+  uint64_t src_len;    // ... when (g & src_mask) < src_len, else 0
+  uint32_t log_domain; // N: log size of the domain the twiddles belong to
+  uint32_t layer0, T, C;
+  uint32_t scale;      // outputs are multiplied by `scale` when != 1
+};
+
+__device__ __forceinline__ uint32_t smem_idx(uint32_t e) { return e + (e >> 4); }
+
+// Circle-layer twiddle for butterfly h, from line layer 1 (x, y pairs).
+__device__ __forceinline__ uint32_t circle_tw(const uint32_t* lt0, uint64_t h) {
+  uint32_t b = __ldg(lt0 + ((h >> 1) ^ 1));
+  return ((h ^ (h >> 1)) & 1) ? m31_neg(b) : b;
+}
+
+__device__ __forceinline__ void ibfly(uint32_t& a, uint32_t& b, uint32_t t) {
+  uint32_t s = m31_add(a, b);
+  b = m31_mul(m31_sub(a, b), t);
+  a = s;
+}
+__device__ __forceinline__ void bfly(uint32_t& a, uint32_t& b, uint32_t t) {
+  uint32_t m = m31_mul(b, t);
+  b = m31_sub(a, m);
+  a = m31_add(a, m);
+}
+
+// One register stage over row bits [s0, s0 + RS) of the tile.
+template <int RS, bool INV>
+__device__ __forceinline__ void fft_stage(uint32_t* sm, const FftPass& p, uint64_t hi, uint32_t s0) {
+  const uint32_t T = p.T, C = p.C;
+  const uint32_t E = 1u << (T + C);
+  const uint32_t groups = E >> RS;
+  const uint32_t cmask = (1u << C) - 1;
+  const uint32_t lowmask = (1u << s0) - 1;
+  for (uint32_t q = threadIdx.x; q < groups; q += blockDim.x) {
+    uint32_t c = q & cmask;
+    uint32_t rest = q >> C;
+    uint32_t low = rest & lowmask;
+    uint32_t high = rest >> s0;
+    uint32_t rowbase = (high << (s0 + RS)) | low;
+    uint32_t v[1 << RS];
+#pragma unroll
+    for (int j = 0; j < (1 << RS); j++) v[j] = sm[smem_idx(((rowbase | ((uint32_t)j << s0)) << C) | c)];
+    // Global row index (in units of 2^layer0) of element j: (hi << T) + row.
+    const uint64_t growbase = (hi << T) + rowbase;
+#pragma unroll
+    for (int kk = 0; kk < RS; kk++) {
+      const int k = INV ? kk : (RS - 1 - kk);
+      const uint32_t layer = p.layer0 + s0 + k;
+#pragma unroll
+      for (int j = 0; j < (1 << RS); j++) {
+        if (j & (1 << k)) continue;
+        uint64_t grow = growbase + ((uint64_t)j << s0);
+        uint32_t t;
+        if (layer == 0) {
+          // circle layer: g = grow (layer0 == 0), h = g >> 1
+          const uint32_t* lt0 = p.tree + (p.tree_len - (1ull << (p.log_domain - 1)));
+          t = circle_tw(lt0, grow >> 1);
+        } else {
+          const uint32_t* lt = p.tree + (p.tree_len - (1ull << (p.log_domain - layer)));
+          t = __ldg(lt + (grow >> (s0 + k + 1)));
+        }
+        if (INV)
+          ibfly(v[j], v[j | (1 << k)], t);
+        else
+          bfly(v[j], v[j | (1 << k)], t);
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < (1 << RS); j++) sm[smem_idx(((rowbase | ((uint32_t)j << s0)) << C) | c)] = v[j];
+  }
+}
+
+template <bool INV>
+__global__ void __launch_bounds__(256) fft_pass_kernel(FftPass p, FftCols cols) {
+  extern __shared__ uint32_t sm[];
+  const uint32_t* __restrict__ src = cols.src[blockIdx.y];
+  uint32_t* __restrict__ dst = cols.dst[blockIdx.y];
+  const uint32_t T = p.T, C = p.C, L0 = p.layer0;
+  const uint64_t tile = blockIdx.x;
+  const uint32_t lo_bits = L0 - C;  // L0 >= C
+  const uint64_t lo = tile & ((1ull << lo_bits) - 1);
+  const uint64_t hi = tile >> lo_bits;
+  const uint64_t base = (hi << (L0 + T)) | (lo << C);
+  const uint32_t E = 1u << (T + C);
+  const uint32_t cmask = (1u << C) - 1;
+
+  for (uint32_t e = threadIdx.x; e < E; e += blockDim.x) {
+    uint64_t g = base + ((uint64_t)(e >> C) << L0) + (e & cmask);
+    uint64_t gi = g & p.src_mask;
+    sm[smem_idx(e)] = gi < p.src_len ? __ldg(src + gi) : 0u;
+  }
+  __syncthreads();
+
+  if (INV) {
+    for (uint32_t s0 = 0; s0 < T;) {
+      uint32_t rs = min(4u, T - s0);
+      switch (rs) {
+        case 4: fft_stage<4, INV>(sm, p, hi, s0); break;
+        case 3: fft_stage<3, INV>(sm, p, hi, s0); break;
+        case 2: fft_stage<2, INV>(sm, p, hi, s0); break;
+        default: fft_stage<1, INV>(sm, p, hi, s0); break;
+      }
+      s0 += rs;
+      __syncthreads();
+    }
+  } else {
+    for (uint32_t top = T; top > 0;) {
+      uint32_t rs = min(4u, top);
+      uint32_t s0 = top - rs;
+      switch (rs) {
+        case 4: fft_stage<4, INV>(sm, p, hi, s0); break;
+        case 3: fft_stage<3, INV>(sm, p, hi, s0); break;
+        case 2: fft_stage<2, INV>(sm, p, hi, s0); break;
+        default: fft_stage<1, INV>(sm, p, hi, s0); break;
+      }
+      top = s0;
+      __syncthreads();
+    }
+  }
+
+  const bool scale = p.scale != 1u;
+  for (uint32_t e = threadIdx.x; e < E; e += blockDim.x) {
+    uint64_t g = base + ((uint64_t)(e >> C) << L0) + (e & cmask);
+    uint32_t v = sm[smem_idx(e)];
+    dst[g] = scale ? m31_mul(v, p.scale) : v;
+  }
+}
+
+// Transforms of log size <= 2 follow the special cases of
+// cpu/circle.rs:35-59 (interpolate) and :215-235 (evaluate); they need the
+// domain's first point (x, y) and run on one thread.
+struct SmallCols {
+  const uint32_t* src[kFftMaxCols];
+  uint32_t* dst[kFftMaxCols];
+  uint32_t x[kFftMaxCols], y[kFftMaxCols];
+  uint32_t log_src[kFftMaxCols], log_dst[kFftMaxCols];
+};
+
+__global__ void small_fft_kernel(SmallCols t, uint32_t n, int inverse) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  uint32_t v[4] = {0, 0, 0, 0};
+  uint32_t ls = t.log_src[i], ld = t.log_dst[i];
+  for (uint32_t k = 0; k < (1u << ls); k++) v[k] = t.src[i][k];
+  uint32_t x = t.x[i], y = t.y[i];
+  if (inverse) {
+    if (ld == 1) {
+      uint32_t yn_inv = m31_inv(m31_mul(y, 2));
+      uint32_t y_inv = m31_mul(yn_inv, 2), n_inv = m31_mul(yn_inv, y);
+      ibfly(v[0], v[1], y_inv);
+      v[0] = m31_mul(v[0], n_inv);
+      v[1] = m31_mul(v[1], n_inv);
+    } else {
+      uint32_t xyn_inv = m31_inv(m31_mul(m31_mul(x, y), 4));
+      uint32_t x_inv = m31_mul(m31_mul(xyn_inv, y), 4);
+      uint32_t y_inv = m31_mul(m31_mul(xyn_inv, x), 4);
+      uint32_t n_inv = m31_mul(m31_mul(xyn_inv, x), y);
+      ibfly(v[0], v[1], y_inv);
+      ibfly(v[2], v[3], m31_neg(y_inv));
+      ibfly(v[0], v[2], x_inv);
+      ibfly(v[1], v[3], x_inv);
+      for (int k = 0; k < 4; k++) v[k] = m31_mul(v[k], n_inv);
+    }
+  } else {
+    if (ld == 1) {
+      bfly(v[0], v[1], y);
+    } else {
+      bfly(v[0], v[2], x);
+      bfly(v[1], v[3], x);
+      bfly(v[0], v[1], y);
+      bfly(v[2], v[3], m31_neg(y));
+    }
+  }
+  for (uint32_t k = 0; k < (1u << ld); k++) t.dst[i][k] = v[k];
+}
+
+// In-place bit reversal: thread i swaps i <-> rev(i) when i < rev(i).
+__global__ void bit_reverse_kernel(uint32_t* v, uint32_t log_n) {
+  uint64_t n = 1ull << log_n;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    uint64_t j = __brevll(i) >> (64 - log_n);
+    if (i < j) {
+      uint32_t a = v[i], b = v[j];
+      v[i] = b;
+      v[j] = a;
+    }
+  }
+}
+
+// ---------------------------------------------------------------- host ----
+
+struct PassPlan {
+  uint32_t layer0, T, C;
+};
+
+// Splits n layers into passes of <= 12 (contiguous) / <= 11 (strided, C = 3)
+// layers, low layers first.
+static std::vector<PassPlan> plan_passes(uint32_t n) {
+  std::vector<PassPlan> plan;
+  if (n <= 12) {
+    plan.push_back({0, n, 0});
+    return plan;
+  }
+  uint32_t parts = n <= 23 ? 2 : 3;
+  uint32_t rest = n;
+  uint32_t l0 = 0;
+  for (uint32_t i = 0; i < parts; i++) {
+    uint32_t t = (rest + (parts - i) - 1) / (parts - i);
+    plan.push_back({l0, t, l0 == 0 ? 0u : 3u});
+    l0 += t;
+    rest -= t;
+  }
+  return plan;
+}
+
+static uint32_t host_pow2_inv(uint32_t log_n) { return m31_inv(m31_reduce_u32(1u << log_n)); }
+
+// Domain first point for CanonicCoset-like half cosets (host).
+static void index_point(uint64_t idx, uint32_t& x, uint32_t& y) {
+  uint32_t gx = 2, gy = 1268011823u;
+  x = 1;
+  y = 0;
+  idx &= (1ull << 31) - 1;
+  for (int b = 0; b < 31; b++) {
+    if ((idx >> b) & 1) {
+      uint32_t nx = m31_sub(m31_mul(x, gx), m31_mul(y, gy));
+      uint32_t ny = m31_add(m31_mul(x, gy), m31_mul(y, gx));
+      x = nx;
+      y = ny;
+    }
+    uint32_t dx = m31_sub(m31_mul(gx, gx), m31_mul(gy, gy));
+    uint32_t dy = m31_add(m31_mul(gx, gy), m31_mul(gy, gx));
+    gx = dx;
+    gy = dy;
+  }
+}
+
+template <bool INV>
+static int launch_pass(const FftPass& p, const std::vector<const uint32_t*>& srcs, const std::vector<uint32_t*>& dsts,
+                       uint64_t total_log, cudaStream_t s, char* err, size_t err_len) {
+  uint64_t tiles = 1ull << (total_log - p.T - p.C);
+  size_t E = (size_t)1 << (p.T + p.C);
+  size_t smem = (E + E / 16 + 1) * sizeof(uint32_t);
+  static bool attr_set[2] = {false, false};
+  if (!attr_set[INV]) {
+    STWO_CUDA_TRY(cudaFuncSetAttribute(fft_pass_kernel<INV>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    attr_set[INV] = true;
+  }
+  STWO_ARG_CHECK(tiles <= 0x7fffffffull, "too many tiles");
+  for (size_t c0 = 0; c0 < srcs.size(); c0 += kFftMaxCols) {
+    FftCols cols;
+    size_t nc = std::min<size_t>(kFftMaxCols, srcs.size() - c0);
+    for (size_t i = 0; i < nc; i++) {
+      cols.src[i] = srcs[c0 + i];
+      cols.dst[i] = dsts[c0 + i];
+    }
+    dim3 grid((unsigned)tiles, (unsigned)nc);
+    fft_pass_kernel<INV><<<grid, 256, smem, s>>>(p, cols);
+    STWO_CHECK_LAUNCH();
+  }
+  return STWO_B200_OK;
+}
+
+}  // namespace stwo_b200
+
+using namespace stwo_b200;
+
+static int interpolate_impl(const uint32_t* const* d_src, uint32_t* const* d_cols, const uint32_t* log_sizes,
+                            const uint64_t* half_initial_indices, uint32_t n_cols, const uint32_t* d_itwiddles,
+                            uint32_t tree_log_size, cudaStream_t s, char* err, size_t err_len) {
+  STWO_ARG_CHECK(n_cols == 0 || (d_src && d_cols && log_sizes), "null column arrays");
+  // Group columns by log size: one launch per (size, pass).
+  std::vector<uint32_t> order(n_cols);
+  for (uint32_t i = 0; i < n_cols; i++) order[i] = i;
+  std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return log_sizes[a] < log_sizes[b]; });
+  SmallCols small;
+  uint32_t n_small = 0;
+  for (size_t a = 0; a < order.size();) {
+    uint32_t n = log_sizes[order[a]];
+    size_t b = a;
+    while (b < order.size() && log_sizes[order[b]] == n) b++;
+    STWO_ARG_CHECK(n <= 30, "column log size %u too large", n);
+    if (n == 0) {
+      a = b;
+      continue;
+    }
+    if (n <= 2) {
+      for (size_t i = a; i < b; i++) {
+        uint32_t c = order[i];
+        uint64_t hi = half_initial_indices ? half_initial_indices[c] : (1ull << (31 - (n + 1)));
+        if (n_small == kFftMaxCols) {
+          small_fft_kernel<<<1, kFftMaxCols, 0, s>>>(small, n_small, 1);
+          STWO_CHECK_LAUNCH();
+          n_small = 0;
+        }
+        small.src[n_small] = d_src[c];
+        small.dst[n_small] = d_cols[c];
+        index_point(hi, small.x[n_small], small.y[n_small]);
+        small.log_src[n_small] = n;
+        small.log_dst[n_small] = n;
+        n_small++;
+      }
+      a = b;
+      continue;
+    }
+    STWO_ARG_CHECK(d_itwiddles && n - 1 <= tree_log_size, "twiddle tree (log %u) too small for log size %u",
+                   tree_log_size, n);
+    std::vector<const uint32_t*> srcs;
+    std::vector<uint32_t*> dsts;
+    for (size_t i = a; i < b; i++) {
+      srcs.push_back(d_src[order[i]]);
+      dsts.push_back(d_cols[order[i]]);
+    }
+    std::vector<const uint32_t*> inplace(dsts.begin(), dsts.end());
+    auto plan = plan_passes(n);
+    for (size_t pi = 0; pi < plan.size(); pi++) {
+      FftPass p;
+      p.tree = d_itwiddles;
+      p.tree_len = 1ull << tree_log_size;
+      p.src_mask = ~0ull;
+      p.src_len = ~0ull;
+      p.log_domain = n;
+      p.layer0 = plan[pi].layer0;
+      p.T = plan[pi].T;
+      p.C = plan[pi].C;
+      p.scale = (pi + 1 == plan.size()) ? host_pow2_inv(n) : 1u;
+      int rc = launch_pass<true>(p, pi == 0 ? srcs : inplace, dsts, n, s, err, err_len);
+      if (rc) return rc;
+    }
+    a = b;
+  }
+  if (n_small) {
+    small_fft_kernel<<<1, kFftMaxCols, 0, s>>>(small, n_small, 1);
+    STWO_CHECK_LAUNCH();
+  }
+  return ok(err, err_len);
+}
+
+extern "C" int stwo_b200_interpolate_columns(uint32_t* const* d_cols, const uint32_t* log_sizes,
+                                             const uint64_t* half_initial_indices, uint32_t n_cols,
+                                             const uint32_t* d_itwiddles, uint32_t tree_log_size, void* stream,
+                                             char* err, size_t err_len) {
+  int rc = interpolate_impl(d_cols, d_cols, log_sizes, half_initial_indices, n_cols, d_itwiddles, tree_log_size,
+                            as_stream(stream), err, err_len);
+  return rc ? rc : ok(err, err_len);
+}
+
+extern "C" int stwo_b200_interpolate_columns_into(const uint32_t* const* d_evals, uint32_t* const* d_coeffs,
+                                                  const uint32_t* log_sizes, const uint64_t* half_initial_indices,
+                                                  uint32_t n_cols, const uint32_t* d_itwiddles,
+                                                  uint32_t tree_log_size, void* stream, char* err, size_t err_len) {
+  int rc = interpolate_impl(d_evals, d_coeffs, log_sizes, half_initial_indices, n_cols, d_itwiddles, tree_log_size,
+                            as_stream(stream), err, err_len);
+  return rc ? rc : ok(err, err_len);
+}
+
+extern "C" int stwo_b200_evaluate_polynomials(const uint32_t* const* d_coeffs, const uint32_t* log_sizes,
+                                              uint32_t n_cols, uint32_t log_blowup, uint32_t* const* d_evals,
+                                              const uint32_t* d_twiddles, uint32_t tree_log_size, void* stream,
+                                              char* err, size_t err_len) {
+  cudaStream_t s = as_stream(stream);
+  STWO_ARG_CHECK(n_cols == 0 || (d_coeffs && log_sizes && d_evals), "null column arrays");
+  std::vector<uint32_t> order(n_cols);
+  for (uint32_t i = 0; i < n_cols; i++) order[i] = i;
+  std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return log_sizes[a] < log_sizes[b]; });
+  SmallCols small;
+  uint32_t n_small = 0;
+  for (size_t a = 0; a < order.size();) {
+    uint32_t n = log_sizes[order[a]];
+    size_t b = a;
+    while (b < order.size() && log_sizes[order[b]] == n) b++;
+    uint32_t N = n + log_blowup;
+    STWO_ARG_CHECK(N <= 30, "evaluation log size %u too large", N);
+    STWO_ARG_CHECK(N >= 1, "evaluation domain log size must be >= 1");
+    if (N <= 2) {
+      for (size_t i = a; i < b; i++) {
+        uint32_t c = order[i];
+        if (n_small == kFftMaxCols) {
+          small_fft_kernel<<<1, kFftMaxCols, 0, s>>>(small, n_small, 0);
+          STWO_CHECK_LAUNCH();
+          n_small = 0;
+        }
+        small.src[n_small] = d_coeffs[c];
+        small.dst[n_small] = d_evals[c];
+        index_point(1ull << (31 - (N + 1)), small.x[n_small], small.y[n_small]);
+        small.log_src[n_small] = n;
+        small.log_dst[n_small] = N;
+        n_small++;
+      }
+      a = b;
+      continue;
+    }
+    STWO_ARG_CHECK(d_twiddles && N - 1 <= tree_log_size, "twiddle tree (log %u) too small for log size %u",
+                   tree_log_size, N);
+    std::vector<const uint32_t*> srcs;
+    std::vector<uint32_t*> dsts;
+    for (size_t i = a; i < b; i++) {
+      srcs.push_back(d_coeffs[order[i]]);
+      dsts.push_back(d_evals[order[i]]);
+    }
+    // simd/circle.rs:403-411: below log 5 the CPU path zero-extends the
+    // coefficients and runs every layer of the big domain; otherwise each of
+    // the 2^blowup subdomains transforms a copy of the coefficients with the
+    // layers below n only (simd/circle.rs:413-440).
+    const bool cpu_path = n < 5;
+    const uint32_t layers = cpu_path ? N : n;
+    auto plan = plan_passes(layers);
+    for (size_t k = plan.size(); k-- > 0;) {
+      FftPass p;
+      p.tree = d_twiddles;
+      p.tree_len = 1ull << tree_log_size;
+      p.log_domain = N;
+      p.layer0 = plan[k].layer0;
+      p.T = plan[k].T;
+      p.C = plan[k].C;
+      p.scale = 1u;
+      const bool first = (k + 1 == plan.size());
+      if (first) {
+        p.src_mask = cpu_path ? ((1ull << N) - 1) : ((1ull << n) - 1);
+        p.src_len = 1ull << n;
+        int rc = launch_pass<false>(p, srcs, dsts, N, s, err, err_len);
+        if (rc) return rc;
+      } else {
+        p.src_mask = ~0ull;
+        p.src_len = ~0ull;
+        std::vector<const uint32_t*> inplace(dsts.begin(), dsts.end());
+        int rc = launch_pass<false>(p, inplace, dsts, N, s, err, err_len);
+        if (rc) return rc;
+      }
+    }
+    a = b;
+  }
+  if (n_small) {
+    small_fft_kernel<<<1, kFftMaxCols, 0, s>>>(small, n_small, 0);
+    STWO_CHECK_LAUNCH();
+  }
+  return ok(err, err_len);
+}
+
+extern "C" int stwo_b200_bit_reverse_column(uint32_t* d_col, uint32_t log_size, void* stream, char* err,
+                                            size_t err_len) {
+  STWO_ARG_CHECK(log_size <= 31, "log size %u too large", log_size);
+  if (log_size == 0) return ok(err, err_len);
+  uint64_t n = 1ull << log_size;
+  uint64_t blocks = std::min<uint64_t>((n + 255) / 256, 148 * 32);
+  bit_reverse_kernel<<<(unsigned)blocks, 256, 0, as_stream(stream)>>>(d_col, log_size);
+  STWO_CHECK_LAUNCH();
+  return ok(err, err_len);
+}

@@ -1,0 +1,250 @@
+// FRI folds for sm_100a: fold_line, fold_circle_into_line, decompose.
+//
+// QM31 columns are four M31 coordinate columns; each kernel streams them with
+// one thread per output (fold) or per element (decompose).
+//  fold_line (crates/stwo/src/prover/backend/cpu/fri.rs:67-92, simd/fri.rs:32-122):
+//    f' = (f(x) + f(-x)) + alpha * (f(x) - f(-x)) * x^-1, fold_step layers fused
+//    with alpha <- alpha^2 per layer; x^-1 from the inverse twiddle tree.
+//  fold_circle_into_line (cpu/fri.rs:95-123, simd/fri.rs:124-172):
+//    dst <- dst * alpha^2 + (f(p) + f(-p)) + alpha * (f(p) - f(-p)) * p.y^-1.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+
+#include "common.cuh"
+#include "field.cuh"
+
+namespace stwo_b200 {
+
+struct Cols4 {
+  const uint32_t* c[4];
+};
+struct Cols4W {
+  uint32_t* c[4];
+};
+
+__device__ __forceinline__ qm31 load_q(const Cols4& s, uint64_t i) {
+  return {__ldg(s.c[0] + i), __ldg(s.c[1] + i), __ldg(s.c[2] + i), __ldg(s.c[3] + i)};
+}
+__device__ __forceinline__ void store_q(const Cols4W& d, uint64_t i, qm31 v) {
+  d.c[0][i] = v.a;
+  d.c[1][i] = v.b;
+  d.c[2][i] = v.c;
+  d.c[3][i] = v.d;
+}
+
+constexpr int kMaxFoldStep = 6;
+struct FoldAlphas {
+  qm31 a[kMaxFoldStep];
+};
+
+// One thread per output; reads 2^fold_step consecutive inputs.
+__global__ void fold_line_kernel(Cols4 in, uint32_t log_m, uint32_t fold_step, FoldAlphas alphas,
+                                 const uint32_t* itw, uint64_t tw_len, Cols4W out) {
+  uint64_t n_out = 1ull << (log_m - fold_step);
+  for (uint64_t o = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; o < n_out; o += (uint64_t)gridDim.x * blockDim.x) {
+    if (fold_step == 1) {
+      const uint32_t* lt = itw + (tw_len - (1ull << log_m));
+      qm31 fx = load_q(in, 2 * o), fnx = load_q(in, 2 * o + 1);
+      qm31 f0 = qm31_add(fx, fnx);
+      qm31 f1 = qm31_mul_m31(qm31_sub(fx, fnx), __ldg(lt + o));
+      store_q(out, o, qm31_add(f0, qm31_mul(alphas.a[0], f1)));
+      continue;
+    }
+    qm31 v[1 << kMaxFoldStep];
+    const uint32_t w = 1u << fold_step;
+    for (uint32_t j = 0; j < w; j++) v[j] = load_q(in, o * w + j);
+    for (uint32_t s = 0; s < fold_step; s++) {
+      const uint32_t* lt = itw + (tw_len - (1ull << (log_m - s)));
+      uint32_t pairs = w >> (s + 1);
+      for (uint32_t j = 0; j < pairs; j++) {
+        qm31 fx = v[2 * j], fnx = v[2 * j + 1];
+        qm31 f0 = qm31_add(fx, fnx);
+        qm31 f1 = qm31_mul_m31(qm31_sub(fx, fnx), __ldg(lt + o * pairs + j));
+        v[j] = qm31_add(f0, qm31_mul(alphas.a[s], f1));
+      }
+    }
+    store_q(out, o, v[0]);
+  }
+}
+
+// Circle-layer inverse twiddle of pair i, derived from line layer 1 of the
+// source domain: [y, -y, -x, x] (simd/fft/mod.rs:61-97).
+__device__ __forceinline__ uint32_t circle_itw(const uint32_t* lt0, uint64_t i) {
+  uint32_t b = __ldg(lt0 + ((i >> 1) ^ 1));
+  return ((i ^ (i >> 1)) & 1) ? m31_neg(b) : b;
+}
+
+struct SmallYinv {
+  uint32_t v[8];
+};
+
+__global__ void fold_circle_kernel(Cols4W dst, Cols4 src, uint32_t log_n, qm31 alpha, qm31 alpha_sq,
+                                   const uint32_t* itw, uint64_t tw_len, SmallYinv small) {
+  uint64_t n_out = 1ull << (log_n - 1);
+  const uint32_t* lt0 = log_n > 4 ? itw + (tw_len - (1ull << (log_n - 1))) : nullptr;
+  const Cols4 dr{{dst.c[0], dst.c[1], dst.c[2], dst.c[3]}};
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n_out; i += (uint64_t)gridDim.x * blockDim.x) {
+    uint32_t yinv = log_n > 4 ? circle_itw(lt0, i) : small.v[i];
+    qm31 fp = load_q(src, 2 * i), fnp = load_q(src, 2 * i + 1);
+    qm31 f0 = qm31_add(fp, fnp);
+    qm31 f1 = qm31_mul_m31(qm31_sub(fp, fnp), yinv);
+    qm31 fprime = qm31_add(f0, qm31_mul(alpha, f1));
+    qm31 d = load_q(dr, i);
+    store_q(dst, i, qm31_add(qm31_mul(d, alpha_sq), fprime));
+  }
+}
+
+// decompose: per-block signed sums (+ on [0, 16*half_a), - on [16*half_a,
+// 16*range)), then lambda = sum / n, then g = f -/+ lambda.
+__global__ void decompose_sums_kernel(Cols4 in, uint64_t split, uint64_t end, uint32_t* partial) {
+  __shared__ uint32_t red[4][256];
+  uint32_t acc[4] = {0, 0, 0, 0};
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < end; i += (uint64_t)gridDim.x * blockDim.x) {
+    qm31 v = load_q(in, i);
+    uint32_t w[4] = {v.a, v.b, v.c, v.d};
+#pragma unroll
+    for (int k = 0; k < 4; k++) acc[k] = i < split ? m31_add(acc[k], w[k]) : m31_sub(acc[k], w[k]);
+  }
+#pragma unroll
+  for (int k = 0; k < 4; k++) red[k][threadIdx.x] = acc[k];
+  __syncthreads();
+  for (uint32_t s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) {
+#pragma unroll
+      for (int k = 0; k < 4; k++) red[k][threadIdx.x] = m31_add(red[k][threadIdx.x], red[k][threadIdx.x + s]);
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < 4; k++) partial[blockIdx.x * 4 + k] = red[k][0];
+  }
+}
+
+__global__ void decompose_finish_kernel(const uint32_t* partial, uint32_t n_blocks, uint32_t inv_n, uint32_t* lambda) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  uint32_t s[4] = {0, 0, 0, 0};
+  for (uint32_t b = 0; b < n_blocks; b++)
+    for (int k = 0; k < 4; k++) s[k] = m31_add(s[k], partial[b * 4 + k]);
+  for (int k = 0; k < 4; k++) lambda[k] = m31_mul(s[k], inv_n);
+}
+
+__global__ void decompose_apply_kernel(Cols4 in, uint64_t n, uint64_t split, const uint32_t* lambda, Cols4W out) {
+  qm31 l{lambda[0], lambda[1], lambda[2], lambda[3]};
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    qm31 v = load_q(in, i);
+    store_q(out, i, i < split ? qm31_sub(v, l) : qm31_add(v, l));
+  }
+}
+
+static unsigned grid_for(uint64_t n, unsigned threads) {
+  uint64_t b = (n + threads - 1) / threads;
+  return (unsigned)std::min<uint64_t>(std::max<uint64_t>(b, 1), 148ull * 64);
+}
+
+static void host_point(uint64_t idx, uint32_t& x, uint32_t& y) {
+  uint32_t gx = 2, gy = 1268011823u;
+  x = 1;
+  y = 0;
+  idx &= (1ull << 31) - 1;
+  for (int b = 0; b < 31; b++) {
+    if ((idx >> b) & 1) {
+      uint32_t nx = m31_sub(m31_mul(x, gx), m31_mul(y, gy));
+      uint32_t ny = m31_add(m31_mul(x, gy), m31_mul(y, gx));
+      x = nx;
+      y = ny;
+    }
+    uint32_t dx = m31_sub(m31_mul(gx, gx), m31_mul(gy, gy));
+    uint32_t dy = m31_add(m31_mul(gx, gy), m31_mul(gy, gx));
+    gx = dx;
+    gy = dy;
+  }
+}
+
+}  // namespace stwo_b200
+
+using namespace stwo_b200;
+
+extern "C" int stwo_b200_fold_line(const uint32_t* const* d_in4, uint32_t log_size, const uint32_t* alpha,
+                                   uint32_t fold_step, const uint32_t* d_itwiddles, uint32_t tree_log_size,
+                                   uint32_t* const* d_out4, void* stream, char* err, size_t err_len) {
+  STWO_ARG_CHECK(d_in4 && d_out4 && alpha, "null argument");
+  STWO_ARG_CHECK(fold_step >= 1 && fold_step <= (uint32_t)kMaxFoldStep && fold_step <= log_size,
+                 "fold_step %u invalid for log size %u", fold_step, log_size);
+  STWO_ARG_CHECK(d_itwiddles && log_size <= tree_log_size, "twiddle tree (log %u) too small for line log size %u",
+                 tree_log_size, log_size);
+  Cols4 in{{d_in4[0], d_in4[1], d_in4[2], d_in4[3]}};
+  Cols4W out{{d_out4[0], d_out4[1], d_out4[2], d_out4[3]}};
+  FoldAlphas al;
+  qm31 a{alpha[0], alpha[1], alpha[2], alpha[3]};
+  for (uint32_t s = 0; s < fold_step; s++) {
+    al.a[s] = a;
+    a = qm31_mul(a, a);
+  }
+  uint64_t n_out = 1ull << (log_size - fold_step);
+  fold_line_kernel<<<grid_for(n_out, 256), 256, 0, as_stream(stream)>>>(in, log_size, fold_step, al, d_itwiddles,
+                                                                        1ull << tree_log_size, out);
+  STWO_CHECK_LAUNCH();
+  return ok(err, err_len);
+}
+
+extern "C" int stwo_b200_fold_circle_into_line(uint32_t* const* d_dst4, const uint32_t* const* d_src4,
+                                               uint32_t log_size, uint64_t half_initial_index, const uint32_t* alpha,
+                                               const uint32_t* d_itwiddles, uint32_t tree_log_size, void* stream,
+                                               char* err, size_t err_len) {
+  STWO_ARG_CHECK(d_dst4 && d_src4 && alpha, "null argument");
+  STWO_ARG_CHECK(log_size >= 1 && log_size <= 30, "bad log size %u", log_size);
+  SmallYinv small{};
+  if (log_size <= 4) {
+    // simd/fri.rs:130-140: CPU path, y^-1 of circle domain point bitrev(2i).
+    uint64_t half_size = 1ull << (log_size - 1);
+    uint64_t step = 1ull << (31 - (log_size - 1));
+    for (uint64_t i = 0; i < half_size; i++) {
+      uint64_t pos = bitrev32((uint32_t)(i << 1), log_size);
+      uint64_t idx = pos < half_size ? (half_initial_index + step * pos)
+                                     : ((1ull << 31) - ((half_initial_index + step * (pos - half_size)) & ((1ull << 31) - 1)));
+      uint32_t x, y;
+      host_point(idx, x, y);
+      small.v[i] = m31_inv(y);
+    }
+  } else {
+    STWO_ARG_CHECK(d_itwiddles && log_size - 1 <= tree_log_size, "twiddle tree (log %u) too small for log size %u",
+                   tree_log_size, log_size);
+  }
+  Cols4W dst{{d_dst4[0], d_dst4[1], d_dst4[2], d_dst4[3]}};
+  Cols4 src{{d_src4[0], d_src4[1], d_src4[2], d_src4[3]}};
+  qm31 a{alpha[0], alpha[1], alpha[2], alpha[3]};
+  uint64_t n_out = 1ull << (log_size - 1);
+  fold_circle_kernel<<<grid_for(n_out, 256), 256, 0, as_stream(stream)>>>(
+      dst, src, log_size, a, qm31_mul(a, a), d_itwiddles, d_itwiddles ? (1ull << tree_log_size) : 0, small);
+  STWO_CHECK_LAUNCH();
+  return ok(err, err_len);
+}
+
+extern "C" int stwo_b200_decompose(const uint32_t* const* d_in4, uint32_t log_size, uint32_t* const* d_out4,
+                                   uint32_t* lambda_out, void* stream, char* err, size_t err_len) {
+  STWO_ARG_CHECK(d_in4 && d_out4 && lambda_out, "null argument");
+  STWO_ARG_CHECK(log_size <= 30, "bad log size %u", log_size);
+  cudaStream_t s = as_stream(stream);
+  uint64_t n = 1ull << log_size;
+  uint64_t range = n / 16, half_a = range / 2;
+  uint64_t split_sum = 16 * half_a, end_sum = 16 * range;
+  uint64_t split_apply = 16 * (((n + 15) / 16) / 2);
+  Cols4 in{{d_in4[0], d_in4[1], d_in4[2], d_in4[3]}};
+  Cols4W out{{d_out4[0], d_out4[1], d_out4[2], d_out4[3]}};
+  unsigned blocks = grid_for(std::max<uint64_t>(end_sum, 1), 256);
+  uint32_t* scratch = nullptr;
+  STWO_CUDA_TRY(cudaMallocAsync(&scratch, (blocks * 4 + 4) * sizeof(uint32_t), s));
+  uint32_t* lam = scratch + blocks * 4;
+  decompose_sums_kernel<<<blocks, 256, 0, s>>>(in, split_sum, end_sum, scratch);
+  STWO_CHECK_LAUNCH();
+  decompose_finish_kernel<<<1, 32, 0, s>>>(scratch, blocks, m31_inv(m31_reduce_u32((uint32_t)n)), lam);
+  STWO_CHECK_LAUNCH();
+  decompose_apply_kernel<<<grid_for(n, 256), 256, 0, s>>>(in, n, split_apply, lam, out);
+  STWO_CHECK_LAUNCH();
+  STWO_CUDA_TRY(cudaMemcpyAsync(lambda_out, lam, 16, cudaMemcpyDeviceToHost, s));
+  STWO_CUDA_TRY(cudaFreeAsync(scratch, s));
+  STWO_CUDA_TRY(cudaStreamSynchronize(s));
+  return ok(err, err_len);
+}

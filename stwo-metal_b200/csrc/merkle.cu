@@ -1,0 +1,320 @@
+// Blake2s Merkle trees for sm_100a: lifted leaves, node layers and the
+// mixed-degree commit_on_layer.
+//
+// Lifted leaf i (crates/stwo/src/prover/backend/cpu/merkle_lifted.rs:44-78)
+// is Blake2s-256 of the byte stream LE32(col_c[lift(i, L - log_c)]) over the
+// columns sorted by length, lift(i, r) = ((i >> (r+1)) << 1) + (i & 1).  One
+// thread per leaf absorbs 16 columns per compression; for every column a warp
+// reads 32 consecutive (or pairwise repeated) words, so loads are coalesced
+// without a shared-memory transpose.  Node layers hash 64-byte child pairs with
+// one final compression (core/vcs_lifted/blake2_merkle.rs:18-25); a block
+// builds up to 8 layers of a subtree in shared memory per launch.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "blake2s.cuh"
+#include "common.cuh"
+#include "field.cuh"
+
+namespace stwo_b200 {
+
+constexpr int kLeafMaxCols = 1024;
+struct LeafCols {
+  const uint32_t* col[kLeafMaxCols];
+  uint8_t shift[kLeafMaxCols];  // L - log_size
+};
+
+__device__ __forceinline__ void store_hash(uint8_t* out, uint64_t i, const uint32_t h[8], bool m31) {
+  uint4* o = reinterpret_cast<uint4*>(out + i * 32);
+  uint32_t w[8];
+#pragma unroll
+  for (int k = 0; k < 8; k++) w[k] = m31 ? m31_reduce_u32(h[k]) : h[k];
+  o[0] = make_uint4(w[0], w[1], w[2], w[3]);
+  o[1] = make_uint4(w[4], w[5], w[6], w[7]);
+}
+
+__device__ __forceinline__ uint64_t lift_index(uint64_t i, uint32_t r) {
+  return r == 0 ? i : (((i >> (r + 1)) << 1) + (i & 1));
+}
+
+// Leaves for columns [c_begin, c_end) of `t`; `state` (nullable) carries the
+// chaining value between launches when a tree has more than kLeafMaxCols
+// columns; only the last launch finalizes.
+__global__ void __launch_bounds__(256) lifted_leaves_kernel(LeafCols t, uint32_t n_cols, uint32_t L, int m31,
+                                                           uint32_t bytes_before, uint32_t total_bytes,
+                                                           uint32_t* state, int is_first, int is_last, uint8_t* out) {
+  uint64_t n = 1ull << L;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    uint32_t h[8];
+    if (is_first) {
+      blake2s_init(h);
+    } else {
+#pragma unroll
+      for (int k = 0; k < 8; k++) h[k] = state[k * n + i];
+    }
+    uint32_t m[16];
+    uint32_t done = bytes_before;
+    if (n_cols == 0 && is_last) {
+#pragma unroll
+      for (int k = 0; k < 16; k++) m[k] = 0;
+      blake2s_compress(h, m, done, true);
+    }
+    for (uint32_t c0 = 0; c0 < n_cols; c0 += 16) {
+#pragma unroll
+      for (int k = 0; k < 16; k++) {
+        uint32_t c = c0 + k;
+        m[k] = c < n_cols ? __ldg(t.col[c] + lift_index(i, t.shift[c])) : 0u;
+      }
+      uint32_t nb = min(16u, n_cols - c0) * 4;
+      done += nb;
+      blake2s_compress(h, m, done, is_last && done == total_bytes);
+    }
+    if (is_last) {
+      store_hash(out, i, h, m31 != 0);
+    } else {
+#pragma unroll
+      for (int k = 0; k < 8; k++) state[k * n + i] = h[k];
+    }
+  }
+}
+
+// Hashes `levels` consecutive node layers.  Block b hashes `width` parents
+// of `in` (2^in_log hashes) at the first level, keeps them in shared memory
+// and continues up its subtree; every produced layer lv goes to outs[lv].
+struct NodeOuts {
+  uint8_t* out[8];
+};
+
+__global__ void __launch_bounds__(256) node_layers_kernel(const uint8_t* in, uint32_t in_log, uint32_t levels, int m31,
+                                                         NodeOuts outs) {
+  __shared__ uint32_t buf[2][256 * 8];
+  // level 0: parents of `in`
+  uint64_t parents0 = 1ull << (in_log - 1);
+  uint32_t width = parents0 < 256 ? (uint32_t)parents0 : 256u;  // parents of this block at level 0
+  uint64_t first_parent = (uint64_t)blockIdx.x * width;
+  uint32_t tid = threadIdx.x;
+  int cur = 0;
+  if (tid < width) {
+    uint64_t p = first_parent + tid;
+    const uint4* src = reinterpret_cast<const uint4*>(in + p * 64);
+    uint32_t m[16];
+    uint4 a = src[0], b = src[1], c = src[2], d = src[3];
+    m[0] = a.x; m[1] = a.y; m[2] = a.z; m[3] = a.w;
+    m[4] = b.x; m[5] = b.y; m[6] = b.z; m[7] = b.w;
+    m[8] = c.x; m[9] = c.y; m[10] = c.z; m[11] = c.w;
+    m[12] = d.x; m[13] = d.y; m[14] = d.z; m[15] = d.w;
+    uint32_t h[8];
+    blake2s_init(h);
+    blake2s_compress(h, m, 64, true);
+    if (m31) {
+#pragma unroll
+      for (int k = 0; k < 8; k++) h[k] = m31_reduce_u32(h[k]);
+    }
+    store_hash(outs.out[0], p, h, false);
+#pragma unroll
+    for (int k = 0; k < 8; k++) buf[cur][tid * 8 + k] = h[k];
+  }
+  __syncthreads();
+  for (uint32_t lv = 1; lv < levels; lv++) {
+    width >>= 1;
+    if (width == 0) break;
+    uint64_t first = first_parent >> lv;
+    if (tid < width) {
+      uint32_t m[16];
+#pragma unroll
+      for (int k = 0; k < 16; k++) m[k] = buf[cur][tid * 16 + k];
+      uint32_t h[8];
+      blake2s_init(h);
+      blake2s_compress(h, m, 64, true);
+      if (m31) {
+#pragma unroll
+        for (int k = 0; k < 8; k++) h[k] = m31_reduce_u32(h[k]);
+      }
+      store_hash(outs.out[lv], first + tid, h, false);
+#pragma unroll
+      for (int k = 0; k < 8; k++) buf[cur ^ 1][tid * 8 + k] = h[k];
+    }
+    cur ^= 1;
+    __syncthreads();
+  }
+}
+
+// Mixed-degree node: Blake2s(prev[2i] || prev[2i+1] || LE32 cols[c][i] ...).
+__global__ void __launch_bounds__(256) commit_on_layer_kernel(uint32_t log_size, const uint8_t* prev, LeafCols t,
+                                                             uint32_t n_cols, int m31, uint8_t* out) {
+  uint64_t n = 1ull << log_size;
+  const uint32_t total = (prev ? 64u : 0u) + 4u * n_cols;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    uint32_t h[8];
+    blake2s_init(h);
+    uint32_t m[16];
+    uint32_t done = 0;
+    uint32_t c0 = 0;
+    if (prev) {
+      const uint4* src = reinterpret_cast<const uint4*>(prev + i * 64);
+      uint4 a = src[0], b = src[1], c = src[2], d = src[3];
+      m[0] = a.x; m[1] = a.y; m[2] = a.z; m[3] = a.w;
+      m[4] = b.x; m[5] = b.y; m[6] = b.z; m[7] = b.w;
+      m[8] = c.x; m[9] = c.y; m[10] = c.z; m[11] = c.w;
+      m[12] = d.x; m[13] = d.y; m[14] = d.z; m[15] = d.w;
+      done = 64;
+      blake2s_compress(h, m, done, done == total);
+    }
+    if (total == 0) {
+#pragma unroll
+      for (int k = 0; k < 16; k++) m[k] = 0;
+      blake2s_compress(h, m, 0, true);
+    }
+    for (; c0 < n_cols; c0 += 16) {
+#pragma unroll
+      for (int k = 0; k < 16; k++) {
+        uint32_t c = c0 + k;
+        m[k] = c < n_cols ? __ldg(t.col[c] + i) : 0u;
+      }
+      done += min(16u, n_cols - c0) * 4;
+      blake2s_compress(h, m, done, done == total);
+    }
+    store_hash(out, i, h, m31 != 0);
+  }
+}
+
+static unsigned grid_for(uint64_t n, unsigned threads) {
+  uint64_t b = (n + threads - 1) / threads;
+  return (unsigned)std::min<uint64_t>(std::max<uint64_t>(b, 1), 148ull * 64);
+}
+
+int build_leaves_impl(const uint32_t* const* d_cols, const uint32_t* log_sizes, uint32_t n_cols, uint32_t L,
+                      int m31, uint8_t* d_leaves, cudaStream_t s, char* err, size_t err_len) {
+  STWO_ARG_CHECK(d_leaves != nullptr, "null leaves");
+  if (n_cols == 0) {
+    LeafCols t{};
+    lifted_leaves_kernel<<<1, 32, 0, s>>>(t, 0, 0, m31, 0, 0, nullptr, 1, 1, d_leaves);
+    STWO_CHECK_LAUNCH();
+    return STWO_B200_OK;
+  }
+  STWO_ARG_CHECK(L <= 30, "lifting log size %u too large", L);
+  for (uint32_t c = 0; c < n_cols; c++) {
+    STWO_ARG_CHECK(log_sizes[c] >= 1, "A column must be of length >= 2.");
+    STWO_ARG_CHECK(log_sizes[c] <= L, "column log size %u exceeds lifting log size %u", log_sizes[c], L);
+    STWO_ARG_CHECK(c == 0 || log_sizes[c - 1] <= log_sizes[c], "columns must be sorted by length");
+  }
+  uint64_t n = 1ull << L;
+  uint32_t total_bytes = 4u * n_cols;
+  uint32_t* state = nullptr;
+  const uint32_t chunks = (n_cols + kLeafMaxCols - 1) / kLeafMaxCols;
+  if (chunks > 1) STWO_CUDA_TRY(cudaMallocAsync(&state, n * 32, s));
+  for (uint32_t ch = 0; ch < chunks; ch++) {
+    LeafCols t;
+    uint32_t c0 = ch * kLeafMaxCols;
+    uint32_t nc = std::min<uint32_t>(kLeafMaxCols, n_cols - c0);
+    for (uint32_t k = 0; k < nc; k++) {
+      t.col[k] = d_cols[c0 + k];
+      t.shift[k] = (uint8_t)(L - log_sizes[c0 + k]);
+    }
+    lifted_leaves_kernel<<<grid_for(n, 256), 256, 0, s>>>(t, nc, L, m31, 4u * c0, total_bytes, state, ch == 0,
+                                                          ch + 1 == chunks, d_leaves);
+    STWO_CHECK_LAUNCH();
+  }
+  if (state) STWO_CUDA_TRY(cudaFreeAsync(state, s));
+  return STWO_B200_OK;
+}
+
+// Builds layers [in_log - 1 .. stop_log] from layer `in` (2^in_log hashes);
+// outs_by_log[k] is the destination of layer log k.
+int build_node_layers_impl(const uint8_t* in, uint32_t in_log, uint32_t stop_log, int m31,
+                           uint8_t* const* outs_by_log, cudaStream_t s, char* err, size_t err_len) {
+  uint32_t cur_log = in_log;
+  const uint8_t* cur = in;
+  while (cur_log > stop_log) {
+    uint32_t levels = std::min<uint32_t>(8, cur_log - stop_log);
+    uint64_t parents0 = 1ull << (cur_log - 1);
+    uint32_t width = (uint32_t)std::min<uint64_t>(256, parents0);
+    // a block produces width >> (lv) parents at level lv; keep it >= 1
+    while (levels > 1 && (width >> (levels - 1)) == 0) levels--;
+    NodeOuts o;
+    for (uint32_t lv = 0; lv < levels; lv++) o.out[lv] = outs_by_log[cur_log - 1 - lv];
+    unsigned blocks = (unsigned)(parents0 / width);
+    node_layers_kernel<<<blocks, 256, 0, s>>>(cur, cur_log, levels, m31, o);
+    STWO_CHECK_LAUNCH();
+    cur = outs_by_log[cur_log - levels];
+    cur_log -= levels;
+  }
+  return STWO_B200_OK;
+}
+
+}  // namespace stwo_b200
+
+using namespace stwo_b200;
+
+extern "C" int stwo_b200_merkle_build_leaves(const uint32_t* const* d_cols, const uint32_t* log_sizes,
+                                             uint32_t n_cols, uint32_t lifting_log_size, int m31_output,
+                                             uint8_t* d_leaves, void* stream, char* err, size_t err_len) {
+  int rc = build_leaves_impl(d_cols, log_sizes, n_cols, lifting_log_size, m31_output, d_leaves, as_stream(stream),
+                             err, err_len);
+  return rc ? rc : ok(err, err_len);
+}
+
+extern "C" int stwo_b200_merkle_build_next_layer(const uint8_t* d_prev, uint32_t prev_log_size, int m31_output,
+                                                 uint8_t* d_out, void* stream, char* err, size_t err_len) {
+  STWO_ARG_CHECK(prev_log_size >= 1 && prev_log_size <= 31, "bad layer log size %u", prev_log_size);
+  std::vector<uint8_t*> outs(prev_log_size, nullptr);
+  outs[prev_log_size - 1] = d_out;
+  int rc = build_node_layers_impl(d_prev, prev_log_size, prev_log_size - 1, m31_output, outs.data(),
+                                  as_stream(stream), err, err_len);
+  return rc ? rc : ok(err, err_len);
+}
+
+extern "C" int stwo_b200_merkle_build_layers(const uint32_t* const* d_cols, const uint32_t* log_sizes,
+                                             uint32_t n_cols, uint32_t lifting_log_size, int m31_output,
+                                             uint8_t* const* d_layers, void* stream, char* err, size_t err_len) {
+  cudaStream_t s = as_stream(stream);
+  STWO_ARG_CHECK(d_layers != nullptr, "null layers");
+  if (n_cols == 0) {
+    STWO_ARG_CHECK(lifting_log_size == 0, "empty commitment needs lifting_log_size 0");
+    int rc = build_leaves_impl(nullptr, nullptr, 0, 0, m31_output, d_layers[0], s, err, err_len);
+    return rc ? rc : ok(err, err_len);
+  }
+  // prover/vcs_lifted/ops.rs:37 stable sort by length.
+  std::vector<uint32_t> order(n_cols);
+  for (uint32_t i = 0; i < n_cols; i++) order[i] = i;
+  std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return log_sizes[a] < log_sizes[b]; });
+  std::vector<const uint32_t*> cols(n_cols);
+  std::vector<uint32_t> logs(n_cols);
+  for (uint32_t i = 0; i < n_cols; i++) {
+    cols[i] = d_cols[order[i]];
+    logs[i] = log_sizes[order[i]];
+  }
+  const uint32_t L = lifting_log_size;
+  int rc = build_leaves_impl(cols.data(), logs.data(), n_cols, L, m31_output, d_layers[L], s, err, err_len);
+  if (rc) return rc;
+  rc = build_node_layers_impl(d_layers[L], L, 0, m31_output, d_layers, s, err, err_len);
+  return rc ? rc : ok(err, err_len);
+}
+
+extern "C" int stwo_b200_merkle_build_nodes(uint8_t* const* d_layers, uint32_t lifting_log_size, int m31_output,
+                                            void* stream, char* err, size_t err_len) {
+  STWO_ARG_CHECK(d_layers != nullptr, "null layers");
+  STWO_ARG_CHECK(lifting_log_size <= 31, "bad lifting log size");
+  int rc = build_node_layers_impl(d_layers[lifting_log_size], lifting_log_size, 0, m31_output, d_layers,
+                                  as_stream(stream), err, err_len);
+  return rc ? rc : ok(err, err_len);
+}
+
+extern "C" int stwo_b200_commit_on_layer(uint32_t log_size, const uint8_t* d_prev, const uint32_t* const* d_cols,
+                                         uint32_t n_cols, int m31_output, uint8_t* d_out, void* stream, char* err,
+                                         size_t err_len) {
+  STWO_ARG_CHECK(log_size <= 30, "log size %u too large", log_size);
+  STWO_ARG_CHECK(n_cols <= kLeafMaxCols, "at most %d columns per layer", kLeafMaxCols);
+  LeafCols t;
+  for (uint32_t c = 0; c < n_cols; c++) {
+    t.col[c] = d_cols[c];
+    t.shift[c] = 0;
+  }
+  uint64_t n = 1ull << log_size;
+  commit_on_layer_kernel<<<grid_for(n, 256), 256, 0, as_stream(stream)>>>(log_size, d_prev, t, n_cols, m31_output,
+                                                                           d_out);
+  STWO_CHECK_LAUNCH();
+  return ok(err, err_len);
+}

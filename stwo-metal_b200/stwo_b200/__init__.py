@@ -1,0 +1,11 @@
+"""stwo_b200 -- B200-native (sm_100a) backend for stwo's commit + FRI path.
+
+The compute lives in ``libstwo_b200.so`` (hand-written CUDA kernels behind the
+flat C ABI of ``include/stwo_b200.h``); this package is its Python view.
+"""
+from . import ffi
+from .backend import (B200Backend, DeviceBuffer, DeviceColumn, SecureColumn, TwiddleTree, canonic_half_coset,
+                      layer_to_host, sync)
+
+__all__ = ["ffi", "B200Backend", "DeviceBuffer", "DeviceColumn", "SecureColumn", "TwiddleTree",
+           "canonic_half_coset", "layer_to_host", "sync"]

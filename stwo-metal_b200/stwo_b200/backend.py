@@ -1,0 +1,261 @@
+"""Python view of the B200 backend: device columns and stwo's Backend ops.
+
+Mirrors the trait surface of ``crates/stwo/src/prover/backend/mod.rs`` (ColumnOps,
+PolyOps, MerkleOpsLifted, MerkleOps, FriOps) over the C ABI in
+``include/stwo_b200.h``.  Columns live in device memory (:class:`DeviceColumn`);
+host copies happen only through :meth:`DeviceColumn.from_host` /
+:meth:`DeviceColumn.to_host`.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import ffi
+
+P = (1 << 31) - 1
+
+
+def as_stream(stream):
+    """cudaStream_t for ctypes: None (legacy default stream), an int handle
+    (e.g. torch.cuda.Stream().cuda_stream) or a c_void_p."""
+    if stream is None or isinstance(stream, C.c_void_p):
+        return stream
+    return C.c_void_p(int(stream))
+
+
+class DeviceBuffer:
+    """Device memory from the stream-ordered pool; freed on close()/GC."""
+
+    def __init__(self, nbytes: int, stream=None):
+        ffi.init()
+        self.nbytes = int(nbytes)
+        stream = as_stream(stream)
+        self.stream = stream
+        ptr = C.c_void_p()
+        ffi.call("stwo_b200_alloc", C.c_size_t(self.nbytes), C.byref(ptr), stream)
+        self.ptr = ptr.value or 0
+
+    def close(self):
+        if getattr(self, "ptr", 0):
+            ffi.call("stwo_b200_free", C.c_void_p(self.ptr), self.stream)
+            self.ptr = 0
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def upload(self, host: np.ndarray, offset: int = 0):
+        host = np.ascontiguousarray(host)
+        assert offset + host.nbytes <= self.nbytes
+        ffi.call("stwo_b200_memcpy_h2d", C.c_void_p(self.ptr + offset), host.ctypes.data_as(C.c_void_p),
+                 C.c_size_t(host.nbytes), self.stream)
+        sync(self.stream)
+
+    def download(self, dtype=np.uint32, count=None, offset: int = 0) -> np.ndarray:
+        dtype = np.dtype(dtype)
+        if count is None:
+            count = (self.nbytes - offset) // dtype.itemsize
+        out = np.empty(count, dtype)
+        ffi.call("stwo_b200_memcpy_d2h", out.ctypes.data_as(C.c_void_p), C.c_void_p(self.ptr + offset),
+                 C.c_size_t(out.nbytes), self.stream)
+        sync(self.stream)
+        return out
+
+
+def sync(stream=None):
+    ffi.call("stwo_b200_stream_sync", as_stream(stream))
+
+
+class DeviceColumn(DeviceBuffer):
+    """A column of M31 words on the device (Col<B200Backend, BaseField>)."""
+
+    def __init__(self, length: int, stream=None):
+        super().__init__(4 * length, stream)
+        self.length = int(length)
+
+    @property
+    def log_size(self) -> int:
+        return self.length.bit_length() - 1
+
+    @classmethod
+    def from_host(cls, values, stream=None) -> "DeviceColumn":
+        values = np.ascontiguousarray(values, dtype=np.uint32)
+        col = cls(values.size, stream)
+        if values.size:
+            col.upload(values)
+        return col
+
+    def to_host(self) -> np.ndarray:
+        return self.download(np.uint32, self.length)
+
+
+class SecureColumn:
+    """QM31 column as four M31 coordinate columns (SecureColumnByCoords)."""
+
+    def __init__(self, cols):
+        self.cols = list(cols)
+        assert len(self.cols) == 4
+
+    @classmethod
+    def from_host(cls, coords, stream=None):
+        return cls([DeviceColumn.from_host(c, stream) for c in coords])
+
+    @classmethod
+    def empty(cls, length, stream=None):
+        return cls([DeviceColumn(length, stream) for _ in range(4)])
+
+    def to_host(self):
+        return [c.to_host() for c in self.cols]
+
+    @property
+    def length(self):
+        return self.cols[0].length
+
+
+@dataclass
+class TwiddleTree:
+    """PolyOps::Twiddles: tree of the root coset (canonical values)."""
+    root_initial_index: int
+    log_size: int
+    twiddles: DeviceColumn
+    itwiddles: DeviceColumn
+
+
+def _ptr_array(cols):
+    return (C.c_void_p * max(1, len(cols)))(*[c.ptr for c in cols])
+
+
+def _u32_array(vals):
+    return (C.c_uint32 * max(1, len(vals)))(*[int(v) for v in vals])
+
+
+def canonic_half_coset(log_size: int):
+    """(initial_index, log_size) of CanonicCoset(log_size).half_coset."""
+    return 1 << (31 - (log_size + 1)), log_size - 1
+
+
+class B200Backend:
+    """The Backend trait surface on one B200 (all ops enqueue on `stream`)."""
+
+    def __init__(self, stream=None):
+        ffi.init()
+        self.stream = as_stream(stream)
+
+    # ---- PolyOps::precompute_twiddles --------------------------------------
+    def precompute_twiddles(self, initial_index: int, log_size: int) -> TwiddleTree:
+        tw = DeviceColumn(1 << log_size, self.stream)
+        itw = DeviceColumn(1 << log_size, self.stream)
+        ffi.call("stwo_b200_precompute_twiddles", C.c_uint64(initial_index), C.c_uint32(log_size),
+                 C.c_void_p(tw.ptr), C.c_void_p(itw.ptr), self.stream)
+        return TwiddleTree(initial_index, log_size, tw, itw)
+
+    # ---- ColumnOps::bit_reverse_column --------------------------------------
+    def bit_reverse_column(self, col: DeviceColumn):
+        ffi.call("stwo_b200_bit_reverse_column", C.c_void_p(col.ptr), C.c_uint32(col.log_size), self.stream)
+
+    # ---- PolyOps::interpolate_columns (in place) ------------------------------
+    def interpolate_columns(self, cols, tree: TwiddleTree, half_initial_indices=None):
+        his = None
+        if half_initial_indices is not None:
+            his = (C.c_uint64 * len(cols))(*half_initial_indices)
+        ffi.call("stwo_b200_interpolate_columns", _ptr_array(cols), _u32_array([c.log_size for c in cols]), his,
+                 C.c_uint32(len(cols)), C.c_void_p(tree.itwiddles.ptr), C.c_uint32(tree.log_size), self.stream)
+        return cols
+
+    def interpolate_columns_into(self, evals, coeffs, tree: TwiddleTree):
+        """Out-of-place interpolate: evals stay intact, coeffs receive the result."""
+        ffi.call("stwo_b200_interpolate_columns_into", _ptr_array(evals), _ptr_array(coeffs),
+                 _u32_array([c.log_size for c in evals]), None, C.c_uint32(len(evals)),
+                 C.c_void_p(tree.itwiddles.ptr), C.c_uint32(tree.log_size), self.stream)
+        return coeffs
+
+    def evaluate_polynomials_into(self, coeffs, log_blowup: int, tree: TwiddleTree, outs):
+        ffi.call("stwo_b200_evaluate_polynomials", _ptr_array(coeffs), _u32_array([c.log_size for c in coeffs]),
+                 C.c_uint32(len(coeffs)), C.c_uint32(log_blowup), _ptr_array(outs), C.c_void_p(tree.twiddles.ptr),
+                 C.c_uint32(tree.log_size), self.stream)
+        return outs
+
+    # ---- PolyOps::evaluate_polynomials ---------------------------------------
+    def evaluate_polynomials(self, coeffs, log_blowup: int, tree: TwiddleTree):
+        outs = [DeviceColumn(c.length << log_blowup, self.stream) for c in coeffs]
+        ffi.call("stwo_b200_evaluate_polynomials", _ptr_array(coeffs), _u32_array([c.log_size for c in coeffs]),
+                 C.c_uint32(len(coeffs)), C.c_uint32(log_blowup), _ptr_array(outs), C.c_void_p(tree.twiddles.ptr),
+                 C.c_uint32(tree.log_size), self.stream)
+        return outs
+
+    # ---- MerkleOpsLifted ----------------------------------------------------
+    def build_leaves(self, cols, lifting_log_size: int, m31_output: bool = False) -> DeviceBuffer:
+        n = (1 << lifting_log_size) if cols else 1
+        out = DeviceBuffer(32 * n, self.stream)
+        ffi.call("stwo_b200_merkle_build_leaves", _ptr_array(cols), _u32_array([c.log_size for c in cols]),
+                 C.c_uint32(len(cols)), C.c_uint32(lifting_log_size), C.c_int(int(m31_output)), C.c_void_p(out.ptr),
+                 self.stream)
+        return out
+
+    def build_next_layer(self, prev: DeviceBuffer, m31_output: bool = False) -> DeviceBuffer:
+        n = prev.nbytes // 32
+        out = DeviceBuffer(32 * (n // 2), self.stream)
+        ffi.call("stwo_b200_merkle_build_next_layer", C.c_void_p(prev.ptr), C.c_uint32(n.bit_length() - 1),
+                 C.c_int(int(m31_output)), C.c_void_p(out.ptr), self.stream)
+        return out
+
+    def build_merkle_layers(self, cols, lifting_log_size: int, m31_output: bool = False):
+        """Layers root first: layers[k] holds 2^k hashes."""
+        layers = [DeviceBuffer(32 << k, self.stream) for k in range(lifting_log_size + 1)]
+        ffi.call("stwo_b200_merkle_build_layers", _ptr_array(cols), _u32_array([c.log_size for c in cols]),
+                 C.c_uint32(len(cols)), C.c_uint32(lifting_log_size), C.c_int(int(m31_output)),
+                 _ptr_array(layers), self.stream)
+        return layers
+
+    def build_leaves_into(self, cols, lifting_log_size: int, out: DeviceBuffer, m31_output: bool = False):
+        ffi.call("stwo_b200_merkle_build_leaves", _ptr_array(cols), _u32_array([c.log_size for c in cols]),
+                 C.c_uint32(len(cols)), C.c_uint32(lifting_log_size), C.c_int(int(m31_output)), C.c_void_p(out.ptr),
+                 self.stream)
+        return out
+
+    def build_nodes(self, layers, m31_output: bool = False):
+        """Fills layers[L-1..0] from the leaves in layers[L]."""
+        ffi.call("stwo_b200_merkle_build_nodes", _ptr_array(layers), C.c_uint32(len(layers) - 1),
+                 C.c_int(int(m31_output)), self.stream)
+        return layers
+
+    # ---- MerkleOps::commit_on_layer ------------------------------------------
+    def commit_on_layer(self, log_size: int, prev, cols, m31_output: bool = False) -> DeviceBuffer:
+        out = DeviceBuffer(32 << log_size, self.stream)
+        ffi.call("stwo_b200_commit_on_layer", C.c_uint32(log_size), C.c_void_p(prev.ptr if prev else 0),
+                 _ptr_array(cols), C.c_uint32(len(cols)), C.c_int(int(m31_output)), C.c_void_p(out.ptr), self.stream)
+        return out
+
+    # ---- FriOps ---------------------------------------------------------------
+    def fold_line(self, ev: SecureColumn, alpha, tree: TwiddleTree, fold_step: int = 1) -> SecureColumn:
+        out = SecureColumn.empty(ev.length >> fold_step, self.stream)
+        ffi.call("stwo_b200_fold_line", _ptr_array(ev.cols), C.c_uint32(ev.cols[0].log_size), _u32_array(alpha),
+                 C.c_uint32(fold_step), C.c_void_p(tree.itwiddles.ptr), C.c_uint32(tree.log_size),
+                 _ptr_array(out.cols), self.stream)
+        return out
+
+    def fold_circle_into_line(self, dst: SecureColumn, src: SecureColumn, alpha, tree: TwiddleTree,
+                              half_initial_index=None):
+        log_n = src.cols[0].log_size
+        if half_initial_index is None:
+            half_initial_index = canonic_half_coset(log_n)[0]
+        ffi.call("stwo_b200_fold_circle_into_line", _ptr_array(dst.cols), _ptr_array(src.cols), C.c_uint32(log_n),
+                 C.c_uint64(half_initial_index), _u32_array(alpha), C.c_void_p(tree.itwiddles.ptr),
+                 C.c_uint32(tree.log_size), self.stream)
+        return dst
+
+    def decompose(self, ev: SecureColumn):
+        out = SecureColumn.empty(ev.length, self.stream)
+        lam = (C.c_uint32 * 4)()
+        ffi.call("stwo_b200_decompose", _ptr_array(ev.cols), C.c_uint32(ev.cols[0].log_size), _ptr_array(out.cols),
+                 lam, self.stream)
+        return out, np.array(list(lam), np.uint32)
+
+
+def layer_to_host(buf: DeviceBuffer) -> np.ndarray:
+    return buf.download(np.uint8).reshape(-1, 32)

@@ -1,0 +1,28 @@
+"""The C-ABI library loads and exports every symbol include/stwo_b200.h
+declares (no GPU needed: nothing is called)."""
+import ctypes
+import pytest
+
+from stwo_b200 import ffi
+
+
+def test_library_builds_and_loads():
+    lib = ffi.load()
+    assert "sm_100a" in ffi.version()
+    assert lib is not None
+
+
+def test_every_declared_symbol_is_exported():
+    names = ffi.declared_symbols()
+    assert len(names) >= 20
+    lib = ffi.load()
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_init_fails_loudly_without_gpu():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("GPU present")
+    with pytest.raises(ffi.B200Error):
+        ffi.call("stwo_b200_init", ctypes.c_int(0))

@@ -1,0 +1,217 @@
+"""GPU parity: every B200 kernel against the CPU oracle, bit-exact, through
+the C ABI.  Sizes cover the reference's edge cases: tiny domains (log 1-5,
+where SimdBackend falls back to CPU code), log 16/17 (the SIMD transpose
+boundary), columns < 16, = 16 and 17 (Blake2s block boundary), uneven size
+groups and P-valued words."""
+import numpy as np
+import pytest
+
+from stwo_b200 import B200Backend, DeviceColumn, SecureColumn, layer_to_host
+
+pytestmark = pytest.mark.gpu
+P = (1 << 31) - 1
+
+
+@pytest.fixture(scope="module")
+def be():
+    return B200Backend()
+
+
+def rng(seed):
+    return np.random.default_rng(seed)
+
+
+def rand_col(r, log_n):
+    return r.integers(0, P, 1 << log_n, dtype=np.uint32)
+
+
+@pytest.mark.parametrize("log_size", [0, 1, 2, 3, 5, 10, 16, 21])
+def test_twiddles(be, oracle, log_size):
+    init = 1 << (31 - (log_size + 2))
+    tree = be.precompute_twiddles(init, log_size)
+    tw, itw = oracle.precompute_twiddles(init, log_size)
+    assert (tree.twiddles.to_host() == tw).all()
+    assert (tree.itwiddles.to_host() == itw).all()
+
+
+@pytest.mark.parametrize("log_n", [1, 2, 5, 10, 17, 20])
+def test_bit_reverse(be, oracle, log_n):
+    v = rand_col(rng(log_n), log_n)
+    c = DeviceColumn.from_host(v)
+    be.bit_reverse_column(c)
+    assert (c.to_host() == oracle.bit_reverse(v)).all()
+
+
+LOGS = [1, 2, 3, 4, 5, 6, 8, 11, 12, 13, 16, 17, 20, 22]
+
+
+@pytest.fixture(scope="module")
+def big_tree(be, oracle):
+    init, lg = oracle.canonic_half_coset_root(25)
+    tw, itw = oracle.precompute_twiddles(init, lg)
+    return be.precompute_twiddles(init, lg), tw, itw
+
+
+@pytest.mark.parametrize("log_n", LOGS)
+def test_interpolate(be, oracle, big_tree, log_n):
+    tree, tw, itw = big_tree
+    vals = [rand_col(rng(1000 + log_n + k), log_n) for k in range(3)]
+    cols = [DeviceColumn.from_host(v) for v in vals]
+    be.interpolate_columns(cols, tree)
+    for v, c in zip(vals, cols):
+        assert (c.to_host() == oracle.interpolate(v, itw)).all()
+
+
+@pytest.mark.parametrize("log_n", LOGS)
+@pytest.mark.parametrize("log_blowup", [0, 1, 2])
+def test_evaluate(be, oracle, big_tree, log_n, log_blowup):
+    tree, tw, itw = big_tree
+    coeffs = [rand_col(rng(2000 + log_n), log_n)]
+    outs = be.evaluate_polynomials([DeviceColumn.from_host(coeffs[0])], log_blowup, tree)
+    ref = oracle.evaluate(coeffs[0], log_n + log_blowup, tw)
+    assert (outs[0].to_host() == ref).all()
+
+
+def test_uneven_batch_roundtrip(be, oracle, big_tree):
+    tree, tw, itw = big_tree
+    r = rng(7)
+    logs = [int(x) for x in r.integers(3, 15, 40)]
+    vals = [rand_col(r, l) for l in logs]
+    cols = [DeviceColumn.from_host(v) for v in vals]
+    be.interpolate_columns(cols, tree)
+    evs = be.evaluate_polynomials(cols, 2, tree)
+    for v, c, e, l in zip(vals, cols, evs, logs):
+        co = oracle.interpolate(v, itw)
+        assert (c.to_host() == co).all()
+        assert (e.to_host() == oracle.evaluate(co, l + 2, tw)).all()
+
+
+def test_p_valued_inputs(be, oracle, big_tree):
+    # Words equal to P (the redundant zero) propagate exactly like SimdBackend.
+    tree, tw, itw = big_tree
+    for log_n in [3, 6, 12, 14]:
+        v = rand_col(rng(log_n), log_n)
+        v[::3] = P
+        v[1::7] = 0
+        c = DeviceColumn.from_host(v)
+        be.interpolate_columns([c], tree)
+        assert (c.to_host() == oracle.interpolate(v, itw)).all()
+        e = be.evaluate_polynomials([DeviceColumn.from_host(v)], 1, tree)[0]
+        assert (e.to_host() == oracle.evaluate(v, log_n + 1, tw)).all()
+
+
+@pytest.mark.parametrize("logs,L", [
+    ([4, 4, 4], 4),
+    ([2, 3, 4], 4),
+    ([5] * 16, 5),
+    ([5] * 17, 5),
+    ([3, 7, 7, 1, 9, 9, 9, 2] + [6] * 20, 11),
+    ([10] * 33, 12),
+])
+@pytest.mark.parametrize("m31", [False, True])
+def test_merkle_layers(be, oracle, logs, L, m31):
+    r = rng(sum(logs) + L)
+    vals = [rand_col(r, l) for l in logs]
+    cols = [DeviceColumn.from_host(v) for v in vals]
+    layers = be.build_merkle_layers(cols, L, m31)
+    ref = oracle.merkle_build_layers(vals, L, m31)
+    for k in range(L + 1):
+        assert (layer_to_host(layers[k]) == ref[k]).all(), k
+
+
+def test_merkle_empty(be, oracle):
+    layers = be.build_merkle_layers([], 0)
+    assert (layer_to_host(layers[0]) == oracle.merkle_build_layers([], 0)[0]).all()
+
+
+def test_merkle_many_columns_chunked(be, oracle):
+    # More columns than one leaf launch holds: the chaining state is carried.
+    r = rng(99)
+    logs = [4] * 1100 + [6] * 30
+    vals = [rand_col(r, l) for l in logs]
+    cols = [DeviceColumn.from_host(v) for v in vals]
+    layers = be.build_merkle_layers(cols, 7)
+    ref = oracle.merkle_build_layers(vals, 7)
+    assert (layer_to_host(layers[0]) == ref[0]).all()
+    assert (layer_to_host(layers[7]) == ref[7]).all()
+
+
+def test_build_leaves_and_next_layer(be, oracle):
+    r = rng(5)
+    vals = [rand_col(r, l) for l in [3, 5, 5, 8]]
+    cols = [DeviceColumn.from_host(v) for v in vals]
+    leaves = be.build_leaves(cols, 9)
+    ref = oracle.merkle_build_leaves(vals, 9)
+    assert (layer_to_host(leaves) == ref).all()
+    nxt = be.build_next_layer(leaves)
+    assert (layer_to_host(nxt) == oracle.merkle_next_layer(ref)).all()
+
+
+@pytest.mark.parametrize("with_prev", [False, True])
+@pytest.mark.parametrize("n_cols", [0, 1, 16, 17])
+def test_commit_on_layer(be, oracle, with_prev, n_cols):
+    r = rng(n_cols * 2 + with_prev)
+    log_size = 6
+    vals = [rand_col(r, log_size) for _ in range(n_cols)]
+    prev_host = r.integers(0, 256, (2 << log_size, 32), dtype=np.uint8) if with_prev else None
+    prev = None
+    if with_prev:
+        from stwo_b200 import DeviceBuffer
+        prev = DeviceBuffer(prev_host.nbytes)
+        prev.upload(prev_host)
+    out = be.commit_on_layer(log_size, prev, [DeviceColumn.from_host(v) for v in vals])
+    ref = oracle.commit_on_layer(log_size, prev_host, vals)
+    assert (layer_to_host(out) == ref).all()
+
+
+def test_mixed_degree_commit_matches_oracle(be, oracle):
+    r = rng(11)
+    logs = [6, 4, 6, 2, 5]
+    vals = [rand_col(r, l) for l in logs]
+    ref = oracle.mixed_degree_commit(vals)
+    order = sorted(range(len(vals)), key=lambda i: -logs[i])
+    prev = None
+    for log_size in range(6, -1, -1):
+        cs = [DeviceColumn.from_host(vals[i]) for i in order if logs[i] == log_size]
+        prev = be.commit_on_layer(log_size, prev, cs)
+        assert (layer_to_host(prev) == ref[log_size]).all()
+
+
+@pytest.mark.parametrize("log_m", [1, 2, 4, 5, 9, 16])
+@pytest.mark.parametrize("fold_step", [1, 2, 3])
+def test_fold_line(be, oracle, big_tree, log_m, fold_step):
+    if fold_step > log_m:
+        pytest.skip("fold_step > log size")
+    tree, tw, itw = big_tree
+    r = rng(log_m * 10 + fold_step)
+    coords = [rand_col(r, log_m) for _ in range(4)]
+    alpha = r.integers(0, P, 4, dtype=np.uint32)
+    out = be.fold_line(SecureColumn.from_host(coords), alpha, tree, fold_step)
+    ref = oracle.fold_line(coords, itw, alpha, fold_step)
+    for a, b in zip(out.to_host(), ref):
+        assert (a == b).all()
+
+
+@pytest.mark.parametrize("log_n", [1, 2, 3, 4, 5, 6, 12, 18])
+def test_fold_circle_into_line(be, oracle, big_tree, log_n):
+    tree, tw, itw = big_tree
+    r = rng(300 + log_n)
+    src = [rand_col(r, log_n) for _ in range(4)]
+    dst = [rand_col(r, log_n - 1) for _ in range(4)]
+    alpha = r.integers(0, P, 4, dtype=np.uint32)
+    d = SecureColumn.from_host(dst)
+    be.fold_circle_into_line(d, SecureColumn.from_host(src), alpha, tree)
+    ref = oracle.fold_circle_into_line(dst, src, itw, alpha)
+    for a, b in zip(d.to_host(), ref):
+        assert (a == b).all()
+
+
+@pytest.mark.parametrize("log_n", [2, 4, 5, 10, 15])
+def test_decompose(be, oracle, log_n):
+    r = rng(400 + log_n)
+    coords = [rand_col(r, log_n) for _ in range(4)]
+    g, lam = be.decompose(SecureColumn.from_host(coords))
+    gr, lr = oracle.decompose(coords)
+    assert (lam == lr).all()
+    for a, b in zip(g.to_host(), gr):
+        assert (a == b).all()
