@@ -38,6 +38,7 @@ struct FftPass {
   uint32_t log_domain; // N: log size of the domain the twiddles belong to
   uint32_t layer0, T, C;
   uint32_t scale;      // outputs are multiplied by `scale` when != 1
+  uint32_t vec_io;     // 16-byte global loads/stores are legal for this launch
 };
 
 __device__ __forceinline__ uint32_t smem_idx(uint32_t e) { return e + (e >> 4); }
@@ -59,42 +60,34 @@ __device__ __forceinline__ void bfly(uint32_t& a, uint32_t& b, uint32_t t) {
   a = m31_add(a, m);
 }
 
-// One register stage over row bits [s0, s0 + RS) of the tile.
+// One register stage over tile row bits [s0, s0 + RS).  Twiddles come from
+// the per-tile table `tws`: layer lam (relative to layer0) at offset
+// 2^T - 2^(T - lam), indexed by row >> (lam + 1).
 template <int RS, bool INV>
-__device__ __forceinline__ void fft_stage(uint32_t* sm, const FftPass& p, uint64_t hi, uint32_t s0) {
-  const uint32_t T = p.T, C = p.C;
+__device__ __forceinline__ void fft_stage(uint32_t* __restrict__ sm, const uint32_t* __restrict__ tws, uint32_t T,
+                                          uint32_t C, uint32_t s0) {
   const uint32_t E = 1u << (T + C);
   const uint32_t groups = E >> RS;
   const uint32_t cmask = (1u << C) - 1;
   const uint32_t lowmask = (1u << s0) - 1;
   for (uint32_t q = threadIdx.x; q < groups; q += blockDim.x) {
-    uint32_t c = q & cmask;
-    uint32_t rest = q >> C;
-    uint32_t low = rest & lowmask;
-    uint32_t high = rest >> s0;
-    uint32_t rowbase = (high << (s0 + RS)) | low;
+    const uint32_t c = q & cmask;
+    const uint32_t rest = q >> C;
+    const uint32_t low = rest & lowmask;
+    const uint32_t high = rest >> s0;
+    const uint32_t rowbase = (high << (s0 + RS)) | low;
     uint32_t v[1 << RS];
 #pragma unroll
     for (int j = 0; j < (1 << RS); j++) v[j] = sm[smem_idx(((rowbase | ((uint32_t)j << s0)) << C) | c)];
-    // Global row index (in units of 2^layer0) of element j: (hi << T) + row.
-    const uint64_t growbase = (hi << T) + rowbase;
 #pragma unroll
     for (int kk = 0; kk < RS; kk++) {
       const int k = INV ? kk : (RS - 1 - kk);
-      const uint32_t layer = p.layer0 + s0 + k;
+      const uint32_t lam = s0 + k;
+      const uint32_t* tl = tws + ((1u << T) - (1u << (T - lam)));
 #pragma unroll
       for (int j = 0; j < (1 << RS); j++) {
         if (j & (1 << k)) continue;
-        uint64_t grow = growbase + ((uint64_t)j << s0);
-        uint32_t t;
-        if (layer == 0) {
-          // circle layer: g = grow (layer0 == 0), h = g >> 1
-          const uint32_t* lt0 = p.tree + (p.tree_len - (1ull << (p.log_domain - 1)));
-          t = circle_tw(lt0, grow >> 1);
-        } else {
-          const uint32_t* lt = p.tree + (p.tree_len - (1ull << (p.log_domain - layer)));
-          t = __ldg(lt + (grow >> (s0 + k + 1)));
-        }
+        const uint32_t t = tl[(rowbase | ((uint32_t)j << s0)) >> (lam + 1)];
         if (INV)
           ibfly(v[j], v[j | (1 << k)], t);
         else
@@ -107,58 +100,103 @@ __device__ __forceinline__ void fft_stage(uint32_t* sm, const FftPass& p, uint64
 }
 
 template <bool INV>
-__global__ void __launch_bounds__(256) fft_pass_kernel(FftPass p, FftCols cols) {
-  extern __shared__ uint32_t sm[];
+__global__ void __launch_bounds__(256, 3) fft_pass_kernel(FftPass p, FftCols cols) {
+  extern __shared__ uint32_t smem[];
+  const uint32_t T = p.T, C = p.C, L0 = p.layer0;
+  const uint32_t E = 1u << (T + C);
+  uint32_t* __restrict__ sm = smem;
+  uint32_t* __restrict__ tws = smem + E + (E >> 4) + 1;
   const uint32_t* __restrict__ src = cols.src[blockIdx.y];
   uint32_t* __restrict__ dst = cols.dst[blockIdx.y];
-  const uint32_t T = p.T, C = p.C, L0 = p.layer0;
   const uint64_t tile = blockIdx.x;
   const uint32_t lo_bits = L0 - C;  // L0 >= C
   const uint64_t lo = tile & ((1ull << lo_bits) - 1);
   const uint64_t hi = tile >> lo_bits;
   const uint64_t base = (hi << (L0 + T)) | (lo << C);
-  const uint32_t E = 1u << (T + C);
   const uint32_t cmask = (1u << C) - 1;
 
-  for (uint32_t e = threadIdx.x; e < E; e += blockDim.x) {
-    uint64_t g = base + ((uint64_t)(e >> C) << L0) + (e & cmask);
-    uint64_t gi = g & p.src_mask;
-    sm[smem_idx(e)] = gi < p.src_len ? __ldg(src + gi) : 0u;
+  // Stage this tile's twiddles: layer lam needs 2^(T-1-lam) consecutive
+  // entries starting at hi << (T-1-lam) of tree layer L0 + lam.
+  for (uint32_t lam = 0; lam < T; lam++) {
+    const uint32_t cnt = 1u << (T - 1 - lam);
+    const uint32_t off = (1u << T) - (1u << (T - lam));
+    const uint64_t h0 = hi << (T - 1 - lam);
+    const uint32_t layer = L0 + lam;
+    if (layer == 0) {
+      const uint32_t* lt0 = p.tree + (p.tree_len - (1ull << (p.log_domain - 1)));
+      for (uint32_t i = threadIdx.x; i < cnt; i += blockDim.x) tws[off + i] = circle_tw(lt0, h0 + i);
+    } else {
+      const uint32_t* lt = p.tree + (p.tree_len - (1ull << (p.log_domain - layer))) + h0;
+      for (uint32_t i = threadIdx.x; i < cnt; i += blockDim.x) tws[off + i] = __ldg(lt + i);
+    }
+  }
+
+  // Load the tile; rows of 2^C >= 4 words (or contiguous tiles) use 16-byte loads.
+  if (p.vec_io) {
+    for (uint32_t e = threadIdx.x * 4; e < E; e += blockDim.x * 4) {
+      const uint64_t g = base + ((uint64_t)(e >> C) << L0) + (e & cmask);
+      const uint64_t gi = g & p.src_mask;
+      const uint4 w = gi < p.src_len ? __ldg(reinterpret_cast<const uint4*>(src + gi)) : make_uint4(0, 0, 0, 0);
+      sm[smem_idx(e)] = w.x;
+      sm[smem_idx(e + 1)] = w.y;
+      sm[smem_idx(e + 2)] = w.z;
+      sm[smem_idx(e + 3)] = w.w;
+    }
+  } else {
+    for (uint32_t e = threadIdx.x; e < E; e += blockDim.x) {
+      const uint64_t g = base + ((uint64_t)(e >> C) << L0) + (e & cmask);
+      const uint64_t gi = g & p.src_mask;
+      sm[smem_idx(e)] = gi < p.src_len ? __ldg(src + gi) : 0u;
+    }
   }
   __syncthreads();
 
   if (INV) {
     for (uint32_t s0 = 0; s0 < T;) {
-      uint32_t rs = min(4u, T - s0);
+      const uint32_t rs = min(4u, T - s0);
       switch (rs) {
-        case 4: fft_stage<4, INV>(sm, p, hi, s0); break;
-        case 3: fft_stage<3, INV>(sm, p, hi, s0); break;
-        case 2: fft_stage<2, INV>(sm, p, hi, s0); break;
-        default: fft_stage<1, INV>(sm, p, hi, s0); break;
+        case 4: fft_stage<4, INV>(sm, tws, T, C, s0); break;
+        case 3: fft_stage<3, INV>(sm, tws, T, C, s0); break;
+        case 2: fft_stage<2, INV>(sm, tws, T, C, s0); break;
+        default: fft_stage<1, INV>(sm, tws, T, C, s0); break;
       }
       s0 += rs;
       __syncthreads();
     }
   } else {
     for (uint32_t top = T; top > 0;) {
-      uint32_t rs = min(4u, top);
-      uint32_t s0 = top - rs;
+      const uint32_t rs = min(4u, top);
+      const uint32_t s0 = top - rs;
       switch (rs) {
-        case 4: fft_stage<4, INV>(sm, p, hi, s0); break;
-        case 3: fft_stage<3, INV>(sm, p, hi, s0); break;
-        case 2: fft_stage<2, INV>(sm, p, hi, s0); break;
-        default: fft_stage<1, INV>(sm, p, hi, s0); break;
+        case 4: fft_stage<4, INV>(sm, tws, T, C, s0); break;
+        case 3: fft_stage<3, INV>(sm, tws, T, C, s0); break;
+        case 2: fft_stage<2, INV>(sm, tws, T, C, s0); break;
+        default: fft_stage<1, INV>(sm, tws, T, C, s0); break;
       }
       top = s0;
       __syncthreads();
     }
   }
 
-  const bool scale = p.scale != 1u;
-  for (uint32_t e = threadIdx.x; e < E; e += blockDim.x) {
-    uint64_t g = base + ((uint64_t)(e >> C) << L0) + (e & cmask);
-    uint32_t v = sm[smem_idx(e)];
-    dst[g] = scale ? m31_mul(v, p.scale) : v;
+  const uint32_t scale = p.scale;
+  if (p.vec_io) {
+    for (uint32_t e = threadIdx.x * 4; e < E; e += blockDim.x * 4) {
+      const uint64_t g = base + ((uint64_t)(e >> C) << L0) + (e & cmask);
+      uint4 w = make_uint4(sm[smem_idx(e)], sm[smem_idx(e + 1)], sm[smem_idx(e + 2)], sm[smem_idx(e + 3)]);
+      if (scale != 1u) {
+        w.x = m31_mul(w.x, scale);
+        w.y = m31_mul(w.y, scale);
+        w.z = m31_mul(w.z, scale);
+        w.w = m31_mul(w.w, scale);
+      }
+      *reinterpret_cast<uint4*>(dst + g) = w;
+    }
+  } else {
+    for (uint32_t e = threadIdx.x; e < E; e += blockDim.x) {
+      const uint64_t g = base + ((uint64_t)(e >> C) << L0) + (e & cmask);
+      const uint32_t v = sm[smem_idx(e)];
+      dst[g] = scale != 1u ? m31_mul(v, scale) : v;
+    }
   }
 }
 
@@ -276,7 +314,7 @@ static int launch_pass(const FftPass& p, const std::vector<const uint32_t*>& src
                        uint64_t total_log, cudaStream_t s, char* err, size_t err_len) {
   uint64_t tiles = 1ull << (total_log - p.T - p.C);
   size_t E = (size_t)1 << (p.T + p.C);
-  size_t smem = (E + E / 16 + 1) * sizeof(uint32_t);
+  size_t smem = (E + E / 16 + 1 + ((size_t)1 << p.T)) * sizeof(uint32_t);
   static bool attr_set[2] = {false, false};
   if (!attr_set[INV]) {
     STWO_CUDA_TRY(cudaFuncSetAttribute(fft_pass_kernel<INV>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
@@ -286,12 +324,18 @@ static int launch_pass(const FftPass& p, const std::vector<const uint32_t*>& src
   for (size_t c0 = 0; c0 < srcs.size(); c0 += kFftMaxCols) {
     FftCols cols;
     size_t nc = std::min<size_t>(kFftMaxCols, srcs.size() - c0);
+    bool aligned = true;
     for (size_t i = 0; i < nc; i++) {
       cols.src[i] = srcs[c0 + i];
       cols.dst[i] = dsts[c0 + i];
+      aligned = aligned && (reinterpret_cast<uintptr_t>(cols.src[i]) % 16 == 0) &&
+                (reinterpret_cast<uintptr_t>(cols.dst[i]) % 16 == 0);
     }
+    FftPass q = p;
+    q.vec_io = aligned && (p.C >= 2 || p.layer0 == 0) && E >= 4 && (p.src_mask & 3) == 3 &&
+               (p.src_len == ~0ull || p.src_len % 4 == 0);
     dim3 grid((unsigned)tiles, (unsigned)nc);
-    fft_pass_kernel<INV><<<grid, 256, smem, s>>>(p, cols);
+    fft_pass_kernel<INV><<<grid, 256, smem, s>>>(q, cols);
     STWO_CHECK_LAUNCH();
   }
   return STWO_B200_OK;
