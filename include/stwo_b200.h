@@ -140,6 +140,12 @@ int stwo_b200_merkle_build_layers(const uint32_t* const* d_cols, const uint32_t*
 int stwo_b200_merkle_build_nodes(uint8_t* const* d_layers, uint32_t lifting_log_size, int m31_output,
                                  void* stream, char* err, size_t err_len);
 
+/* Throughput probe (no reference counterpart): `blocks` x 256 threads each
+ * chain `iters` Blake2s compressions in registers.  compressions / elapsed
+ * time is the integer-pipe ceiling the leaf kernel is measured against. */
+int stwo_b200_blake2s_probe(uint32_t blocks, uint32_t iters, uint32_t* d_out, void* stream, char* err,
+                            size_t err_len);
+
 /* ------------------------------------------------------------ MerkleOps -- */
 /* MerkleOps<Blake2sMerkleHasherGeneric<m31_output>>::commit_on_layer
  * (prover/vcs/ops.rs:24-28; cpu/blake2s.rs:13-26): node i = Blake2s(

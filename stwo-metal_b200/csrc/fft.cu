@@ -83,15 +83,19 @@ __device__ __forceinline__ void fft_stage(uint32_t* __restrict__ sm, const uint3
     for (int kk = 0; kk < RS; kk++) {
       const int k = INV ? kk : (RS - 1 - kk);
       const uint32_t lam = s0 + k;
-      const uint32_t* tl = tws + ((1u << T) - (1u << (T - lam)));
+      // Butterfly (j, j | 2^k) uses twiddle (high << (RS-1-k)) + (j >> (k+1)):
+      // 2^(RS-1-k) distinct values per group.
+      const uint32_t* tl = tws + ((1u << T) - (1u << (T - lam))) + (high << (RS - 1 - k));
+      uint32_t t[1 << (RS - 1)];
+#pragma unroll
+      for (int m = 0; m < (1 << (RS - 1 - k)); m++) t[m] = tl[m];
 #pragma unroll
       for (int j = 0; j < (1 << RS); j++) {
         if (j & (1 << k)) continue;
-        const uint32_t t = tl[(rowbase | ((uint32_t)j << s0)) >> (lam + 1)];
         if (INV)
-          ibfly(v[j], v[j | (1 << k)], t);
+          ibfly(v[j], v[j | (1 << k)], t[j >> (k + 1)]);
         else
-          bfly(v[j], v[j | (1 << k)], t);
+          bfly(v[j], v[j | (1 << k)], t[j >> (k + 1)]);
       }
     }
 #pragma unroll
@@ -100,7 +104,7 @@ __device__ __forceinline__ void fft_stage(uint32_t* __restrict__ sm, const uint3
 }
 
 template <bool INV>
-__global__ void __launch_bounds__(256, 3) fft_pass_kernel(FftPass p, FftCols cols) {
+__global__ void __launch_bounds__(256, 4) fft_pass_kernel(FftPass p, FftCols cols) {
   extern __shared__ uint32_t smem[];
   const uint32_t T = p.T, C = p.C, L0 = p.layer0;
   const uint32_t E = 1u << (T + C);
@@ -335,7 +339,9 @@ static int launch_pass(const FftPass& p, const std::vector<const uint32_t*>& src
     q.vec_io = aligned && (p.C >= 2 || p.layer0 == 0) && E >= 4 && (p.src_mask & 3) == 3 &&
                (p.src_len == ~0ull || p.src_len % 4 == 0);
     dim3 grid((unsigned)tiles, (unsigned)nc);
-    fft_pass_kernel<INV><<<grid, 256, smem, s>>>(q, cols);
+    // one radix-16 group per thread per stage for small tiles
+    const unsigned threads = E <= 2048 ? 128 : 256;
+    fft_pass_kernel<INV><<<grid, threads, smem, s>>>(q, cols);
     STWO_CHECK_LAUNCH();
   }
   return STWO_B200_OK;

@@ -180,6 +180,25 @@ __global__ void __launch_bounds__(256) commit_on_layer_kernel(uint32_t log_size,
   }
 }
 
+// Blake2s throughput probe: every thread chains `iters` compressions on
+// register-resident data (no memory traffic), giving the integer-pipe ceiling
+// for exactly the op mix the leaf and node kernels execute.
+__global__ void __launch_bounds__(256) blake2s_probe_kernel(uint32_t iters, uint32_t* out) {
+  uint32_t h[8];
+  blake2s_init(h);
+  uint32_t m[16];
+#pragma unroll
+  for (int k = 0; k < 16; k++) m[k] = threadIdx.x * 16 + k + blockIdx.x;
+  for (uint32_t it = 0; it < iters; it++) {
+    blake2s_compress(h, m, 64 * (it + 1), false);
+    m[it & 15] ^= h[0];
+  }
+  uint32_t x = 0;
+#pragma unroll
+  for (int k = 0; k < 8; k++) x ^= h[k];
+  if (x == 0x12345678u) out[0] = x;  // keeps the chain live
+}
+
 static unsigned grid_for(uint64_t n, unsigned threads) {
   uint64_t b = (n + threads - 1) / threads;
   return (unsigned)std::min<uint64_t>(std::max<uint64_t>(b, 1), 148ull * 64);
@@ -300,6 +319,14 @@ extern "C" int stwo_b200_merkle_build_nodes(uint8_t* const* d_layers, uint32_t l
   int rc = build_node_layers_impl(d_layers[lifting_log_size], lifting_log_size, 0, m31_output, d_layers,
                                   as_stream(stream), err, err_len);
   return rc ? rc : ok(err, err_len);
+}
+
+extern "C" int stwo_b200_blake2s_probe(uint32_t blocks, uint32_t iters, uint32_t* d_out, void* stream, char* err,
+                                       size_t err_len) {
+  STWO_ARG_CHECK(blocks >= 1 && d_out, "bad probe arguments");
+  blake2s_probe_kernel<<<blocks, 256, 0, as_stream(stream)>>>(iters, d_out);
+  STWO_CHECK_LAUNCH();
+  return ok(err, err_len);
 }
 
 extern "C" int stwo_b200_commit_on_layer(uint32_t log_size, const uint8_t* d_prev, const uint32_t* const* d_cols,
