@@ -35,6 +35,7 @@ def lib():
         _lib = C.CDLL(_LIB_PATH)
         _lib.oracle_last_error.restype = C.c_char_p
         _lib.oracle_channel_grind.restype = C.c_uint64
+        _lib.oracle_last_intermediate.restype = C.c_size_t
     return _lib
 
 
@@ -319,3 +320,51 @@ class Channel:
 
     def grind(self, bits: int) -> int:
         return int(lib().oracle_channel_grind(C.byref(self.s), C.c_uint32(bits)))
+
+
+class WideFibConfig(C.Structure):
+    _fields_ = [("log_n_rows", C.c_uint32), ("n_cols", C.c_uint32), ("log_blowup", C.c_uint32),
+                ("pow_bits", C.c_uint32), ("n_queries", C.c_uint32), ("log_last_layer_degree_bound", C.c_uint32),
+                ("line_fold_step", C.c_uint32), ("m31_channel", C.c_int32)]
+
+
+def wide_fib_config(log_n_rows: int, n_cols: int = 100, log_blowup: int = 1, pow_bits: int = 10, n_queries: int = 3,
+                    log_last_layer_degree_bound: int = 0, line_fold_step: int = 1, m31_channel: bool = False):
+    return WideFibConfig(log_n_rows, n_cols, log_blowup, pow_bits, n_queries, log_last_layer_degree_bound,
+                         line_fold_step, int(m31_channel))
+
+
+def wide_fib_inputs(log_n_rows: int, seed: int):
+    """First two trace columns, uniform in [0, P) (seeded numpy PCG64)."""
+    r = np.random.default_rng(seed)
+    return (r.integers(0, P, 1 << log_n_rows, dtype=np.uint32), r.integers(0, P, 1 << log_n_rows, dtype=np.uint32))
+
+
+def prove_wide_fib(cfg: WideFibConfig, a, b) -> bytes:
+    a, b = _u32(a), _u32(b)
+    n = C.c_size_t()
+    _check(lib().oracle_prove_wide_fib(C.byref(cfg), _p(a), _p(b), C.byref(n)))
+    out = (C.c_uint8 * n.value)()
+    lib().oracle_last_proof(out)
+    return bytes(out)
+
+
+def last_intermediate(which: int, k: int) -> np.ndarray:
+    n = lib().oracle_last_intermediate(C.c_int(which), C.c_int(k), None)
+    out = np.zeros(n, np.uint32)
+    lib().oracle_last_intermediate(C.c_int(which), C.c_int(k), _p(out))
+    return out
+
+
+def last_roots(n_trees: int = 3):
+    out = (C.c_uint8 * (32 * n_trees))()
+    lib().oracle_last_roots(out)
+    return [bytes(out[32 * i:32 * (i + 1)]) for i in range(n_trees)]
+
+
+def verify_wide_fib(proof: bytes, log_n_rows: int, n_cols: int, m31: bool = False):
+    """Returns None when the proof verifies, else the rejection reason."""
+    buf = (C.c_uint8 * len(proof)).from_buffer_copy(proof)
+    rc = lib().oracle_verify_wide_fib(buf, C.c_size_t(len(proof)), C.c_uint32(log_n_rows), C.c_uint32(n_cols),
+                                      C.c_int(int(m31)))
+    return None if rc == 0 else lib().oracle_last_error().decode()

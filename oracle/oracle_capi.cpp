@@ -223,3 +223,50 @@ int oracle_channel_verify_pow(const OracleChannelState* s, uint32_t bits, uint64
 uint64_t oracle_channel_grind(const OracleChannelState* s, uint32_t bits) { return load(s).grind(bits); }
 
 }  // extern "C"
+
+// ---- Wide-Fibonacci prove (Blake2s Merkle channel) ----
+#include "stwo_oracle_prove.hpp"
+
+struct OracleWideFibConfig {
+  uint32_t log_n_rows, n_cols, log_blowup, pow_bits, n_queries, log_last_layer_degree_bound, line_fold_step;
+  int32_t m31_channel;
+};
+
+static WideFibConfig to_cfg(const OracleWideFibConfig* c) {
+  WideFibConfig w;
+  w.log_n_rows = c->log_n_rows; w.n_cols = c->n_cols; w.log_blowup = c->log_blowup; w.pow_bits = c->pow_bits;
+  w.n_queries = c->n_queries; w.log_last_layer_degree_bound = c->log_last_layer_degree_bound;
+  w.line_fold_step = c->line_fold_step; w.m31_channel = c->m31_channel != 0;
+  return w;
+}
+
+static std::vector<uint8_t> g_last_proof;
+static ProveTrace g_last_trace;
+
+// Proves; the serialized proof is kept until the next call (oracle_last_proof).
+extern "C" int oracle_prove_wide_fib(const OracleWideFibConfig* cfg, const uint32_t* a, const uint32_t* b,
+                                     size_t* proof_len) {
+  return guard([&] {
+    g_last_trace = ProveTrace{};
+    Proof p = prove_wide_fib(to_cfg(cfg), a, b, &g_last_trace);
+    g_last_proof = serialize(p);
+    *proof_len = g_last_proof.size();
+  });
+}
+extern "C" void oracle_last_proof(uint8_t* out) { std::memcpy(out, g_last_proof.data(), g_last_proof.size()); }
+// Intermediates of the last prove: which = 0 composition evals (coord k), 1 quotients (coord k).
+extern "C" size_t oracle_last_intermediate(int which, int k, uint32_t* out) {
+  const auto& v = which == 0 ? g_last_trace.composition_evals : g_last_trace.quotients;
+  if (k < 0 || (size_t)k >= v.size()) return 0;
+  if (out) std::memcpy(out, v[k].data(), v[k].size() * 4);
+  return v[k].size();
+}
+extern "C" void oracle_last_roots(uint8_t* out) {
+  for (size_t i = 0; i < g_last_trace.roots.size(); i++) std::memcpy(out + 32 * i, g_last_trace.roots[i].data(), 32);
+}
+
+// 0 = accepted; -1 = rejected (reason via oracle_last_error()).
+extern "C" int oracle_verify_wide_fib(const uint8_t* proof, size_t len, uint32_t log_n_rows, uint32_t n_cols,
+                                      int m31) {
+  return guard([&] { verify_wide_fib(proof, len, log_n_rows, n_cols, m31 != 0); });
+}

@@ -271,3 +271,29 @@ def test_decompose_small_lambda_zero(oracle):
     assert (lam == 0).all()
     for k in range(4):
         assert (g[k] == cols[k]).all()
+
+
+@pytest.mark.parametrize("log_n,cols,m31", [(4, 100, False), (5, 8, True), (8, 100, False), (6, 3, False),
+                                            (10, 16, False)])
+def test_wide_fib_prove_verify(oracle, log_n, cols, m31):
+    # examples/src/wide_fibonacci/mod.rs:188-244: prove then verify; tampered
+    # proofs are rejected.
+    a, b = oracle.wide_fib_inputs(log_n, 7)
+    cfg = oracle.wide_fib_config(log_n, cols, m31_channel=m31)
+    proof = oracle.prove_wide_fib(cfg, a, b)
+    assert oracle.verify_wide_fib(proof, log_n, cols, m31) is None
+    assert oracle.prove_wide_fib(cfg, a, b) == proof  # deterministic
+    rng = np.random.default_rng(log_n)
+    for pos in rng.integers(8, len(proof), 12):
+        bad = bytearray(proof)
+        bad[int(pos)] ^= 0x10
+        assert oracle.verify_wide_fib(bytes(bad), log_n, cols, m31) is not None
+
+
+def test_wide_fib_trace_definition(oracle):
+    # col[i+2] = col[i]^2 + col[i+1]^2: the committed trace root changes with
+    # the inputs, and the empty preprocessed tree root is Blake2s("").
+    a, b = oracle.wide_fib_inputs(5, 1)
+    oracle.prove_wide_fib(oracle.wide_fib_config(5, 10), a, b)
+    roots = oracle.last_roots()
+    assert roots[0] == hashlib.blake2s(b"").digest()
