@@ -181,6 +181,40 @@ int stwo_b200_fold_circle_into_line(uint32_t* const* d_dst4, const uint32_t* con
 int stwo_b200_decompose(const uint32_t* const* d_in4, uint32_t log_size, uint32_t* const* d_out4,
                         uint32_t* lambda_out, void* stream, char* err, size_t err_len);
 
+/* ----------------------------------------------------- Wide-Fibonacci prove */
+/* PcsConfig + FriConfig fields of crates/stwo/src/core/pcs/mod.rs:31-80 and
+ * core/fri.rs:31-80 (defaults: pow_bits 10, log_blowup 1, n_queries 3,
+ * log_last_layer_degree_bound 0, line_fold_step 1), plus the AIR shape
+ * (examples/src/wide_fibonacci/mod.rs:80-101) and the channel flavour
+ * (0 = Blake2sMerkleChannel, 1 = Blake2sM31MerkleChannel). */
+typedef struct stwo_b200_wide_fib_config {
+  uint32_t log_n_rows;
+  uint32_t n_cols;
+  uint32_t log_blowup;
+  uint32_t pow_bits;
+  uint32_t n_queries;
+  uint32_t log_last_layer_degree_bound;
+  uint32_t line_fold_step;
+  int32_t m31_channel;
+} stwo_b200_wide_fib_config;
+
+/* A prover owns every device buffer of one proof shape (twiddles, trace,
+ * trees, FRI layers) and reuses them across proofs on `stream`. */
+typedef struct stwo_b200_prover stwo_b200_prover;
+int stwo_b200_prover_create(const stwo_b200_wide_fib_config* cfg, stwo_b200_prover** out, void* stream, char* err,
+                            size_t err_len);
+int stwo_b200_prover_destroy(stwo_b200_prover* prover, char* err, size_t err_len);
+
+/* stwo::prover::prove::<B200Backend, Blake2sMerkleChannel> of the
+ * Wide-Fibonacci component (crates/stwo/src/prover/mod.rs:32-138, driven as in
+ * the reference harness fixtures/standalone-benchmarks/src/bin/
+ * wide_fibonacci_simd_prove.rs:117-150: empty preprocessed tree, trace tree,
+ * prove).  d_a / d_b: the first two trace columns (2^log_n_rows words each,
+ * device memory).  Writes the canonical proof bytes to proof_out (host) when
+ * non-NULL and its length to *proof_len.  Synchronises the prover's stream. */
+int stwo_b200_prove_wide_fib(stwo_b200_prover* prover, const uint32_t* d_a, const uint32_t* d_b,
+                             uint8_t* proof_out, size_t proof_cap, size_t* proof_len, char* err, size_t err_len);
+
 #ifdef __cplusplus
 }
 #endif

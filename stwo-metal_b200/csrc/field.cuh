@@ -84,3 +84,69 @@ __host__ __device__ __forceinline__ qm31 qm31_mul(qm31 x, qm31 y) {
 }
 
 }  // namespace stwo_b200
+
+namespace stwo_b200 {
+
+// ---- host/device helpers beyond the kernels' hot arithmetic ----
+__host__ __device__ __forceinline__ bool qm31_eq(qm31 x, qm31 y) {
+  return x.a == y.a && x.b == y.b && x.c == y.c && x.d == y.d;
+}
+__host__ __device__ __forceinline__ qm31 qm31_from_m31(uint32_t v) { return {v, 0, 0, 0}; }
+__host__ __device__ __forceinline__ qm31 qm31_one() { return {1, 0, 0, 0}; }
+__host__ __device__ __forceinline__ qm31 qm31_zero() { return {0, 0, 0, 0}; }
+__host__ __device__ __forceinline__ qm31 qm31_neg(qm31 x) { return {m31_neg(x.a), m31_neg(x.b), m31_neg(x.c), m31_neg(x.d)}; }
+// Complex conjugate over CM31: (x0 + x1 u) -> (x0 - x1 u) (core/fields/mod.rs:413-415).
+__host__ __device__ __forceinline__ qm31 qm31_conj(qm31 x) { return {x.a, x.b, m31_neg(x.c), m31_neg(x.d)}; }
+__host__ __device__ __forceinline__ cm31 cm31_neg(cm31 x) { return {m31_neg(x.a), m31_neg(x.b)}; }
+__host__ __device__ inline cm31 cm31_inv(cm31 x) {  // (a - bi) / (a^2 + b^2)
+  uint32_t d = m31_inv(m31_add(m31_sqr(x.a), m31_sqr(x.b)));
+  return cm31_mul({x.a, m31_neg(x.b)}, {d, 0});
+}
+__host__ __device__ inline qm31 qm31_inv(qm31 x) {  // core/fields/qm31.rs:125-133
+  cm31 x0{x.a, x.b}, x1{x.c, x.d};
+  cm31 b2 = cm31_mul(x1, x1);
+  cm31 ib2{m31_neg(b2.b), b2.a};
+  cm31 denom = cm31_sub(cm31_mul(x0, x0), cm31_add(cm31_add(b2, b2), ib2));
+  cm31 di = cm31_inv(denom);
+  cm31 r0 = cm31_mul(x0, di), r1 = cm31_mul(cm31_neg(x1), di);
+  return {r0.a, r0.b, r1.a, r1.b};
+}
+__host__ __device__ __forceinline__ qm31 qm31_mul_cm31(qm31 x, cm31 c) {
+  cm31 a = cm31_mul({x.a, x.b}, c), b = cm31_mul({x.c, x.d}, c);
+  return {a.a, a.b, b.a, b.b};
+}
+
+// Circle points over M31 and QM31.
+struct cpoint {
+  uint32_t x, y;
+};
+__host__ __device__ __forceinline__ cpoint cpoint_add(cpoint p, cpoint q) {
+  return {m31_sub(m31_mul(p.x, q.x), m31_mul(p.y, q.y)), m31_add(m31_mul(p.x, q.y), m31_mul(p.y, q.x))};
+}
+struct spoint {
+  qm31 x, y;
+};
+__host__ __device__ inline spoint spoint_add(spoint p, spoint q) {
+  return {qm31_sub(qm31_mul(p.x, q.x), qm31_mul(p.y, q.y)), qm31_add(qm31_mul(p.x, q.y), qm31_mul(p.y, q.x))};
+}
+__host__ __device__ inline qm31 qm31_double_x(qm31 x) {
+  qm31 s = qm31_mul(x, x);
+  return qm31_sub(qm31_add(s, s), qm31_one());
+}
+__host__ __device__ inline spoint spoint_repeated_double(spoint p, uint32_t n) {
+  for (uint32_t i = 0; i < n; i++) p = spoint_add(p, p);
+  return p;
+}
+
+// Circle point of index i (GEN^i, GEN = M31_CIRCLE_GEN of crates/stwo/src/core/circle.rs:202-205).
+__host__ __device__ inline cpoint index_to_cpoint(uint64_t idx) {
+  cpoint g{2u, 1268011823u}, r{1u, 0u};
+  idx &= (1ull << 31) - 1;
+  for (int b = 0; b < 31; b++) {
+    if ((idx >> b) & 1) r = cpoint_add(r, g);
+    g = cpoint_add(g, g);
+  }
+  return r;
+}
+
+}  // namespace stwo_b200

@@ -1,0 +1,945 @@
+// The B200 Wide-Fibonacci prover: stwo's prove flow (crates/stwo/src/prover/mod.rs:41-138)
+// for the Wide-Fibonacci AIR (examples/src/wide_fibonacci/mod.rs:27-101) over the
+// Blake2s Merkle channel, with every column-sized step on the device:
+//   trace generation, interpolate / evaluate (fft.cu), lifted Merkle commits
+//   (merkle.cu), the composition polynomial, OODS sampling, FRI quotients, the
+//   FRI folds (fri.cu), proof-of-work grinding and the decommitment gathers.
+// The host keeps the Fiat-Shamir channel and assembles the proof; it waits on
+// the device only where the transcript needs a device value (roots, sampled
+// values, the last FRI layer, the nonce, the decommitted values).
+// Device buffers are allocated once per prover (resident between proofs).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "blake2s.cuh"
+#include "channel.hpp"
+#include "common.cuh"
+#include "field.cuh"
+
+namespace stwo_b200 {
+
+int build_leaves_impl(const uint32_t* const* d_cols, const uint32_t* log_sizes, uint32_t n_cols, uint32_t L,
+                      int m31, uint8_t* d_leaves, cudaStream_t s, char* err, size_t err_len);
+int build_node_layers_impl(const uint8_t* in, uint32_t in_log, uint32_t stop_log, int m31,
+                           uint8_t* const* outs_by_log, cudaStream_t s, char* err, size_t err_len);
+
+// ----------------------------------------------------------------- kernels --
+
+// One thread per row: col[i+2] = col[i]^2 + col[i+1]^2 (wide_fibonacci/mod.rs:27-50).
+__global__ void wide_fib_trace_kernel(const uint32_t* __restrict__ a, const uint32_t* __restrict__ b,
+                                      uint32_t* __restrict__ cols, uint32_t n_cols, uint64_t rows) {
+  for (uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; r < rows; r += (uint64_t)gridDim.x * blockDim.x) {
+    uint32_t x = __ldg(a + r), y = __ldg(b + r);
+    cols[r] = x;
+    cols[rows + r] = y;
+    for (uint32_t c = 2; c < n_cols; c++) {
+      uint32_t z = m31_add(m31_sqr(x), m31_sqr(y));
+      cols[(uint64_t)c * rows + r] = z;
+      x = y;
+      y = z;
+    }
+  }
+}
+
+// Composition evaluation at every point of the evaluation domain
+// (constraint-framework/src/prover/component_prover.rs:91-160): for constraint
+// k (0-based) c_{k+2} - (c_k^2 + c_{k+1}^2) weighted by powers[k] (already
+// reversed), times the vanishing inverse of the point's trace-coset class.
+__global__ void composition_kernel(const uint32_t* __restrict__ evals, uint64_t col_stride, uint32_t n_cons,
+                                   const qm31* __restrict__ powers, const uint32_t* __restrict__ denom_inv,
+                                   uint32_t log_n, uint64_t n_points, uint32_t* __restrict__ out) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n_points;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    uint32_t a = __ldg(evals + i), b = __ldg(evals + col_stride + i);
+    qm31 row = qm31_zero();
+    for (uint32_t k = 0; k < n_cons; k++) {
+      uint32_t c = __ldg(evals + (uint64_t)(k + 2) * col_stride + i);
+      uint32_t cons = m31_sub(c, m31_add(m31_sqr(a), m31_sqr(b)));
+      row = qm31_add(row, qm31_mul_m31(powers[k], cons));
+      a = b;
+      b = c;
+    }
+    qm31 v = qm31_mul_m31(row, __ldg(denom_inv + (i >> log_n)));
+    out[i] = v.a;
+    out[n_points + i] = v.b;
+    out[2 * n_points + i] = v.c;
+    out[3 * n_points + i] = v.d;
+  }
+}
+
+// Polynomial values at one secure point: sum_j coeff_j * w_j where
+// w_j = prod over set bits b of j of f_b, f = [y, x, pi(x), pi^2(x), ...]
+// (the coefficient fold of prover/backend/cpu/circle.rs:82-99).  w_j =
+// w_hi[j >> h] * w_lo[j & (2^h - 1)].  Block (chunk, group) accumulates up to
+// kEvalGroup polynomials over a chunk of j.
+constexpr int kEvalGroup = 8;
+constexpr int kMaxPolys = 1024;
+struct PolyTable {
+  const uint32_t* p[kMaxPolys];
+};
+
+__global__ void __launch_bounds__(256) batch_eval_kernel(PolyTable t, uint32_t n_polys, uint32_t log_n, uint32_t h,
+                                                        const qm31* __restrict__ w_lo, const qm31* __restrict__ w_hi,
+                                                        qm31* __restrict__ partial) {
+  const uint32_t group = blockIdx.y;
+  const uint32_t p0 = group * kEvalGroup;
+  const uint32_t np = min((uint32_t)kEvalGroup, n_polys - p0);
+  const uint64_t n = 1ull << log_n;
+  const uint64_t lo_mask = (1ull << h) - 1;
+  qm31 acc[kEvalGroup];
+#pragma unroll
+  for (int q = 0; q < kEvalGroup; q++) acc[q] = qm31_zero();
+  for (uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; j < n; j += (uint64_t)gridDim.x * blockDim.x) {
+    qm31 w = qm31_mul(w_hi[j >> h], w_lo[j & lo_mask]);
+#pragma unroll
+    for (int q = 0; q < kEvalGroup; q++)
+      if (q < (int)np) acc[q] = qm31_add(acc[q], qm31_mul_m31(w, __ldg(t.p[p0 + q] + j)));
+  }
+  __shared__ qm31 red[256];
+  for (uint32_t q = 0; q < np; q++) {
+    red[threadIdx.x] = acc[q];
+    __syncthreads();
+    for (uint32_t s = blockDim.x / 2; s > 0; s >>= 1) {
+      if (threadIdx.x < s) red[threadIdx.x] = qm31_add(red[threadIdx.x], red[threadIdx.x + s]);
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) partial[(uint64_t)(p0 + q) * gridDim.x + blockIdx.x] = red[0];
+    __syncthreads();
+  }
+}
+
+__global__ void reduce_partials_kernel(const qm31* __restrict__ partial, uint32_t n_chunks, uint32_t n_polys,
+                                       qm31* __restrict__ out) {
+  uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n_polys) return;
+  qm31 s = qm31_zero();
+  for (uint32_t c = 0; c < n_chunks; c++) s = qm31_add(s, partial[(uint64_t)p * n_chunks + c]);
+  out[p] = s;
+}
+
+// FRI quotient of one sample batch (all columns sampled at point z, same
+// size): q(p) = [c * sum_k alpha^k f_k(p) - B - A * p.y] / den(p), den(p) =
+// (Re z.x - p.x) Im z.y - (Re z.y - p.y) Im z.x in CM31.  Equal, value for
+// value, to the line-coefficient form of prover/backend/simd/quotients.rs:34-164
+// with core/constraints.rs:119-134 coefficients.
+struct QuotientParams {
+  qm31 c, A, B;
+  cm31 prx, pix, pry, piy;
+  cpoint init;           // first point of the half coset
+  cpoint step_pow[31];   // step * 2^b
+  uint32_t log_size;     // lifting domain
+};
+
+__global__ void __launch_bounds__(256) quotient_kernel(QuotientParams q, PolyTable cols, uint32_t n_cols,
+                                                      const qm31* __restrict__ alpha_pows, uint32_t* __restrict__ out) {
+  const uint64_t n = 1ull << q.log_size;
+  const uint64_t half = n >> 1;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    qm31 acc = qm31_zero();
+    for (uint32_t k = 0; k < n_cols; k++) acc = qm31_add(acc, qm31_mul_m31(alpha_pows[k], __ldg(cols.p[k] + i)));
+    // domain point at bit-reversed position i (core/poly/circle/domain.rs:56-66)
+    uint64_t j = __brevll(i) >> (64 - q.log_size);
+    uint64_t jj = j < half ? j : j - half;
+    cpoint pt = q.init;
+    for (uint32_t b = 0; b + 1 < q.log_size; b++)
+      if ((jj >> b) & 1) pt = cpoint_add(pt, q.step_pow[b]);
+    if (j >= half) pt.y = m31_neg(pt.y);  // -index is the conjugate point
+    qm31 num = qm31_sub(qm31_mul(q.c, acc), q.B);
+    qm31 full = qm31_sub(num, qm31_mul_m31(q.A, pt.y));
+    cm31 den = cm31_sub(cm31_mul(cm31_sub(q.prx, cm31{pt.x, 0}), q.piy),
+                        cm31_mul(cm31_sub(q.pry, cm31{pt.y, 0}), q.pix));
+    qm31 v = qm31_mul_cm31(full, cm31_inv(den));
+    out[i] = v.a;
+    out[n + i] = v.b;
+    out[2 * n + i] = v.c;
+    out[3 * n + i] = v.d;
+  }
+}
+
+// Proof-of-work search over nonces (hi << 32) | (low_base + t)
+// (prover/backend/simd/grind.rs:62-96): a hit needs trailing_zeros(word 0 of
+// Blake2s(prefixed_digest || LE64(nonce))) >= bits; the smallest hit wins.
+struct Digest8 {
+  uint32_t w[8];
+};
+__global__ void grind_kernel(Digest8 pre, uint32_t hi, uint32_t low_base, uint32_t bits, int m31,
+                             uint32_t* __restrict__ found) {
+  uint32_t low = low_base + blockIdx.x * blockDim.x + threadIdx.x;
+  uint32_t m[16];
+#pragma unroll
+  for (int k = 0; k < 8; k++) m[k] = pre.w[k];
+  m[8] = low;
+  m[9] = hi;
+#pragma unroll
+  for (int k = 10; k < 16; k++) m[k] = 0;
+  uint32_t h[8];
+  blake2s_init(h);
+  blake2s_compress(h, m, 40, true);
+  uint32_t w0 = m31 ? m31_reduce_u32(h[0]) : h[0];
+  uint32_t tz = w0 == 0 ? 32u : (uint32_t)__ffs(w0) - 1;
+  if (tz >= bits) atomicMin(found, low);
+}
+
+__global__ void gather_kernel(const uint64_t* __restrict__ addrs, uint32_t n, uint32_t* __restrict__ out) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = *reinterpret_cast<const uint32_t*>(addrs[i]);
+}
+
+static unsigned grid1d(uint64_t n, unsigned threads) {
+  uint64_t b = (n + threads - 1) / threads;
+  return (unsigned)std::min<uint64_t>(std::max<uint64_t>(b, 1), 148ull * 32);
+}
+
+// ------------------------------------------------------------- host side ----
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+};
+
+struct MerkleTree {  // lifted tree layers in one buffer, root first
+  uint8_t* base = nullptr;
+  uint32_t L = 0;
+  uint8_t* layer(uint32_t k) const { return base + (((size_t)1 << k) - 1) * 32; }
+  static size_t bytes_for(uint32_t L) { return (((size_t)2 << L) - 1) * 32; }
+};
+
+struct FriLayerBuf {
+  uint32_t log_size;
+  uint32_t* coords;  // 4 x 2^log_size
+  MerkleTree tree;
+  uint32_t fold_step;
+};
+
+struct GatherPlan {
+  std::vector<uint64_t> addrs;
+  size_t add_word(const void* p) {
+    addrs.push_back(reinterpret_cast<uint64_t>(p));
+    return addrs.size() - 1;
+  }
+  size_t add_hash(const uint8_t* p) {
+    size_t first = addrs.size();
+    for (int k = 0; k < 8; k++) addrs.push_back(reinterpret_cast<uint64_t>(p + 4 * k));
+    return first;
+  }
+};
+
+// Witness node (layer log, index) list of a lifted Merkle decommitment in
+// proof order (prover/vcs_lifted/prover.rs:114-185).
+static std::vector<std::pair<uint32_t, size_t>> witness_nodes(std::vector<size_t> queries, uint32_t L) {
+  std::vector<std::pair<uint32_t, size_t>> out;
+  queries.erase(std::unique(queries.begin(), queries.end()), queries.end());
+  std::vector<size_t> prev = queries;
+  for (uint32_t layer_log = L; layer_log-- > 0;) {
+    std::vector<size_t> cur;
+    for (size_t i = 0; i < prev.size();) {
+      size_t first = prev[i];
+      bool pair = (i + 1 < prev.size()) && ((first ^ 1) == prev[i + 1]);
+      if (!pair) out.push_back({layer_log + 1, first ^ 1});
+      cur.push_back(first >> 1);
+      i += pair ? 2 : 1;
+    }
+    prev = cur;
+  }
+  return out;
+}
+
+struct ProofOut {
+  std::vector<uint8_t> bytes;
+  void u32(uint32_t v) { for (int i = 0; i < 4; i++) bytes.push_back((v >> (8 * i)) & 0xFF); }
+  void u64(uint64_t v) { for (int i = 0; i < 8; i++) bytes.push_back((v >> (8 * i)) & 0xFF); }
+  void q(const qm31& x) { u32(x.a); u32(x.b); u32(x.c); u32(x.d); }
+  void h(const uint8_t* p) { bytes.insert(bytes.end(), p, p + 32); }
+};
+
+class WideFibProver {
+ public:
+  stwo_b200_wide_fib_config cfg;
+  uint32_t log_n, N, blowup, eval_log, L1, L2, lift, tree_log;
+  cudaStream_t s;
+
+  uint32_t *d_tw = nullptr, *d_itw = nullptr;
+  uint32_t* d_coeffs = nullptr;   // N x 2^log_n (trace, then coefficients)
+  uint32_t* d_evals = nullptr;    // N x 2^L1
+  uint32_t* d_ext = nullptr;      // N x 2^eval_log when eval_log != L1
+  MerkleTree t1, t2, tq;
+  uint32_t* d_comp = nullptr;     // 4 x 2^eval_log (evals, then coefficients)
+  uint32_t* d_comp_lde = nullptr; // 8 x 2^L2
+  uint32_t* d_quot = nullptr;     // 4 x 2^lift
+  std::vector<FriLayerBuf> fri;   // inner layers
+  uint32_t* d_last = nullptr;     // 4 x 2^last_log
+  qm31* d_small = nullptr;        // powers / weights / partials / alpha powers
+  uint32_t* d_denom = nullptr;
+  uint32_t* d_found = nullptr;
+  uint64_t* d_gather_addr = nullptr;
+  uint32_t* d_gather_out = nullptr;
+  size_t gather_cap = 0;
+  qm31* h_pinned = nullptr;       // staging for small uploads / downloads
+  size_t h_pinned_bytes = 0;
+  std::vector<void*> allocs;
+
+  ~WideFibProver() {
+    for (void* p : allocs) cudaFree(p);
+    if (h_pinned) cudaFreeHost(h_pinned);
+  }
+
+  int alloc(void** p, size_t bytes, char* err, size_t err_len) {
+    STWO_CUDA_TRY(cudaMalloc(p, std::max<size_t>(bytes, 16)));
+    allocs.push_back(*p);
+    return 0;
+  }
+
+  int init(const stwo_b200_wide_fib_config& c, cudaStream_t stream, char* err, size_t err_len) {
+    cfg = c;
+    s = stream;
+    log_n = c.log_n_rows;
+    N = c.n_cols;
+    blowup = c.log_blowup;
+    STWO_ARG_CHECK(N >= 3 && N <= kMaxPolys - 8, "n_cols %u out of range [3, %d]", N, kMaxPolys - 8);
+    STWO_ARG_CHECK(log_n >= 4 && log_n + blowup <= 28, "log_n_rows %u / log_blowup %u out of range", log_n, blowup);
+    STWO_ARG_CHECK(blowup >= 1 && blowup <= 16, "log_blowup %u out of range", blowup);
+    STWO_ARG_CHECK(c.line_fold_step >= 1 && c.line_fold_step <= 6, "line_fold_step %u unsupported", c.line_fold_step);
+    STWO_ARG_CHECK(c.pow_bits <= 32, "pow_bits > 32 is not supported");
+    STWO_ARG_CHECK(c.n_queries >= 1 && c.n_queries <= 4096, "n_queries %u out of range", c.n_queries);
+    STWO_ARG_CHECK(c.log_last_layer_degree_bound <= 10, "log_last_layer_degree_bound out of range");
+    eval_log = log_n + 1;           // max_constraint_log_degree_bound of Wide-Fibonacci
+    L1 = log_n + blowup;            // trace tree
+    L2 = eval_log - 1 + blowup;     // composition tree (lifting size)
+    lift = L2;
+    STWO_ARG_CHECK(L1 <= lift, "trace tree larger than the lifting domain");
+    STWO_ARG_CHECK(lift - 1 >= c.log_last_layer_degree_bound + blowup, "domain too small for the FRI config");
+    tree_log = log_n + blowup;      // twiddles of CanonicCoset(log_n + 1 + blowup).half_coset
+    int rc;
+    if ((rc = alloc((void**)&d_tw, 4ull << tree_log, err, err_len))) return rc;
+    if ((rc = alloc((void**)&d_itw, 4ull << tree_log, err, err_len))) return rc;
+    rc = stwo_b200_precompute_twiddles(1ull << (31 - (tree_log + 1)), tree_log, d_tw, d_itw, s, err, err_len);
+    if (rc) return rc;
+    if ((rc = alloc((void**)&d_coeffs, (4ull * N) << log_n, err, err_len))) return rc;
+    if ((rc = alloc((void**)&d_evals, (4ull * N) << L1, err, err_len))) return rc;
+    if (eval_log != L1 && (rc = alloc((void**)&d_ext, (4ull * N) << eval_log, err, err_len))) return rc;
+    t1.L = L1;
+    if ((rc = alloc((void**)&t1.base, MerkleTree::bytes_for(L1), err, err_len))) return rc;
+    t2.L = L2;
+    if ((rc = alloc((void**)&t2.base, MerkleTree::bytes_for(L2), err, err_len))) return rc;
+    tq.L = lift;
+    if ((rc = alloc((void**)&tq.base, MerkleTree::bytes_for(lift), err, err_len))) return rc;
+    if ((rc = alloc((void**)&d_comp, 16ull << eval_log, err, err_len))) return rc;
+    if ((rc = alloc((void**)&d_comp_lde, 32ull << L2, err, err_len))) return rc;
+    if ((rc = alloc((void**)&d_quot, 16ull << lift, err, err_len))) return rc;
+    // FRI inner layers (prover/fri.rs:188-262).
+    uint32_t last_log = c.log_last_layer_degree_bound + blowup;
+    uint32_t cur = lift - 1;
+    if (cur != last_log) {
+      while (cur > last_log + c.line_fold_step) {
+        fri.push_back({cur, nullptr, {}, c.line_fold_step});
+        cur -= c.line_fold_step;
+      }
+      fri.push_back({cur, nullptr, {}, cur - last_log});
+      cur = last_log;
+    }
+    // the first inner layer receives the circle fold; the others the line folds
+    for (auto& l : fri) {
+      if ((rc = alloc((void**)&l.coords, 16ull << l.log_size, err, err_len))) return rc;
+      l.tree.L = l.log_size;
+      if ((rc = alloc((void**)&l.tree.base, MerkleTree::bytes_for(l.log_size), err, err_len))) return rc;
+    }
+    if ((rc = alloc((void**)&d_last, 16ull << last_log, err, err_len))) return rc;
+    size_t small_q = std::max<size_t>(4096, 2 * (1u << 12) + (size_t)kMaxPolys * 1024);
+    if ((rc = alloc((void**)&d_small, small_q * sizeof(qm31), err, err_len))) return rc;
+    if ((rc = alloc((void**)&d_denom, 4ull << (eval_log - log_n), err, err_len))) return rc;
+    if ((rc = alloc((void**)&d_found, 64, err, err_len))) return rc;
+    h_pinned_bytes = std::max<size_t>(small_q * sizeof(qm31), 16ull << last_log);
+    STWO_CUDA_TRY(cudaMallocHost((void**)&h_pinned, h_pinned_bytes));
+    STWO_CUDA_TRY(cudaStreamSynchronize(s));
+    return 0;
+  }
+
+  int ensure_gather(size_t n, char* err, size_t err_len) {
+    if (n <= gather_cap) return 0;
+    int rc;
+    size_t cap = std::max<size_t>(n, 4096);
+    if ((rc = alloc((void**)&d_gather_addr, cap * 8, err, err_len))) return rc;
+    if ((rc = alloc((void**)&d_gather_out, cap * 4, err, err_len))) return rc;
+    gather_cap = cap;
+    return 0;
+  }
+
+  int download_root(const MerkleTree& t, Hash32& root, char* err, size_t err_len) {
+    STWO_CUDA_TRY(cudaMemcpyAsync(h_pinned, t.layer(0), 32, cudaMemcpyDeviceToHost, s));
+    STWO_CUDA_TRY(cudaStreamSynchronize(s));
+    std::memcpy(root.data(), h_pinned, 32);
+    return 0;
+  }
+
+  int commit_columns(uint32_t* const* cols, const std::vector<uint32_t>& logs, MerkleTree& t, char* err,
+                     size_t err_len) {
+    std::vector<uint8_t*> layers(t.L + 1);
+    for (uint32_t k = 0; k <= t.L; k++) layers[k] = t.layer(k);
+    return stwo_b200_merkle_build_layers(const_cast<const uint32_t* const*>(cols), logs.data(), (uint32_t)logs.size(),
+                                         t.L, cfg.m31_channel, layers.data(), s, err, err_len);
+  }
+
+  int prove(const uint32_t* d_a, const uint32_t* d_b, ProofOut& out, char* err, size_t err_len);
+};
+
+int WideFibProver::prove(const uint32_t* d_a, const uint32_t* d_b, ProofOut& out, char* err, size_t err_len) {
+  const bool m31 = cfg.m31_channel != 0;
+  HostChannel ch(m31);
+  int rc;
+  const uint64_t rows = 1ull << log_n;
+  // ---- tree 0: empty preprocessed trace -> Blake2s("") ----
+  Hash32 root0;
+  {
+    HostBlake2s e;
+    root0 = e.finalize(m31);
+  }
+  ch.mix_root(root0);
+
+  // ---- tree 1: trace ----
+  wide_fib_trace_kernel<<<grid1d(rows, 256), 256, 0, s>>>(d_a, d_b, d_coeffs, N, rows);
+  STWO_CHECK_LAUNCH();
+  std::vector<uint32_t*> coeff_ptrs(N), eval_ptrs(N);
+  std::vector<uint32_t> logs_n(N, log_n), logs_1(N, L1);
+  for (uint32_t c = 0; c < N; c++) {
+    coeff_ptrs[c] = d_coeffs + (uint64_t)c * rows;
+    eval_ptrs[c] = d_evals + ((uint64_t)c << L1);
+  }
+  if ((rc = stwo_b200_interpolate_columns(coeff_ptrs.data(), logs_n.data(), nullptr, N, d_itw, tree_log, s, err,
+                                          err_len)))
+    return rc;
+  if ((rc = stwo_b200_evaluate_polynomials(const_cast<const uint32_t* const*>(coeff_ptrs.data()), logs_n.data(), N,
+                                           blowup, eval_ptrs.data(), d_tw, tree_log, s, err, err_len)))
+    return rc;
+  if ((rc = commit_columns(eval_ptrs.data(), logs_1, t1, err, err_len))) return rc;
+  Hash32 root1;
+  if ((rc = download_root(t1, root1, err, err_len))) return rc;
+  ch.mix_root(root1);
+
+  // ---- composition (prover/mod.rs:57-77) ----
+  const qm31 random_coeff = ch.draw_secure_felt();
+  const uint32_t n_cons = N - 2;
+  {
+    qm31* pw = h_pinned;
+    qm31 acc = qm31_one();
+    for (uint32_t k = 0; k < n_cons; k++) {
+      pw[n_cons - 1 - k] = acc;  // reversed powers
+      acc = qm31_mul(acc, random_coeff);
+    }
+    STWO_CUDA_TRY(cudaMemcpyAsync(d_small, pw, n_cons * sizeof(qm31), cudaMemcpyHostToDevice, s));
+    // vanishing inverses of the 2^(eval_log - log_n) trace-coset classes, bit-reversed
+    uint32_t log_expand = eval_log - log_n;
+    uint32_t* dn = reinterpret_cast<uint32_t*>(h_pinned + n_cons + 1);
+    for (uint32_t j = 0; j < (1u << log_expand); j++) {
+      // eval_domain.at(j): half coset of CanonicCoset(eval_log)
+      uint64_t init = 1ull << (31 - (eval_log + 1)), step = 1ull << (31 - (eval_log - 1));
+      uint64_t half = 1ull << (eval_log - 1);
+      uint64_t idx = j < half ? (init + step * j) : ((1ull << 31) - ((init + step * (j - half)) & ((1ull << 31) - 1)));
+      cpoint p = index_to_cpoint(idx);
+      // coset_vanishing(CanonicCoset(log_n).coset, p) (core/constraints.rs:12-34)
+      uint64_t cinit = 1ull << (31 - (log_n + 1)), cstep = 1ull << (31 - log_n);
+      cpoint ci = index_to_cpoint(cinit);
+      cpoint sh = cpoint_add(cpoint_add(p, cpoint{ci.x, m31_neg(ci.y)}), index_to_cpoint(cstep >> 1));
+      uint32_t x = sh.x;
+      for (uint32_t i = 1; i < log_n; i++) x = m31_sub(m31_add(m31_sqr(x), m31_sqr(x)), 1);
+      dn[bitrev32(j, log_expand)] = m31_inv(x);
+    }
+    STWO_CUDA_TRY(cudaMemcpyAsync(d_denom, dn, 4ull << log_expand, cudaMemcpyHostToDevice, s));
+  }
+  const uint32_t* comp_src = d_evals;
+  uint64_t comp_stride = 1ull << L1;
+  if (eval_log != L1) {
+    std::vector<uint32_t*> ext_ptrs(N);
+    for (uint32_t c = 0; c < N; c++) ext_ptrs[c] = d_ext + ((uint64_t)c << eval_log);
+    if ((rc = stwo_b200_evaluate_polynomials(const_cast<const uint32_t* const*>(coeff_ptrs.data()), logs_n.data(), N,
+                                             eval_log - log_n, ext_ptrs.data(), d_tw, tree_log, s, err, err_len)))
+      return rc;
+    comp_src = d_ext;
+    comp_stride = 1ull << eval_log;
+  }
+  const uint64_t n_eval = 1ull << eval_log;
+  composition_kernel<<<grid1d(n_eval, 256), 256, 0, s>>>(comp_src, comp_stride, n_cons, d_small, d_denom, log_n,
+                                                         n_eval, d_comp);
+  STWO_CHECK_LAUNCH();
+  std::vector<uint32_t*> comp_cols(4);
+  std::vector<uint32_t> logs_e(4, eval_log);
+  for (int k = 0; k < 4; k++) comp_cols[k] = d_comp + ((uint64_t)k << eval_log);
+  if ((rc = stwo_b200_interpolate_columns(comp_cols.data(), logs_e.data(), nullptr, 4, d_itw, tree_log, s, err,
+                                          err_len)))
+    return rc;
+  // split_at_mid (natural coefficient order): left = first half, right = second half.
+  std::vector<uint32_t*> split(8), lde(8);
+  std::vector<uint32_t> logs_h(8, eval_log - 1), logs_2(8, L2);
+  for (int k = 0; k < 4; k++) {
+    split[k] = comp_cols[k];
+    split[4 + k] = comp_cols[k] + (n_eval >> 1);
+  }
+  for (int k = 0; k < 8; k++) lde[k] = d_comp_lde + ((uint64_t)k << L2);
+  if ((rc = stwo_b200_evaluate_polynomials(const_cast<const uint32_t* const*>(split.data()), logs_h.data(), 8, blowup,
+                                           lde.data(), d_tw, tree_log, s, err, err_len)))
+    return rc;
+  if ((rc = commit_columns(lde.data(), logs_2, t2, err, err_len))) return rc;
+  Hash32 root2;
+  if ((rc = download_root(t2, root2, err, err_len))) return rc;
+  ch.mix_root(root2);
+
+  // ---- OODS point and sampled values (prover/mod.rs:80-119, pcs/mod.rs:512-689) ----
+  spoint oods;
+  {
+    qm31 t = ch.draw_secure_felt();
+    qm31 t2s = qm31_mul(t, t);
+    qm31 inv1 = qm31_inv(qm31_add(t2s, qm31_one()));
+    oods = {qm31_mul(qm31_add(qm31_one(), qm31_neg(t2s)), inv1), qm31_mul(qm31_add(t, t), inv1)};
+  }
+  const uint32_t max_log_degree_bound = lift - blowup;
+  std::vector<qm31> sampled(N + 8);
+  {
+    // Every column is committed at the lifting size, so all 108 polynomials
+    // (log_n coefficients each) are sampled at the OODS point itself.
+    STWO_ARG_CHECK(L1 == lift && eval_log - 1 == log_n, "sampling assumes one column size");
+    const uint32_t lg = log_n, h = lg / 2;
+    qm31 f[32];
+    f[0] = oods.y;
+    qm31 x = oods.x;
+    for (uint32_t b = 1; b < lg; b++) {
+      f[b] = x;
+      x = qm31_double_x(x);
+    }
+    qm31* w_lo = h_pinned;
+    qm31* w_hi = h_pinned + (1u << h);
+    w_lo[0] = qm31_one();
+    for (uint32_t t = 1; t < (1u << h); t++) w_lo[t] = qm31_mul(w_lo[t & (t - 1)], f[__builtin_ctz(t)]);
+    w_hi[0] = qm31_one();
+    for (uint32_t t = 1; t < (1u << (lg - h)); t++) w_hi[t] = qm31_mul(w_hi[t & (t - 1)], f[h + __builtin_ctz(t)]);
+    size_t n_w = (1u << h) + (1u << (lg - h));
+    STWO_CUDA_TRY(cudaMemcpyAsync(d_small, h_pinned, n_w * sizeof(qm31), cudaMemcpyHostToDevice, s));
+    PolyTable pt;
+    uint32_t np = N + 8;
+    for (uint32_t c = 0; c < N; c++) pt.p[c] = coeff_ptrs[c];
+    for (int k = 0; k < 8; k++) pt.p[N + k] = split[k];
+    const uint32_t chunks = 128;
+    qm31* d_partial = d_small + n_w;
+    dim3 grid(chunks, (np + kEvalGroup - 1) / kEvalGroup);
+    batch_eval_kernel<<<grid, 256, 0, s>>>(pt, np, lg, h, d_small, d_small + (1u << h), d_partial);
+    STWO_CHECK_LAUNCH();
+    qm31* d_vals = d_partial + (size_t)np * chunks;
+    reduce_partials_kernel<<<(np + 127) / 128, 128, 0, s>>>(d_partial, chunks, np, d_vals);
+    STWO_CHECK_LAUNCH();
+    STWO_CUDA_TRY(cudaMemcpyAsync(h_pinned, d_vals, np * sizeof(qm31), cudaMemcpyDeviceToHost, s));
+    STWO_CUDA_TRY(cudaStreamSynchronize(s));
+    std::memcpy(sampled.data(), h_pinned, np * sizeof(qm31));
+  }
+  ch.mix_felts(sampled.data(), sampled.size());
+
+  // Sanity check (prover/mod.rs:123-138): the composition value rebuilt from
+  // the split halves equals the constraint quotient at the OODS point.
+  {
+    const qm31 basis[4] = {qm31_one(), {0, 1, 0, 0}, {0, 0, 1, 0}, {0, 0, 0, 1}};
+    qm31 left = qm31_zero(), right = qm31_zero();
+    for (int k = 0; k < 4; k++) {
+      left = qm31_add(left, qm31_mul(sampled[N + k], basis[k]));
+      right = qm31_add(right, qm31_mul(sampled[N + 4 + k], basis[k]));
+    }
+    qm31 comp = qm31_add(left, qm31_mul(spoint_repeated_double(oods, max_log_degree_bound - 1).x, right));
+    // coset_vanishing(CanonicCoset(max_log_degree_bound).coset, oods)
+    uint64_t cinit = 1ull << (31 - (max_log_degree_bound + 1)), cstep = 1ull << (31 - max_log_degree_bound);
+    cpoint ci = index_to_cpoint(cinit), hs = index_to_cpoint(cstep >> 1);
+    spoint sp = spoint_add(spoint_add(oods, {qm31_from_m31(ci.x), qm31_from_m31(m31_neg(ci.y))}),
+                           {qm31_from_m31(hs.x), qm31_from_m31(hs.y)});
+    qm31 vx = sp.x;
+    for (uint32_t i = 1; i < max_log_degree_bound; i++) vx = qm31_double_x(vx);
+    qm31 dinv = qm31_inv(vx);
+    qm31 acc = qm31_zero();
+    for (uint32_t k = 0; k < n_cons; k++) {
+      qm31 a = sampled[k], b = sampled[k + 1], c = sampled[k + 2];
+      qm31 cons = qm31_sub(c, qm31_add(qm31_mul(a, a), qm31_mul(b, b)));
+      acc = qm31_add(qm31_mul(acc, random_coeff), qm31_mul(cons, dinv));
+    }
+    if (!qm31_eq(acc, comp))
+      return set_err(err, err_len, STWO_B200_ESTATE, "ConstraintsNotSatisfied: composition OODS mismatch");
+  }
+
+  // ---- FRI quotients (pcs/mod.rs:112-118, quotient_ops.rs:134-233) ----
+  const qm31 qcoeff = ch.draw_secure_felt();
+  {
+    QuotientParams qp;
+    qm31 cz = qm31_sub(qm31_conj(oods.y), oods.y);
+    qm31 A = qm31_zero(), B = qm31_zero();
+    qm31* ap = h_pinned;
+    qm31 pk = qm31_one();
+    const uint32_t nq = N + 8;
+    for (uint32_t k = 0; k < nq; k++) {
+      qm31 v = sampled[k];
+      qm31 a = qm31_sub(qm31_conj(v), v);
+      qm31 b = qm31_sub(qm31_mul(v, cz), qm31_mul(a, oods.y));
+      A = qm31_add(A, qm31_mul(pk, a));
+      B = qm31_add(B, qm31_mul(pk, b));
+      ap[k] = pk;
+      pk = qm31_mul(pk, qcoeff);
+    }
+    qp.c = cz;
+    qp.A = A;
+    qp.B = B;
+    qp.prx = {oods.x.a, oods.x.b};
+    qp.pix = {oods.x.c, oods.x.d};
+    qp.pry = {oods.y.a, oods.y.b};
+    qp.piy = {oods.y.c, oods.y.d};
+    qp.log_size = lift;
+    qp.init = index_to_cpoint(1ull << (31 - (lift + 1)));
+    cpoint st = index_to_cpoint(1ull << (31 - (lift - 1)));
+    for (int b = 0; b < 31; b++) {
+      qp.step_pow[b] = st;
+      st = cpoint_add(st, st);
+    }
+    STWO_CUDA_TRY(cudaMemcpyAsync(d_small, ap, nq * sizeof(qm31), cudaMemcpyHostToDevice, s));
+    PolyTable cols;
+    for (uint32_t c = 0; c < N; c++) cols.p[c] = eval_ptrs[c];
+    for (int k = 0; k < 8; k++) cols.p[N + k] = lde[k];
+    quotient_kernel<<<grid1d(1ull << lift, 256), 256, 0, s>>>(qp, cols, nq, d_small, d_quot);
+    STWO_CHECK_LAUNCH();
+  }
+
+  // ---- FRI commit (prover/fri.rs:133-291) ----
+  std::vector<Hash32> fri_roots;
+  {
+    std::vector<uint32_t*> q4(4);
+    for (int k = 0; k < 4; k++) q4[k] = d_quot + ((uint64_t)k << lift);
+    if ((rc = commit_columns(q4.data(), std::vector<uint32_t>(4, lift), tq, err, err_len))) return rc;
+    Hash32 r;
+    if ((rc = download_root(tq, r, err, err_len))) return rc;
+    fri_roots.push_back(r);
+    ch.mix_root(r);
+  }
+  const uint32_t last_log = cfg.log_last_layer_degree_bound + blowup;
+  {
+    qm31 alpha = ch.draw_secure_felt();
+    uint32_t* dst = fri.empty() ? d_last : fri[0].coords;
+    uint32_t dlog = lift - 1;
+    STWO_CUDA_TRY(cudaMemsetAsync(dst, 0, 16ull << dlog, s));
+    std::vector<uint32_t*> d4(4);
+    std::vector<const uint32_t*> s4(4);
+    for (int k = 0; k < 4; k++) {
+      d4[k] = dst + ((uint64_t)k << dlog);
+      s4[k] = d_quot + ((uint64_t)k << lift);
+    }
+    uint32_t al[4] = {alpha.a, alpha.b, alpha.c, alpha.d};
+    if ((rc = stwo_b200_fold_circle_into_line(d4.data(), s4.data(), lift, 1ull << (31 - (lift + 1)), al, d_itw,
+                                              tree_log, s, err, err_len)))
+      return rc;
+  }
+  for (size_t li = 0; li < fri.size(); li++) {
+    FriLayerBuf& l = fri[li];
+    std::vector<uint32_t*> c4(4);
+    for (int k = 0; k < 4; k++) c4[k] = l.coords + ((uint64_t)k << l.log_size);
+    if ((rc = commit_columns(c4.data(), std::vector<uint32_t>(4, l.log_size), l.tree, err, err_len))) return rc;
+    Hash32 r;
+    if ((rc = download_root(l.tree, r, err, err_len))) return rc;
+    fri_roots.push_back(r);
+    ch.mix_root(r);
+    qm31 alpha = ch.draw_secure_felt();
+    uint32_t* nxt = (li + 1 < fri.size()) ? fri[li + 1].coords : d_last;
+    uint32_t nlog = l.log_size - l.fold_step;
+    std::vector<uint32_t*> o4(4);
+    for (int k = 0; k < 4; k++) o4[k] = nxt + ((uint64_t)k << nlog);
+    uint32_t al[4] = {alpha.a, alpha.b, alpha.c, alpha.d};
+    if ((rc = stwo_b200_fold_line(const_cast<const uint32_t* const*>(c4.data()), l.log_size, al, l.fold_step, d_itw,
+                                  tree_log, o4.data(), s, err, err_len)))
+      return rc;
+  }
+  // Last layer (prover/fri.rs:274-291).
+  std::vector<qm31> last_coeffs;
+  {
+    const uint64_t n_last = 1ull << last_log;
+    STWO_CUDA_TRY(cudaMemcpyAsync(h_pinned, d_last, 16 * n_last, cudaMemcpyDeviceToHost, s));
+    STWO_CUDA_TRY(cudaStreamSynchronize(s));
+    const uint32_t* hv = reinterpret_cast<const uint32_t*>(h_pinned);
+    std::vector<qm31> v(n_last);
+    for (uint64_t i = 0; i < n_last; i++) v[i] = {hv[i], hv[n_last + i], hv[2 * n_last + i], hv[3 * n_last + i]};
+    // LineEvaluation::interpolate (prover/line.rs:54-99): bit-reverse, line IFFT, 1/n.
+    for (uint64_t i = 0; i < n_last; i++) {
+      uint64_t j = bitrev32((uint32_t)i, last_log);
+      if (j > i) std::swap(v[i], v[j]);
+    }
+    // line domain: half coset of CanonicCoset(lift) doubled down to last_log
+    uint64_t dinit = (1ull << (31 - (lift + 1))) << (lift - 1 - last_log);
+    uint64_t dstep = 1ull << (31 - last_log);
+    for (uint32_t lg = last_log; lg >= 1; lg--) {
+      uint64_t sz = 1ull << lg;
+      for (uint64_t c0 = 0; c0 < n_last; c0 += sz)
+        for (uint64_t i = 0; i < sz / 2; i++) {
+          uint32_t xi = m31_inv(index_to_cpoint(dinit + dstep * i).x);
+          qm31 l = v[c0 + i], r = v[c0 + i + sz / 2];
+          v[c0 + i] = qm31_add(l, r);
+          v[c0 + i + sz / 2] = qm31_mul_m31(qm31_sub(l, r), xi);
+        }
+      dinit = (dinit * 2) & ((1ull << 31) - 1);
+      dstep = (dstep * 2) & ((1ull << 31) - 1);
+    }
+    uint32_t ninv = m31_inv(m31_reduce_u32((uint32_t)n_last));
+    for (auto& x : v) x = qm31_mul_m31(x, ninv);
+    for (uint64_t i = 0; i < n_last; i++) {  // into ordered coefficients
+      uint64_t j = bitrev32((uint32_t)i, last_log);
+      if (j > i) std::swap(v[i], v[j]);
+    }
+    size_t bound = 1ull << cfg.log_last_layer_degree_bound;
+    for (size_t i = bound; i < v.size(); i++)
+      if (!qm31_eq(v[i], qm31_zero())) return set_err(err, err_len, STWO_B200_ESTATE, "invalid degree");
+    v.resize(bound);
+    last_coeffs = v;
+    ch.mix_felts(last_coeffs.data(), last_coeffs.size());
+  }
+
+  // ---- proof of work (pcs/mod.rs:140-142) ----
+  uint64_t nonce = 0;
+  {
+    Hash32 pre = ch.pow_prefixed(cfg.pow_bits);
+    Digest8 d;
+    std::memcpy(d.w, pre.data(), 32);
+    bool found = false;
+    for (uint32_t hi = 0; !found; hi++) {
+      for (uint32_t base = 0; base < (1u << 20) && !found; base += 1u << 16) {
+        uint32_t init = 0xFFFFFFFFu;
+        STWO_CUDA_TRY(cudaMemcpyAsync(d_found, &init, 4, cudaMemcpyHostToDevice, s));
+        grind_kernel<<<(1u << 16) / 256, 256, 0, s>>>(d, hi, base, cfg.pow_bits, m31, d_found);
+        STWO_CHECK_LAUNCH();
+        uint32_t* hf = reinterpret_cast<uint32_t*>(h_pinned);
+        STWO_CUDA_TRY(cudaMemcpyAsync(hf, d_found, 4, cudaMemcpyDeviceToHost, s));
+        STWO_CUDA_TRY(cudaStreamSynchronize(s));
+        if (*hf != 0xFFFFFFFFu) {
+          nonce = ((uint64_t)hi << 32) | *hf;
+          found = true;
+        }
+      }
+      if (hi == 0x7ffffffeu && !found) return set_err(err, err_len, STWO_B200_ESTATE, "grind found no nonce");
+    }
+  }
+  ch.mix_u64(nonce);
+
+  // ---- queries (core/queries.rs:11-58) ----
+  std::vector<size_t> queries;
+  {
+    size_t mask = ((size_t)1 << lift) - 1;
+    while (queries.size() < cfg.n_queries) {
+      auto w = ch.draw_u32s();
+      for (uint32_t x : w)
+        if (queries.size() < cfg.n_queries) queries.push_back(x & mask);
+    }
+    std::sort(queries.begin(), queries.end());
+    queries.erase(std::unique(queries.begin(), queries.end()), queries.end());
+  }
+
+  // ---- decommitments: one gather of every needed word ----
+  GatherPlan g;
+  struct FriDecommit {
+    std::vector<size_t> positions;       // subset positions
+    std::vector<bool> is_query;
+    std::vector<size_t> value_slot;      // 4 words per position
+    std::vector<std::pair<uint32_t, size_t>> nodes;
+    std::vector<size_t> node_slot;
+  };
+  auto plan_fri = [&](const uint32_t* coords, uint32_t log_size, const MerkleTree& tree,
+                      const std::vector<size_t>& q, uint32_t fold_step) {
+    FriDecommit d;
+    for (size_t i = 0; i < q.size();) {
+      size_t j = i;
+      while (j < q.size() && (q[j] >> fold_step) == (q[i] >> fold_step)) j++;
+      size_t start = (q[i] >> fold_step) << fold_step;
+      size_t k = i;
+      for (size_t pos = start; pos < start + ((size_t)1 << fold_step); pos++) {
+        bool isq = k < j && q[k] == pos;
+        if (isq) k++;
+        d.positions.push_back(pos);
+        d.is_query.push_back(isq);
+        size_t slot = g.add_word(coords + pos);
+        for (int c = 1; c < 4; c++) g.add_word(coords + ((uint64_t)c << log_size) + pos);
+        d.value_slot.push_back(slot);
+      }
+      i = j;
+    }
+    d.nodes = witness_nodes(d.positions, tree.L);
+    for (auto& nd : d.nodes) d.node_slot.push_back(g.add_hash(tree.layer(nd.first) + nd.second * 32));
+    return d;
+  };
+  std::vector<FriDecommit> fri_dec;
+  fri_dec.push_back(plan_fri(d_quot, lift, tq, queries, 1));
+  {
+    std::vector<size_t> lq;
+    for (size_t q : queries)
+      if (lq.empty() || lq.back() != (q >> 1)) lq.push_back(q >> 1);
+    for (auto& l : fri) {
+      fri_dec.push_back(plan_fri(l.coords, l.log_size, l.tree, lq, l.fold_step));
+      std::vector<size_t> nq;
+      for (size_t q : lq)
+        if (nq.empty() || nq.back() != (q >> l.fold_step)) nq.push_back(q >> l.fold_step);
+      lq = nq;
+    }
+  }
+  // trees 1 and 2 at the lifting size: queried values and witness nodes
+  struct TreeDecommit {
+    std::vector<size_t> value_slot;  // column-major: col * n_q + qi
+    std::vector<std::pair<uint32_t, size_t>> nodes;
+    std::vector<size_t> node_slot;
+  };
+  auto plan_tree = [&](const std::vector<uint32_t*>& cols, uint32_t log_size, const MerkleTree& tree) {
+    TreeDecommit d;
+    // prepare_query_positions_for_tree (core/pcs/utils.rs:195-213) and the
+    // lifted read index (prover/vcs_lifted/prover.rs:83-109)
+    std::vector<size_t> tq;
+    for (size_t p : queries) tq.push_back(((p >> (lift - tree.L + 1)) << 1) + (p & 1));
+    for (size_t c = 0; c < cols.size(); c++)
+      for (size_t p : tq) {
+        size_t shift = tree.L - log_size;
+        d.value_slot.push_back(g.add_word(cols[c] + (((p >> (shift + 1)) << 1) + (p & 1))));
+      }
+    d.nodes = witness_nodes(tq, tree.L);
+    for (auto& nd : d.nodes) d.node_slot.push_back(g.add_hash(tree.layer(nd.first) + nd.second * 32));
+    return d;
+  };
+  TreeDecommit td1 = plan_tree(eval_ptrs, L1, t1);
+  TreeDecommit td2 = plan_tree(lde, L2, t2);
+  if ((rc = ensure_gather(g.addrs.size(), err, err_len))) return rc;
+  {
+    size_t n = g.addrs.size();
+    std::vector<uint32_t> words(n);
+    // upload addresses through the pinned staging buffer in chunks
+    size_t chunk = h_pinned_bytes / 8;
+    for (size_t off = 0; off < n; off += chunk) {
+      size_t m = std::min(chunk, n - off);
+      std::memcpy(h_pinned, g.addrs.data() + off, m * 8);
+      STWO_CUDA_TRY(cudaMemcpyAsync(d_gather_addr + off, h_pinned, m * 8, cudaMemcpyHostToDevice, s));
+      STWO_CUDA_TRY(cudaStreamSynchronize(s));
+    }
+    gather_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(d_gather_addr, (uint32_t)n, d_gather_out);
+    STWO_CHECK_LAUNCH();
+    size_t wchunk = h_pinned_bytes / 4;
+    for (size_t off = 0; off < n; off += wchunk) {
+      size_t m = std::min(wchunk, n - off);
+      STWO_CUDA_TRY(cudaMemcpyAsync(h_pinned, d_gather_out + off, m * 4, cudaMemcpyDeviceToHost, s));
+      STWO_CUDA_TRY(cudaStreamSynchronize(s));
+      std::memcpy(words.data() + off, h_pinned, m * 4);
+    }
+    // ---- serialize (canonical layout, struct field order of
+    // core/pcs/quotients.rs:27-35 and core/fri.rs:361-395) ----
+    auto hash_at = [&](size_t slot, ProofOut& o) { o.h(reinterpret_cast<const uint8_t*>(words.data() + slot)); };
+    const char magic[8] = {'S', 'T', 'W', 'O', 'P', 'R', 'F', '1'};
+    out.bytes.assign(magic, magic + 8);
+    out.u32(cfg.pow_bits);
+    out.u32(cfg.log_blowup);
+    out.u32(cfg.log_last_layer_degree_bound);
+    out.u64(cfg.n_queries);
+    out.u32(cfg.line_fold_step);
+    out.bytes.push_back(0);  // lifting_log_size: None
+    out.u64(3);
+    out.h(root0.data());
+    out.h(root1.data());
+    out.h(root2.data());
+    // sampled values: tree 0 (no columns), tree 1 (N), tree 2 (8)
+    out.u64(3);
+    out.u64(0);
+    out.u64(N);
+    for (uint32_t c = 0; c < N; c++) {
+      out.u64(1);
+      out.q(sampled[c]);
+    }
+    out.u64(8);
+    for (int k = 0; k < 8; k++) {
+      out.u64(1);
+      out.q(sampled[N + k]);
+    }
+    // decommitments
+    out.u64(3);
+    out.u64(0);
+    out.u64(td1.nodes.size());
+    for (size_t s2 : td1.node_slot) hash_at(s2, out);
+    out.u64(td2.nodes.size());
+    for (size_t s2 : td2.node_slot) hash_at(s2, out);
+    // queried values
+    const size_t nq = queries.size();
+    out.u64(3);
+    out.u64(0);
+    out.u64(N);
+    for (uint32_t c = 0; c < N; c++) {
+      out.u64(nq);
+      for (size_t qi = 0; qi < nq; qi++) out.u32(words[td1.value_slot[c * nq + qi]]);
+    }
+    out.u64(8);
+    for (int c = 0; c < 8; c++) {
+      out.u64(nq);
+      for (size_t qi = 0; qi < nq; qi++) out.u32(words[td2.value_slot[c * nq + qi]]);
+    }
+    out.u64(nonce);
+    auto fri_layer = [&](const FriDecommit& d, const Hash32& root) {
+      size_t n_w = 0;
+      for (bool b : d.is_query) n_w += b ? 0 : 1;
+      out.u64(n_w);
+      for (size_t i = 0; i < d.positions.size(); i++)
+        if (!d.is_query[i]) {
+          size_t sl = d.value_slot[i];
+          out.q({words[sl], words[sl + 1], words[sl + 2], words[sl + 3]});
+        }
+      out.u64(d.nodes.size());
+      for (size_t s2 : d.node_slot) hash_at(s2, out);
+      out.h(root.data());
+    };
+    fri_layer(fri_dec[0], fri_roots[0]);
+    out.u64(fri.size());
+    for (size_t li = 0; li < fri.size(); li++) fri_layer(fri_dec[li + 1], fri_roots[li + 1]);
+    // last layer poly: bit-reversed storage order
+    std::vector<qm31> lp = last_coeffs;
+    uint32_t lg = 0;
+    while (((size_t)1 << lg) < lp.size()) lg++;
+    for (size_t i = 0; i < lp.size(); i++) {
+      size_t j = bitrev32((uint32_t)i, lg);
+      if (j > i) std::swap(lp[i], lp[j]);
+    }
+    out.u64(lp.size());
+    for (auto& x : lp) out.q(x);
+  }
+  return 0;
+}
+
+}  // namespace stwo_b200
+
+using namespace stwo_b200;
+
+struct stwo_b200_prover {
+  std::unique_ptr<WideFibProver> impl;
+};
+
+extern "C" int stwo_b200_prover_create(const stwo_b200_wide_fib_config* cfg, stwo_b200_prover** out, void* stream,
+                                       char* err, size_t err_len) {
+  STWO_ARG_CHECK(cfg && out, "null argument");
+  *out = nullptr;
+  auto p = std::make_unique<stwo_b200_prover>();
+  p->impl = std::make_unique<WideFibProver>();
+  int rc = p->impl->init(*cfg, as_stream(stream), err, err_len);
+  if (rc) return rc;
+  *out = p.release();
+  return ok(err, err_len);
+}
+
+extern "C" int stwo_b200_prover_destroy(stwo_b200_prover* p, char* err, size_t err_len) {
+  if (p) {
+    cudaStreamSynchronize(p->impl->s);
+    delete p;
+  }
+  return ok(err, err_len);
+}
+
+extern "C" int stwo_b200_prove_wide_fib(stwo_b200_prover* p, const uint32_t* d_a, const uint32_t* d_b,
+                                        uint8_t* proof_out, size_t proof_cap, size_t* proof_len, char* err,
+                                        size_t err_len) {
+  STWO_ARG_CHECK(p && d_a && d_b && proof_len, "null argument");
+  ProofOut out;
+  int rc = p->impl->prove(d_a, d_b, out, err, err_len);
+  if (rc) return rc;
+  *proof_len = out.bytes.size();
+  if (proof_out) {
+    STWO_ARG_CHECK(proof_cap >= out.bytes.size(), "proof buffer too small (%zu < %zu)", proof_cap, out.bytes.size());
+    std::memcpy(proof_out, out.bytes.data(), out.bytes.size());
+  }
+  return ok(err, err_len);
+}

@@ -4,8 +4,9 @@ The compute lives in ``libstwo_b200.so`` (hand-written CUDA kernels behind the
 flat C ABI of ``include/stwo_b200.h``); this package is its Python view.
 """
 from . import ffi
+from .prover import WideFibConfig, WideFibProver, wide_fib_config
 from .backend import (B200Backend, DeviceBuffer, DeviceColumn, SecureColumn, TwiddleTree, canonic_half_coset,
                       layer_to_host, sync)
 
-__all__ = ["ffi", "B200Backend", "DeviceBuffer", "DeviceColumn", "SecureColumn", "TwiddleTree",
+__all__ = ["ffi", "WideFibConfig", "WideFibProver", "wide_fib_config", "B200Backend", "DeviceBuffer", "DeviceColumn", "SecureColumn", "TwiddleTree",
            "canonic_half_coset", "layer_to_host", "sync"]
