@@ -316,7 +316,8 @@ class WideFibProver {
     int rc;
     if ((rc = alloc((void**)&d_tw, 4ull << tree_log, err, err_len))) return rc;
     if ((rc = alloc((void**)&d_itw, 4ull << tree_log, err, err_len))) return rc;
-    rc = stwo_b200_precompute_twiddles(1ull << (31 - (tree_log + 1)), tree_log, d_tw, d_itw, s, err, err_len);
+    // CanonicCoset(tree_log + 1).half_coset = half_odds(tree_log): initial index 2^(31 - (tree_log + 2)).
+    rc = stwo_b200_precompute_twiddles(1ull << (31 - (tree_log + 2)), tree_log, d_tw, d_itw, s, err, err_len);
     if (rc) return rc;
     if ((rc = alloc((void**)&d_coeffs, (4ull * N) << log_n, err, err_len))) return rc;
     if ((rc = alloc((void**)&d_evals, (4ull * N) << L1, err, err_len))) return rc;
