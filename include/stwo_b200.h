@@ -215,6 +215,18 @@ int stwo_b200_prover_destroy(stwo_b200_prover* prover, char* err, size_t err_len
 int stwo_b200_prove_wide_fib(stwo_b200_prover* prover, const uint32_t* d_a, const uint32_t* d_b,
                              uint8_t* proof_out, size_t proof_cap, size_t* proof_len, char* err, size_t err_len);
 
+/* Per-phase device time (CUDA events on the prover's stream), accumulated over
+ * the proofs made since timing was enabled.  Phases, in order: 0 trace
+ * generation, 1 trace interpolate, 2 trace evaluate, 3 trace Merkle,
+ * 4 composition, 5 composition interpolate, 6 composition evaluate,
+ * 7 composition Merkle, 8 OODS sampling, 9 FRI quotients, 10 FRI Merkle,
+ * 11 FRI folds, 12 grind, 13 decommit (each phase spans to the next one,
+ * host channel work included).  No reference counterpart (the reference's
+ * env-gated timers STWO_METAL_PROFILE_* play this role). */
+int stwo_b200_prover_set_timing(stwo_b200_prover* prover, int enable, char* err, size_t err_len);
+int stwo_b200_prover_phase_times(stwo_b200_prover* prover, double* ms_out, uint32_t n, uint32_t* proofs, char* err,
+                                 size_t err_len);
+
 #ifdef __cplusplus
 }
 #endif

@@ -256,8 +256,55 @@ struct ProofOut {
   void h(const uint8_t* p) { bytes.insert(bytes.end(), p, p + 32); }
 };
 
+// Phases timed with CUDA events when timing is enabled
+// (stwo_b200_prover_phase_times).
+enum Phase {
+  kTraceGen, kTraceInterpolate, kTraceEvaluate, kTraceMerkle, kComposition, kCompInterpolate, kCompEvaluate,
+  kCompMerkle, kOodsSampling, kQuotients, kFriMerkle, kFriFold, kGrind, kDecommit, kNumPhases
+};
+
 class WideFibProver {
  public:
+  bool timing = false;
+  std::vector<cudaEvent_t> ev_pool;
+  std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> marks;
+  size_t ev_used = 0;
+  double phase_ms[kNumPhases] = {0};
+  uint32_t proofs_timed = 0;
+
+  cudaEvent_t next_event() {
+    if (ev_used == ev_pool.size()) {
+      cudaEvent_t e;
+      cudaEventCreate(&e);
+      ev_pool.push_back(e);
+    }
+    return ev_pool[ev_used++];
+  }
+  // Opens phase `ph` at the current point of the stream; closes the previous.
+  int open_phase = -1;
+  cudaEvent_t open_event = nullptr;
+  void phase(int ph) {
+    if (!timing) return;
+    cudaEvent_t e = next_event();
+    cudaEventRecord(e, s);
+    if (open_phase >= 0) marks.push_back({open_phase, {open_event, e}});
+    open_phase = ph;
+    open_event = e;
+  }
+  void finish_timing() {
+    if (!timing) return;
+    phase(-1);
+    cudaStreamSynchronize(s);
+    for (auto& m : marks) {
+      float ms = 0;
+      cudaEventElapsedTime(&ms, m.second.first, m.second.second);
+      phase_ms[m.first] += ms;
+    }
+    marks.clear();
+    ev_used = 0;
+    open_phase = -1;
+    proofs_timed++;
+  }
   stwo_b200_wide_fib_config cfg;
   uint32_t log_n, N, blowup, eval_log, L1, L2, lift, tree_log;
   cudaStream_t s;
@@ -283,6 +330,7 @@ class WideFibProver {
   std::vector<void*> allocs;
 
   ~WideFibProver() {
+    for (cudaEvent_t e : ev_pool) cudaEventDestroy(e);
     for (void* p : allocs) cudaFree(p);
     if (h_pinned) cudaFreeHost(h_pinned);
   }
@@ -401,6 +449,7 @@ int WideFibProver::prove(const uint32_t* d_a, const uint32_t* d_b, ProofOut& out
   ch.mix_root(root0);
 
   // ---- tree 1: trace ----
+  phase(kTraceGen);
   wide_fib_trace_kernel<<<grid1d(rows, 256), 256, 0, s>>>(d_a, d_b, d_coeffs, N, rows);
   STWO_CHECK_LAUNCH();
   std::vector<uint32_t*> coeff_ptrs(N), eval_ptrs(N);
@@ -409,12 +458,15 @@ int WideFibProver::prove(const uint32_t* d_a, const uint32_t* d_b, ProofOut& out
     coeff_ptrs[c] = d_coeffs + (uint64_t)c * rows;
     eval_ptrs[c] = d_evals + ((uint64_t)c << L1);
   }
+  phase(kTraceInterpolate);
   if ((rc = stwo_b200_interpolate_columns(coeff_ptrs.data(), logs_n.data(), nullptr, N, d_itw, tree_log, s, err,
                                           err_len)))
     return rc;
+  phase(kTraceEvaluate);
   if ((rc = stwo_b200_evaluate_polynomials(const_cast<const uint32_t* const*>(coeff_ptrs.data()), logs_n.data(), N,
                                            blowup, eval_ptrs.data(), d_tw, tree_log, s, err, err_len)))
     return rc;
+  phase(kTraceMerkle);
   if ((rc = commit_columns(eval_ptrs.data(), logs_1, t1, err, err_len))) return rc;
   Hash32 root1;
   if ((rc = download_root(t1, root1, err, err_len))) return rc;
@@ -423,6 +475,7 @@ int WideFibProver::prove(const uint32_t* d_a, const uint32_t* d_b, ProofOut& out
   // ---- composition (prover/mod.rs:57-77) ----
   const qm31 random_coeff = ch.draw_secure_felt();
   const uint32_t n_cons = N - 2;
+  phase(kComposition);
   {
     qm31* pw = h_pinned;
     qm31 acc = qm31_one();
@@ -468,9 +521,11 @@ int WideFibProver::prove(const uint32_t* d_a, const uint32_t* d_b, ProofOut& out
   std::vector<uint32_t*> comp_cols(4);
   std::vector<uint32_t> logs_e(4, eval_log);
   for (int k = 0; k < 4; k++) comp_cols[k] = d_comp + ((uint64_t)k << eval_log);
+  phase(kCompInterpolate);
   if ((rc = stwo_b200_interpolate_columns(comp_cols.data(), logs_e.data(), nullptr, 4, d_itw, tree_log, s, err,
                                           err_len)))
     return rc;
+  phase(kCompEvaluate);
   // split_at_mid (natural coefficient order): left = first half, right = second half.
   std::vector<uint32_t*> split(8), lde(8);
   std::vector<uint32_t> logs_h(8, eval_log - 1), logs_2(8, L2);
@@ -482,6 +537,7 @@ int WideFibProver::prove(const uint32_t* d_a, const uint32_t* d_b, ProofOut& out
   if ((rc = stwo_b200_evaluate_polynomials(const_cast<const uint32_t* const*>(split.data()), logs_h.data(), 8, blowup,
                                            lde.data(), d_tw, tree_log, s, err, err_len)))
     return rc;
+  phase(kCompMerkle);
   if ((rc = commit_columns(lde.data(), logs_2, t2, err, err_len))) return rc;
   Hash32 root2;
   if ((rc = download_root(t2, root2, err, err_len))) return rc;
@@ -516,6 +572,7 @@ int WideFibProver::prove(const uint32_t* d_a, const uint32_t* d_b, ProofOut& out
     w_hi[0] = qm31_one();
     for (uint32_t t = 1; t < (1u << (lg - h)); t++) w_hi[t] = qm31_mul(w_hi[t & (t - 1)], f[h + __builtin_ctz(t)]);
     size_t n_w = (1u << h) + (1u << (lg - h));
+    phase(kOodsSampling);
     STWO_CUDA_TRY(cudaMemcpyAsync(d_small, h_pinned, n_w * sizeof(qm31), cudaMemcpyHostToDevice, s));
     PolyTable pt;
     uint32_t np = N + 8;
@@ -595,6 +652,7 @@ int WideFibProver::prove(const uint32_t* d_a, const uint32_t* d_b, ProofOut& out
       qp.step_pow[b] = st;
       st = cpoint_add(st, st);
     }
+    phase(kQuotients);
     STWO_CUDA_TRY(cudaMemcpyAsync(d_small, ap, nq * sizeof(qm31), cudaMemcpyHostToDevice, s));
     PolyTable cols;
     for (uint32_t c = 0; c < N; c++) cols.p[c] = eval_ptrs[c];
@@ -608,6 +666,7 @@ int WideFibProver::prove(const uint32_t* d_a, const uint32_t* d_b, ProofOut& out
   {
     std::vector<uint32_t*> q4(4);
     for (int k = 0; k < 4; k++) q4[k] = d_quot + ((uint64_t)k << lift);
+    phase(kFriMerkle);
     if ((rc = commit_columns(q4.data(), std::vector<uint32_t>(4, lift), tq, err, err_len))) return rc;
     Hash32 r;
     if ((rc = download_root(tq, r, err, err_len))) return rc;
@@ -627,6 +686,7 @@ int WideFibProver::prove(const uint32_t* d_a, const uint32_t* d_b, ProofOut& out
       s4[k] = d_quot + ((uint64_t)k << lift);
     }
     uint32_t al[4] = {alpha.a, alpha.b, alpha.c, alpha.d};
+    phase(kFriFold);
     if ((rc = stwo_b200_fold_circle_into_line(d4.data(), s4.data(), lift, 1ull << (31 - (lift + 1)), al, d_itw,
                                               tree_log, s, err, err_len)))
       return rc;
@@ -635,6 +695,7 @@ int WideFibProver::prove(const uint32_t* d_a, const uint32_t* d_b, ProofOut& out
     FriLayerBuf& l = fri[li];
     std::vector<uint32_t*> c4(4);
     for (int k = 0; k < 4; k++) c4[k] = l.coords + ((uint64_t)k << l.log_size);
+    phase(kFriMerkle);
     if ((rc = commit_columns(c4.data(), std::vector<uint32_t>(4, l.log_size), l.tree, err, err_len))) return rc;
     Hash32 r;
     if ((rc = download_root(l.tree, r, err, err_len))) return rc;
@@ -646,6 +707,7 @@ int WideFibProver::prove(const uint32_t* d_a, const uint32_t* d_b, ProofOut& out
     std::vector<uint32_t*> o4(4);
     for (int k = 0; k < 4; k++) o4[k] = nxt + ((uint64_t)k << nlog);
     uint32_t al[4] = {alpha.a, alpha.b, alpha.c, alpha.d};
+    phase(kFriFold);
     if ((rc = stwo_b200_fold_line(const_cast<const uint32_t* const*>(c4.data()), l.log_size, al, l.fold_step, d_itw,
                                   tree_log, o4.data(), s, err, err_len)))
       return rc;
@@ -695,6 +757,7 @@ int WideFibProver::prove(const uint32_t* d_a, const uint32_t* d_b, ProofOut& out
 
   // ---- proof of work (pcs/mod.rs:140-142) ----
   uint64_t nonce = 0;
+  phase(kGrind);
   {
     Hash32 pre = ch.pow_prefixed(cfg.pow_bits);
     Digest8 d;
@@ -733,6 +796,7 @@ int WideFibProver::prove(const uint32_t* d_a, const uint32_t* d_b, ProofOut& out
   }
 
   // ---- decommitments: one gather of every needed word ----
+  phase(kDecommit);
   GatherPlan g;
   struct FriDecommit {
     std::vector<size_t> positions;       // subset positions
@@ -899,6 +963,7 @@ int WideFibProver::prove(const uint32_t* d_a, const uint32_t* d_b, ProofOut& out
     out.u64(lp.size());
     for (auto& x : lp) out.q(x);
   }
+  finish_timing();
   return 0;
 }
 
@@ -927,6 +992,22 @@ extern "C" int stwo_b200_prover_destroy(stwo_b200_prover* p, char* err, size_t e
     cudaStreamSynchronize(p->impl->s);
     delete p;
   }
+  return ok(err, err_len);
+}
+
+extern "C" int stwo_b200_prover_set_timing(stwo_b200_prover* p, int enable, char* err, size_t err_len) {
+  STWO_ARG_CHECK(p, "null prover");
+  p->impl->timing = enable != 0;
+  for (double& x : p->impl->phase_ms) x = 0;
+  p->impl->proofs_timed = 0;
+  return ok(err, err_len);
+}
+
+extern "C" int stwo_b200_prover_phase_times(stwo_b200_prover* p, double* ms_out, uint32_t n, uint32_t* proofs,
+                                            char* err, size_t err_len) {
+  STWO_ARG_CHECK(p && ms_out, "null argument");
+  for (uint32_t i = 0; i < n && i < (uint32_t)kNumPhases; i++) ms_out[i] = p->impl->phase_ms[i];
+  if (proofs) *proofs = p->impl->proofs_timed;
   return ok(err, err_len);
 }
 
