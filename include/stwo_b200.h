@@ -181,6 +181,19 @@ int stwo_b200_fold_circle_into_line(uint32_t* const* d_dst4, const uint32_t* con
 int stwo_b200_decompose(const uint32_t* const* d_in4, uint32_t log_size, uint32_t* const* d_out4,
                         uint32_t* lambda_out, void* stream, char* err, size_t err_len);
 
+/* FriOps::decompose without device allocation.  No counterpart in the
+ * reference: for callers that cannot let the library allocate device memory
+ * mid-run (a prover service whose admission controller has already divided
+ * HBM between requests, or a host runtime that owns every device
+ * allocation).  Same results as stwo_b200_decompose; the reduction scratch
+ * (18,960 bytes) is a fixed device array that every GPU loading the library
+ * keeps until exit.  Inputs up to 2^30 elements per coordinate; larger sizes
+ * are rejected.  The first call on a device looks up the array's device
+ * address (make it before any stream capture).  Calls share the array:
+ * calls that overlap on the GPU race.  Synchronises `stream`. */
+int stwo_b200_decompose_noalloc(const uint32_t* const* d_in4, uint32_t log_size, uint32_t* const* d_out4,
+                                uint32_t* lambda_out, void* stream, char* err, size_t err_len);
+
 /* ----------------------------------------------------- Wide-Fibonacci prove */
 /* PcsConfig + FriConfig fields of crates/stwo/src/core/pcs/mod.rs:31-80 and
  * core/fri.rs:31-80 (defaults: pow_bits 10, log_blowup 1, n_queries 3,

@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 
 #include "common.cuh"
 #include "field.cuh"
@@ -245,6 +246,90 @@ extern "C" int stwo_b200_decompose(const uint32_t* const* d_in4, uint32_t log_si
   STWO_CHECK_LAUNCH();
   STWO_CUDA_TRY(cudaMemcpyAsync(lambda_out, lam, 16, cudaMemcpyDeviceToHost, s));
   STWO_CUDA_TRY(cudaFreeAsync(scratch, s));
+  STWO_CUDA_TRY(cudaStreamSynchronize(s));
+  return ok(err, err_len);
+}
+
+// ---------------------------------------------------------------------------
+// decompose without allocation.
+//
+// Some callers cannot let a library allocate device memory while they run: a
+// prover service whose admission controller has already divided the GPU's
+// memory between requests (a cudaMalloc from inside a request could fail
+// under that pressure or bypass the accounting), or a host runtime that owns
+// every device allocation itself.  stwo_b200_decompose_noalloc gives them
+// FriOps::decompose with its reduction scratch in the fixed array below
+// instead of cudaMallocAsync.
+//
+// The array is a file-scope __device__ symbol: every GPU that loads this
+// library holds its kNoAllocScratchWords words until the process exits.  In
+// host code the symbol's name is a host-side stand-in, not a device address,
+// so the address is fetched once per device with cudaGetSymbolAddress (with
+// that device current) and cached; the first call on a device does that
+// set-up, so make it before any stream capture.  All calls on a device share
+// the array and it keeps the last call's contents: each call overwrites every
+// word it reads, and calls that overlap on the GPU (different streams, or
+// host threads without ordering) race on it.
+namespace stwo_b200 {
+
+constexpr uint32_t kNoAllocBlocks = 148 * 8;                  // reduction blocks (one wave)
+constexpr uint32_t kNoAllocScratchWords = kNoAllocBlocks * 4 + 4;  // partials + lambda: 18,960 bytes
+static __device__ __align__(256) uint32_t g_decompose_scratch[kNoAllocScratchWords];
+
+static uint32_t* noalloc_scratch(int device, char* err, size_t err_len, int* rc) {
+  static std::atomic<uint32_t*> cache[64];
+  *rc = STWO_B200_OK;
+  if (device < 0 || device >= 64) {
+    *rc = set_err(err, err_len, STWO_B200_ESTATE, "device ordinal %d out of range", device);
+    return nullptr;
+  }
+  uint32_t* p = cache[device].load(std::memory_order_acquire);
+  if (p) return p;
+  void* addr = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&addr, g_decompose_scratch);
+  if (e != cudaSuccess) {
+    *rc = set_err(err, err_len, STWO_B200_ECUDA, "cudaGetSymbolAddress(decompose scratch): %s",
+                  cudaGetErrorString(e));
+    return nullptr;
+  }
+  p = static_cast<uint32_t*>(addr);
+  cache[device].store(p, std::memory_order_release);
+  return p;
+}
+
+}  // namespace stwo_b200
+
+extern "C" int stwo_b200_decompose_noalloc(const uint32_t* const* d_in4, uint32_t log_size, uint32_t* const* d_out4,
+                                           uint32_t* lambda_out, void* stream, char* err, size_t err_len) {
+  STWO_ARG_CHECK(d_in4 && d_out4 && lambda_out, "null argument");
+  STWO_ARG_CHECK(log_size <= 30, "log size %u exceeds the maximum of 30 (2^30 elements per coordinate)", log_size);
+  cudaStream_t s = as_stream(stream);
+  int device = 0;
+  STWO_CUDA_TRY(cudaGetDevice(&device));
+  int rc;
+  uint32_t* scratch = noalloc_scratch(device, err, err_len, &rc);
+  if (!scratch) return rc;
+  uint64_t n = 1ull << log_size;
+  uint64_t range = n / 16, half_a = range / 2;
+  uint64_t split_sum = 16 * half_a, end_sum = 16 * range;
+  uint64_t split_apply = 16 * (((n + 15) / 16) / 2);
+  unsigned blocks = (unsigned)std::min<uint64_t>(std::max<uint64_t>((end_sum + 255) / 256, 1), kNoAllocBlocks);
+  // blocks * 4 partial words + 4 lambda words must fit the fixed array.
+  STWO_ARG_CHECK((uint64_t)blocks * 4 + 4 <= kNoAllocScratchWords, "scratch of %u words exceeds the maximum of %u",
+                 blocks * 4 + 4, kNoAllocScratchWords);
+  uint32_t* lam = scratch + blocks * 4;
+  Cols4 in{{d_in4[0], d_in4[1], d_in4[2], d_in4[3]}};
+  Cols4W out{{d_out4[0], d_out4[1], d_out4[2], d_out4[3]}};
+  // Every partial word read below is written first by decompose_sums_kernel
+  // (one word per block and coordinate, zero sums included), so no clearing
+  // is needed between calls.
+  decompose_sums_kernel<<<blocks, 256, 0, s>>>(in, split_sum, end_sum, scratch);
+  STWO_CHECK_LAUNCH();
+  decompose_finish_kernel<<<1, 32, 0, s>>>(scratch, blocks, m31_inv(m31_reduce_u32((uint32_t)n)), lam);
+  STWO_CHECK_LAUNCH();
+  decompose_apply_kernel<<<grid_for(n, 256), 256, 0, s>>>(in, n, split_apply, lam, out);
+  STWO_CHECK_LAUNCH();
+  STWO_CUDA_TRY(cudaMemcpyAsync(lambda_out, lam, 16, cudaMemcpyDeviceToHost, s));
   STWO_CUDA_TRY(cudaStreamSynchronize(s));
   return ok(err, err_len);
 }
