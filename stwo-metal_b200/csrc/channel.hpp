@@ -107,6 +107,7 @@ class HostChannel {
  public:
   explicit HostChannel(bool m31_output) : m31_(m31_output) { digest_.fill(0); }
   const Hash32& digest() const { return digest_; }
+  uint32_t n_draws() const { return n_draws_; }
   bool m31() const { return m31_; }
 
   void mix_root(const Hash32& root) {  // core/vcs_lifted/blake2_merkle.rs:49-56

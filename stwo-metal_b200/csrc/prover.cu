@@ -189,6 +189,132 @@ __global__ void gather_kernel(const uint64_t* __restrict__ addrs, uint32_t n, ui
   if (i < n) out[i] = *reinterpret_cast<const uint32_t*>(addrs[i]);
 }
 
+// ---- device-side Fiat-Shamir steps of the FRI commit ----
+// The channel state lives in device memory so the FRI layer loop (commit a
+// layer, mix its root, draw the folding alpha, fold) is enqueued without host
+// round trips (core/channel/blake2s.rs:25-120, core/vcs_lifted/blake2_merkle.rs:49-56).
+struct DevChannel {
+  uint32_t digest[8];
+  uint32_t n_draws;
+  uint32_t m31;
+  uint32_t error;  // set when a secure-felt draw exhausted its retry bound
+  uint32_t pad;
+};
+
+__device__ void dev_finalize(uint32_t h[8], bool m31) {
+  if (m31)
+    for (int k = 0; k < 8; k++) h[k] = m31_reduce_u32(h[k]);
+}
+
+// mix_root (digest <- H(digest || root)), then draw_secure_felt into *alpha.
+__global__ void channel_mix_root_draw_kernel(DevChannel* ch, const uint8_t* root, qm31* alpha) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  uint32_t m[16];
+  for (int k = 0; k < 8; k++) m[k] = ch->digest[k];
+  const uint32_t* r = reinterpret_cast<const uint32_t*>(root);
+  for (int k = 0; k < 8; k++) m[8 + k] = r[k];
+  uint32_t h[8];
+  blake2s_init(h);
+  blake2s_compress(h, m, 64, true);
+  dev_finalize(h, ch->m31 != 0);
+  for (int k = 0; k < 8; k++) ch->digest[k] = h[k];
+  uint32_t n_draws = 0;
+  // draw_base_felts: retry until all 8 words are below 2P (probability of a
+  // retry ~2^-28 per draw); bounded, with an error flag instead of a hang.
+  for (int attempt = 0; attempt < 64; attempt++) {
+    for (int k = 0; k < 8; k++) m[k] = ch->digest[k];
+    m[8] = n_draws;
+    for (int k = 9; k < 16; k++) m[k] = 0;
+    n_draws++;
+    blake2s_init(h);
+    blake2s_compress(h, m, 37, true);
+    dev_finalize(h, ch->m31 != 0);
+    bool okw = true;
+    for (int k = 0; k < 8; k++) okw = okw && h[k] < 2 * M31_P;
+    if (okw) {
+      *alpha = {m31_reduce_u32(h[0]), m31_reduce_u32(h[1]), m31_reduce_u32(h[2]), m31_reduce_u32(h[3])};
+      ch->n_draws = n_draws;
+      return;
+    }
+  }
+  ch->error = 1;
+  ch->n_draws = n_draws;
+  *alpha = qm31_zero();
+}
+
+// fold_line with alpha read from device memory (prover/backend/cpu/fri.rs:67-92).
+__global__ void fold_line_dev_kernel(const uint32_t* __restrict__ in, uint32_t log_m, uint32_t fold_step,
+                                     const qm31* __restrict__ d_alpha, const uint32_t* __restrict__ itw,
+                                     uint64_t tw_len, uint32_t* __restrict__ out) {
+  const uint64_t n_in = 1ull << log_m;
+  const uint64_t n_out = n_in >> fold_step;
+  qm31 a0 = *d_alpha;
+  if (fold_step == 1) {
+    const uint32_t* lt = itw + (tw_len - (1ull << log_m));
+    for (uint64_t o = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; o < n_out;
+         o += (uint64_t)gridDim.x * blockDim.x) {
+      qm31 fx = {__ldg(in + 2 * o), __ldg(in + n_in + 2 * o), __ldg(in + 2 * n_in + 2 * o), __ldg(in + 3 * n_in + 2 * o)};
+      qm31 fnx = {__ldg(in + 2 * o + 1), __ldg(in + n_in + 2 * o + 1), __ldg(in + 2 * n_in + 2 * o + 1),
+                  __ldg(in + 3 * n_in + 2 * o + 1)};
+      qm31 v = qm31_add(qm31_add(fx, fnx), qm31_mul(a0, qm31_mul_m31(qm31_sub(fx, fnx), __ldg(lt + o))));
+      out[o] = v.a;
+      out[n_out + o] = v.b;
+      out[2 * n_out + o] = v.c;
+      out[3 * n_out + o] = v.d;
+    }
+    return;
+  }
+  for (uint64_t o = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; o < n_out; o += (uint64_t)gridDim.x * blockDim.x) {
+    qm31 v[1 << 6];
+    const uint32_t w = 1u << fold_step;
+    for (uint32_t j = 0; j < w; j++) {
+      uint64_t i = o * w + j;
+      v[j] = {__ldg(in + i), __ldg(in + n_in + i), __ldg(in + 2 * n_in + i), __ldg(in + 3 * n_in + i)};
+    }
+    qm31 a = a0;
+    for (uint32_t st = 0; st < fold_step; st++) {
+      const uint32_t* lt = itw + (tw_len - (1ull << (log_m - st)));
+      uint32_t pairs = w >> (st + 1);
+      for (uint32_t j = 0; j < pairs; j++) {
+        qm31 fx = v[2 * j], fnx = v[2 * j + 1];
+        qm31 f0 = qm31_add(fx, fnx);
+        qm31 f1 = qm31_mul_m31(qm31_sub(fx, fnx), __ldg(lt + o * pairs + j));
+        v[j] = qm31_add(f0, qm31_mul(a, f1));
+      }
+      a = qm31_mul(a, a);
+    }
+    out[o] = v[0].a;
+    out[n_out + o] = v[0].b;
+    out[2 * n_out + o] = v[0].c;
+    out[3 * n_out + o] = v[0].d;
+  }
+}
+
+// First FRI layer: dst = 0 * alpha^2 + fold(src) = fold(src) (prover/fri.rs:74-85
+// with a zero line evaluation), alpha from device memory; log_n > 4.
+__global__ void fold_circle_first_dev_kernel(const uint32_t* __restrict__ src, uint32_t log_n,
+                                             const qm31* __restrict__ d_alpha, const uint32_t* __restrict__ itw,
+                                             uint64_t tw_len, uint32_t* __restrict__ dst) {
+  const uint64_t n_in = 1ull << log_n, n_out = n_in >> 1;
+  const uint32_t* lt0 = itw + (tw_len - (1ull << (log_n - 1)));
+  qm31 alpha = *d_alpha;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n_out; i += (uint64_t)gridDim.x * blockDim.x) {
+    uint32_t b = __ldg(lt0 + ((i >> 1) ^ 1));
+    uint32_t yinv = ((i ^ (i >> 1)) & 1) ? m31_neg(b) : b;
+    qm31 fp = {__ldg(src + 2 * i), __ldg(src + n_in + 2 * i), __ldg(src + 2 * n_in + 2 * i),
+               __ldg(src + 3 * n_in + 2 * i)};
+    qm31 fnp = {__ldg(src + 2 * i + 1), __ldg(src + n_in + 2 * i + 1), __ldg(src + 2 * n_in + 2 * i + 1),
+                __ldg(src + 3 * n_in + 2 * i + 1)};
+    qm31 f0 = qm31_add(fp, fnp);
+    qm31 f1 = qm31_mul_m31(qm31_sub(fp, fnp), yinv);
+    qm31 v = qm31_add(qm31_zero(), qm31_add(f0, qm31_mul(alpha, f1)));
+    dst[i] = v.a;
+    dst[n_out + i] = v.b;
+    dst[2 * n_out + i] = v.c;
+    dst[3 * n_out + i] = v.d;
+  }
+}
+
 static unsigned grid1d(uint64_t n, unsigned threads) {
   uint64_t b = (n + threads - 1) / threads;
   return (unsigned)std::min<uint64_t>(std::max<uint64_t>(b, 1), 148ull * 32);
@@ -322,10 +448,14 @@ class WideFibProver {
   qm31* d_small = nullptr;        // powers / weights / partials / alpha powers
   uint32_t* d_denom = nullptr;
   uint32_t* d_found = nullptr;
+  DevChannel* d_chan = nullptr;
+  qm31* d_alphas = nullptr;       // folding alphas of the FRI layers
   uint64_t* d_gather_addr = nullptr;
   uint32_t* d_gather_out = nullptr;
   size_t gather_cap = 0;
   qm31* h_pinned = nullptr;       // staging for small uploads / downloads
+  DevChannel* h_chan = nullptr;   // staging of the device channel state (own region: the
+                                  // quotient upload from h_pinned may still be in flight)
   size_t h_pinned_bytes = 0;
   std::vector<void*> allocs;
 
@@ -333,6 +463,7 @@ class WideFibProver {
     for (cudaEvent_t e : ev_pool) cudaEventDestroy(e);
     for (void* p : allocs) cudaFree(p);
     if (h_pinned) cudaFreeHost(h_pinned);
+    if (h_chan) cudaFreeHost(h_chan);
   }
 
   int alloc(void** p, size_t bytes, char* err, size_t err_len) {
@@ -401,8 +532,11 @@ class WideFibProver {
     if ((rc = alloc((void**)&d_small, small_q * sizeof(qm31), err, err_len))) return rc;
     if ((rc = alloc((void**)&d_denom, 4ull << (eval_log - log_n), err, err_len))) return rc;
     if ((rc = alloc((void**)&d_found, 64, err, err_len))) return rc;
+    if ((rc = alloc((void**)&d_chan, sizeof(DevChannel), err, err_len))) return rc;
+    if ((rc = alloc((void**)&d_alphas, (fri.size() + 2) * sizeof(qm31), err, err_len))) return rc;
     h_pinned_bytes = std::max<size_t>(small_q * sizeof(qm31), 16ull << last_log);
     STWO_CUDA_TRY(cudaMallocHost((void**)&h_pinned, h_pinned_bytes));
+    STWO_CUDA_TRY(cudaMallocHost((void**)&h_chan, sizeof(DevChannel)));
     STWO_CUDA_TRY(cudaStreamSynchronize(s));
     return 0;
   }
@@ -662,34 +796,33 @@ int WideFibProver::prove(const uint32_t* d_a, const uint32_t* d_b, ProofOut& out
   }
 
   // ---- FRI commit (prover/fri.rs:133-291) ----
-  std::vector<Hash32> fri_roots;
+  // The layer loop runs on the device: commit, mix root / draw alpha on the
+  // device channel, fold.  The host replays the transcript afterwards from the
+  // downloaded roots and checks the device alphas against its own.
+  std::vector<Hash32> fri_roots(1 + fri.size());
+  const uint32_t last_log = cfg.log_last_layer_degree_bound + blowup;
   {
+    DevChannel* hc = h_chan;
+    std::memset(hc, 0, sizeof(DevChannel));
+    std::memcpy(hc->digest, ch.digest().data(), 32);
+    hc->n_draws = ch.n_draws();
+    hc->m31 = m31 ? 1 : 0;
+    STWO_CUDA_TRY(cudaMemcpyAsync(d_chan, hc, sizeof(DevChannel), cudaMemcpyHostToDevice, s));
     std::vector<uint32_t*> q4(4);
     for (int k = 0; k < 4; k++) q4[k] = d_quot + ((uint64_t)k << lift);
     phase(kFriMerkle);
     if ((rc = commit_columns(q4.data(), std::vector<uint32_t>(4, lift), tq, err, err_len))) return rc;
-    Hash32 r;
-    if ((rc = download_root(tq, r, err, err_len))) return rc;
-    fri_roots.push_back(r);
-    ch.mix_root(r);
-  }
-  const uint32_t last_log = cfg.log_last_layer_degree_bound + blowup;
-  {
-    qm31 alpha = ch.draw_secure_felt();
-    uint32_t* dst = fri.empty() ? d_last : fri[0].coords;
-    uint32_t dlog = lift - 1;
-    STWO_CUDA_TRY(cudaMemsetAsync(dst, 0, 16ull << dlog, s));
-    std::vector<uint32_t*> d4(4);
-    std::vector<const uint32_t*> s4(4);
-    for (int k = 0; k < 4; k++) {
-      d4[k] = dst + ((uint64_t)k << dlog);
-      s4[k] = d_quot + ((uint64_t)k << lift);
-    }
-    uint32_t al[4] = {alpha.a, alpha.b, alpha.c, alpha.d};
+    channel_mix_root_draw_kernel<<<1, 32, 0, s>>>(d_chan, tq.layer(0), d_alphas);
+    STWO_CHECK_LAUNCH();
     phase(kFriFold);
-    if ((rc = stwo_b200_fold_circle_into_line(d4.data(), s4.data(), lift, 1ull << (31 - (lift + 1)), al, d_itw,
-                                              tree_log, s, err, err_len)))
-      return rc;
+    uint32_t* dst = fri.empty() ? d_last : fri[0].coords;
+    if (lift > 4) {
+      fold_circle_first_dev_kernel<<<grid1d(1ull << (lift - 1), 256), 256, 0, s>>>(d_quot, lift, d_alphas, d_itw,
+                                                                                     1ull << tree_log, dst);
+      STWO_CHECK_LAUNCH();
+    } else {
+      return set_err(err, err_len, STWO_B200_EARG, "lifting domain too small");
+    }
   }
   for (size_t li = 0; li < fri.size(); li++) {
     FriLayerBuf& l = fri[li];
@@ -697,20 +830,41 @@ int WideFibProver::prove(const uint32_t* d_a, const uint32_t* d_b, ProofOut& out
     for (int k = 0; k < 4; k++) c4[k] = l.coords + ((uint64_t)k << l.log_size);
     phase(kFriMerkle);
     if ((rc = commit_columns(c4.data(), std::vector<uint32_t>(4, l.log_size), l.tree, err, err_len))) return rc;
-    Hash32 r;
-    if ((rc = download_root(l.tree, r, err, err_len))) return rc;
-    fri_roots.push_back(r);
-    ch.mix_root(r);
-    qm31 alpha = ch.draw_secure_felt();
+    channel_mix_root_draw_kernel<<<1, 32, 0, s>>>(d_chan, l.tree.layer(0), d_alphas + li + 1);
+    STWO_CHECK_LAUNCH();
+    phase(kFriFold);
     uint32_t* nxt = (li + 1 < fri.size()) ? fri[li + 1].coords : d_last;
     uint32_t nlog = l.log_size - l.fold_step;
-    std::vector<uint32_t*> o4(4);
-    for (int k = 0; k < 4; k++) o4[k] = nxt + ((uint64_t)k << nlog);
-    uint32_t al[4] = {alpha.a, alpha.b, alpha.c, alpha.d};
-    phase(kFriFold);
-    if ((rc = stwo_b200_fold_line(const_cast<const uint32_t* const*>(c4.data()), l.log_size, al, l.fold_step, d_itw,
-                                  tree_log, o4.data(), s, err, err_len)))
-      return rc;
+    fold_line_dev_kernel<<<grid1d(1ull << nlog, 256), 256, 0, s>>>(l.coords, l.log_size, l.fold_step,
+                                                                     d_alphas + li + 1, d_itw, 1ull << tree_log, nxt);
+    STWO_CHECK_LAUNCH();
+  }
+  {
+    // one download: roots, device alphas, channel state; then the host replay
+    uint8_t* hp = reinterpret_cast<uint8_t*>(h_pinned);
+    size_t off = 0;
+    STWO_CUDA_TRY(cudaMemcpyAsync(hp + off, tq.layer(0), 32, cudaMemcpyDeviceToHost, s));
+    off += 32;
+    for (auto& l : fri) {
+      STWO_CUDA_TRY(cudaMemcpyAsync(hp + off, l.tree.layer(0), 32, cudaMemcpyDeviceToHost, s));
+      off += 32;
+    }
+    size_t alpha_off = off;
+    STWO_CUDA_TRY(cudaMemcpyAsync(hp + off, d_alphas, (fri.size() + 1) * sizeof(qm31), cudaMemcpyDeviceToHost, s));
+    off += (fri.size() + 1) * sizeof(qm31);
+    size_t chan_off = off;
+    STWO_CUDA_TRY(cudaMemcpyAsync(hp + off, d_chan, sizeof(DevChannel), cudaMemcpyDeviceToHost, s));
+    STWO_CUDA_TRY(cudaStreamSynchronize(s));
+    const DevChannel* dc = reinterpret_cast<const DevChannel*>(hp + chan_off);
+    if (dc->error) return set_err(err, err_len, STWO_B200_ESTATE, "device channel: draw retry bound exhausted");
+    const qm31* dev_alpha = reinterpret_cast<const qm31*>(hp + alpha_off);
+    for (size_t i = 0; i < fri_roots.size(); i++) {
+      std::memcpy(fri_roots[i].data(), hp + 32 * i, 32);
+      ch.mix_root(fri_roots[i]);
+      qm31 a = ch.draw_secure_felt();
+      if (!qm31_eq(a, dev_alpha[i]))
+        return set_err(err, err_len, STWO_B200_ESTATE, "device and host channels diverged at FRI layer %zu", i);
+    }
   }
   // Last layer (prover/fri.rs:274-291).
   std::vector<qm31> last_coeffs;

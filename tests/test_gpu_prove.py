@@ -56,3 +56,23 @@ def test_invalid_config_rejected():
         WideFibProver(wide_fib_config(2, 100))
     with pytest.raises(ffi.B200Error):
         WideFibProver(wide_fib_config(8, 2))
+
+
+def test_phase_timing_does_not_change_proofs(oracle):
+    # The timed path records CUDA events between phases; proofs must be
+    # unchanged and every phase must have been timed.
+    import ctypes as C
+    from stwo_b200 import ffi
+    log_n, cols = 12, 100
+    a, b = oracle.wide_fib_inputs(log_n, 77)
+    ref = oracle.prove_wide_fib(oracle.wide_fib_config(log_n, cols), a, b)
+    prover = WideFibProver(wide_fib_config(log_n, cols))
+    da, db = DeviceColumn.from_host(a), DeviceColumn.from_host(b)
+    ffi.call("stwo_b200_prover_set_timing", prover.handle, C.c_int(1))
+    for _ in range(4):
+        assert prover.prove(da, db) == ref
+    ms = (C.c_double * 14)()
+    n = C.c_uint32()
+    ffi.call("stwo_b200_prover_phase_times", prover.handle, ms, C.c_uint32(14), C.byref(n))
+    assert n.value == 4
+    assert all(x > 0 for x in ms)
