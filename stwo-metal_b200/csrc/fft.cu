@@ -39,6 +39,8 @@ struct FftPass {
   uint32_t layer0, T, C;
   uint32_t scale;      // outputs are multiplied by `scale` when != 1
   uint32_t vec_io;     // 16-byte global loads/stores are legal for this launch
+  uint32_t cpb;        // columns per block: tiles of the same position share staged twiddles
+  uint32_t n_cols;     // columns in this launch
 };
 
 __device__ __forceinline__ uint32_t smem_idx(uint32_t e) { return e + (e >> 4); }
@@ -65,20 +67,23 @@ __device__ __forceinline__ void bfly(uint32_t& a, uint32_t& b, uint32_t t) {
 // 2^T - 2^(T - lam), indexed by row >> (lam + 1).
 template <int RS, bool INV>
 __device__ __forceinline__ void fft_stage(uint32_t* __restrict__ sm, const uint32_t* __restrict__ tws, uint32_t T,
-                                          uint32_t C, uint32_t s0) {
+                                          uint32_t C, uint32_t s0, uint32_t n_tiles, uint32_t tile_stride) {
   const uint32_t E = 1u << (T + C);
-  const uint32_t groups = E >> RS;
+  const uint32_t log_groups = T + C - RS;
+  const uint32_t groups = n_tiles << log_groups;
   const uint32_t cmask = (1u << C) - 1;
   const uint32_t lowmask = (1u << s0) - 1;
   for (uint32_t q = threadIdx.x; q < groups; q += blockDim.x) {
-    const uint32_t c = q & cmask;
-    const uint32_t rest = q >> C;
+    uint32_t* tile = sm + (q >> log_groups) * tile_stride;
+    const uint32_t qq = q & ((1u << log_groups) - 1);
+    const uint32_t c = qq & cmask;
+    const uint32_t rest = qq >> C;
     const uint32_t low = rest & lowmask;
     const uint32_t high = rest >> s0;
     const uint32_t rowbase = (high << (s0 + RS)) | low;
     uint32_t v[1 << RS];
 #pragma unroll
-    for (int j = 0; j < (1 << RS); j++) v[j] = sm[smem_idx(((rowbase | ((uint32_t)j << s0)) << C) | c)];
+    for (int j = 0; j < (1 << RS); j++) v[j] = tile[smem_idx(((rowbase | ((uint32_t)j << s0)) << C) | c)];
 #pragma unroll
     for (int kk = 0; kk < RS; kk++) {
       const int k = INV ? kk : (RS - 1 - kk);
@@ -99,8 +104,9 @@ __device__ __forceinline__ void fft_stage(uint32_t* __restrict__ sm, const uint3
       }
     }
 #pragma unroll
-    for (int j = 0; j < (1 << RS); j++) sm[smem_idx(((rowbase | ((uint32_t)j << s0)) << C) | c)] = v[j];
+    for (int j = 0; j < (1 << RS); j++) tile[smem_idx(((rowbase | ((uint32_t)j << s0)) << C) | c)] = v[j];
   }
+  (void)E;
 }
 
 template <bool INV>
@@ -108,10 +114,11 @@ __global__ void __launch_bounds__(256, 4) fft_pass_kernel(FftPass p, FftCols col
   extern __shared__ uint32_t smem[];
   const uint32_t T = p.T, C = p.C, L0 = p.layer0;
   const uint32_t E = 1u << (T + C);
+  const uint32_t tile_stride = E + (E >> 4) + 1;
+  const uint32_t col0 = blockIdx.y * p.cpb;
+  const uint32_t n_tiles = min(p.cpb, p.n_cols - col0);
   uint32_t* __restrict__ sm = smem;
-  uint32_t* __restrict__ tws = smem + E + (E >> 4) + 1;
-  const uint32_t* __restrict__ src = cols.src[blockIdx.y];
-  uint32_t* __restrict__ dst = cols.dst[blockIdx.y];
+  uint32_t* __restrict__ tws = smem + p.cpb * tile_stride;
   const uint64_t tile = blockIdx.x;
   const uint32_t lo_bits = L0 - C;  // L0 >= C
   const uint64_t lo = tile & ((1ull << lo_bits) - 1);
@@ -119,8 +126,8 @@ __global__ void __launch_bounds__(256, 4) fft_pass_kernel(FftPass p, FftCols col
   const uint64_t base = (hi << (L0 + T)) | (lo << C);
   const uint32_t cmask = (1u << C) - 1;
 
-  // Stage this tile's twiddles: layer lam needs 2^(T-1-lam) consecutive
-  // entries starting at hi << (T-1-lam) of tree layer L0 + lam.
+  // Stage the twiddles of this tile position: layer lam needs 2^(T-1-lam)
+  // consecutive entries starting at hi << (T-1-lam) of tree layer L0 + lam.
   for (uint32_t lam = 0; lam < T; lam++) {
     const uint32_t cnt = 1u << (T - 1 - lam);
     const uint32_t off = (1u << T) - (1u << (T - lam));
@@ -135,22 +142,26 @@ __global__ void __launch_bounds__(256, 4) fft_pass_kernel(FftPass p, FftCols col
     }
   }
 
-  // Load the tile; rows of 2^C >= 4 words (or contiguous tiles) use 16-byte loads.
-  if (p.vec_io) {
-    for (uint32_t e = threadIdx.x * 4; e < E; e += blockDim.x * 4) {
-      const uint64_t g = base + ((uint64_t)(e >> C) << L0) + (e & cmask);
-      const uint64_t gi = g & p.src_mask;
-      const uint4 w = gi < p.src_len ? __ldg(reinterpret_cast<const uint4*>(src + gi)) : make_uint4(0, 0, 0, 0);
-      sm[smem_idx(e)] = w.x;
-      sm[smem_idx(e + 1)] = w.y;
-      sm[smem_idx(e + 2)] = w.z;
-      sm[smem_idx(e + 3)] = w.w;
-    }
-  } else {
-    for (uint32_t e = threadIdx.x; e < E; e += blockDim.x) {
-      const uint64_t g = base + ((uint64_t)(e >> C) << L0) + (e & cmask);
-      const uint64_t gi = g & p.src_mask;
-      sm[smem_idx(e)] = gi < p.src_len ? __ldg(src + gi) : 0u;
+  // Load the tiles; rows of 2^C >= 4 words (or contiguous tiles) use 16-byte loads.
+  for (uint32_t cc = 0; cc < n_tiles; cc++) {
+    const uint32_t* __restrict__ src = cols.src[col0 + cc];
+    uint32_t* tsm = sm + cc * tile_stride;
+    if (p.vec_io) {
+      for (uint32_t e = threadIdx.x * 4; e < E; e += blockDim.x * 4) {
+        const uint64_t g = base + ((uint64_t)(e >> C) << L0) + (e & cmask);
+        const uint64_t gi = g & p.src_mask;
+        const uint4 w = gi < p.src_len ? __ldg(reinterpret_cast<const uint4*>(src + gi)) : make_uint4(0, 0, 0, 0);
+        tsm[smem_idx(e)] = w.x;
+        tsm[smem_idx(e + 1)] = w.y;
+        tsm[smem_idx(e + 2)] = w.z;
+        tsm[smem_idx(e + 3)] = w.w;
+      }
+    } else {
+      for (uint32_t e = threadIdx.x; e < E; e += blockDim.x) {
+        const uint64_t g = base + ((uint64_t)(e >> C) << L0) + (e & cmask);
+        const uint64_t gi = g & p.src_mask;
+        tsm[smem_idx(e)] = gi < p.src_len ? __ldg(src + gi) : 0u;
+      }
     }
   }
   __syncthreads();
@@ -159,10 +170,10 @@ __global__ void __launch_bounds__(256, 4) fft_pass_kernel(FftPass p, FftCols col
     for (uint32_t s0 = 0; s0 < T;) {
       const uint32_t rs = min(4u, T - s0);
       switch (rs) {
-        case 4: fft_stage<4, INV>(sm, tws, T, C, s0); break;
-        case 3: fft_stage<3, INV>(sm, tws, T, C, s0); break;
-        case 2: fft_stage<2, INV>(sm, tws, T, C, s0); break;
-        default: fft_stage<1, INV>(sm, tws, T, C, s0); break;
+        case 4: fft_stage<4, INV>(sm, tws, T, C, s0, n_tiles, tile_stride); break;
+        case 3: fft_stage<3, INV>(sm, tws, T, C, s0, n_tiles, tile_stride); break;
+        case 2: fft_stage<2, INV>(sm, tws, T, C, s0, n_tiles, tile_stride); break;
+        default: fft_stage<1, INV>(sm, tws, T, C, s0, n_tiles, tile_stride); break;
       }
       s0 += rs;
       __syncthreads();
@@ -172,10 +183,10 @@ __global__ void __launch_bounds__(256, 4) fft_pass_kernel(FftPass p, FftCols col
       const uint32_t rs = min(4u, top);
       const uint32_t s0 = top - rs;
       switch (rs) {
-        case 4: fft_stage<4, INV>(sm, tws, T, C, s0); break;
-        case 3: fft_stage<3, INV>(sm, tws, T, C, s0); break;
-        case 2: fft_stage<2, INV>(sm, tws, T, C, s0); break;
-        default: fft_stage<1, INV>(sm, tws, T, C, s0); break;
+        case 4: fft_stage<4, INV>(sm, tws, T, C, s0, n_tiles, tile_stride); break;
+        case 3: fft_stage<3, INV>(sm, tws, T, C, s0, n_tiles, tile_stride); break;
+        case 2: fft_stage<2, INV>(sm, tws, T, C, s0, n_tiles, tile_stride); break;
+        default: fft_stage<1, INV>(sm, tws, T, C, s0, n_tiles, tile_stride); break;
       }
       top = s0;
       __syncthreads();
@@ -183,23 +194,27 @@ __global__ void __launch_bounds__(256, 4) fft_pass_kernel(FftPass p, FftCols col
   }
 
   const uint32_t scale = p.scale;
-  if (p.vec_io) {
-    for (uint32_t e = threadIdx.x * 4; e < E; e += blockDim.x * 4) {
-      const uint64_t g = base + ((uint64_t)(e >> C) << L0) + (e & cmask);
-      uint4 w = make_uint4(sm[smem_idx(e)], sm[smem_idx(e + 1)], sm[smem_idx(e + 2)], sm[smem_idx(e + 3)]);
-      if (scale != 1u) {
-        w.x = m31_mul(w.x, scale);
-        w.y = m31_mul(w.y, scale);
-        w.z = m31_mul(w.z, scale);
-        w.w = m31_mul(w.w, scale);
+  for (uint32_t cc = 0; cc < n_tiles; cc++) {
+    uint32_t* __restrict__ dst = cols.dst[col0 + cc];
+    const uint32_t* tsm = sm + cc * tile_stride;
+    if (p.vec_io) {
+      for (uint32_t e = threadIdx.x * 4; e < E; e += blockDim.x * 4) {
+        const uint64_t g = base + ((uint64_t)(e >> C) << L0) + (e & cmask);
+        uint4 w = make_uint4(tsm[smem_idx(e)], tsm[smem_idx(e + 1)], tsm[smem_idx(e + 2)], tsm[smem_idx(e + 3)]);
+        if (scale != 1u) {
+          w.x = m31_mul(w.x, scale);
+          w.y = m31_mul(w.y, scale);
+          w.z = m31_mul(w.z, scale);
+          w.w = m31_mul(w.w, scale);
+        }
+        *reinterpret_cast<uint4*>(dst + g) = w;
       }
-      *reinterpret_cast<uint4*>(dst + g) = w;
-    }
-  } else {
-    for (uint32_t e = threadIdx.x; e < E; e += blockDim.x) {
-      const uint64_t g = base + ((uint64_t)(e >> C) << L0) + (e & cmask);
-      const uint32_t v = sm[smem_idx(e)];
-      dst[g] = scale != 1u ? m31_mul(v, scale) : v;
+    } else {
+      for (uint32_t e = threadIdx.x; e < E; e += blockDim.x) {
+        const uint64_t g = base + ((uint64_t)(e >> C) << L0) + (e & cmask);
+        const uint32_t v = tsm[smem_idx(e)];
+        dst[g] = scale != 1u ? m31_mul(v, scale) : v;
+      }
     }
   }
 }
@@ -318,7 +333,11 @@ static int launch_pass(const FftPass& p, const std::vector<const uint32_t*>& src
                        uint64_t total_log, cudaStream_t s, char* err, size_t err_len) {
   uint64_t tiles = 1ull << (total_log - p.T - p.C);
   size_t E = (size_t)1 << (p.T + p.C);
-  size_t smem = (E + E / 16 + 1 + ((size_t)1 << p.T)) * sizeof(uint32_t);
+  // Contiguous passes (small tiles, twiddles as large as the data) share one
+  // staged twiddle table between up to 4 columns of the same tile position.
+  const uint32_t cpb = (p.C == 0 && E <= 4096 && srcs.size() >= 4) ? 4u : 1u;
+  size_t tile_words = E + E / 16 + 1;
+  size_t smem = (cpb * tile_words + ((size_t)1 << p.T)) * sizeof(uint32_t);
   static bool attr_set[2] = {false, false};
   if (!attr_set[INV]) {
     STWO_CUDA_TRY(cudaFuncSetAttribute(fft_pass_kernel<INV>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
@@ -338,9 +357,10 @@ static int launch_pass(const FftPass& p, const std::vector<const uint32_t*>& src
     FftPass q = p;
     q.vec_io = aligned && (p.C >= 2 || p.layer0 == 0) && E >= 4 && (p.src_mask & 3) == 3 &&
                (p.src_len == ~0ull || p.src_len % 4 == 0);
-    dim3 grid((unsigned)tiles, (unsigned)nc);
-    // one radix-16 group per thread per stage for small tiles
-    const unsigned threads = E <= 2048 ? 128 : 256;
+    q.cpb = cpb;
+    q.n_cols = (uint32_t)nc;
+    dim3 grid((unsigned)tiles, (unsigned)((nc + cpb - 1) / cpb));
+    const unsigned threads = (cpb * E) <= 2048 ? 128 : 256;
     fft_pass_kernel<INV><<<grid, threads, smem, s>>>(q, cols);
     STWO_CHECK_LAUNCH();
   }

@@ -29,6 +29,35 @@ int build_node_layers_impl(const uint8_t* in, uint32_t in_log, uint32_t stop_log
 
 // ----------------------------------------------------------------- kernels --
 
+// Exact M31 dot products: products of canonical words (< 2^62) are summed in
+// 64 bits and folded with 2^31 = 1 (mod P) every three terms, then reduced
+// once to the canonical value.  The residue is exact, so the result equals the
+// canonical value SimdBackend's reduced-per-operation arithmetic produces.
+__device__ __forceinline__ uint64_t fold64(uint64_t x) { return (x & M31_P) + (x >> 31); }  // < 2^34
+__device__ __forceinline__ uint32_t reduce_acc(uint64_t x) {
+  x = fold64(fold64(x));  // < P + 8
+  uint32_t y = (uint32_t)x;
+  return y >= M31_P ? y - M31_P : y;
+}
+struct acc4 {
+  uint64_t a, b, c, d;
+};
+__device__ __forceinline__ void acc4_mad(acc4& s, const qm31& w, uint32_t v) {
+  s.a += (uint64_t)w.a * v;
+  s.b += (uint64_t)w.b * v;
+  s.c += (uint64_t)w.c * v;
+  s.d += (uint64_t)w.d * v;
+}
+__device__ __forceinline__ void acc4_fold(acc4& s) {
+  s.a = fold64(s.a);
+  s.b = fold64(s.b);
+  s.c = fold64(s.c);
+  s.d = fold64(s.d);
+}
+__device__ __forceinline__ qm31 acc4_reduce(const acc4& s) {
+  return {reduce_acc(s.a), reduce_acc(s.b), reduce_acc(s.c), reduce_acc(s.d)};
+}
+
 // One thread per row: col[i+2] = col[i]^2 + col[i+1]^2 (wide_fibonacci/mod.rs:27-50).
 __global__ void wide_fib_trace_kernel(const uint32_t* __restrict__ a, const uint32_t* __restrict__ b,
                                       uint32_t* __restrict__ cols, uint32_t n_cols, uint64_t rows) {
@@ -55,15 +84,31 @@ __global__ void composition_kernel(const uint32_t* __restrict__ evals, uint64_t 
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n_points;
        i += (uint64_t)gridDim.x * blockDim.x) {
     uint32_t a = __ldg(evals + i), b = __ldg(evals + col_stride + i);
-    qm31 row = qm31_zero();
-    for (uint32_t k = 0; k < n_cons; k++) {
-      uint32_t c = __ldg(evals + (uint64_t)(k + 2) * col_stride + i);
-      uint32_t cons = m31_sub(c, m31_add(m31_sqr(a), m31_sqr(b)));
-      row = qm31_add(row, qm31_mul_m31(powers[k], cons));
-      a = b;
-      b = c;
+    uint32_t sa = m31_sqr(a), sb = m31_sqr(b);
+    acc4 row{0, 0, 0, 0};
+    uint32_t k = 0;
+    for (; k + 6 <= n_cons; k += 6) {
+      uint32_t cv[6];  // six independent loads in flight per thread
+#pragma unroll
+      for (int u = 0; u < 6; u++) cv[u] = __ldg(evals + (uint64_t)(k + u + 2) * col_stride + i);
+#pragma unroll
+      for (int u = 0; u < 6; u++) {
+        uint32_t cons = m31_sub(cv[u], m31_add(sa, sb));
+        acc4_mad(row, powers[k + u], cons);
+        sa = sb;
+        sb = m31_sqr(cv[u]);
+        if (u == 2 || u == 5) acc4_fold(row);
+      }
     }
-    qm31 v = qm31_mul_m31(row, __ldg(denom_inv + (i >> log_n)));
+    for (; k < n_cons; k++) {  // remainder: fold after every term
+      uint32_t c = __ldg(evals + (uint64_t)(k + 2) * col_stride + i);
+      uint32_t cons = m31_sub(c, m31_add(sa, sb));
+      acc4_mad(row, powers[k], cons);
+      acc4_fold(row);
+      sa = sb;
+      sb = m31_sqr(c);
+    }
+    qm31 v = qm31_mul_m31(acc4_reduce(row), __ldg(denom_inv + (i >> log_n)));
     out[i] = v.a;
     out[n_points + i] = v.b;
     out[2 * n_points + i] = v.c;
@@ -90,18 +135,24 @@ __global__ void __launch_bounds__(256) batch_eval_kernel(PolyTable t, uint32_t n
   const uint32_t np = min((uint32_t)kEvalGroup, n_polys - p0);
   const uint64_t n = 1ull << log_n;
   const uint64_t lo_mask = (1ull << h) - 1;
-  qm31 acc[kEvalGroup];
+  acc4 acc[kEvalGroup];
 #pragma unroll
-  for (int q = 0; q < kEvalGroup; q++) acc[q] = qm31_zero();
+  for (int q = 0; q < kEvalGroup; q++) acc[q] = {0, 0, 0, 0};
+  uint32_t since_fold = 0;
   for (uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; j < n; j += (uint64_t)gridDim.x * blockDim.x) {
     qm31 w = qm31_mul(w_hi[j >> h], w_lo[j & lo_mask]);
 #pragma unroll
     for (int q = 0; q < kEvalGroup; q++)
-      if (q < (int)np) acc[q] = qm31_add(acc[q], qm31_mul_m31(w, __ldg(t.p[p0 + q] + j)));
+      if (q < (int)np) acc4_mad(acc[q], w, __ldg(t.p[p0 + q] + j));
+    if (++since_fold == 3) {
+      since_fold = 0;
+#pragma unroll
+      for (int q = 0; q < kEvalGroup; q++) acc4_fold(acc[q]);
+    }
   }
   __shared__ qm31 red[256];
   for (uint32_t q = 0; q < np; q++) {
-    red[threadIdx.x] = acc[q];
+    red[threadIdx.x] = acc4_reduce(acc[q]);
     __syncthreads();
     for (uint32_t s = blockDim.x / 2; s > 0; s >>= 1) {
       if (threadIdx.x < s) red[threadIdx.x] = qm31_add(red[threadIdx.x], red[threadIdx.x + s]);
@@ -139,8 +190,23 @@ __global__ void __launch_bounds__(256) quotient_kernel(QuotientParams q, PolyTab
   const uint64_t n = 1ull << q.log_size;
   const uint64_t half = n >> 1;
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
-    qm31 acc = qm31_zero();
-    for (uint32_t k = 0; k < n_cols; k++) acc = qm31_add(acc, qm31_mul_m31(alpha_pows[k], __ldg(cols.p[k] + i)));
+    acc4 s4{0, 0, 0, 0};
+    uint32_t k = 0;
+    for (; k + 6 <= n_cols; k += 6) {
+      uint32_t fv[6];  // six independent loads in flight per thread
+#pragma unroll
+      for (int u = 0; u < 6; u++) fv[u] = __ldg(cols.p[k + u] + i);
+#pragma unroll
+      for (int u = 0; u < 6; u++) {
+        acc4_mad(s4, alpha_pows[k + u], fv[u]);
+        if (u == 2 || u == 5) acc4_fold(s4);
+      }
+    }
+    for (; k < n_cols; k++) {  // remainder: fold after every term
+      acc4_mad(s4, alpha_pows[k], __ldg(cols.p[k] + i));
+      acc4_fold(s4);
+    }
+    qm31 acc = acc4_reduce(s4);
     // domain point at bit-reversed position i (core/poly/circle/domain.rs:56-66)
     uint64_t j = __brevll(i) >> (64 - q.log_size);
     uint64_t jj = j < half ? j : j - half;
