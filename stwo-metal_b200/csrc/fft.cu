@@ -43,7 +43,6 @@ struct FftPass {
   uint32_t n_cols;     // columns in this launch
 };
 
-__device__ __forceinline__ uint32_t smem_idx(uint32_t e) { return e + (e >> 4); }
 
 // Circle-layer twiddle for butterfly h, from line layer 1 (x, y pairs).
 __device__ __forceinline__ uint32_t circle_tw(const uint32_t* lt0, uint64_t h) {
@@ -62,35 +61,53 @@ __device__ __forceinline__ void bfly(uint32_t& a, uint32_t& b, uint32_t t) {
   a = m31_add(a, m);
 }
 
-// One register stage over tile row bits [s0, s0 + RS).  Twiddles come from
-// the per-tile table `tws`: layer lam (relative to layer0) at offset
+__host__ __device__ constexpr uint32_t tile_stride_words(uint32_t e) { return e + (e >> 4) + 1; }
+__host__ __device__ constexpr uint32_t smem_off(uint32_t e) { return e + (e >> 4); }
+
+// Threads per block of a pass: one radix-16 group per thread, 32..256.
+__host__ __device__ constexpr int fft_threads(int T, int C, int CPB) {
+  return ((CPB << (T + C)) >> 4) >= 256 ? 256
+         : ((CPB << (T + C)) >> 4) >= 128 ? 128
+         : ((CPB << (T + C)) >> 4) >= 64  ? 64
+                                          : 32;
+}
+
+// One register stage over tile row bits [S0, S0 + RS) of CPB tiles.  Tile
+// shape and stage position are compile-time, so the 2^RS shared-memory
+// offsets of a group are immediates: for disjoint bit sets,
+// smem_off(ebase | J) = smem_off(ebase) + smem_off(J).  Twiddles come from the
+// per-position table `tws`: layer lam (relative to layer0) at offset
 // 2^T - 2^(T - lam), indexed by row >> (lam + 1).
-template <int RS, bool INV>
-__device__ __forceinline__ void fft_stage(uint32_t* __restrict__ sm, const uint32_t* __restrict__ tws, uint32_t T,
-                                          uint32_t C, uint32_t s0, uint32_t n_tiles, uint32_t tile_stride) {
-  const uint32_t E = 1u << (T + C);
-  const uint32_t log_groups = T + C - RS;
-  const uint32_t groups = n_tiles << log_groups;
-  const uint32_t cmask = (1u << C) - 1;
-  const uint32_t lowmask = (1u << s0) - 1;
-  for (uint32_t q = threadIdx.x; q < groups; q += blockDim.x) {
-    uint32_t* tile = sm + (q >> log_groups) * tile_stride;
-    const uint32_t qq = q & ((1u << log_groups) - 1);
-    const uint32_t c = qq & cmask;
+template <bool INV, int T, int C, int CPB, int NT, int RS, int S0>
+__device__ __forceinline__ void tile_stage(uint32_t* __restrict__ sm, const uint32_t* __restrict__ tws,
+                                           uint32_t n_tiles) {
+  constexpr uint32_t E = 1u << (T + C);
+  constexpr uint32_t STRIDE = tile_stride_words(E);
+  constexpr int LG = T + C - RS;
+  constexpr uint32_t GROUPS = (uint32_t)CPB << LG;
+  constexpr int ITERS = (int)((GROUPS + NT - 1) / NT);
+#pragma unroll
+  for (int it = 0; it < ITERS; it++) {
+    const uint32_t q = threadIdx.x + (uint32_t)it * NT;
+    if ((GROUPS % NT) != 0 && q >= GROUPS) break;
+    const uint32_t tile = q >> LG;
+    if (CPB > 1 && tile >= n_tiles) break;
+    const uint32_t qq = q & ((1u << LG) - 1);
+    const uint32_t c = qq & ((1u << C) - 1);
     const uint32_t rest = qq >> C;
-    const uint32_t low = rest & lowmask;
-    const uint32_t high = rest >> s0;
-    const uint32_t rowbase = (high << (s0 + RS)) | low;
+    const uint32_t low = rest & ((1u << S0) - 1);
+    const uint32_t high = rest >> S0;
+    const uint32_t ebase = (((high << (S0 + RS)) | low) << C) | c;
+    uint32_t* __restrict__ g = sm + tile * STRIDE + smem_off(ebase);
     uint32_t v[1 << RS];
 #pragma unroll
-    for (int j = 0; j < (1 << RS); j++) v[j] = tile[smem_idx(((rowbase | ((uint32_t)j << s0)) << C) | c)];
+    for (int j = 0; j < (1 << RS); j++) v[j] = g[smem_off((uint32_t)j << (S0 + C))];
 #pragma unroll
     for (int kk = 0; kk < RS; kk++) {
       const int k = INV ? kk : (RS - 1 - kk);
-      const uint32_t lam = s0 + k;
       // Butterfly (j, j | 2^k) uses twiddle (high << (RS-1-k)) + (j >> (k+1)):
       // 2^(RS-1-k) distinct values per group.
-      const uint32_t* tl = tws + ((1u << T) - (1u << (T - lam))) + (high << (RS - 1 - k));
+      const uint32_t* tl = tws + ((1u << T) - (1u << (T - (S0 + k)))) + (high << (RS - 1 - k));
       uint32_t t[1 << (RS - 1)];
 #pragma unroll
       for (int m = 0; m < (1 << (RS - 1 - k)); m++) t[m] = tl[m];
@@ -104,103 +121,102 @@ __device__ __forceinline__ void fft_stage(uint32_t* __restrict__ sm, const uint3
       }
     }
 #pragma unroll
-    for (int j = 0; j < (1 << RS); j++) tile[smem_idx(((rowbase | ((uint32_t)j << s0)) << C) | c)] = v[j];
+    for (int j = 0; j < (1 << RS); j++) g[smem_off((uint32_t)j << (S0 + C))] = v[j];
   }
-  (void)E;
 }
 
-template <bool INV>
-__global__ void __launch_bounds__(256, 4) fft_pass_kernel(FftPass p, FftCols cols) {
+// IFFT stages bottom-up from S0; RFFT stages top-down from TOP.
+template <int T, int C, int CPB, int NT, int S0>
+__device__ __forceinline__ void inv_stages(uint32_t* sm, const uint32_t* tws, uint32_t n_tiles) {
+  constexpr int RS = (T - S0) < 4 ? (T - S0) : 4;
+  tile_stage<true, T, C, CPB, NT, RS, S0>(sm, tws, n_tiles);
+  __syncthreads();
+  if constexpr (S0 + RS < T) inv_stages<T, C, CPB, NT, S0 + RS>(sm, tws, n_tiles);
+}
+template <int T, int C, int CPB, int NT, int TOP>
+__device__ __forceinline__ void fwd_stages(uint32_t* sm, const uint32_t* tws, uint32_t n_tiles) {
+  constexpr int RS = TOP < 4 ? TOP : 4;
+  tile_stage<false, T, C, CPB, NT, RS, TOP - RS>(sm, tws, n_tiles);
+  __syncthreads();
+  if constexpr (TOP - RS > 0) fwd_stages<T, C, CPB, NT, TOP - RS>(sm, tws, n_tiles);
+}
+
+template <bool INV, int T, int C, int CPB, int NT>
+__global__ void __launch_bounds__(NT, 1024 / NT) fft_pass_kernel(FftPass p, FftCols cols) {
+  constexpr uint32_t E = 1u << (T + C);
+  constexpr uint32_t STRIDE = tile_stride_words(E);
+  constexpr uint32_t CMASK = (1u << C) - 1;
   extern __shared__ uint32_t smem[];
-  const uint32_t T = p.T, C = p.C, L0 = p.layer0;
-  const uint32_t E = 1u << (T + C);
-  const uint32_t tile_stride = E + (E >> 4) + 1;
-  const uint32_t col0 = blockIdx.y * p.cpb;
-  const uint32_t n_tiles = min(p.cpb, p.n_cols - col0);
+  const uint32_t L0 = p.layer0;
+  const uint32_t col0 = blockIdx.y * CPB;
+  const uint32_t n_tiles = CPB == 1 ? 1u : min((uint32_t)CPB, p.n_cols - col0);
   uint32_t* __restrict__ sm = smem;
-  uint32_t* __restrict__ tws = smem + p.cpb * tile_stride;
+  uint32_t* __restrict__ tws = smem + CPB * STRIDE;
   const uint64_t tile = blockIdx.x;
   const uint32_t lo_bits = L0 - C;  // L0 >= C
   const uint64_t lo = tile & ((1ull << lo_bits) - 1);
   const uint64_t hi = tile >> lo_bits;
   const uint64_t base = (hi << (L0 + T)) | (lo << C);
-  const uint32_t cmask = (1u << C) - 1;
 
   // Stage the twiddles of this tile position: layer lam needs 2^(T-1-lam)
   // consecutive entries starting at hi << (T-1-lam) of tree layer L0 + lam.
-  for (uint32_t lam = 0; lam < T; lam++) {
-    const uint32_t cnt = 1u << (T - 1 - lam);
-    const uint32_t off = (1u << T) - (1u << (T - lam));
+#pragma unroll
+  for (int lam = 0; lam < T; lam++) {
+    constexpr uint32_t one = 1;
+    const uint32_t cnt = one << (T - 1 - lam);
+    const uint32_t off = (one << T) - (one << (T - lam));
     const uint64_t h0 = hi << (T - 1 - lam);
     const uint32_t layer = L0 + lam;
     if (layer == 0) {
       const uint32_t* lt0 = p.tree + (p.tree_len - (1ull << (p.log_domain - 1)));
-      for (uint32_t i = threadIdx.x; i < cnt; i += blockDim.x) tws[off + i] = circle_tw(lt0, h0 + i);
+      for (uint32_t i = threadIdx.x; i < cnt; i += NT) tws[off + i] = circle_tw(lt0, h0 + i);
     } else {
       const uint32_t* lt = p.tree + (p.tree_len - (1ull << (p.log_domain - layer))) + h0;
-      for (uint32_t i = threadIdx.x; i < cnt; i += blockDim.x) tws[off + i] = __ldg(lt + i);
+      for (uint32_t i = threadIdx.x; i < cnt; i += NT) tws[off + i] = __ldg(lt + i);
     }
   }
 
   // Load the tiles; rows of 2^C >= 4 words (or contiguous tiles) use 16-byte loads.
   for (uint32_t cc = 0; cc < n_tiles; cc++) {
     const uint32_t* __restrict__ src = cols.src[col0 + cc];
-    uint32_t* tsm = sm + cc * tile_stride;
+    uint32_t* tsm = sm + cc * STRIDE;
     if (p.vec_io) {
-      for (uint32_t e = threadIdx.x * 4; e < E; e += blockDim.x * 4) {
-        const uint64_t g = base + ((uint64_t)(e >> C) << L0) + (e & cmask);
+#pragma unroll 4
+      for (uint32_t e = threadIdx.x * 4; e < E; e += NT * 4) {
+        const uint64_t g = base + ((uint64_t)(e >> C) << L0) + (e & CMASK);
         const uint64_t gi = g & p.src_mask;
         const uint4 w = gi < p.src_len ? __ldg(reinterpret_cast<const uint4*>(src + gi)) : make_uint4(0, 0, 0, 0);
-        tsm[smem_idx(e)] = w.x;
-        tsm[smem_idx(e + 1)] = w.y;
-        tsm[smem_idx(e + 2)] = w.z;
-        tsm[smem_idx(e + 3)] = w.w;
+        uint32_t* d = tsm + smem_off(e);  // e % 4 == 0: the four words share one padding group
+        d[0] = w.x;
+        d[1] = w.y;
+        d[2] = w.z;
+        d[3] = w.w;
       }
     } else {
-      for (uint32_t e = threadIdx.x; e < E; e += blockDim.x) {
-        const uint64_t g = base + ((uint64_t)(e >> C) << L0) + (e & cmask);
+      for (uint32_t e = threadIdx.x; e < E; e += NT) {
+        const uint64_t g = base + ((uint64_t)(e >> C) << L0) + (e & CMASK);
         const uint64_t gi = g & p.src_mask;
-        tsm[smem_idx(e)] = gi < p.src_len ? __ldg(src + gi) : 0u;
+        tsm[smem_off(e)] = gi < p.src_len ? __ldg(src + gi) : 0u;
       }
     }
   }
   __syncthreads();
 
-  if (INV) {
-    for (uint32_t s0 = 0; s0 < T;) {
-      const uint32_t rs = min(4u, T - s0);
-      switch (rs) {
-        case 4: fft_stage<4, INV>(sm, tws, T, C, s0, n_tiles, tile_stride); break;
-        case 3: fft_stage<3, INV>(sm, tws, T, C, s0, n_tiles, tile_stride); break;
-        case 2: fft_stage<2, INV>(sm, tws, T, C, s0, n_tiles, tile_stride); break;
-        default: fft_stage<1, INV>(sm, tws, T, C, s0, n_tiles, tile_stride); break;
-      }
-      s0 += rs;
-      __syncthreads();
-    }
-  } else {
-    for (uint32_t top = T; top > 0;) {
-      const uint32_t rs = min(4u, top);
-      const uint32_t s0 = top - rs;
-      switch (rs) {
-        case 4: fft_stage<4, INV>(sm, tws, T, C, s0, n_tiles, tile_stride); break;
-        case 3: fft_stage<3, INV>(sm, tws, T, C, s0, n_tiles, tile_stride); break;
-        case 2: fft_stage<2, INV>(sm, tws, T, C, s0, n_tiles, tile_stride); break;
-        default: fft_stage<1, INV>(sm, tws, T, C, s0, n_tiles, tile_stride); break;
-      }
-      top = s0;
-      __syncthreads();
-    }
-  }
+  if constexpr (INV)
+    inv_stages<T, C, CPB, NT, 0>(sm, tws, n_tiles);
+  else
+    fwd_stages<T, C, CPB, NT, T>(sm, tws, n_tiles);
 
   const uint32_t scale = p.scale;
   for (uint32_t cc = 0; cc < n_tiles; cc++) {
     uint32_t* __restrict__ dst = cols.dst[col0 + cc];
-    const uint32_t* tsm = sm + cc * tile_stride;
+    const uint32_t* tsm = sm + cc * STRIDE;
     if (p.vec_io) {
-      for (uint32_t e = threadIdx.x * 4; e < E; e += blockDim.x * 4) {
-        const uint64_t g = base + ((uint64_t)(e >> C) << L0) + (e & cmask);
-        uint4 w = make_uint4(tsm[smem_idx(e)], tsm[smem_idx(e + 1)], tsm[smem_idx(e + 2)], tsm[smem_idx(e + 3)]);
+#pragma unroll 4
+      for (uint32_t e = threadIdx.x * 4; e < E; e += NT * 4) {
+        const uint64_t g = base + ((uint64_t)(e >> C) << L0) + (e & CMASK);
+        const uint32_t* d = tsm + smem_off(e);
+        uint4 w = make_uint4(d[0], d[1], d[2], d[3]);
         if (scale != 1u) {
           w.x = m31_mul(w.x, scale);
           w.y = m31_mul(w.y, scale);
@@ -210,9 +226,9 @@ __global__ void __launch_bounds__(256, 4) fft_pass_kernel(FftPass p, FftCols col
         *reinterpret_cast<uint4*>(dst + g) = w;
       }
     } else {
-      for (uint32_t e = threadIdx.x; e < E; e += blockDim.x) {
-        const uint64_t g = base + ((uint64_t)(e >> C) << L0) + (e & cmask);
-        const uint32_t v = tsm[smem_idx(e)];
+      for (uint32_t e = threadIdx.x; e < E; e += NT) {
+        const uint64_t g = base + ((uint64_t)(e >> C) << L0) + (e & CMASK);
+        const uint32_t v = tsm[smem_off(e)];
         dst[g] = scale != 1u ? m31_mul(v, scale) : v;
       }
     }
@@ -328,21 +344,46 @@ static void index_point(uint64_t idx, uint32_t& x, uint32_t& y) {
   }
 }
 
+template <bool INV, int T, int C, int CPB>
+static int launch_tile(const FftPass& q, const FftCols& cols, dim3 grid, cudaStream_t s, char* err, size_t err_len) {
+  constexpr int NT = fft_threads(T, C, CPB);
+  constexpr size_t E = (size_t)1 << (T + C);
+  constexpr size_t smem = ((size_t)CPB * tile_stride_words(E) + ((size_t)1 << T)) * sizeof(uint32_t);
+  static_assert(smem <= 200 * 1024, "FFT tile exceeds shared memory");
+  static bool attr_set = false;
+  if (!attr_set) {
+    STWO_CUDA_TRY(cudaFuncSetAttribute(fft_pass_kernel<INV, T, C, CPB, NT>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    attr_set = true;
+  }
+  fft_pass_kernel<INV, T, C, CPB, NT><<<grid, NT, smem, s>>>(q, cols);
+  STWO_CHECK_LAUNCH();
+  return STWO_B200_OK;
+}
+
+template <bool INV, int C, int CPB>
+static int dispatch_tile(const FftPass& q, const FftCols& cols, dim3 grid, cudaStream_t s, char* err,
+                         size_t err_len) {
+  switch (q.T) {
+#define STWO_FFT_T(TT) \
+  case TT: return launch_tile<INV, TT, C, CPB>(q, cols, grid, s, err, err_len);
+    STWO_FFT_T(1) STWO_FFT_T(2) STWO_FFT_T(3) STWO_FFT_T(4) STWO_FFT_T(5) STWO_FFT_T(6)
+    STWO_FFT_T(7) STWO_FFT_T(8) STWO_FFT_T(9) STWO_FFT_T(10) STWO_FFT_T(11) STWO_FFT_T(12)
+#undef STWO_FFT_T
+    default: break;
+  }
+  return set_err(err, err_len, STWO_B200_EARG, "unsupported FFT pass size T=%u", q.T);
+}
+
 template <bool INV>
 static int launch_pass(const FftPass& p, const std::vector<const uint32_t*>& srcs, const std::vector<uint32_t*>& dsts,
                        uint64_t total_log, cudaStream_t s, char* err, size_t err_len) {
   uint64_t tiles = 1ull << (total_log - p.T - p.C);
   size_t E = (size_t)1 << (p.T + p.C);
+  STWO_ARG_CHECK(p.C == 0 || p.C == 3, "unsupported FFT tile width");
   // Contiguous passes (small tiles, twiddles as large as the data) share one
-  // staged twiddle table between up to 4 columns of the same tile position.
+  // staged twiddle table between 4 columns of the same tile position.
   const uint32_t cpb = (p.C == 0 && E <= 4096 && srcs.size() >= 4) ? 4u : 1u;
-  size_t tile_words = E + E / 16 + 1;
-  size_t smem = (cpb * tile_words + ((size_t)1 << p.T)) * sizeof(uint32_t);
-  static bool attr_set[2] = {false, false};
-  if (!attr_set[INV]) {
-    STWO_CUDA_TRY(cudaFuncSetAttribute(fft_pass_kernel<INV>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-    attr_set[INV] = true;
-  }
   STWO_ARG_CHECK(tiles <= 0x7fffffffull, "too many tiles");
   for (size_t c0 = 0; c0 < srcs.size(); c0 += kFftMaxCols) {
     FftCols cols;
@@ -360,9 +401,14 @@ static int launch_pass(const FftPass& p, const std::vector<const uint32_t*>& src
     q.cpb = cpb;
     q.n_cols = (uint32_t)nc;
     dim3 grid((unsigned)tiles, (unsigned)((nc + cpb - 1) / cpb));
-    const unsigned threads = (cpb * E) <= 2048 ? 128 : 256;
-    fft_pass_kernel<INV><<<grid, threads, smem, s>>>(q, cols);
-    STWO_CHECK_LAUNCH();
+    int rc;
+    if (p.C == 3)
+      rc = dispatch_tile<INV, 3, 1>(q, cols, grid, s, err, err_len);
+    else if (cpb == 4)
+      rc = dispatch_tile<INV, 0, 4>(q, cols, grid, s, err, err_len);
+    else
+      rc = dispatch_tile<INV, 0, 1>(q, cols, grid, s, err, err_len);
+    if (rc) return rc;
   }
   return STWO_B200_OK;
 }
