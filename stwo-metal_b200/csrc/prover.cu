@@ -272,13 +272,12 @@ __device__ void dev_finalize(uint32_t h[8], bool m31) {
     for (int k = 0; k < 8; k++) h[k] = m31_reduce_u32(h[k]);
 }
 
-// mix_root (digest <- H(digest || root)), then draw_secure_felt into *alpha.
-__global__ void channel_mix_root_draw_kernel(DevChannel* ch, const uint8_t* root, qm31* alpha) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+// mix_root (digest <- H(digest || root)), then draw_secure_felt into *alpha;
+// one thread.
+__device__ void dev_mix_root_draw(DevChannel* ch, const uint32_t* root, qm31* alpha) {
   uint32_t m[16];
   for (int k = 0; k < 8; k++) m[k] = ch->digest[k];
-  const uint32_t* r = reinterpret_cast<const uint32_t*>(root);
-  for (int k = 0; k < 8; k++) m[8 + k] = r[k];
+  for (int k = 0; k < 8; k++) m[8 + k] = root[k];
   uint32_t h[8];
   blake2s_init(h);
   blake2s_compress(h, m, 64, true);
@@ -306,6 +305,11 @@ __global__ void channel_mix_root_draw_kernel(DevChannel* ch, const uint8_t* root
   ch->error = 1;
   ch->n_draws = n_draws;
   *alpha = qm31_zero();
+}
+
+__global__ void channel_mix_root_draw_kernel(DevChannel* ch, const uint8_t* root, qm31* alpha) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  dev_mix_root_draw(ch, reinterpret_cast<const uint32_t*>(root), alpha);
 }
 
 // fold_line with alpha read from device memory (prover/backend/cpu/fri.rs:67-92).
@@ -378,6 +382,145 @@ __global__ void fold_circle_first_dev_kernel(const uint32_t* __restrict__ src, u
     dst[n_out + i] = v.b;
     dst[2 * n_out + i] = v.c;
     dst[3 * n_out + i] = v.d;
+  }
+}
+
+// ---- fused FRI tail ----
+// The small FRI layers (log size <= kFriTailLog) are latency-bound: a few
+// thousand compressions each, spread over leaf, node, channel and fold
+// launches.  One CTA runs all of them back to back: per layer it hashes the
+// lifted leaves (4 equal columns, prover/backend/cpu/merkle_lifted.rs:44-78),
+// every node level to the root with the levels in shared memory (and in the
+// tree buffer, for decommitment), mixes the root and draws alpha on the device
+// channel, and folds into the next layer (prover/backend/cpu/fri.rs:67-92).
+// Data written inside the kernel is read back with plain loads, never through
+// the read-only path.
+constexpr uint32_t kFriTailLog = 11;
+constexpr int kFriTailMaxLayers = 32;
+constexpr int kFriTailThreads = 1024;
+constexpr size_t kFriTailSmem = (size_t)3 << (kFriTailLog + 4);  // 2^L + 2^(L-1) hashes of 32 bytes
+struct FriTail {
+  uint32_t* coords[kFriTailMaxLayers];  // 4 x 2^log_size
+  uint8_t* tree[kFriTailMaxLayers];     // MerkleTree base: layer k at ((1 << k) - 1) * 32
+  uint32_t log_size[kFriTailMaxLayers];
+  uint32_t fold_step[kFriTailMaxLayers];
+  uint32_t* last;  // destination of the last fold
+  uint32_t n_layers;
+  uint32_t m31;
+};
+
+__device__ __forceinline__ void put_hash(uint8_t* layer, uint4* smem, uint32_t i, const uint32_t h[8]) {
+  const uint4 a = make_uint4(h[0], h[1], h[2], h[3]);
+  const uint4 b = make_uint4(h[4], h[5], h[6], h[7]);
+  uint4* g = reinterpret_cast<uint4*>(layer + (size_t)i * 32);
+  g[0] = a;
+  g[1] = b;
+  smem[2 * i] = a;
+  smem[2 * i + 1] = b;
+}
+
+__global__ void __launch_bounds__(kFriTailThreads, 1) fri_tail_kernel(FriTail t, DevChannel* ch, qm31* alphas,
+                                                                      const uint32_t* __restrict__ itw,
+                                                                      uint64_t tw_len) {
+  extern __shared__ uint4 tail_smem[];  // ping: 2^kFriTailLog hashes, pong: 2^(kFriTailLog-1)
+  __shared__ qm31 s_alpha;
+  uint4* ping = tail_smem;
+  uint4* pong = tail_smem + (2u << kFriTailLog);
+  const uint32_t tid = threadIdx.x;
+  const bool m31 = t.m31 != 0;
+  for (uint32_t li = 0; li < t.n_layers; li++) {
+    const uint32_t L = t.log_size[li];
+    const uint32_t n = 1u << L;
+    const uint32_t* c = t.coords[li];
+    uint8_t* base = t.tree[li];
+    for (uint32_t i = tid; i < n; i += kFriTailThreads) {
+      uint32_t m[16];
+      m[0] = c[i];
+      m[1] = c[n + i];
+      m[2] = c[2 * n + i];
+      m[3] = c[3 * n + i];
+#pragma unroll
+      for (int k = 4; k < 16; k++) m[k] = 0;
+      uint32_t h[8];
+      blake2s_init(h);
+      blake2s_compress(h, m, 16, true);
+      dev_finalize(h, m31);
+      put_hash(base + ((size_t)n - 1) * 32, ping, i, h);
+    }
+    __syncthreads();
+    uint4* src = ping;
+    uint4* dst = pong;
+    for (int d = (int)L - 1; d >= 0; d--) {
+      const uint32_t np = 1u << d;
+      for (uint32_t p = tid; p < np; p += kFriTailThreads) {
+        uint32_t m[16];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+          const uint4 w = src[4 * p + q];
+          m[4 * q] = w.x;
+          m[4 * q + 1] = w.y;
+          m[4 * q + 2] = w.z;
+          m[4 * q + 3] = w.w;
+        }
+        uint32_t h[8];
+        blake2s_init(h);
+        blake2s_compress(h, m, 64, true);
+        dev_finalize(h, m31);
+        put_hash(base + ((size_t)np - 1) * 32, dst, p, h);
+      }
+      __syncthreads();
+      uint4* tmp = src;
+      src = dst;
+      dst = tmp;
+    }
+    if (tid == 0) {
+      const uint4 a = src[0], b = src[1];
+      const uint32_t root[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+      dev_mix_root_draw(ch, root, alphas + li);
+      s_alpha = alphas[li];
+    }
+    __syncthreads();
+    const qm31 a0 = s_alpha;
+    const uint32_t fs = t.fold_step[li];
+    const uint32_t n_out = n >> fs;
+    uint32_t* out = li + 1 < t.n_layers ? t.coords[li + 1] : t.last;
+    if (fs == 1) {
+      const uint32_t* lt = itw + (tw_len - (1ull << L));
+      for (uint32_t o = tid; o < n_out; o += kFriTailThreads) {
+        const qm31 fx = {c[2 * o], c[n + 2 * o], c[2 * n + 2 * o], c[3 * n + 2 * o]};
+        const qm31 fnx = {c[2 * o + 1], c[n + 2 * o + 1], c[2 * n + 2 * o + 1], c[3 * n + 2 * o + 1]};
+        const qm31 v = qm31_add(qm31_add(fx, fnx), qm31_mul(a0, qm31_mul_m31(qm31_sub(fx, fnx), __ldg(lt + o))));
+        out[o] = v.a;
+        out[n_out + o] = v.b;
+        out[2 * n_out + o] = v.c;
+        out[3 * n_out + o] = v.d;
+      }
+    }
+    for (uint32_t o = tid; fs > 1 && o < n_out; o += kFriTailThreads) {
+      qm31 v[1 << 6];
+      const uint32_t w = 1u << fs;
+      for (uint32_t j = 0; j < w; j++) {
+        const uint32_t i = o * w + j;
+        v[j] = {c[i], c[n + i], c[2 * n + i], c[3 * n + i]};
+      }
+      qm31 a = a0;
+      for (uint32_t st = 0; st < fs; st++) {
+        const uint32_t* lt = itw + (tw_len - (1ull << (L - st)));
+        const uint32_t pairs = w >> (st + 1);
+        for (uint32_t j = 0; j < pairs; j++) {
+          const qm31 fx = v[2 * j], fnx = v[2 * j + 1];
+          const qm31 f0 = qm31_add(fx, fnx);
+          const qm31 f1 = qm31_mul_m31(qm31_sub(fx, fnx), __ldg(lt + o * pairs + j));
+          v[j] = qm31_add(f0, qm31_mul(a, f1));
+        }
+        a = qm31_mul(a, a);
+      }
+      out[o] = v[0].a;
+      out[n_out + o] = v[0].b;
+      out[2 * n_out + o] = v[0].c;
+      out[3 * n_out + o] = v[0].d;
+    }
+    __syncthreads();
   }
 }
 
@@ -541,6 +684,7 @@ class WideFibProver {
   int init(const stwo_b200_wide_fib_config& c, cudaStream_t stream, char* err, size_t err_len) {
     cfg = c;
     s = stream;
+    STWO_CUDA_TRY(cudaFuncSetAttribute(fri_tail_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFriTailSmem));
     log_n = c.log_n_rows;
     N = c.n_cols;
     blowup = c.log_blowup;
@@ -890,7 +1034,9 @@ int WideFibProver::prove(const uint32_t* d_a, const uint32_t* d_b, ProofOut& out
       return set_err(err, err_len, STWO_B200_EARG, "lifting domain too small");
     }
   }
-  for (size_t li = 0; li < fri.size(); li++) {
+  size_t tail0 = fri.size();  // first layer of the fused tail
+  while (tail0 > 0 && fri[tail0 - 1].log_size <= kFriTailLog) tail0--;
+  for (size_t li = 0; li < tail0; li++) {
     FriLayerBuf& l = fri[li];
     std::vector<uint32_t*> c4(4);
     for (int k = 0; k < 4; k++) c4[k] = l.coords + ((uint64_t)k << l.log_size);
@@ -903,6 +1049,23 @@ int WideFibProver::prove(const uint32_t* d_a, const uint32_t* d_b, ProofOut& out
     uint32_t nlog = l.log_size - l.fold_step;
     fold_line_dev_kernel<<<grid1d(1ull << nlog, 256), 256, 0, s>>>(l.coords, l.log_size, l.fold_step,
                                                                      d_alphas + li + 1, d_itw, 1ull << tree_log, nxt);
+    STWO_CHECK_LAUNCH();
+  }
+  if (tail0 < fri.size()) {
+    phase(kFriMerkle);
+    FriTail t;
+    t.n_layers = (uint32_t)(fri.size() - tail0);
+    STWO_ARG_CHECK(t.n_layers <= (uint32_t)kFriTailMaxLayers, "too many FRI layers");
+    for (uint32_t k = 0; k < t.n_layers; k++) {
+      const FriLayerBuf& l = fri[tail0 + k];
+      t.coords[k] = l.coords;
+      t.tree[k] = l.tree.base;
+      t.log_size[k] = l.log_size;
+      t.fold_step[k] = l.fold_step;
+    }
+    t.last = d_last;
+    t.m31 = m31 ? 1u : 0u;
+    fri_tail_kernel<<<1, kFriTailThreads, kFriTailSmem, s>>>(t, d_chan, d_alphas + tail0 + 1, d_itw, 1ull << tree_log);
     STWO_CHECK_LAUNCH();
   }
   {
