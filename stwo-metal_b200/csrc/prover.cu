@@ -313,9 +313,32 @@ __global__ void channel_mix_root_draw_kernel(DevChannel* ch, const uint8_t* root
 }
 
 // fold_line with alpha read from device memory (prover/backend/cpu/fri.rs:67-92).
+// Lifted leaf of one FRI layer element: Blake2s of its 4 coordinates (16
+// bytes), the leaf of a tree over 4 equal-length columns
+// (prover/backend/cpu/merkle_lifted.rs:44-78).
+__device__ __forceinline__ void fri_leaf_store(uint8_t* leaves, uint64_t i, const qm31& v, bool m31) {
+  uint32_t m[16];
+  m[0] = v.a;
+  m[1] = v.b;
+  m[2] = v.c;
+  m[3] = v.d;
+#pragma unroll
+  for (int k = 4; k < 16; k++) m[k] = 0;
+  uint32_t h[8];
+  blake2s_init(h);
+  blake2s_compress(h, m, 16, true);
+  dev_finalize(h, m31);
+  uint4* g = reinterpret_cast<uint4*>(leaves + i * 32);
+  g[0] = make_uint4(h[0], h[1], h[2], h[3]);
+  g[1] = make_uint4(h[4], h[5], h[6], h[7]);
+}
+
+// When `leaves` is not null the fold also writes the leaf hashes of the next
+// layer's tree (its Merkle leaf layer), saving a launch and a re-read.
 __global__ void fold_line_dev_kernel(const uint32_t* __restrict__ in, uint32_t log_m, uint32_t fold_step,
                                      const qm31* __restrict__ d_alpha, const uint32_t* __restrict__ itw,
-                                     uint64_t tw_len, uint32_t* __restrict__ out) {
+                                     uint64_t tw_len, uint32_t* __restrict__ out, uint8_t* __restrict__ leaves,
+                                     int m31) {
   const uint64_t n_in = 1ull << log_m;
   const uint64_t n_out = n_in >> fold_step;
   qm31 a0 = *d_alpha;
@@ -331,6 +354,7 @@ __global__ void fold_line_dev_kernel(const uint32_t* __restrict__ in, uint32_t l
       out[n_out + o] = v.b;
       out[2 * n_out + o] = v.c;
       out[3 * n_out + o] = v.d;
+      if (leaves) fri_leaf_store(leaves, o, v, m31 != 0);
     }
     return;
   }
@@ -357,6 +381,7 @@ __global__ void fold_line_dev_kernel(const uint32_t* __restrict__ in, uint32_t l
     out[n_out + o] = v[0].b;
     out[2 * n_out + o] = v[0].c;
     out[3 * n_out + o] = v[0].d;
+    if (leaves) fri_leaf_store(leaves, o, v[0], m31 != 0);
   }
 }
 
@@ -364,7 +389,8 @@ __global__ void fold_line_dev_kernel(const uint32_t* __restrict__ in, uint32_t l
 // with a zero line evaluation), alpha from device memory; log_n > 4.
 __global__ void fold_circle_first_dev_kernel(const uint32_t* __restrict__ src, uint32_t log_n,
                                              const qm31* __restrict__ d_alpha, const uint32_t* __restrict__ itw,
-                                             uint64_t tw_len, uint32_t* __restrict__ dst) {
+                                             uint64_t tw_len, uint32_t* __restrict__ dst,
+                                             uint8_t* __restrict__ leaves, int m31) {
   const uint64_t n_in = 1ull << log_n, n_out = n_in >> 1;
   const uint32_t* lt0 = itw + (tw_len - (1ull << (log_n - 1)));
   qm31 alpha = *d_alpha;
@@ -382,12 +408,13 @@ __global__ void fold_circle_first_dev_kernel(const uint32_t* __restrict__ src, u
     dst[n_out + i] = v.b;
     dst[2 * n_out + i] = v.c;
     dst[3 * n_out + i] = v.d;
+    if (leaves) fri_leaf_store(leaves, i, v, m31 != 0);
   }
 }
 
 // ---- fused FRI tail ----
-// The small FRI layers (log size <= kFriTailLog) are latency-bound: a few
-// thousand compressions each, spread over leaf, node, channel and fold
+// The small FRI layers (log size <= kFriTailLog) are latency-bound: at most
+// a few hundred compressions each, spread over leaf, node, channel and fold
 // launches.  One CTA runs all of them back to back: per layer it hashes the
 // lifted leaves (4 equal columns, prover/backend/cpu/merkle_lifted.rs:44-78),
 // every node level to the root with the levels in shared memory (and in the
@@ -395,9 +422,9 @@ __global__ void fold_circle_first_dev_kernel(const uint32_t* __restrict__ src, u
 // channel, and folds into the next layer (prover/backend/cpu/fri.rs:67-92).
 // Data written inside the kernel is read back with plain loads, never through
 // the read-only path.
-constexpr uint32_t kFriTailLog = 11;
+constexpr uint32_t kFriTailLog = 8;
 constexpr int kFriTailMaxLayers = 32;
-constexpr int kFriTailThreads = 1024;
+constexpr int kFriTailThreads = 256;  // one thread per leaf of the largest tail layer
 constexpr size_t kFriTailSmem = (size_t)3 << (kFriTailLog + 4);  // 2^L + 2^(L-1) hashes of 32 bytes
 struct FriTail {
   uint32_t* coords[kFriTailMaxLayers];  // 4 x 2^log_size
@@ -417,6 +444,83 @@ __device__ __forceinline__ void put_hash(uint8_t* layer, uint4* smem, uint32_t i
   g[1] = b;
   smem[2 * i] = a;
   smem[2 * i + 1] = b;
+}
+
+// Node levels lg-1 .. 0 of a tree whose level lg (2^lg hashes) is in shared
+// memory at `src`; every level also goes to the tree buffer.  Returns the
+// buffer that holds the root.  Called by all threads of the block.
+__device__ const uint4* tree_levels_smem(uint8_t* base, uint32_t lg, uint4* src, uint4* dst, bool m31) {
+  for (int d = (int)lg - 1; d >= 0; d--) {
+    const uint32_t np = 1u << d;
+    for (uint32_t p = threadIdx.x; p < np; p += blockDim.x) {
+      uint32_t m[16];
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        const uint4 w = src[4 * p + q];
+        m[4 * q] = w.x;
+        m[4 * q + 1] = w.y;
+        m[4 * q + 2] = w.z;
+        m[4 * q + 3] = w.w;
+      }
+      uint32_t h[8];
+      blake2s_init(h);
+      blake2s_compress(h, m, 64, true);
+      dev_finalize(h, m31);
+      put_hash(base + ((size_t)np - 1) * 32, dst, p, h);
+    }
+    __syncthreads();
+    uint4* tmp = src;
+    src = dst;
+    dst = tmp;
+  }
+  return src;
+}
+
+// Top of one FRI layer tree and its Fiat-Shamir step: hashes levels
+// top_log-1 .. 0 from tree level top_log (2^top_log hashes in global memory,
+// top_log <= kFriTailLog), then mixes the root and draws alpha.
+__global__ void __launch_bounds__(kFriTailThreads, 1) tree_top_channel_kernel(uint8_t* base, uint32_t top_log,
+                                                                              DevChannel* ch, qm31* alpha,
+                                                                              int m31) {
+  extern __shared__ uint4 tail_smem[];
+  uint4* ping = tail_smem;
+  uint4* pong = tail_smem + (2u << kFriTailLog);
+  const bool m31b = m31 != 0;
+  const uint4* src = ping;
+  if (top_log == 0) {
+    if (threadIdx.x == 0) {
+      const uint4* r = reinterpret_cast<const uint4*>(base);
+      ping[0] = r[0];
+      ping[1] = r[1];
+    }
+    __syncthreads();
+  } else {
+    const uint32_t np = 1u << (top_log - 1);
+    const uint4* in = reinterpret_cast<const uint4*>(base + (((size_t)1 << top_log) - 1) * 32);
+    for (uint32_t p = threadIdx.x; p < np; p += blockDim.x) {
+      uint32_t m[16];
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        const uint4 w = __ldg(in + 4 * p + q);
+        m[4 * q] = w.x;
+        m[4 * q + 1] = w.y;
+        m[4 * q + 2] = w.z;
+        m[4 * q + 3] = w.w;
+      }
+      uint32_t h[8];
+      blake2s_init(h);
+      blake2s_compress(h, m, 64, true);
+      dev_finalize(h, m31b);
+      put_hash(base + ((size_t)np - 1) * 32, ping, p, h);
+    }
+    __syncthreads();
+    src = tree_levels_smem(base, top_log - 1, ping, pong, m31b);
+  }
+  if (threadIdx.x == 0) {
+    const uint4 a = src[0], b = src[1];
+    const uint32_t root[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+    dev_mix_root_draw(ch, root, alpha);
+  }
 }
 
 __global__ void __launch_bounds__(kFriTailThreads, 1) fri_tail_kernel(FriTail t, DevChannel* ch, qm31* alphas,
@@ -448,31 +552,7 @@ __global__ void __launch_bounds__(kFriTailThreads, 1) fri_tail_kernel(FriTail t,
       put_hash(base + ((size_t)n - 1) * 32, ping, i, h);
     }
     __syncthreads();
-    uint4* src = ping;
-    uint4* dst = pong;
-    for (int d = (int)L - 1; d >= 0; d--) {
-      const uint32_t np = 1u << d;
-      for (uint32_t p = tid; p < np; p += kFriTailThreads) {
-        uint32_t m[16];
-#pragma unroll
-        for (int q = 0; q < 4; q++) {
-          const uint4 w = src[4 * p + q];
-          m[4 * q] = w.x;
-          m[4 * q + 1] = w.y;
-          m[4 * q + 2] = w.z;
-          m[4 * q + 3] = w.w;
-        }
-        uint32_t h[8];
-        blake2s_init(h);
-        blake2s_compress(h, m, 64, true);
-        dev_finalize(h, m31);
-        put_hash(base + ((size_t)np - 1) * 32, dst, p, h);
-      }
-      __syncthreads();
-      uint4* tmp = src;
-      src = dst;
-      dst = tmp;
-    }
+    const uint4* src = tree_levels_smem(base, L, ping, pong, m31);
     if (tid == 0) {
       const uint4 a = src[0], b = src[1];
       const uint32_t root[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
@@ -620,8 +700,17 @@ class WideFibProver {
   cudaEvent_t open_event = nullptr;
   void phase(int ph) {
     if (!timing) return;
+    if (capture_slot >= 0) {  // inside a graph capture: an event-record node
+      cudaEvent_t e = graph_events[graph_ev_next++];
+      cudaEventRecordWithFlags(e, s, cudaEventRecordExternal);
+      graph_phase_seq[capture_slot].push_back({ph, e});
+      return;
+    }
     cudaEvent_t e = next_event();
     cudaEventRecord(e, s);
+    apply_phase(ph, e);
+  }
+  void apply_phase(int ph, cudaEvent_t e) {
     if (open_phase >= 0) marks.push_back({open_phase, {open_event, e}});
     open_phase = ph;
     open_event = e;
@@ -668,11 +757,31 @@ class WideFibProver {
   size_t h_pinned_bytes = 0;
   std::vector<void*> allocs;
 
+  // The prover enqueues on its own non-blocking stream `s` (so the FRI commit
+  // can be a captured CUDA graph), ordered after and before the caller's
+  // stream `user_s` with events.
+  cudaStream_t user_s = nullptr;
+  cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+  // FRI commit graphs, [timing off, timing on], captured on first use.
+  cudaGraphExec_t fri_exec[2] = {nullptr, nullptr};
+  uint64_t fri_graph_launches[2] = {0, 0};
+  std::vector<std::pair<int, cudaEvent_t>> graph_phase_seq[2];
+  std::vector<cudaEvent_t> graph_events;  // created before a capture, owned
+  size_t graph_ev_next = 0;
+  int capture_slot = -1;
+
   ~WideFibProver() {
+    if (s) cudaStreamSynchronize(s);
+    for (int k = 0; k < 2; k++)
+      if (fri_exec[k]) cudaGraphExecDestroy(fri_exec[k]);
+    for (cudaEvent_t e : graph_events) cudaEventDestroy(e);
+    if (ev_in) cudaEventDestroy(ev_in);
+    if (ev_out) cudaEventDestroy(ev_out);
     for (cudaEvent_t e : ev_pool) cudaEventDestroy(e);
     for (void* p : allocs) cudaFree(p);
     if (h_pinned) cudaFreeHost(h_pinned);
     if (h_chan) cudaFreeHost(h_chan);
+    if (s) cudaStreamDestroy(s);
   }
 
   int alloc(void** p, size_t bytes, char* err, size_t err_len) {
@@ -683,8 +792,13 @@ class WideFibProver {
 
   int init(const stwo_b200_wide_fib_config& c, cudaStream_t stream, char* err, size_t err_len) {
     cfg = c;
-    s = stream;
+    user_s = stream;
+    STWO_CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    STWO_CUDA_TRY(cudaEventCreateWithFlags(&ev_in, cudaEventDisableTiming));
+    STWO_CUDA_TRY(cudaEventCreateWithFlags(&ev_out, cudaEventDisableTiming));
     STWO_CUDA_TRY(cudaFuncSetAttribute(fri_tail_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFriTailSmem));
+    STWO_CUDA_TRY(
+        cudaFuncSetAttribute(tree_top_channel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFriTailSmem));
     log_n = c.log_n_rows;
     N = c.n_cols;
     blowup = c.log_blowup;
@@ -761,6 +875,125 @@ class WideFibProver {
     return 0;
   }
 
+  // One FRI layer tree from its leaf level L: grid-wide node launches down to
+  // 2^kFriTailLog hashes, then one CTA for the top levels (latency-bound, a
+  // few hundred compressions), the root mix and the alpha draw on the device
+  // channel.
+  int fri_tree_top(const MerkleTree& t, uint32_t L, qm31* alpha, char* err, size_t err_len) {
+    const uint32_t top = std::min<uint32_t>(L, kFriTailLog);
+    if (L > top) {
+      std::vector<uint8_t*> outs(L);
+      for (uint32_t k = 0; k < L; k++) outs[k] = t.layer(k);
+      int rc = build_node_layers_impl(t.layer(L), L, top, cfg.m31_channel, outs.data(), s, err, err_len);
+      if (rc) return rc;
+    }
+    tree_top_channel_kernel<<<1, kFriTailThreads, kFriTailSmem, s>>>(t.base, top, d_chan, alpha, cfg.m31_channel);
+    STWO_CHECK_LAUNCH();
+    return 0;
+  }
+
+  // FRI commit (prover/fri.rs:133-291) on the device channel: the circle
+  // layer tree, the first fold, every line layer's tree top, alpha draw and
+  // fold, then the fused tail.  Launch parameters depend only on the
+  // configuration and the buffers allocated at init, so the sequence is
+  // captured once as a CUDA graph and replayed.
+  int enqueue_fri(char* err, size_t err_len) {
+    const bool m31 = cfg.m31_channel != 0;
+    int rc;
+    {
+      std::vector<uint32_t*> q4(4);
+      for (int k = 0; k < 4; k++) q4[k] = d_quot + ((uint64_t)k << lift);
+      phase(kFriMerkle);
+      if ((rc = build_leaves_impl(q4.data(), std::vector<uint32_t>(4, lift).data(), 4, lift, m31, tq.layer(lift), s,
+                                  err, err_len)))
+        return rc;
+      if ((rc = fri_tree_top(tq, lift, d_alphas, err, err_len))) return rc;
+    }
+    size_t tail0 = fri.size();  // first layer of the fused tail
+    while (tail0 > 0 && fri[tail0 - 1].log_size <= kFriTailLog) tail0--;
+    {
+      phase(kFriFold);
+      uint32_t* dst = fri.empty() ? d_last : fri[0].coords;
+      uint8_t* leaves = tail0 > 0 ? fri[0].tree.layer(fri[0].log_size) : nullptr;
+      if (lift <= 4) return set_err(err, err_len, STWO_B200_EARG, "lifting domain too small");
+      fold_circle_first_dev_kernel<<<grid1d(1ull << (lift - 1), 256), 256, 0, s>>>(
+          d_quot, lift, d_alphas, d_itw, 1ull << tree_log, dst, leaves, m31 ? 1 : 0);
+      STWO_CHECK_LAUNCH();
+    }
+    for (size_t li = 0; li < tail0; li++) {
+      FriLayerBuf& l = fri[li];
+      phase(kFriMerkle);  // leaves were hashed by the fold that produced this layer
+      if ((rc = fri_tree_top(l.tree, l.log_size, d_alphas + li + 1, err, err_len))) return rc;
+      phase(kFriFold);
+      uint32_t* nxt = (li + 1 < fri.size()) ? fri[li + 1].coords : d_last;
+      uint8_t* leaves = li + 1 < tail0 ? fri[li + 1].tree.layer(fri[li + 1].log_size) : nullptr;
+      uint32_t nlog = l.log_size - l.fold_step;
+      fold_line_dev_kernel<<<grid1d(1ull << nlog, 256), 256, 0, s>>>(l.coords, l.log_size, l.fold_step,
+                                                                       d_alphas + li + 1, d_itw, 1ull << tree_log, nxt,
+                                                                       leaves, m31 ? 1 : 0);
+      STWO_CHECK_LAUNCH();
+    }
+    if (tail0 < fri.size()) {
+      phase(kFriMerkle);
+      FriTail t;
+      t.n_layers = (uint32_t)(fri.size() - tail0);
+      STWO_ARG_CHECK(t.n_layers <= (uint32_t)kFriTailMaxLayers, "too many FRI layers");
+      for (uint32_t k = 0; k < t.n_layers; k++) {
+        const FriLayerBuf& l = fri[tail0 + k];
+        t.coords[k] = l.coords;
+        t.tree[k] = l.tree.base;
+        t.log_size[k] = l.log_size;
+        t.fold_step[k] = l.fold_step;
+      }
+      t.last = d_last;
+      t.m31 = m31 ? 1u : 0u;
+      fri_tail_kernel<<<1, kFriTailThreads, kFriTailSmem, s>>>(t, d_chan, d_alphas + tail0 + 1, d_itw, 1ull << tree_log);
+      STWO_CHECK_LAUNCH();
+    }
+    return 0;
+  }
+
+  int run_fri(char* err, size_t err_len) {
+    const int k = timing ? 1 : 0;
+    if (!fri_exec[k]) {
+      const uint64_t before = g_kernel_launches.load();
+      graph_phase_seq[k].clear();
+      if (timing) {
+        const size_t need = graph_ev_next + 2 * fri.size() + 8;  // phase() calls in enqueue_fri
+        while (graph_events.size() < need) {
+          cudaEvent_t e;
+          STWO_CUDA_TRY(cudaEventCreate(&e));
+          graph_events.push_back(e);
+        }
+      }
+      STWO_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+      capture_slot = k;
+      int rc = enqueue_fri(err, err_len);
+      capture_slot = -1;
+      cudaGraph_t g = nullptr;
+      cudaError_t ce = cudaStreamEndCapture(s, &g);
+      const uint64_t n = g_kernel_launches.load() - before;
+      g_kernel_launches.fetch_sub(n);  // nothing ran during capture
+      if (rc) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+      }
+      if (ce != cudaSuccess) return set_err(err, err_len, STWO_B200_ECUDA, "FRI graph capture: %s", cudaGetErrorString(ce));
+      ce = cudaGraphInstantiate(&fri_exec[k], g, 0);
+      cudaGraphDestroy(g);
+      if (ce != cudaSuccess) {
+        fri_exec[k] = nullptr;
+        return set_err(err, err_len, STWO_B200_ECUDA, "FRI graph instantiate: %s", cudaGetErrorString(ce));
+      }
+      fri_graph_launches[k] = n;
+    }
+    STWO_CUDA_TRY(cudaGraphLaunch(fri_exec[k], s));
+    g_kernel_launches.fetch_add(fri_graph_launches[k]);
+    if (timing)
+      for (auto& pe : graph_phase_seq[k]) apply_phase(pe.first, pe.second);
+    return 0;
+  }
+
   int download_root(const MerkleTree& t, Hash32& root, char* err, size_t err_len) {
     STWO_CUDA_TRY(cudaMemcpyAsync(h_pinned, t.layer(0), 32, cudaMemcpyDeviceToHost, s));
     STWO_CUDA_TRY(cudaStreamSynchronize(s));
@@ -776,10 +1009,18 @@ class WideFibProver {
                                          t.L, cfg.m31_channel, layers.data(), s, err, err_len);
   }
 
-  int prove(const uint32_t* d_a, const uint32_t* d_b, ProofOut& out, char* err, size_t err_len);
+  int prove(const uint32_t* d_a, const uint32_t* d_b, ProofOut& out, char* err, size_t err_len) {
+    STWO_CUDA_TRY(cudaEventRecord(ev_in, user_s));
+    STWO_CUDA_TRY(cudaStreamWaitEvent(s, ev_in, 0));
+    const int rc = prove_body(d_a, d_b, out, err, err_len);
+    cudaEventRecord(ev_out, s);
+    cudaStreamWaitEvent(user_s, ev_out, 0);
+    return rc;
+  }
+  int prove_body(const uint32_t* d_a, const uint32_t* d_b, ProofOut& out, char* err, size_t err_len);
 };
 
-int WideFibProver::prove(const uint32_t* d_a, const uint32_t* d_b, ProofOut& out, char* err, size_t err_len) {
+int WideFibProver::prove_body(const uint32_t* d_a, const uint32_t* d_b, ProofOut& out, char* err, size_t err_len) {
   const bool m31 = cfg.m31_channel != 0;
   HostChannel ch(m31);
   int rc;
@@ -1018,56 +1259,8 @@ int WideFibProver::prove(const uint32_t* d_a, const uint32_t* d_b, ProofOut& out
     hc->n_draws = ch.n_draws();
     hc->m31 = m31 ? 1 : 0;
     STWO_CUDA_TRY(cudaMemcpyAsync(d_chan, hc, sizeof(DevChannel), cudaMemcpyHostToDevice, s));
-    std::vector<uint32_t*> q4(4);
-    for (int k = 0; k < 4; k++) q4[k] = d_quot + ((uint64_t)k << lift);
-    phase(kFriMerkle);
-    if ((rc = commit_columns(q4.data(), std::vector<uint32_t>(4, lift), tq, err, err_len))) return rc;
-    channel_mix_root_draw_kernel<<<1, 32, 0, s>>>(d_chan, tq.layer(0), d_alphas);
-    STWO_CHECK_LAUNCH();
-    phase(kFriFold);
-    uint32_t* dst = fri.empty() ? d_last : fri[0].coords;
-    if (lift > 4) {
-      fold_circle_first_dev_kernel<<<grid1d(1ull << (lift - 1), 256), 256, 0, s>>>(d_quot, lift, d_alphas, d_itw,
-                                                                                     1ull << tree_log, dst);
-      STWO_CHECK_LAUNCH();
-    } else {
-      return set_err(err, err_len, STWO_B200_EARG, "lifting domain too small");
-    }
   }
-  size_t tail0 = fri.size();  // first layer of the fused tail
-  while (tail0 > 0 && fri[tail0 - 1].log_size <= kFriTailLog) tail0--;
-  for (size_t li = 0; li < tail0; li++) {
-    FriLayerBuf& l = fri[li];
-    std::vector<uint32_t*> c4(4);
-    for (int k = 0; k < 4; k++) c4[k] = l.coords + ((uint64_t)k << l.log_size);
-    phase(kFriMerkle);
-    if ((rc = commit_columns(c4.data(), std::vector<uint32_t>(4, l.log_size), l.tree, err, err_len))) return rc;
-    channel_mix_root_draw_kernel<<<1, 32, 0, s>>>(d_chan, l.tree.layer(0), d_alphas + li + 1);
-    STWO_CHECK_LAUNCH();
-    phase(kFriFold);
-    uint32_t* nxt = (li + 1 < fri.size()) ? fri[li + 1].coords : d_last;
-    uint32_t nlog = l.log_size - l.fold_step;
-    fold_line_dev_kernel<<<grid1d(1ull << nlog, 256), 256, 0, s>>>(l.coords, l.log_size, l.fold_step,
-                                                                     d_alphas + li + 1, d_itw, 1ull << tree_log, nxt);
-    STWO_CHECK_LAUNCH();
-  }
-  if (tail0 < fri.size()) {
-    phase(kFriMerkle);
-    FriTail t;
-    t.n_layers = (uint32_t)(fri.size() - tail0);
-    STWO_ARG_CHECK(t.n_layers <= (uint32_t)kFriTailMaxLayers, "too many FRI layers");
-    for (uint32_t k = 0; k < t.n_layers; k++) {
-      const FriLayerBuf& l = fri[tail0 + k];
-      t.coords[k] = l.coords;
-      t.tree[k] = l.tree.base;
-      t.log_size[k] = l.log_size;
-      t.fold_step[k] = l.fold_step;
-    }
-    t.last = d_last;
-    t.m31 = m31 ? 1u : 0u;
-    fri_tail_kernel<<<1, kFriTailThreads, kFriTailSmem, s>>>(t, d_chan, d_alphas + tail0 + 1, d_itw, 1ull << tree_log);
-    STWO_CHECK_LAUNCH();
-  }
+  if ((rc = run_fri(err, err_len))) return rc;
   {
     // one download: roots, device alphas, channel state; then the host replay
     uint8_t* hp = reinterpret_cast<uint8_t*>(h_pinned);
