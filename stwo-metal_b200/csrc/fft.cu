@@ -344,6 +344,261 @@ static void index_point(uint64_t idx, uint32_t& x, uint32_t& y) {
   }
 }
 
+// ---- warp-per-column 1024-point passes (T = 10) ----
+// A warp owns one column of a 1024-row tile: 32 values per lane.  Layers
+// 0..4 (row bits 0..4) run with the tile held lane-major (v[j] = row
+// lane*32 + j); layers 5..9 with it held row-major (v[j] = row j*32 + lane).
+// The two layouts exchange through a warp-private 32 x 33 shared-memory
+// region (conflict-free both ways), so a warp needs no block barrier once the
+// block's twiddles are staged.  Butterflies, twiddle indices (row >> (lam+1)
+// of tree layer layer0 + lam) and layer order are those of fft_stage.
+constexpr int kWarpCols = 8;                  // warps (columns) per block
+constexpr uint32_t kColWords = 1024 + 32 + 1;  // padded column region
+
+// Layers 0..4 on v[j] = row lane*32 + j.
+template <bool INV>
+__device__ __forceinline__ void warp_phase_lo(uint32_t (&v)[32], const uint32_t* __restrict__ tws, uint32_t lane) {
+#pragma unroll
+  for (int kk = 0; kk < 5; kk++) {
+    const int lam = INV ? kk : 4 - kk;
+    // row >> (lam + 1) = (lane << (4 - lam)) + (j >> (lam + 1))
+    const uint32_t* tl = tws + (1024u - (1024u >> lam)) + (lane << (4 - lam));
+    uint32_t t[16];
+#pragma unroll
+    for (int m = 0; m < (1 << (4 - lam)); m++) t[m] = tl[m];
+#pragma unroll
+    for (int j = 0; j < 32; j++) {
+      if (j & (1 << lam)) continue;
+      if (INV)
+        ibfly(v[j], v[j | (1 << lam)], t[j >> (lam + 1)]);
+      else
+        bfly(v[j], v[j | (1 << lam)], t[j >> (lam + 1)]);
+    }
+  }
+}
+
+// Layers 5..9 on v[j] = row j*32 + lane: row >> (lam + 1) = j >> (lam - 4),
+// the same twiddle for every lane.
+template <bool INV>
+__device__ __forceinline__ void warp_phase_hi(uint32_t (&v)[32], const uint32_t* __restrict__ tws) {
+#pragma unroll
+  for (int kk = 0; kk < 5; kk++) {
+    const int k = INV ? kk : 4 - kk;  // bit of j
+    const uint32_t* tl = tws + (1024u - (1024u >> (5 + k)));
+    uint32_t t[16];
+#pragma unroll
+    for (int m = 0; m < (1 << (4 - k)); m++) t[m] = tl[m];
+#pragma unroll
+    for (int j = 0; j < 32; j++) {
+      if (j & (1 << k)) continue;
+      if (INV)
+        ibfly(v[j], v[j | (1 << k)], t[j >> (k + 1)]);
+      else
+        bfly(v[j], v[j | (1 << k)], t[j >> (k + 1)]);
+    }
+  }
+}
+
+__device__ __forceinline__ void warp_lo_to_hi(uint32_t (&v)[32], uint32_t* col, uint32_t lane) {
+#pragma unroll
+  for (int j = 0; j < 32; j++) col[lane * 33 + j] = v[j];
+  __syncwarp();
+#pragma unroll
+  for (int j = 0; j < 32; j++) v[j] = col[j * 33 + lane];
+  __syncwarp();
+}
+__device__ __forceinline__ void warp_hi_to_lo(uint32_t (&v)[32], uint32_t* col, uint32_t lane) {
+#pragma unroll
+  for (int j = 0; j < 32; j++) col[j * 33 + lane] = v[j];
+  __syncwarp();
+#pragma unroll
+  for (int j = 0; j < 32; j++) v[j] = col[lane * 33 + j];
+  __syncwarp();
+}
+
+// Stages the 1023 twiddles of a 10-layer tile position (as fft_pass_kernel).
+__device__ __forceinline__ void stage_tws10(const FftPass& p, uint64_t hi, uint32_t* tws) {
+#pragma unroll
+  for (int lam = 0; lam < 10; lam++) {
+    const uint32_t cnt = 1u << (9 - lam);
+    const uint32_t off = 1024u - (1024u >> lam);
+    const uint64_t h0 = hi << (9 - lam);
+    const uint32_t layer = p.layer0 + lam;
+    if (layer == 0) {
+      const uint32_t* lt0 = p.tree + (p.tree_len - (1ull << (p.log_domain - 1)));
+      for (uint32_t i = threadIdx.x; i < cnt; i += blockDim.x) tws[off + i] = circle_tw(lt0, h0 + i);
+    } else {
+      const uint32_t* lt = p.tree + (p.tree_len - (1ull << (p.log_domain - layer))) + h0;
+      for (uint32_t i = threadIdx.x; i < cnt; i += blockDim.x) tws[off + i] = __ldg(lt + i);
+    }
+  }
+}
+
+// Contiguous pass (layer0 = 0, C = 0): 1024 consecutive words of a column per
+// warp, straight between global memory and registers.  Needs 16-byte aligned
+// columns and no source masking.
+template <bool INV>
+__global__ void __launch_bounds__(256, 4) fft_warp_contig_kernel(FftPass p, FftCols cols) {
+  extern __shared__ uint32_t smem[];
+  uint32_t* tws = smem;
+  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  uint32_t* col = smem + 1024 + warp * (32 * 33);
+  const uint64_t hi = blockIdx.x;
+  stage_tws10(p, hi, tws);
+  __syncthreads();
+  const uint32_t c = blockIdx.y * kWarpCols + warp;
+  if (c >= p.n_cols) return;  // no block barrier follows
+  const uint32_t* __restrict__ src = cols.src[c];
+  uint32_t* __restrict__ dst = cols.dst[c];
+  const uint64_t base = hi << 10;
+  const uint32_t scale = p.scale;
+  uint32_t v[32];
+  if (INV) {
+    const uint4* s4 = reinterpret_cast<const uint4*>(src + base + lane * 32);
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+      const uint4 w = __ldg(s4 + q);
+      v[4 * q] = w.x;
+      v[4 * q + 1] = w.y;
+      v[4 * q + 2] = w.z;
+      v[4 * q + 3] = w.w;
+    }
+    warp_phase_lo<true>(v, tws, lane);
+    warp_lo_to_hi(v, col, lane);
+    warp_phase_hi<true>(v, tws);
+#pragma unroll
+    for (int j = 0; j < 32; j++) dst[base + j * 32 + lane] = scale != 1u ? m31_mul(v[j], scale) : v[j];
+  } else {
+#pragma unroll
+    for (int j = 0; j < 32; j++) v[j] = __ldg(src + base + j * 32 + lane);
+    warp_phase_hi<false>(v, tws);
+    warp_hi_to_lo(v, col, lane);
+    warp_phase_lo<false>(v, tws, lane);
+    uint4* d4 = reinterpret_cast<uint4*>(dst + base + lane * 32);
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+      uint4 w = make_uint4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+      if (scale != 1u) {
+        w.x = m31_mul(w.x, scale);
+        w.y = m31_mul(w.y, scale);
+        w.z = m31_mul(w.z, scale);
+        w.w = m31_mul(w.w, scale);
+      }
+      d4[q] = w;
+    }
+  }
+}
+
+// Strided pass (C = 3, layer0 >= 3): the block stages a 1024 x 8 tile of one
+// column; warp w transforms tile column w.
+template <bool INV>
+__global__ void __launch_bounds__(256, 4) fft_warp_strided_kernel(FftPass p, FftCols cols) {
+  extern __shared__ uint32_t smem[];
+  uint32_t* tws = smem;
+  uint32_t* tile = smem + 1024;  // 8 column regions of kColWords
+  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t L0 = p.layer0;
+  const uint64_t t = blockIdx.x;
+  const uint32_t lo_bits = L0 - 3;
+  const uint64_t lo = t & ((1ull << lo_bits) - 1);
+  const uint64_t hi = t >> lo_bits;
+  const uint64_t base = (hi << (L0 + 10)) | (lo << 3);
+  const uint32_t* __restrict__ src = cols.src[blockIdx.y];
+  uint32_t* __restrict__ dst = cols.dst[blockIdx.y];
+  stage_tws10(p, hi, tws);
+  if (p.vec_io) {
+#pragma unroll 4
+    for (uint32_t e = threadIdx.x * 4; e < 8192; e += 1024) {
+      const uint32_t row = e >> 3, c0 = e & 7;
+      const uint64_t gi = (base + ((uint64_t)row << L0) + c0) & p.src_mask;
+      const uint4 w = gi < p.src_len ? __ldg(reinterpret_cast<const uint4*>(src + gi)) : make_uint4(0, 0, 0, 0);
+      const uint32_t r = row + (row >> 5);
+      tile[c0 * kColWords + r] = w.x;
+      tile[(c0 + 1) * kColWords + r] = w.y;
+      tile[(c0 + 2) * kColWords + r] = w.z;
+      tile[(c0 + 3) * kColWords + r] = w.w;
+    }
+  } else {
+    for (uint32_t e = threadIdx.x; e < 8192; e += 256) {
+      const uint32_t row = e >> 3, c0 = e & 7;
+      const uint64_t gi = (base + ((uint64_t)row << L0) + c0) & p.src_mask;
+      tile[c0 * kColWords + row + (row >> 5)] = gi < p.src_len ? __ldg(src + gi) : 0u;
+    }
+  }
+  __syncthreads();
+  uint32_t* cw = tile + warp * kColWords;
+  uint32_t v[32];
+  if (INV) {
+#pragma unroll
+    for (int j = 0; j < 32; j++) v[j] = cw[lane * 33 + j];
+    warp_phase_lo<true>(v, tws, lane);
+    warp_lo_to_hi(v, cw, lane);
+    warp_phase_hi<true>(v, tws);
+#pragma unroll
+    for (int j = 0; j < 32; j++) cw[j * 33 + lane] = v[j];
+  } else {
+#pragma unroll
+    for (int j = 0; j < 32; j++) v[j] = cw[j * 33 + lane];
+    warp_phase_hi<false>(v, tws);
+    warp_hi_to_lo(v, cw, lane);
+    warp_phase_lo<false>(v, tws, lane);
+#pragma unroll
+    for (int j = 0; j < 32; j++) cw[lane * 33 + j] = v[j];
+  }
+  __syncthreads();
+  const uint32_t scale = p.scale;
+  if (p.vec_io) {
+#pragma unroll 4
+    for (uint32_t e = threadIdx.x * 4; e < 8192; e += 1024) {
+      const uint32_t row = e >> 3, c0 = e & 7;
+      const uint32_t r = row + (row >> 5);
+      uint4 w = make_uint4(tile[c0 * kColWords + r], tile[(c0 + 1) * kColWords + r], tile[(c0 + 2) * kColWords + r],
+                           tile[(c0 + 3) * kColWords + r]);
+      if (scale != 1u) {
+        w.x = m31_mul(w.x, scale);
+        w.y = m31_mul(w.y, scale);
+        w.z = m31_mul(w.z, scale);
+        w.w = m31_mul(w.w, scale);
+      }
+      *reinterpret_cast<uint4*>(dst + base + ((uint64_t)row << L0) + c0) = w;
+    }
+  } else {
+    for (uint32_t e = threadIdx.x; e < 8192; e += 256) {
+      const uint32_t row = e >> 3, c0 = e & 7;
+      const uint32_t v1 = tile[c0 * kColWords + row + (row >> 5)];
+      dst[base + ((uint64_t)row << L0) + c0] = scale != 1u ? m31_mul(v1, scale) : v1;
+    }
+  }
+}
+
+template <bool INV>
+static int launch_warp_pass(const FftPass& q, const FftCols& cols, uint64_t tiles, size_t nc, cudaStream_t s,
+                            char* err, size_t err_len) {
+  if (q.C == 0) {
+    constexpr size_t smem = (1024 + kWarpCols * 32 * 33) * sizeof(uint32_t);
+    static bool attr = false;
+    if (!attr) {
+      STWO_CUDA_TRY(cudaFuncSetAttribute(fft_warp_contig_kernel<INV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem));
+      attr = true;
+    }
+    dim3 grid((unsigned)tiles, (unsigned)((nc + kWarpCols - 1) / kWarpCols));
+    fft_warp_contig_kernel<INV><<<grid, 32 * kWarpCols, smem, s>>>(q, cols);
+  } else {
+    constexpr size_t smem = (1024 + 8 * kColWords) * sizeof(uint32_t);
+    static bool attr = false;
+    if (!attr) {
+      STWO_CUDA_TRY(cudaFuncSetAttribute(fft_warp_strided_kernel<INV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem));
+      attr = true;
+    }
+    dim3 grid((unsigned)tiles, (unsigned)nc);
+    fft_warp_strided_kernel<INV><<<grid, 256, smem, s>>>(q, cols);
+  }
+  STWO_CHECK_LAUNCH();
+  return STWO_B200_OK;
+}
+
 template <bool INV, int T, int C, int CPB>
 static int launch_tile(const FftPass& q, const FftCols& cols, dim3 grid, cudaStream_t s, char* err, size_t err_len) {
   constexpr int NT = fft_threads(T, C, CPB);
@@ -402,7 +657,12 @@ static int launch_pass(const FftPass& p, const std::vector<const uint32_t*>& src
     q.n_cols = (uint32_t)nc;
     dim3 grid((unsigned)tiles, (unsigned)((nc + cpb - 1) / cpb));
     int rc;
-    if (p.C == 3)
+    const bool warp_contig = p.T == 10 && p.C == 0 && p.layer0 == 0 && aligned && p.src_mask == ~0ull &&
+                             p.src_len == ~0ull;
+    const bool warp_strided = p.T == 10 && p.C == 3 && p.layer0 >= 3;
+    if (warp_contig || warp_strided)
+      rc = launch_warp_pass<INV>(q, cols, tiles, nc, s, err, err_len);
+    else if (p.C == 3)
       rc = dispatch_tile<INV, 3, 1>(q, cols, grid, s, err, err_len);
     else if (cpb == 4)
       rc = dispatch_tile<INV, 0, 4>(q, cols, grid, s, err, err_len);
