@@ -19,6 +19,7 @@
 #include "channel.hpp"
 #include "common.cuh"
 #include "field.cuh"
+#include "stream.cuh"
 
 namespace stwo_b200 {
 
@@ -116,60 +117,154 @@ __global__ void composition_kernel(const uint32_t* __restrict__ evals, uint64_t 
   }
 }
 
+__device__ __forceinline__ uint4 ldg4(const uint32_t* p) { return __ldg(reinterpret_cast<const uint4*>(p)); }
+__device__ __forceinline__ uint32_t u4get(const uint4& v, int r) {
+  return r == 0 ? v.x : r == 1 ? v.y : r == 2 ? v.z : v.w;
+}
+
+// composition_kernel for 4 consecutive points per thread: 16-byte loads keep
+// four times the bytes in flight per load, which this memory-latency-bound
+// loop needs.  Same arithmetic per point.  n_points % 4 == 0, columns
+// 16-byte aligned.
+__global__ void __launch_bounds__(256) composition4_kernel(const uint32_t* __restrict__ evals, uint64_t col_stride,
+                                                          uint32_t n_cons, const qm31* __restrict__ powers,
+                                                          const uint32_t* __restrict__ denom_inv, uint32_t log_n,
+                                                          uint64_t n_points, uint32_t* __restrict__ out) {
+  const uint64_t n4 = n_points >> 2;
+  for (uint64_t q = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; q < n4; q += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t i = q << 2;
+    const uint4 a = ldg4(evals + i), b = ldg4(evals + col_stride + i);
+    uint32_t sa[4], sb[4];
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+      sa[r] = m31_sqr(u4get(a, r));
+      sb[r] = m31_sqr(u4get(b, r));
+    }
+    acc4 row[4];
+#pragma unroll
+    for (int r = 0; r < 4; r++) row[r] = {0, 0, 0, 0};
+    uint32_t k = 0;
+    for (; k + 6 <= n_cons; k += 6) {
+      uint4 cv[6];
+#pragma unroll
+      for (int u = 0; u < 6; u++) cv[u] = ldg4(evals + (uint64_t)(k + u + 2) * col_stride + i);
+#pragma unroll
+      for (int u = 0; u < 6; u++) {
+        const qm31 pw = powers[k + u];
+#pragma unroll
+        for (int r = 0; r < 4; r++) {
+          const uint32_t c = u4get(cv[u], r);
+          acc4_mad(row[r], pw, m31_sub(c, m31_add(sa[r], sb[r])));
+          sa[r] = sb[r];
+          sb[r] = m31_sqr(c);
+        }
+        if (u == 2 || u == 5) {
+#pragma unroll
+          for (int r = 0; r < 4; r++) acc4_fold(row[r]);
+        }
+      }
+    }
+    for (; k < n_cons; k++) {  // remainder: fold after every term
+      const uint4 cv = ldg4(evals + (uint64_t)(k + 2) * col_stride + i);
+      const qm31 pw = powers[k];
+#pragma unroll
+      for (int r = 0; r < 4; r++) {
+        const uint32_t c = u4get(cv, r);
+        acc4_mad(row[r], pw, m31_sub(c, m31_add(sa[r], sb[r])));
+        acc4_fold(row[r]);
+        sa[r] = sb[r];
+        sb[r] = m31_sqr(c);
+      }
+    }
+    qm31 v[4];
+#pragma unroll
+    for (int r = 0; r < 4; r++) v[r] = qm31_mul_m31(acc4_reduce(row[r]), __ldg(denom_inv + ((i + r) >> log_n)));
+    *reinterpret_cast<uint4*>(out + i) = make_uint4(v[0].a, v[1].a, v[2].a, v[3].a);
+    *reinterpret_cast<uint4*>(out + n_points + i) = make_uint4(v[0].b, v[1].b, v[2].b, v[3].b);
+    *reinterpret_cast<uint4*>(out + 2 * n_points + i) = make_uint4(v[0].c, v[1].c, v[2].c, v[3].c);
+    *reinterpret_cast<uint4*>(out + 3 * n_points + i) = make_uint4(v[0].d, v[1].d, v[2].d, v[3].d);
+  }
+}
+
 // Polynomial values at one secure point: sum_j coeff_j * w_j where
 // w_j = prod over set bits b of j of f_b, f = [y, x, pi(x), pi^2(x), ...]
-// (the coefficient fold of prover/backend/cpu/circle.rs:82-99).  w_j =
-// w_hi[j >> h] * w_lo[j & (2^h - 1)].  Block (chunk, group) accumulates up to
-// kEvalGroup polynomials over a chunk of j.
-constexpr int kEvalGroup = 8;
+// (the coefficient fold of prover/backend/cpu/circle.rs:82-99), w_j =
+// w_hi[j >> h] * w_lo[j & (2^h - 1)]; see oods_eval_kernel.
 constexpr int kMaxPolys = 1024;
 struct PolyTable {
   const uint32_t* p[kMaxPolys];
 };
 
-__global__ void __launch_bounds__(256) batch_eval_kernel(PolyTable t, uint32_t n_polys, uint32_t log_n, uint32_t h,
-                                                        const qm31* __restrict__ w_lo, const qm31* __restrict__ w_hi,
-                                                        qm31* __restrict__ partial) {
-  const uint32_t group = blockIdx.y;
-  const uint32_t p0 = group * kEvalGroup;
-  const uint32_t np = min((uint32_t)kEvalGroup, n_polys - p0);
+// OODS sampling for every polynomial of one size: the block stages the
+// weights w_j of a 1024-index chunk in shared memory, then each warp takes one
+// polynomial at a time and reduces its chunk (coalesced loads, 8 in flight per
+// lane) to one partial sum per (polynomial, chunk).  Sums are exact field sums,
+// so the grouping does not change the result.
+constexpr uint32_t kOodsChunk = 1024;
+__global__ void __launch_bounds__(256) oods_eval_kernel(PolyTable t, uint32_t n_polys, uint32_t log_n, uint32_t h,
+                                                       const qm31* __restrict__ w_lo, const qm31* __restrict__ w_hi,
+                                                       qm31* __restrict__ partial) {
+  __shared__ uint4 ws[kOodsChunk];
   const uint64_t n = 1ull << log_n;
+  const uint32_t chunk = n < kOodsChunk ? (uint32_t)n : kOodsChunk;
+  const uint64_t j0 = (uint64_t)blockIdx.x * chunk;
   const uint64_t lo_mask = (1ull << h) - 1;
-  acc4 acc[kEvalGroup];
-#pragma unroll
-  for (int q = 0; q < kEvalGroup; q++) acc[q] = {0, 0, 0, 0};
-  uint32_t since_fold = 0;
-  for (uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; j < n; j += (uint64_t)gridDim.x * blockDim.x) {
-    qm31 w = qm31_mul(w_hi[j >> h], w_lo[j & lo_mask]);
-#pragma unroll
-    for (int q = 0; q < kEvalGroup; q++)
-      if (q < (int)np) acc4_mad(acc[q], w, __ldg(t.p[p0 + q] + j));
-    if (++since_fold == 3) {
-      since_fold = 0;
-#pragma unroll
-      for (int q = 0; q < kEvalGroup; q++) acc4_fold(acc[q]);
-    }
+  for (uint32_t k = threadIdx.x; k < chunk; k += blockDim.x) {
+    const uint64_t j = j0 + k;
+    const qm31 w = qm31_mul(w_hi[j >> h], w_lo[j & lo_mask]);
+    ws[k] = make_uint4(w.a, w.b, w.c, w.d);
   }
-  __shared__ qm31 red[256];
-  for (uint32_t q = 0; q < np; q++) {
-    red[threadIdx.x] = acc4_reduce(acc[q]);
-    __syncthreads();
-    for (uint32_t s = blockDim.x / 2; s > 0; s >>= 1) {
-      if (threadIdx.x < s) red[threadIdx.x] = qm31_add(red[threadIdx.x], red[threadIdx.x + s]);
-      __syncthreads();
+  __syncthreads();
+  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t n_warps = blockDim.x >> 5;
+  for (uint32_t p = warp; p < n_polys; p += n_warps) {
+    const uint32_t* __restrict__ col = t.p[p] + j0;
+    acc4 s{0, 0, 0, 0};
+    if (chunk == kOodsChunk) {
+#pragma unroll 1
+      for (uint32_t b = 0; b < kOodsChunk; b += 256) {
+        uint32_t v[8];
+#pragma unroll
+        for (int u = 0; u < 8; u++) v[u] = __ldg(col + b + u * 32 + lane);
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+          const uint4 w = ws[b + u * 32 + lane];
+          acc4_mad(s, qm31{w.x, w.y, w.z, w.w}, v[u]);
+          if (u == 2 || u == 5 || u == 7) acc4_fold(s);
+        }
+      }
+    } else {
+      for (uint32_t k = lane; k < chunk; k += 32) {
+        const uint4 w = ws[k];
+        acc4_mad(s, qm31{w.x, w.y, w.z, w.w}, __ldg(col + k));
+        acc4_fold(s);
+      }
     }
-    if (threadIdx.x == 0) partial[(uint64_t)(p0 + q) * gridDim.x + blockIdx.x] = red[0];
-    __syncthreads();
+    qm31 v = acc4_reduce(s);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const qm31 u = {__shfl_xor_sync(0xffffffffu, v.a, o), __shfl_xor_sync(0xffffffffu, v.b, o),
+                      __shfl_xor_sync(0xffffffffu, v.c, o), __shfl_xor_sync(0xffffffffu, v.d, o)};
+      v = qm31_add(v, u);
+    }
+    if (lane == 0) partial[(uint64_t)p * gridDim.x + blockIdx.x] = v;
   }
 }
 
-__global__ void reduce_partials_kernel(const qm31* __restrict__ partial, uint32_t n_chunks, uint32_t n_polys,
-                                       qm31* __restrict__ out) {
-  uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= n_polys) return;
+// out[p] = sum of partial[p][0 .. n_chunks); one block per polynomial.
+__global__ void __launch_bounds__(256) oods_reduce_kernel(const qm31* __restrict__ partial, uint32_t n_chunks,
+                                                         qm31* __restrict__ out) {
+  __shared__ qm31 red[256];
+  const uint32_t p = blockIdx.x;
   qm31 s = qm31_zero();
-  for (uint32_t c = 0; c < n_chunks; c++) s = qm31_add(s, partial[(uint64_t)p * n_chunks + c]);
-  out[p] = s;
+  for (uint32_t c = threadIdx.x; c < n_chunks; c += blockDim.x) s = qm31_add(s, partial[(uint64_t)p * n_chunks + c]);
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (uint32_t k = blockDim.x / 2; k > 0; k >>= 1) {
+    if (threadIdx.x < k) red[threadIdx.x] = qm31_add(red[threadIdx.x], red[threadIdx.x + k]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[p] = red[0];
 }
 
 // FRI quotient of one sample batch (all columns sampled at point z, same
@@ -183,6 +278,7 @@ struct QuotientParams {
   cpoint init;           // first point of the half coset
   cpoint step_pow[31];   // step * 2^b
   uint32_t log_size;     // lifting domain
+  cpoint tile_pts[256];  // m * step * 2^(log_size - tile bits), m < rows/4 (quotient_tma_kernel)
 };
 
 __global__ void __launch_bounds__(256) quotient_kernel(QuotientParams q, PolyTable cols, uint32_t n_cols,
@@ -223,6 +319,267 @@ __global__ void __launch_bounds__(256) quotient_kernel(QuotientParams q, PolyTab
     out[n + i] = v.b;
     out[2 * n + i] = v.c;
     out[3 * n + i] = v.d;
+  }
+}
+
+// quotient_kernel for 4 consecutive rows per thread: 16-byte column loads and
+// one shared inversion for the four denominators (their norms are inverted
+// together with Montgomery's trick; exact, so equal to four cm31_inv).
+// n % 4 == 0, columns 16-byte aligned.
+__device__ __forceinline__ cpoint quotient_point(const QuotientParams& q, uint64_t i) {
+  const uint64_t n = 1ull << q.log_size, half = n >> 1;
+  const uint64_t j = __brevll(i) >> (64 - q.log_size);
+  const uint64_t jj = j < half ? j : j - half;
+  cpoint pt = q.init;
+  for (uint32_t b = 0; b + 1 < q.log_size; b++)
+    if ((jj >> b) & 1) pt = cpoint_add(pt, q.step_pow[b]);
+  if (j >= half) pt.y = m31_neg(pt.y);
+  return pt;
+}
+
+__global__ void __launch_bounds__(256) quotient4_kernel(QuotientParams q, PolyTable cols, uint32_t n_cols,
+                                                       const qm31* __restrict__ alpha_pows, uint32_t* __restrict__ out) {
+  const uint64_t n = 1ull << q.log_size;
+  const uint64_t n4 = n >> 2;
+  for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < n4; t += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t i = t << 2;
+    acc4 s4[4];
+#pragma unroll
+    for (int r = 0; r < 4; r++) s4[r] = {0, 0, 0, 0};
+    uint32_t k = 0;
+    for (; k + 6 <= n_cols; k += 6) {
+      uint4 fv[6];
+#pragma unroll
+      for (int u = 0; u < 6; u++) fv[u] = ldg4(cols.p[k + u] + i);
+#pragma unroll
+      for (int u = 0; u < 6; u++) {
+        const qm31 ap = alpha_pows[k + u];
+#pragma unroll
+        for (int r = 0; r < 4; r++) acc4_mad(s4[r], ap, u4get(fv[u], r));
+        if (u == 2 || u == 5) {
+#pragma unroll
+          for (int r = 0; r < 4; r++) acc4_fold(s4[r]);
+        }
+      }
+    }
+    for (; k < n_cols; k++) {  // remainder: fold after every term
+      const uint4 fv = ldg4(cols.p[k] + i);
+      const qm31 ap = alpha_pows[k];
+#pragma unroll
+      for (int r = 0; r < 4; r++) {
+        acc4_mad(s4[r], ap, u4get(fv, r));
+        acc4_fold(s4[r]);
+      }
+    }
+    qm31 full[4];
+    cm31 den[4];
+    uint32_t norm[4];
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+      const cpoint pt = quotient_point(q, i + r);
+      const qm31 num = qm31_sub(qm31_mul(q.c, acc4_reduce(s4[r])), q.B);
+      full[r] = qm31_sub(num, qm31_mul_m31(q.A, pt.y));
+      den[r] = cm31_sub(cm31_mul(cm31_sub(q.prx, cm31{pt.x, 0}), q.piy),
+                        cm31_mul(cm31_sub(q.pry, cm31{pt.y, 0}), q.pix));
+      norm[r] = m31_add(m31_sqr(den[r].a), m31_sqr(den[r].b));
+    }
+    // Montgomery batch inversion of the four norms.
+    const uint32_t p01 = m31_mul(norm[0], norm[1]);
+    const uint32_t p012 = m31_mul(p01, norm[2]);
+    uint32_t inv = m31_inv(m31_mul(p012, norm[3]));
+    uint32_t ninv[4];
+    ninv[3] = m31_mul(inv, p012);
+    inv = m31_mul(inv, norm[3]);
+    ninv[2] = m31_mul(inv, p01);
+    inv = m31_mul(inv, norm[2]);
+    ninv[1] = m31_mul(inv, norm[0]);
+    ninv[0] = m31_mul(inv, norm[1]);
+    qm31 v[4];
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+      const cm31 di = cm31_mul({den[r].a, m31_neg(den[r].b)}, {ninv[r], 0});
+      v[r] = qm31_mul_cm31(full[r], di);
+    }
+    *reinterpret_cast<uint4*>(out + i) = make_uint4(v[0].a, v[1].a, v[2].a, v[3].a);
+    *reinterpret_cast<uint4*>(out + n + i) = make_uint4(v[0].b, v[1].b, v[2].b, v[3].b);
+    *reinterpret_cast<uint4*>(out + 2 * n + i) = make_uint4(v[0].c, v[1].c, v[2].c, v[3].c);
+    *reinterpret_cast<uint4*>(out + 3 * n + i) = make_uint4(v[0].d, v[1].d, v[2].d, v[3].d);
+  }
+}
+
+// ---- TMA column-streaming versions ----
+// A block owns kStreamRows consecutive rows; thread t owns rows 4t .. 4t+3.
+// Columns arrive kStreamG at a time through the shared-memory ring of
+// ColumnRing (cp.async.bulk, mbarrier completion), so the DRAM reads of the
+// next groups overlap the arithmetic of the current one.  Same arithmetic
+// per point as composition_kernel / quotient_kernel.
+constexpr int kStreamTileBits = 9, kStreamRows = 1 << kStreamTileBits, kStreamG = 6, kStreamS = 3;
+constexpr int kStreamThreads = kStreamRows / 4;  // four rows per thread
+constexpr uint32_t kStreamErrWord = 8;  // word of the prover's flag buffer set by a timed-out stage
+constexpr size_t kStreamRing = (size_t)kStreamS * kStreamG * kStreamRows * sizeof(uint32_t);
+constexpr uint32_t kStreamMaxW = 1024;  // QM31 weights staged in shared memory
+constexpr size_t kStreamSmem = kStreamRing + kStreamMaxW * sizeof(uint4);
+
+__device__ __forceinline__ void stage_weights(uint4* sw, const qm31* __restrict__ w, uint32_t n) {
+  for (uint32_t k = threadIdx.x; k < n; k += blockDim.x) sw[k] = make_uint4(w[k].a, w[k].b, w[k].c, w[k].d);
+}
+
+__global__ void __launch_bounds__(kStreamThreads) composition_tma_kernel(
+    const uint32_t* __restrict__ evals, uint64_t col_stride, uint32_t n_cons, const qm31* __restrict__ powers,
+    const uint32_t* __restrict__ denom_inv, uint32_t log_n, uint64_t n_points, uint32_t* __restrict__ out,
+    uint32_t* err) {
+  extern __shared__ __align__(128) uint32_t smem[];
+  __shared__ uint64_t bars[kStreamS];
+  uint4* sw = reinterpret_cast<uint4*>(smem + kStreamRing / sizeof(uint32_t));
+  const uint32_t t4 = threadIdx.x * 4;
+  auto col = [evals, col_stride](uint32_t c) { return evals + (uint64_t)c * col_stride; };
+  ColumnRing<kStreamG, kStreamS, kStreamRows> ring(smem, bars, n_cons + 2, (uint32_t)(n_points / kStreamRows));
+  stage_weights(sw, powers, n_cons);
+  __syncthreads();
+  ring.start(col);
+  for (uint32_t t = 0; t < ring.my_tiles; t++) {
+    uint32_t sa[4] = {0, 0, 0, 0}, sb[4] = {0, 0, 0, 0};
+    acc4 row[4];
+#pragma unroll
+    for (int r = 0; r < 4; r++) row[r] = {0, 0, 0, 0};
+    // Constraint k = c - 2 of column c = 6g + j: folding after j = 1 and
+    // j = 4 leaves at most three products between folds.
+    for (uint32_t g = 0; g < ring.n_groups; g++) {
+      const uint32_t gg = t * ring.n_groups + g;
+      if (!ring.wait(gg, err)) return;
+      const uint32_t nc = ring.cols_in(g);
+#pragma unroll
+      for (int j = 0; j < kStreamG; j++) {
+        if ((uint32_t)j < nc) {
+          const uint32_t c = g * kStreamG + j;
+          const uint4 v = *reinterpret_cast<const uint4*>(ring.seg(gg, j) + t4);
+          if (c >= 2) {
+            const uint4 pw4 = sw[c - 2];
+            const qm31 pw{pw4.x, pw4.y, pw4.z, pw4.w};
+#pragma unroll
+            for (int r = 0; r < 4; r++) {
+              const uint32_t x = u4get(v, r);
+              acc4_mad(row[r], pw, m31_sub(x, m31_add(sa[r], sb[r])));
+              sa[r] = sb[r];
+              sb[r] = m31_sqr(x);
+            }
+          } else {
+#pragma unroll
+            for (int r = 0; r < 4; r++) {
+              sa[r] = sb[r];
+              sb[r] = m31_sqr(u4get(v, r));
+            }
+          }
+        }
+        if (j == 1 || j == 4) {
+#pragma unroll
+          for (int r = 0; r < 4; r++) acc4_fold(row[r]);
+        }
+      }
+      ring.release(gg, col);
+    }
+    const uint64_t i = ring.tile_row0(t) + t4;
+    qm31 v[4];
+#pragma unroll
+    for (int r = 0; r < 4; r++) v[r] = qm31_mul_m31(acc4_reduce(row[r]), __ldg(denom_inv + ((i + r) >> log_n)));
+    *reinterpret_cast<uint4*>(out + i) = make_uint4(v[0].a, v[1].a, v[2].a, v[3].a);
+    *reinterpret_cast<uint4*>(out + n_points + i) = make_uint4(v[0].b, v[1].b, v[2].b, v[3].b);
+    *reinterpret_cast<uint4*>(out + 2 * n_points + i) = make_uint4(v[0].c, v[1].c, v[2].c, v[3].c);
+    *reinterpret_cast<uint4*>(out + 3 * n_points + i) = make_uint4(v[0].d, v[1].d, v[2].d, v[3].d);
+  }
+}
+
+// Rows 4t .. 4t+3 of a tile (R = 2^b rows, t < R/4): with r0 a multiple of
+// R, the bit-reversed positions are j(r0 + 4t + e) = J0 + bitrev_{b-2}(t) *
+// 2^(log-b) + bitrev2(e) * 2^(log-2).  e = 0, 2 lie below the half (jj = J0 +
+// bitrev_{b-2}(t) * 2^(log-b) and that + 2^(log-2)); e = 1, 3 are their
+// conjugates in the upper half.  So the two points are B +
+// tile_pts[bitrev_{b-2}(t)] and that + step * 2^(log-2), B = init + J0 * step.
+__global__ void __launch_bounds__(kStreamThreads) quotient_tma_kernel(QuotientParams q, PolyTable cols,
+                                                                     uint32_t n_cols,
+                                                                     const qm31* __restrict__ alpha_pows,
+                                                                     uint32_t* __restrict__ out, uint32_t* err) {
+  extern __shared__ __align__(128) uint32_t smem[];
+  __shared__ uint64_t bars[kStreamS];
+  __shared__ cpoint s_base;
+  uint4* sw = reinterpret_cast<uint4*>(smem + kStreamRing / sizeof(uint32_t));
+  const uint64_t n = 1ull << q.log_size;
+  const uint32_t t4 = threadIdx.x * 4;
+  const PolyTable* tab = &cols;
+  auto col = [tab](uint32_t c) { return tab->p[c]; };
+  ColumnRing<kStreamG, kStreamS, kStreamRows> ring(smem, bars, n_cols, (uint32_t)(n / kStreamRows));
+  stage_weights(sw, alpha_pows, n_cols);
+  __syncthreads();
+  ring.start(col);
+  for (uint32_t t = 0; t < ring.my_tiles; t++) {
+    const uint64_t r0 = ring.tile_row0(t);
+    if (threadIdx.x == 0) {  // read by all threads only after the first release barrier of the tile
+      const uint64_t J0 = __brevll(r0) >> (64 - q.log_size);
+      cpoint b = q.init;
+      for (uint32_t k = 0; k + 1 < q.log_size; k++)
+        if ((J0 >> k) & 1) b = cpoint_add(b, q.step_pow[k]);
+      s_base = b;
+    }
+    acc4 s4[4];
+#pragma unroll
+    for (int r = 0; r < 4; r++) s4[r] = {0, 0, 0, 0};
+    for (uint32_t g = 0; g < ring.n_groups; g++) {
+      const uint32_t gg = t * ring.n_groups + g;
+      if (!ring.wait(gg, err)) return;
+      const uint32_t nc = ring.cols_in(g);
+#pragma unroll
+      for (int j = 0; j < kStreamG; j++) {
+        if ((uint32_t)j < nc) {
+          const uint32_t c = g * kStreamG + j;
+          const uint4 v = *reinterpret_cast<const uint4*>(ring.seg(gg, j) + t4);
+          const uint4 a4 = sw[c];
+          const qm31 ap{a4.x, a4.y, a4.z, a4.w};
+#pragma unroll
+          for (int r = 0; r < 4; r++) acc4_mad(s4[r], ap, u4get(v, r));
+        }
+        if (j == 2 || j == 5) {
+#pragma unroll
+          for (int r = 0; r < 4; r++) acc4_fold(s4[r]);
+        }
+      }
+      ring.release(gg, col);
+    }
+    const cpoint p0 = cpoint_add(s_base, q.tile_pts[__brev(threadIdx.x) >> (32 - (kStreamTileBits - 2))]);
+    const cpoint p2 = cpoint_add(p0, q.step_pow[q.log_size - 2]);
+    const uint32_t xs[4] = {p0.x, p0.x, p2.x, p2.x};
+    const uint32_t ys[4] = {p0.y, m31_neg(p0.y), p2.y, m31_neg(p2.y)};
+    qm31 full[4];
+    cm31 den[4];
+    uint32_t norm[4];
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+      const qm31 num = qm31_sub(qm31_mul(q.c, acc4_reduce(s4[r])), q.B);
+      full[r] = qm31_sub(num, qm31_mul_m31(q.A, ys[r]));
+      den[r] = cm31_sub(cm31_mul(cm31_sub(q.prx, cm31{xs[r], 0}), q.piy),
+                        cm31_mul(cm31_sub(q.pry, cm31{ys[r], 0}), q.pix));
+      norm[r] = m31_add(m31_sqr(den[r].a), m31_sqr(den[r].b));
+    }
+    // Montgomery batch inversion of the four norms.
+    const uint32_t p01 = m31_mul(norm[0], norm[1]);
+    const uint32_t p012 = m31_mul(p01, norm[2]);
+    uint32_t inv = m31_inv(m31_mul(p012, norm[3]));
+    uint32_t ninv[4];
+    ninv[3] = m31_mul(inv, p012);
+    inv = m31_mul(inv, norm[3]);
+    ninv[2] = m31_mul(inv, p01);
+    inv = m31_mul(inv, norm[2]);
+    ninv[1] = m31_mul(inv, norm[0]);
+    ninv[0] = m31_mul(inv, norm[1]);
+    qm31 v[4];
+#pragma unroll
+    for (int r = 0; r < 4; r++)
+      v[r] = qm31_mul_cm31(full[r], cm31_mul({den[r].a, m31_neg(den[r].b)}, {ninv[r], 0}));
+    const uint64_t i = r0 + t4;
+    *reinterpret_cast<uint4*>(out + i) = make_uint4(v[0].a, v[1].a, v[2].a, v[3].a);
+    *reinterpret_cast<uint4*>(out + n + i) = make_uint4(v[0].b, v[1].b, v[2].b, v[3].b);
+    *reinterpret_cast<uint4*>(out + 2 * n + i) = make_uint4(v[0].c, v[1].c, v[2].c, v[3].c);
+    *reinterpret_cast<uint4*>(out + 3 * n + i) = make_uint4(v[0].d, v[1].d, v[2].d, v[3].d);
+    __syncthreads();  // s_base of this tile read by every thread before thread 0 rewrites it
   }
 }
 
@@ -604,6 +961,19 @@ __global__ void __launch_bounds__(kFriTailThreads, 1) fri_tail_kernel(FriTail t,
   }
 }
 
+// Persistent grid of the column-streaming kernels: as many blocks as are
+// resident at once (occupancy of this kernel with its shared memory), never
+// more blocks than tiles.
+template <typename K>
+static unsigned stream_grid(K kernel, size_t smem, uint32_t n_tiles) {
+  int dev = 0, sms = 148, per_sm = 1;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kStreamThreads, smem);
+  const uint32_t resident = (uint32_t)std::max(1, sms) * (uint32_t)std::max(1, per_sm);
+  return std::max(1u, std::min(n_tiles, resident));
+}
+
 static unsigned grid1d(uint64_t n, unsigned threads) {
   uint64_t b = (n + threads - 1) / threads;
   return (unsigned)std::min<uint64_t>(std::max<uint64_t>(b, 1), 148ull * 32);
@@ -751,6 +1121,7 @@ class WideFibProver {
   uint64_t* d_gather_addr = nullptr;
   uint32_t* d_gather_out = nullptr;
   size_t gather_cap = 0;
+  qm31* d_oods_partial = nullptr;  // OODS partial sums (polynomials x chunks)
   qm31* h_pinned = nullptr;       // staging for small uploads / downloads
   DevChannel* h_chan = nullptr;   // staging of the device channel state (own region: the
                                   // quotient upload from h_pinned may still be in flight)
@@ -799,6 +1170,10 @@ class WideFibProver {
     STWO_CUDA_TRY(cudaFuncSetAttribute(fri_tail_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFriTailSmem));
     STWO_CUDA_TRY(
         cudaFuncSetAttribute(tree_top_channel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFriTailSmem));
+    STWO_CUDA_TRY(
+        cudaFuncSetAttribute(composition_tma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kStreamSmem));
+    STWO_CUDA_TRY(
+        cudaFuncSetAttribute(quotient_tma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kStreamSmem));
     log_n = c.log_n_rows;
     N = c.n_cols;
     blowup = c.log_blowup;
@@ -854,6 +1229,9 @@ class WideFibProver {
     if ((rc = alloc((void**)&d_last, 16ull << last_log, err, err_len))) return rc;
     size_t small_q = std::max<size_t>(4096, 2 * (1u << 12) + (size_t)kMaxPolys * 1024);
     if ((rc = alloc((void**)&d_small, small_q * sizeof(qm31), err, err_len))) return rc;
+    // OODS partial sums: one per (polynomial, 1024-index chunk)
+    const size_t oods_chunks = log_n > 10 ? (size_t)1 << (log_n - 10) : 1;
+    if ((rc = alloc((void**)&d_oods_partial, (size_t)(N + 8) * oods_chunks * sizeof(qm31), err, err_len))) return rc;
     if ((rc = alloc((void**)&d_denom, 4ull << (eval_log - log_n), err, err_len))) return rc;
     if ((rc = alloc((void**)&d_found, 64, err, err_len))) return rc;
     if ((rc = alloc((void**)&d_chan, sizeof(DevChannel), err, err_len))) return rc;
@@ -1025,6 +1403,7 @@ int WideFibProver::prove_body(const uint32_t* d_a, const uint32_t* d_b, ProofOut
   HostChannel ch(m31);
   int rc;
   const uint64_t rows = 1ull << log_n;
+  STWO_CUDA_TRY(cudaMemsetAsync(d_found + kStreamErrWord, 0, 4, s));
   // ---- tree 0: empty preprocessed trace -> Blake2s("") ----
   Hash32 root0;
   {
@@ -1100,8 +1479,18 @@ int WideFibProver::prove_body(const uint32_t* d_a, const uint32_t* d_b, ProofOut
     comp_stride = 1ull << eval_log;
   }
   const uint64_t n_eval = 1ull << eval_log;
-  composition_kernel<<<grid1d(n_eval, 256), 256, 0, s>>>(comp_src, comp_stride, n_cons, d_small, d_denom, log_n,
-                                                         n_eval, d_comp);
+  if (n_eval % kStreamRows == 0 && n_cons <= kStreamMaxW && comp_stride % 4 == 0 &&
+      reinterpret_cast<uintptr_t>(comp_src) % 16 == 0)
+    composition_tma_kernel<<<stream_grid(composition_tma_kernel, kStreamRing + n_cons * sizeof(uint4),
+                                         (uint32_t)(n_eval / kStreamRows)),
+                             kStreamThreads, kStreamRing + n_cons * sizeof(uint4), s>>>(
+        comp_src, comp_stride, n_cons, d_small, d_denom, log_n, n_eval, d_comp, d_found + kStreamErrWord);
+  else if (n_eval % 4 == 0 && comp_stride % 4 == 0 && reinterpret_cast<uintptr_t>(comp_src) % 16 == 0)
+    composition4_kernel<<<grid1d(n_eval / 4, 256), 256, 0, s>>>(comp_src, comp_stride, n_cons, d_small, d_denom,
+                                                                log_n, n_eval, d_comp);
+  else
+    composition_kernel<<<grid1d(n_eval, 256), 256, 0, s>>>(comp_src, comp_stride, n_cons, d_small, d_denom, log_n,
+                                                           n_eval, d_comp);
   STWO_CHECK_LAUNCH();
   std::vector<uint32_t*> comp_cols(4);
   std::vector<uint32_t> logs_e(4, eval_log);
@@ -1163,13 +1552,11 @@ int WideFibProver::prove_body(const uint32_t* d_a, const uint32_t* d_b, ProofOut
     uint32_t np = N + 8;
     for (uint32_t c = 0; c < N; c++) pt.p[c] = coeff_ptrs[c];
     for (int k = 0; k < 8; k++) pt.p[N + k] = split[k];
-    const uint32_t chunks = 128;
-    qm31* d_partial = d_small + n_w;
-    dim3 grid(chunks, (np + kEvalGroup - 1) / kEvalGroup);
-    batch_eval_kernel<<<grid, 256, 0, s>>>(pt, np, lg, h, d_small, d_small + (1u << h), d_partial);
+    const uint32_t chunks = lg > 10 ? 1u << (lg - 10) : 1u;  // kOodsChunk indices each
+    qm31* d_vals = d_small + n_w;
+    oods_eval_kernel<<<chunks, 256, 0, s>>>(pt, np, lg, h, d_small, d_small + (1u << h), d_oods_partial);
     STWO_CHECK_LAUNCH();
-    qm31* d_vals = d_partial + (size_t)np * chunks;
-    reduce_partials_kernel<<<(np + 127) / 128, 128, 0, s>>>(d_partial, chunks, np, d_vals);
+    oods_reduce_kernel<<<np, 256, 0, s>>>(d_oods_partial, chunks, d_vals);
     STWO_CHECK_LAUNCH();
     STWO_CUDA_TRY(cudaMemcpyAsync(h_pinned, d_vals, np * sizeof(qm31), cudaMemcpyDeviceToHost, s));
     STWO_CUDA_TRY(cudaStreamSynchronize(s));
@@ -1242,7 +1629,22 @@ int WideFibProver::prove_body(const uint32_t* d_a, const uint32_t* d_b, ProofOut
     PolyTable cols;
     for (uint32_t c = 0; c < N; c++) cols.p[c] = eval_ptrs[c];
     for (int k = 0; k < 8; k++) cols.p[N + k] = lde[k];
-    quotient_kernel<<<grid1d(1ull << lift, 256), 256, 0, s>>>(qp, cols, nq, d_small, d_quot);
+    bool aligned = lift >= 2;
+    for (uint32_t c = 0; c < nq; c++) aligned = aligned && reinterpret_cast<uintptr_t>(cols.p[c]) % 16 == 0;
+    if (aligned && lift >= (uint32_t)kStreamTileBits + 1 && nq <= kStreamMaxW) {
+      cpoint g = qp.step_pow[lift - kStreamTileBits], acc = {1, 0};
+      for (int m = 0; m < kStreamRows / 4; m++) {
+        qp.tile_pts[m] = acc;
+        acc = cpoint_add(acc, g);
+      }
+      quotient_tma_kernel<<<stream_grid(quotient_tma_kernel, kStreamRing + nq * sizeof(uint4),
+                                        (uint32_t)((1ull << lift) / kStreamRows)),
+                            kStreamThreads, kStreamRing + nq * sizeof(uint4), s>>>(
+          qp, cols, nq, d_small, d_quot, d_found + kStreamErrWord);
+    } else if (aligned)
+      quotient4_kernel<<<grid1d(1ull << (lift - 2), 256), 256, 0, s>>>(qp, cols, nq, d_small, d_quot);
+    else
+      quotient_kernel<<<grid1d(1ull << lift, 256), 256, 0, s>>>(qp, cols, nq, d_small, d_quot);
     STWO_CHECK_LAUNCH();
   }
 
@@ -1276,9 +1678,14 @@ int WideFibProver::prove_body(const uint32_t* d_a, const uint32_t* d_b, ProofOut
     off += (fri.size() + 1) * sizeof(qm31);
     size_t chan_off = off;
     STWO_CUDA_TRY(cudaMemcpyAsync(hp + off, d_chan, sizeof(DevChannel), cudaMemcpyDeviceToHost, s));
+    off += sizeof(DevChannel);
+    const size_t flag_off = off;
+    STWO_CUDA_TRY(cudaMemcpyAsync(hp + off, d_found + kStreamErrWord, 4, cudaMemcpyDeviceToHost, s));
     STWO_CUDA_TRY(cudaStreamSynchronize(s));
     const DevChannel* dc = reinterpret_cast<const DevChannel*>(hp + chan_off);
     if (dc->error) return set_err(err, err_len, STWO_B200_ESTATE, "device channel: draw retry bound exhausted");
+    if (*reinterpret_cast<const uint32_t*>(hp + flag_off))
+      return set_err(err, err_len, STWO_B200_ETIMEOUT, "column stream: a bulk copy did not complete in time");
     const qm31* dev_alpha = reinterpret_cast<const qm31*>(hp + alpha_off);
     for (size_t i = 0; i < fri_roots.size(); i++) {
       std::memcpy(fri_roots[i].data(), hp + 32 * i, 32);
