@@ -429,8 +429,8 @@ PROVE_PHASES = ["trace_gen", "trace_interpolate", "trace_evaluate", "trace_merkl
                 "quotients", "fri_merkle", "fri_fold", "grind", "decommit"]
 
 
-def prove_spec():
-    return dict(name="wide_fib_prove", log_n=20, n_cols=100, log_blowup=1, pow_bits=10, n_queries=3,
+def prove_spec(log_n=20, n_cols=100):
+    return dict(name="wide_fib_prove", log_n=log_n, n_cols=n_cols, log_blowup=1, pow_bits=10, n_queries=3,
                 log_last_layer=0, line_fold_step=1, seed=2)
 
 
@@ -446,7 +446,8 @@ def prove_config_json(spec, world):
             "pow_bits": spec["pow_bits"], "n_queries": spec["n_queries"],
             "fri": "circle fold + line folds by 2 to last layer log degree 0",
             "channel": "Blake2sMerkleChannel", "inputs": "col0/col1 uniform [0, 2^31-1) per row, seed 2",
-            "l2": "inputs larger than L2 (400 MB trace, 800 MB evaluations; no flush)",
+            "l2": (f"inputs larger than L2 ({(spec['n_cols'] << spec['log_n']) * 4 >> 20} MB trace, "
+                   f"{(spec['n_cols'] << spec['log_n']) * 8 >> 20} MB evaluations; no flush)"),
             "parallelism": f"replicas x{world}"}
 
 
@@ -464,7 +465,7 @@ def cpu_prove(spec, a, b, threads=None):
 def run_prove_reference(args, world, rank):
     if rank != 0:
         return
-    spec = prove_spec()
+    spec = prove_spec(args.log_n_rows, args.n_cols)
     a, b = prove_inputs(spec)
     cells = spec["n_cols"] << spec["log_n"]
     secs = []
@@ -482,7 +483,7 @@ def run_prove_reference(args, world, rank):
         "data": "synthetic (seeded numpy PCG64)", "config": prove_config_json(spec, args.gpus),
         "p50_prove_ms": 1000 * statistics.median(secs), "p99_prove_ms": 1000 * max(secs),
         "cpu_baseline": {"value": value, "unit": "proved trace cells/s", "cores": n_threads, "kind": "port",
-                         "sample": "each step: the whole Wide-Fibonacci 100 x 2^20 proof (SimdBackend restatement, "
+                         "sample": f"each step: the whole Wide-Fibonacci {spec['n_cols']} x 2^{spec['log_n']} proof (SimdBackend restatement, "
                                    "C++ oracle, OpenMP)"},
         "e2e": {"value": value, "unit": "proved trace cells/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -498,7 +499,7 @@ def run_prove_b200(args, world, rank, local):
     torch.cuda.set_device(local)
     ffi.init(local)
     stream = torch.cuda.Stream()
-    spec = prove_spec()
+    spec = prove_spec(args.log_n_rows, args.n_cols)
     a_host, b_host = prove_inputs(spec)
     cells = spec["n_cols"] << spec["log_n"]
     prover = WideFibProver(wide_fib_config(spec["log_n"], spec["n_cols"], spec["log_blowup"], spec["pow_bits"],
@@ -652,7 +653,7 @@ def run_prove_b200(args, world, rank, local):
         "bit_exact_vs_oracle": proof == cpu_proof,
         "cpu_baseline": {"value": cells / cpu_s, "unit": "proved trace cells/s", "cores": cpu_threads,
                          "kind": "port",
-                         "sample": "one whole Wide-Fibonacci 100 x 2^20 proof (SimdBackend restatement, C++ oracle, "
+                         "sample": f"one whole Wide-Fibonacci {spec['n_cols']} x 2^{spec['log_n']} proof (SimdBackend restatement, C++ oracle, "
                                    "OpenMP), same inputs; its proof bytes are compared with the GPU's"},
     }
     print(json.dumps(line), flush=True)
@@ -666,6 +667,8 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="wide_fib_prove",
                     choices=["wide_fib_prove", "commit_uneven", "commit_plain"])
+    ap.add_argument("--log-n-rows", type=int, default=20, help="wide_fib_prove: log2 of the trace rows")
+    ap.add_argument("--n-cols", type=int, default=100, help="wide_fib_prove: trace columns")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world, rank, local = dist_setup()

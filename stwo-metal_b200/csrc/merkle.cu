@@ -87,6 +87,9 @@ struct NodeOuts {
   uint8_t* out[8];
 };
 
+// LAT selects the shortest-dependency Blake2s form, for launches of a few
+// blocks where one compression's latency (not throughput) sets the time.
+template <bool LAT>
 __global__ void __launch_bounds__(256) node_layers_kernel(const uint8_t* in, uint32_t in_log, uint32_t levels, int m31,
                                                          NodeOuts outs) {
   __shared__ uint32_t buf[2][256 * 8];
@@ -107,7 +110,10 @@ __global__ void __launch_bounds__(256) node_layers_kernel(const uint8_t* in, uin
     m[12] = d.x; m[13] = d.y; m[14] = d.z; m[15] = d.w;
     uint32_t h[8];
     blake2s_init(h);
-    blake2s_compress(h, m, 64, true);
+    if (LAT)
+      blake2s_compress_lat(h, m, 64, true);
+    else
+      blake2s_compress(h, m, 64, true);
     if (m31) {
 #pragma unroll
       for (int k = 0; k < 8; k++) h[k] = m31_reduce_u32(h[k]);
@@ -127,6 +133,9 @@ __global__ void __launch_bounds__(256) node_layers_kernel(const uint8_t* in, uin
       for (int k = 0; k < 16; k++) m[k] = buf[cur][tid * 16 + k];
       uint32_t h[8];
       blake2s_init(h);
+      if (LAT)
+      blake2s_compress_lat(h, m, 64, true);
+    else
       blake2s_compress(h, m, 64, true);
       if (m31) {
 #pragma unroll
@@ -255,7 +264,10 @@ int build_node_layers_impl(const uint8_t* in, uint32_t in_log, uint32_t stop_log
     NodeOuts o;
     for (uint32_t lv = 0; lv < levels; lv++) o.out[lv] = outs_by_log[cur_log - 1 - lv];
     unsigned blocks = (unsigned)(parents0 / width);
-    node_layers_kernel<<<blocks, 256, 0, s>>>(cur, cur_log, levels, m31, o);
+    if (blocks <= 148)
+      node_layers_kernel<true><<<blocks, 256, 0, s>>>(cur, cur_log, levels, m31, o);
+    else
+      node_layers_kernel<false><<<blocks, 256, 0, s>>>(cur, cur_log, levels, m31, o);
     STWO_CHECK_LAUNCH();
     cur = outs_by_log[cur_log - levels];
     cur_log -= levels;

@@ -637,7 +637,7 @@ __device__ void dev_mix_root_draw(DevChannel* ch, const uint32_t* root, qm31* al
   for (int k = 0; k < 8; k++) m[8 + k] = root[k];
   uint32_t h[8];
   blake2s_init(h);
-  blake2s_compress(h, m, 64, true);
+  blake2s_compress_lat(h, m, 64, true);
   dev_finalize(h, ch->m31 != 0);
   for (int k = 0; k < 8; k++) ch->digest[k] = h[k];
   uint32_t n_draws = 0;
@@ -649,7 +649,7 @@ __device__ void dev_mix_root_draw(DevChannel* ch, const uint32_t* root, qm31* al
     for (int k = 9; k < 16; k++) m[k] = 0;
     n_draws++;
     blake2s_init(h);
-    blake2s_compress(h, m, 37, true);
+    blake2s_compress_lat(h, m, 37, true);
     dev_finalize(h, ch->m31 != 0);
     bool okw = true;
     for (int k = 0; k < 8; k++) okw = okw && h[k] < 2 * M31_P;
@@ -821,7 +821,7 @@ __device__ const uint4* tree_levels_smem(uint8_t* base, uint32_t lg, uint4* src,
       }
       uint32_t h[8];
       blake2s_init(h);
-      blake2s_compress(h, m, 64, true);
+      blake2s_compress_lat(h, m, 64, true);
       dev_finalize(h, m31);
       put_hash(base + ((size_t)np - 1) * 32, dst, p, h);
     }
@@ -866,7 +866,7 @@ __global__ void __launch_bounds__(kFriTailThreads, 1) tree_top_channel_kernel(ui
       }
       uint32_t h[8];
       blake2s_init(h);
-      blake2s_compress(h, m, 64, true);
+      blake2s_compress_lat(h, m, 64, true);
       dev_finalize(h, m31b);
       put_hash(base + ((size_t)np - 1) * 32, ping, p, h);
     }
@@ -904,7 +904,7 @@ __global__ void __launch_bounds__(kFriTailThreads, 1) fri_tail_kernel(FriTail t,
       for (int k = 4; k < 16; k++) m[k] = 0;
       uint32_t h[8];
       blake2s_init(h);
-      blake2s_compress(h, m, 16, true);
+      blake2s_compress_lat(h, m, 16, true);
       dev_finalize(h, m31);
       put_hash(base + ((size_t)n - 1) * 32, ping, i, h);
     }
