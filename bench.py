@@ -239,6 +239,21 @@ def run_b200(args, spec, world, rank, local):
     n_leaf_blocks = (len(logs) + 15) // 16
     torch.cuda.synchronize()
 
+    # Committer forms (commit_uneven): per-column launches, batched launches,
+    # batched + CUDA graph; the pass plans of every size group are autotuned
+    # first (process-wide, so every form below runs with them).
+    cms, tuned = None, None
+    if spec["name"] == "commit_uneven":
+        from stwo_b200 import Committer, fft_get_plan
+        cms = {"per_column": Committer(logs, blowup, tree, per_column=True, stream=stream.cuda_stream),
+               "batched": Committer(logs, blowup, tree, stream=stream.cuda_stream),
+               "batched_graph": Committer(logs, blowup, tree, graph=True, stream=stream.cuda_stream)}
+        t_tune = time.perf_counter()
+        cms["batched_graph"].autotune(inputs, coeffs, evals, reps=2)
+        torch.cuda.synchronize()
+        tuned = {"seconds": time.perf_counter() - t_tune,
+                 "plans": {str(n): fft_get_plan(n) for n in sorted(set(logs))}}
+
     phases = ["bitrev", "ifft", "rfft", "leaves", "nodes"]
 
     def step(evs=None):
@@ -364,6 +379,32 @@ def run_b200(args, spec, world, rank, local):
     torch.cuda.synchronize()
     probe_rate = pb * 256 * pit / (p0.elapsed_time(p1) * 1e-3)
 
+    forms = None
+    if cms is not None:
+        forms = {}
+        for name, cm in cms.items():
+            with torch.cuda.stream(stream):
+                for _ in range(args.warmup):
+                    cm.commit(inputs, coeffs, evals, layers)
+            torch.cuda.synchronize()
+            l0 = ffi.launch_count()
+            f0 = torch.cuda.Event(enable_timing=True)
+            f1 = torch.cuda.Event(enable_timing=True)
+            with torch.cuda.stream(stream):
+                f0.record(stream)
+                for _ in range(args.steps):
+                    cm.commit(inputs, coeffs, evals, layers)
+                f1.record(stream)
+            torch.cuda.synchronize()
+            f_ms = max_over_ranks(f0.elapsed_time(f1) / args.steps, world)
+            assert bytes(layer_to_host(layers[0])[0]) == root, f"{name} root differs"
+            forms[name] = {"ms_per_step": f_ms, "committed_cells_per_s": cells / (f_ms * 1e-3),
+                           "launches_per_step": (ffi.launch_count() - l0) / args.steps}
+            cm.close()
+        forms["batched_over_per_column"] = forms["per_column"]["ms_per_step"] / forms["batched"]["ms_per_step"]
+        forms["graph_over_per_column"] = forms["per_column"]["ms_per_step"] / forms["batched_graph"]["ms_per_step"]
+        forms["autotune"] = tuned
+
     if rank != 0:
         return
     hbm_peak, peak_kind = load_peaks()
@@ -420,6 +461,8 @@ def run_b200(args, spec, world, rank, local):
                          "sample": cpu_sample + "; SimdBackend restatement (C++ oracle, OpenMP)"},
         "root": root.hex(),
     }
+    if forms is not None:
+        line["forms"] = forms
     print(json.dumps(line), flush=True)
 
 

@@ -194,6 +194,51 @@ int stwo_b200_decompose(const uint32_t* const* d_in4, uint32_t log_size, uint32_
 int stwo_b200_decompose_noalloc(const uint32_t* const* d_in4, uint32_t log_size, uint32_t* const* d_out4,
                                 uint32_t* lambda_out, void* stream, char* err, size_t err_len);
 
+/* --------------------------------------------------------- FFT pass plans */
+/* Pass plan of every n-layer circle FFT: n_passes (1-4) layer counts of 1-12,
+ * low layers first, summing to n; the first at least 3 when there are several
+ * (the later passes are strided).  n_passes = 0 restores the default split.
+ * Process-wide; results do not depend on the plan.  No reference counterpart:
+ * the SIMD backend's radix-8 loop structure is fixed (simd/fft/ifft.rs:33-57);
+ * these are the autotuner's knobs. */
+int stwo_b200_fft_set_plan(uint32_t log_size, const uint32_t* pass_layers, uint32_t n_passes, char* err,
+                           size_t err_len);
+int stwo_b200_fft_get_plan(uint32_t log_size, uint32_t* pass_layers, uint32_t cap, uint32_t* n_passes, char* err,
+                           size_t err_len);
+
+/* --------------------------------------------------------- trace commit -- */
+/* CommitmentTreeProver::new for one column set (crates/stwo/src/prover/pcs/
+ * mod.rs:707-781): interpolate_columns (prover/poly/circle/ops.rs:29-40) from
+ * bit-reversed canonic-coset evaluations, evaluate_polynomials on the
+ * log_blowup domain (ops.rs:110-211), then the lifted Blake2s tree of the
+ * evaluations (prover/vcs_lifted/prover.rs:33-42) with lifting log size
+ * max(log_sizes) + log_blowup.  flags: */
+#define STWO_B200_COMMIT_PER_COLUMN 1u /* launches per column (the plain form) */
+#define STWO_B200_COMMIT_GRAPH 2u      /* capture once per buffer set, replay */
+typedef struct stwo_b200_committer stwo_b200_committer;
+int stwo_b200_committer_create(const uint32_t* log_sizes, uint32_t n_cols, uint32_t log_blowup, int m31_output,
+                               const uint32_t* d_twiddles, const uint32_t* d_itwiddles, uint32_t tree_log_size,
+                               uint32_t flags, stwo_b200_committer** out, char* err, size_t err_len);
+int stwo_b200_committer_destroy(stwo_b200_committer* committer, char* err, size_t err_len);
+int stwo_b200_committer_lifting_log_size(const stwo_b200_committer* committer, uint32_t* out, char* err,
+                                         size_t err_len);
+/* d_evals[i]: column i (2^log_sizes[i] words, read only); d_coeffs[i] and
+ * d_ldes[i] (2^(log_sizes[i]+log_blowup) words) receive its coefficients and
+ * evaluations; d_layers[k] (2^k hashes of 32 bytes, k = 0..lifting log size)
+ * the tree, root first.  Ordered after the work already on `stream`, and the
+ * work on `stream` after it. */
+int stwo_b200_committer_commit(stwo_b200_committer* committer, const uint32_t* const* d_evals,
+                               uint32_t* const* d_coeffs, uint32_t* const* d_ldes, uint8_t* const* d_layers,
+                               void* stream, char* err, size_t err_len);
+/* Times every candidate pass plan of each (log_size, column count) group of
+ * the committer on these buffers (reps timed runs each) and keeps the fastest
+ * as the process-wide plan; cache_path (optional) is read first and written
+ * with the choices ("log_size n_columns T1,T2,..." per line).  Clobbers
+ * d_coeffs and d_ldes.  No reference counterpart. */
+int stwo_b200_committer_autotune(stwo_b200_committer* committer, const uint32_t* const* d_evals,
+                                 uint32_t* const* d_coeffs, uint32_t* const* d_ldes, const char* cache_path,
+                                 uint32_t reps, char* err, size_t err_len);
+
 /* ----------------------------------------------------- Wide-Fibonacci prove */
 /* PcsConfig + FriConfig fields of crates/stwo/src/core/pcs/mod.rs:31-80 and
  * core/fri.rs:31-80 (defaults: pow_bits 10, log_blowup 1, n_queries 3,

@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <mutex>
 #include <vector>
 
 #include "common.cuh"
@@ -302,22 +303,52 @@ struct PassPlan {
   uint32_t layer0, T, C;
 };
 
-// Splits n layers into passes of <= 12 (contiguous) / <= 11 (strided, C = 3)
-// layers, low layers first.
+// Pass plans: per transform size n, the layer counts of its passes, low
+// layers first (the first pass is contiguous, C = 0; the others strided,
+// C = 3).  A plan set with stwo_b200_fft_set_plan (the autotuner's choice)
+// overrides the default split.
+static std::mutex g_plan_mu;
+static std::vector<uint32_t> g_plan_override[31];
+
+static bool plan_is_valid(uint32_t n, const uint32_t* t, uint32_t k) {
+  if (n == 0 || n > 30 || k == 0 || k > 4) return false;
+  uint32_t sum = 0;
+  for (uint32_t i = 0; i < k; i++) {
+    if (t[i] < 1 || t[i] > 12) return false;
+    sum += t[i];
+  }
+  // strided passes need layer0 >= C = 3
+  return sum == n && (k == 1 || t[0] >= 3);
+}
+
+// Default: passes of <= 12 layers, two up to 23 layers, three above.
+static std::vector<uint32_t> default_split(uint32_t n) {
+  if (n <= 12) return {n};
+  uint32_t parts = n <= 23 ? 2 : 3;
+  std::vector<uint32_t> t;
+  uint32_t rest = n;
+  for (uint32_t i = 0; i < parts; i++) {
+    uint32_t x = (rest + (parts - i) - 1) / (parts - i);
+    t.push_back(x);
+    rest -= x;
+  }
+  return t;
+}
+
+static std::vector<uint32_t> split_for(uint32_t n) {
+  {
+    std::lock_guard<std::mutex> g(g_plan_mu);
+    if (n <= 30 && !g_plan_override[n].empty()) return g_plan_override[n];
+  }
+  return default_split(n);
+}
+
 static std::vector<PassPlan> plan_passes(uint32_t n) {
   std::vector<PassPlan> plan;
-  if (n <= 12) {
-    plan.push_back({0, n, 0});
-    return plan;
-  }
-  uint32_t parts = n <= 23 ? 2 : 3;
-  uint32_t rest = n;
   uint32_t l0 = 0;
-  for (uint32_t i = 0; i < parts; i++) {
-    uint32_t t = (rest + (parts - i) - 1) / (parts - i);
+  for (uint32_t t : split_for(n)) {
     plan.push_back({l0, t, l0 == 0 ? 0u : 3u});
     l0 += t;
-    rest -= t;
   }
   return plan;
 }
@@ -846,6 +877,35 @@ extern "C" int stwo_b200_evaluate_polynomials(const uint32_t* const* d_coeffs, c
     small_fft_kernel<<<1, kFftMaxCols, 0, s>>>(small, n_small, 0);
     STWO_CHECK_LAUNCH();
   }
+  return ok(err, err_len);
+}
+
+extern "C" int stwo_b200_fft_set_plan(uint32_t log_size, const uint32_t* pass_layers, uint32_t n_passes, char* err,
+                                      size_t err_len) {
+  STWO_ARG_CHECK(log_size >= 1 && log_size <= 30, "log size %u out of range", log_size);
+  if (n_passes == 0) {
+    std::lock_guard<std::mutex> g(g_plan_mu);
+    g_plan_override[log_size].clear();
+    return ok(err, err_len);
+  }
+  STWO_ARG_CHECK(pass_layers != nullptr, "null plan");
+  STWO_ARG_CHECK(plan_is_valid(log_size, pass_layers, n_passes),
+                 "invalid plan for log size %u: 1-4 passes of 1-12 layers summing to the size, first >= 3 if split",
+                 log_size);
+  std::lock_guard<std::mutex> g(g_plan_mu);
+  g_plan_override[log_size].assign(pass_layers, pass_layers + n_passes);
+  return ok(err, err_len);
+}
+
+extern "C" int stwo_b200_fft_get_plan(uint32_t log_size, uint32_t* pass_layers, uint32_t cap, uint32_t* n_passes,
+                                      char* err, size_t err_len) {
+  STWO_ARG_CHECK(log_size >= 1 && log_size <= 30, "log size %u out of range", log_size);
+  STWO_ARG_CHECK(n_passes != nullptr, "null n_passes");
+  const std::vector<uint32_t> t = split_for(log_size);
+  *n_passes = (uint32_t)t.size();
+  STWO_ARG_CHECK(pass_layers == nullptr || cap >= t.size(), "plan has %zu passes, capacity %u", t.size(), cap);
+  if (pass_layers)
+    for (size_t i = 0; i < t.size(); i++) pass_layers[i] = t[i];
   return ok(err, err_len);
 }
 

@@ -259,3 +259,65 @@ class B200Backend:
 
 def layer_to_host(buf: DeviceBuffer) -> np.ndarray:
     return buf.download(np.uint8).reshape(-1, 32)
+
+
+# ---- FFT pass plans (the autotuner's knobs) ---------------------------------
+def fft_set_plan(log_size: int, passes) -> None:
+    """Process-wide pass plan of n-layer FFTs; ``passes=()`` restores the default."""
+    passes = list(passes)
+    ffi.call("stwo_b200_fft_set_plan", C.c_uint32(log_size), _u32_array(passes), C.c_uint32(len(passes)))
+
+
+def fft_get_plan(log_size: int) -> list:
+    buf = (C.c_uint32 * 4)()
+    n = C.c_uint32(0)
+    ffi.call("stwo_b200_fft_get_plan", C.c_uint32(log_size), buf, C.c_uint32(4), C.byref(n))
+    return [int(buf[i]) for i in range(n.value)]
+
+
+# ---- trace commitment --------------------------------------------------------
+class Committer:
+    """CommitmentTreeProver::new for one column set (crates/stwo/src/prover/pcs/
+    mod.rs:707-781): interpolate, evaluate on the blowup domain, lifted Blake2s
+    tree.  ``per_column`` launches every column on its own (the plain form);
+    otherwise columns of one size share launches, and ``graph`` captures the
+    whole commit once per buffer set and replays it."""
+
+    def __init__(self, log_sizes, log_blowup: int, tree: TwiddleTree, m31: bool = False, per_column: bool = False,
+                 graph: bool = False, stream=None):
+        ffi.init()
+        self.stream = as_stream(stream)
+        self.log_sizes = [int(x) for x in log_sizes]
+        flags = (1 if per_column else 0) | (2 if graph else 0)
+        h = C.c_void_p()
+        ffi.call("stwo_b200_committer_create", _u32_array(self.log_sizes), C.c_uint32(len(self.log_sizes)),
+                 C.c_uint32(log_blowup), C.c_int(1 if m31 else 0), C.c_void_p(tree.twiddles.ptr),
+                 C.c_void_p(tree.itwiddles.ptr), C.c_uint32(tree.log_size), C.c_uint32(flags), C.byref(h))
+        self._h = h
+        L = C.c_uint32(0)
+        ffi.call("stwo_b200_committer_lifting_log_size", h, C.byref(L))
+        self.lifting_log_size = L.value
+
+    def new_layers(self):
+        return [DeviceBuffer(32 << k, self.stream) for k in range(self.lifting_log_size + 1)]
+
+    def commit(self, evals, coeffs, ldes, layers):
+        ffi.call("stwo_b200_committer_commit", self._h, _ptr_array(evals), _ptr_array(coeffs), _ptr_array(ldes),
+                 _ptr_array(layers), self.stream)
+        return layers
+
+    def autotune(self, evals, coeffs, ldes, cache_path: str | None = None, reps: int = 3):
+        path = cache_path.encode() if cache_path else None
+        ffi.call("stwo_b200_committer_autotune", self._h, _ptr_array(evals), _ptr_array(coeffs), _ptr_array(ldes),
+                 C.c_char_p(path), C.c_uint32(reps))
+
+    def close(self):
+        if self._h:
+            ffi.call("stwo_b200_committer_destroy", self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
