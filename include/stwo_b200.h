@@ -285,6 +285,30 @@ int stwo_b200_prover_set_timing(stwo_b200_prover* prover, int enable, char* err,
 int stwo_b200_prover_phase_times(stwo_b200_prover* prover, double* ms_out, uint32_t n, uint32_t* proofs, char* err,
                                  size_t err_len);
 
+/* ------------------------------------------------ FRI commit + decommit -- */
+/* FriProver::commit + decommit (crates/stwo/src/prover/fri.rs:133-350) of one
+ * secure column on CanonicCoset(log_size), with the folding alphas supplied
+ * instead of drawn from a channel: a lifted Blake2s tree of the circle layer,
+ * the circle-to-line fold (FriOps::fold_circle_into_line), then per line layer
+ * its tree and a fold by 2 (FriOps::fold_line) down to a single value; then
+ * the decommitment of the query positions.  d_itwiddles: an inverse twiddle
+ * tree covering log_size - 1 (e.g. of CanonicCoset(log_size + 1).half_coset).
+ * Buffers for every layer and tree are allocated at create. */
+typedef struct stwo_b200_fri_prover stwo_b200_fri_prover;
+int stwo_b200_fri_prover_create(uint32_t log_size, int m31_output, const uint32_t* d_itwiddles,
+                                uint32_t tree_log_size, void* stream, stwo_b200_fri_prover** out, char* err,
+                                size_t err_len);
+int stwo_b200_fri_prover_destroy(stwo_b200_fri_prover* prover, char* err, size_t err_len);
+/* d_coords4: the column's 4 coordinate columns (device, 2^log_size words each,
+ * bit-reversed circle-domain order); alphas: log_size QM31 values (host, 4
+ * words each; alpha 0 folds the circle layer); queries: sorted distinct
+ * positions in [0, 2^log_size).  Writes the FriProof bytes (first layer,
+ * inner layers, last-layer value; the proof's canonical layout) to proof_out
+ * when non-NULL and their length to *proof_len.  Synchronises its stream. */
+int stwo_b200_fri_prove_seeded(stwo_b200_fri_prover* prover, const uint32_t* const* d_coords4,
+                               const uint32_t* alphas, const uint64_t* queries, uint32_t n_queries,
+                               uint8_t* proof_out, size_t proof_cap, size_t* proof_len, char* err, size_t err_len);
+
 #ifdef __cplusplus
 }
 #endif

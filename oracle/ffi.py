@@ -349,6 +349,33 @@ def prove_wide_fib(cfg: WideFibConfig, a, b) -> bytes:
     return bytes(out)
 
 
+def fri_inputs(log_n: int, seed: int, n_queries: int = 70):
+    """Seeded FRI-heavy inputs: 4 coordinate columns uniform in [0, P), one QM31
+    folding alpha per fold (log_n of them, as a (log_n, 4) array), and the
+    sorted distinct query positions drawn from n_queries uniform draws."""
+    r = np.random.default_rng(seed)
+    n = 1 << log_n
+    coords = [r.integers(0, P, n, dtype=np.uint32) for _ in range(4)]
+    alphas = r.integers(0, P, (log_n, 4), dtype=np.uint32)
+    queries = np.unique(r.integers(0, n, n_queries, dtype=np.uint64))
+    return coords, alphas, queries
+
+
+def fri_prove_seeded(coords, log_n: int, alphas, queries, m31: bool = False) -> bytes:
+    """FriProver commit + decommit of one secure column with the given alphas
+    (FriProof bytes: first layer, inner layers, last-layer value)."""
+    arrs = [_u32(c) for c in coords]
+    a = np.ascontiguousarray(alphas, dtype=np.uint32).reshape(-1)
+    q = np.ascontiguousarray(queries, dtype=np.uint64)
+    n = C.c_size_t()
+    _check(lib().oracle_fri_prove_seeded(_ptrs(arrs), C.c_uint32(log_n), _p(a),
+                                         q.ctypes.data_as(C.POINTER(C.c_uint64)), C.c_size_t(q.size),
+                                         C.c_int(1 if m31 else 0), C.byref(n)))
+    out = (C.c_uint8 * n.value)()
+    lib().oracle_last_proof(out)
+    return bytes(out)
+
+
 def last_intermediate(which: int, k: int) -> np.ndarray:
     n = lib().oracle_last_intermediate(C.c_int(which), C.c_int(k), None)
     out = np.zeros(n, np.uint32)

@@ -254,6 +254,19 @@ extern "C" int oracle_prove_wide_fib(const OracleWideFibConfig* cfg, const uint3
   });
 }
 extern "C" void oracle_last_proof(uint8_t* out) { std::memcpy(out, g_last_proof.data(), g_last_proof.size()); }
+// FRI-heavy workload: alphas = log_n QM31 values (4 words each); the proof
+// bytes are kept until the next call (oracle_last_proof).
+extern "C" int oracle_fri_prove_seeded(const uint32_t* const* coords4, uint32_t log_n, const uint32_t* alphas,
+                                       const uint64_t* queries, size_t n_queries, int m31, size_t* proof_len) {
+  return guard([&] {
+    std::vector<QM31> a(log_n);
+    for (uint32_t k = 0; k < log_n; k++)
+      a[k] = QM31::from(alphas[4 * k], alphas[4 * k + 1], alphas[4 * k + 2], alphas[4 * k + 3]);
+    const uint32_t* c[4] = {coords4[0], coords4[1], coords4[2], coords4[3]};
+    g_last_proof = fri_prove_seeded(c, log_n, a.data(), std::vector<size_t>(queries, queries + n_queries), m31 != 0);
+    *proof_len = g_last_proof.size();
+  });
+}
 // Intermediates of the last prove: which = 0 composition evals (coord k), 1 quotients (coord k).
 extern "C" size_t oracle_last_intermediate(int which, int k, uint32_t* out) {
   const auto& v = which == 0 ? g_last_trace.composition_evals : g_last_trace.quotients;

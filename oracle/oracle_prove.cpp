@@ -504,6 +504,14 @@ static void put_u32(std::vector<uint8_t>& o, uint32_t v) { for (int i = 0; i < 4
 static void put_u64(std::vector<uint8_t>& o, uint64_t v) { for (int i = 0; i < 8; i++) o.push_back((v >> (8 * i)) & 0xFF); }
 static void put_q(std::vector<uint8_t>& o, const QM31& q) { for (uint32_t c : q.coords()) put_u32(o, c); }
 static void put_h(std::vector<uint8_t>& o, const Hash& h) { o.insert(o.end(), h.begin(), h.end()); }
+// FriLayerProof field order (core/fri.rs:361-395).
+static void put_fri_layer(std::vector<uint8_t>& o, const FriLayerProofO& l) {
+  put_u64(o, l.fri_witness.size());
+  for (auto& q : l.fri_witness) put_q(o, q);
+  put_u64(o, l.hash_witness.size());
+  for (auto& h : l.hash_witness) put_h(o, h);
+  put_h(o, l.commitment);
+}
 
 std::vector<uint8_t> serialize(const Proof& p) {
   std::vector<uint8_t> o;
@@ -531,13 +539,7 @@ std::vector<uint8_t> serialize(const Proof& p) {
     for (auto& c : t) { put_u64(o, c.size()); for (uint32_t v : c) put_u32(o, v); }
   }
   put_u64(o, p.proof_of_work);
-  auto layer = [&](const FriLayerProofO& l) {
-    put_u64(o, l.fri_witness.size());
-    for (auto& q : l.fri_witness) put_q(o, q);
-    put_u64(o, l.hash_witness.size());
-    for (auto& h : l.hash_witness) put_h(o, h);
-    put_h(o, l.commitment);
-  };
+  auto layer = [&](const FriLayerProofO& l) { put_fri_layer(o, l); };
   layer(p.fri_first);
   put_u64(o, p.fri_inner.size());
   for (auto& l : p.fri_inner) layer(l);
@@ -547,6 +549,77 @@ std::vector<uint8_t> serialize(const Proof& p) {
   bit_reverse(lp.data(), lg);
   put_u64(o, lp.size());
   for (auto& q : lp) put_q(o, q);
+  return o;
+}
+
+// FRI-heavy workload: FriProver::commit (prover/fri.rs:133-291) of one secure
+// column on CanonicCoset(log_n) with the folding alphas supplied instead of
+// drawn from a channel: circle-to-line fold, then line folds by 2 down to a
+// single value (a last layer of log size 0), a lifted Blake2s tree for every
+// layer folded from; then the decommitment of the sorted, distinct query
+// positions (prover/fri.rs:294-350, 459-488).  Serialized as the FriProof part
+// of serialize(): first layer, inner layers, last-layer polynomial (here the
+// one folded value, its own interpolant).
+std::vector<uint8_t> fri_prove_seeded(const uint32_t* const coords[4], uint32_t log_n, const QM31* alphas,
+                                      std::vector<size_t> queries, bool m31) {
+  if (log_n < 2 || log_n > 28) throw std::runtime_error("log_n out of range");
+  std::sort(queries.begin(), queries.end());
+  queries.erase(std::unique(queries.begin(), queries.end()), queries.end());
+  for (size_t q : queries)
+    if (q >> log_n) throw std::runtime_error("query out of range");
+  TwiddleTree tw = precompute_twiddles(canonic_half_coset(log_n + 1));
+  struct Layer { std::vector<std::vector<uint32_t>> coords; std::vector<std::vector<Hash>> layers; };
+  const size_t n = (size_t)1 << log_n;
+  Layer first;
+  for (int k = 0; k < 4; k++) first.coords.emplace_back(coords[k], coords[k] + n);
+  {
+    std::vector<const uint32_t*> p4{first.coords[0].data(), first.coords[1].data(), first.coords[2].data(),
+                                    first.coords[3].data()};
+    first.layers = build_merkle_layers(p4, {log_n, log_n, log_n, log_n}, log_n, m31);
+  }
+  uint32_t cur_log = log_n - 1;
+  std::vector<std::vector<uint32_t>> cur(4, std::vector<uint32_t>((size_t)1 << cur_log, 0));
+  {
+    uint32_t* d[4] = {cur[0].data(), cur[1].data(), cur[2].data(), cur[3].data()};
+    const uint32_t* s[4] = {coords[0], coords[1], coords[2], coords[3]};
+    fold_circle_into_line(d, s, canonic_half_coset(log_n), tw.itw.data(), tw.itw.size(), alphas[0]);
+  }
+  std::vector<Layer> inner;
+  for (uint32_t k = 1; cur_log >= 1; k++) {
+    Layer l;
+    l.coords = cur;
+    std::vector<const uint32_t*> p4{l.coords[0].data(), l.coords[1].data(), l.coords[2].data(), l.coords[3].data()};
+    l.layers = build_merkle_layers(p4, {cur_log, cur_log, cur_log, cur_log}, cur_log, m31);
+    std::vector<std::vector<uint32_t>> nxt(4, std::vector<uint32_t>((size_t)1 << (cur_log - 1)));
+    const uint32_t* in[4] = {cur[0].data(), cur[1].data(), cur[2].data(), cur[3].data()};
+    uint32_t* out[4] = {nxt[0].data(), nxt[1].data(), nxt[2].data(), nxt[3].data()};
+    fold_line(in, cur_log, tw.itw.data(), tw.itw.size(), alphas[k], 1, out);
+    cur.swap(nxt);
+    cur_log -= 1;
+    inner.push_back(std::move(l));
+  }
+  const QM31 last = QM31::from(cur[0][0], cur[1][0], cur[2][0], cur[3][0]);
+  auto decommit = [&](const Layer& l, const std::vector<size_t>& q) {
+    FriLayerProofO out;
+    std::vector<size_t> pos;
+    decommit_positions_and_witness(l.coords, q, 1, pos, out.fri_witness);
+    std::vector<std::vector<uint32_t>> qv;
+    uint32_t lg = (uint32_t)l.layers.size() - 1;
+    std::vector<const uint32_t*> p4{l.coords[0].data(), l.coords[1].data(), l.coords[2].data(), l.coords[3].data()};
+    merkle_decommit(l.layers, pos, p4, {lg, lg, lg, lg}, qv, out.hash_witness);
+    out.commitment = l.layers[0][0];
+    return out;
+  };
+  std::vector<uint8_t> o;
+  put_fri_layer(o, decommit(first, queries));
+  put_u64(o, inner.size());
+  std::vector<size_t> lq = fold_queries(queries, 1);
+  for (auto& l : inner) {
+    put_fri_layer(o, decommit(l, lq));
+    lq = fold_queries(lq, 1);
+  }
+  put_u64(o, 1);
+  put_q(o, last);
   return o;
 }
 

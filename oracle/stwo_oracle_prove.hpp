@@ -62,6 +62,8 @@ void merkle_decommit(const std::vector<std::vector<Hash>>& layers_root_first, st
                      std::vector<std::vector<uint32_t>>& queried_values, std::vector<Hash>& witness);
 Proof prove_wide_fib(const WideFibConfig& cfg, const uint32_t* in_a, const uint32_t* in_b, ProveTrace* dbg);
 std::vector<uint8_t> serialize(const Proof& p);
+std::vector<uint8_t> fri_prove_seeded(const uint32_t* const coords[4], uint32_t log_n, const QM31* alphas,
+                                      std::vector<size_t> queries, bool m31);
 void verify_wide_fib(const uint8_t* data, size_t n, uint32_t log_n_rows, uint32_t n_cols, bool m31);
 
 }  // namespace oracle

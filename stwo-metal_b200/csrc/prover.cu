@@ -1950,6 +1950,181 @@ int WideFibProver::prove_body(const uint32_t* d_a, const uint32_t* d_b, ProofOut
   return 0;
 }
 
+// ---- FRI-heavy path: FriProver commit + decommit with given alphas ----
+// One secure column on CanonicCoset(log_n) (4 coordinate columns): lifted
+// Blake2s tree of the circle layer, circle-to-line fold, then per line layer
+// its tree and a fold by 2, down to one value; then the decommitment of the
+// query positions (prover/fri.rs:133-350; alphas supplied instead of drawn).
+// Output: the FriProof bytes (first layer, inner layers, last-layer value) in
+// the proof's canonical layout.  All buffers are allocated once per size.
+struct SeededFriProver {
+  uint32_t n = 0, tree_log = 0;
+  int m31 = 0;
+  const uint32_t* itw = nullptr;
+  cudaStream_t user_s = nullptr, s = nullptr;
+  cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+  std::vector<uint32_t*> line;   // line[k]: 4 x 2^(n-1-k) words, k = 0..n-1 (line[n-1]: the last value)
+  std::vector<MerkleTree> trees;  // trees[0]: circle layer (L = n); trees[k]: line[k-1] (L = n-k)
+  std::vector<void*> allocs;
+  uint64_t* d_gather_addr = nullptr;
+  uint32_t* d_gather_out = nullptr;
+  size_t gather_cap = 0;
+
+  ~SeededFriProver() {
+    if (s) cudaStreamSynchronize(s);
+    for (void* p : allocs) cudaFree(p);
+    if (ev_in) cudaEventDestroy(ev_in);
+    if (ev_out) cudaEventDestroy(ev_out);
+    if (s) cudaStreamDestroy(s);
+  }
+  int alloc(void** p, size_t bytes, char* err, size_t err_len) {
+    STWO_CUDA_TRY(cudaMalloc(p, std::max<size_t>(bytes, 16)));
+    allocs.push_back(*p);
+    return 0;
+  }
+  int init(uint32_t log_n, int m31_output, const uint32_t* d_itw, uint32_t tree_log_size, cudaStream_t stream,
+           char* err, size_t err_len) {
+    STWO_ARG_CHECK(log_n >= 2 && log_n <= 28, "log_size %u out of range [2, 28]", log_n);
+    STWO_ARG_CHECK(d_itw && log_n - 1 <= tree_log_size, "twiddle tree (log %u) too small", tree_log_size);
+    n = log_n;
+    m31 = m31_output;
+    itw = d_itw;
+    tree_log = tree_log_size;
+    user_s = stream;
+    STWO_CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    STWO_CUDA_TRY(cudaEventCreateWithFlags(&ev_in, cudaEventDisableTiming));
+    STWO_CUDA_TRY(cudaEventCreateWithFlags(&ev_out, cudaEventDisableTiming));
+    int rc;
+    line.resize(n);
+    for (uint32_t k = 0; k < n; k++)
+      if ((rc = alloc((void**)&line[k], 16ull << (n - 1 - k), err, err_len))) return rc;
+    trees.resize(n);
+    for (uint32_t k = 0; k < n; k++) {
+      trees[k].L = n - k;
+      if ((rc = alloc((void**)&trees[k].base, MerkleTree::bytes_for(n - k), err, err_len))) return rc;
+    }
+    return 0;
+  }
+  static std::vector<uint32_t*> cols4(uint32_t* base, uint32_t log_size) {
+    std::vector<uint32_t*> c(4);
+    for (int k = 0; k < 4; k++) c[k] = base + ((uint64_t)k << log_size);
+    return c;
+  }
+  int commit_layer(const uint32_t* const* c4, const MerkleTree& t, char* err, size_t err_len) {
+    std::vector<uint8_t*> layers(t.L + 1);
+    for (uint32_t k = 0; k <= t.L; k++) layers[k] = t.layer(k);
+    const uint32_t lg[4] = {t.L, t.L, t.L, t.L};
+    return stwo_b200_merkle_build_layers(c4, lg, 4, t.L, m31, layers.data(), s, err, err_len);
+  }
+
+  int prove(const uint32_t* const* d_coords, const uint32_t* alphas, const uint64_t* queries_in, uint32_t n_q,
+            ProofOut& out, char* err, size_t err_len) {
+    std::vector<size_t> queries(queries_in, queries_in + n_q);
+    for (uint32_t i = 0; i < n_q; i++) {
+      STWO_ARG_CHECK(queries[i] >> n == 0, "query %zu out of range", queries[i]);
+      STWO_ARG_CHECK(i == 0 || queries[i] > queries[i - 1], "queries must be sorted and distinct");
+    }
+    STWO_CUDA_TRY(cudaEventRecord(ev_in, user_s));
+    STWO_CUDA_TRY(cudaStreamWaitEvent(s, ev_in, 0));
+    int rc;
+    // ---- commit (prover/fri.rs:133-291) ----
+    if ((rc = commit_layer(d_coords, trees[0], err, err_len))) return rc;
+    STWO_CUDA_TRY(cudaMemsetAsync(line[0], 0, 16ull << (n - 1), s));  // fold_circle_into_line accumulates
+    auto l0 = cols4(line[0], n - 1);
+    if ((rc = stwo_b200_fold_circle_into_line(l0.data(), d_coords, n, 1ull << (31 - (n + 1)), alphas, itw, tree_log,
+                                              s, err, err_len)))
+      return rc;
+    for (uint32_t k = 1; k < n; k++) {
+      const uint32_t L = n - k;  // log size of line[k-1]
+      auto cur = cols4(line[k - 1], L);
+      auto nxt = cols4(line[k], L - 1);
+      if ((rc = commit_layer(cur.data(), trees[k], err, err_len))) return rc;
+      if ((rc = stwo_b200_fold_line(const_cast<const uint32_t* const*>(cur.data()), L, alphas + 4 * k, 1, itw,
+                                    tree_log, nxt.data(), s, err, err_len)))
+        return rc;
+    }
+    // ---- decommit (prover/fri.rs:294-350, 459-488): one gather ----
+    GatherPlan g;
+    struct LayerPlan {
+      std::vector<bool> is_query;
+      std::vector<size_t> value_slot, node_slot;
+    };
+    auto plan = [&](const uint32_t* const* c4, const MerkleTree& t, const std::vector<size_t>& q) {
+      LayerPlan d;
+      std::vector<size_t> positions;
+      for (size_t i = 0; i < q.size();) {
+        size_t j = i;
+        while (j < q.size() && (q[j] >> 1) == (q[i] >> 1)) j++;
+        const size_t start = (q[i] >> 1) << 1;
+        size_t k = i;
+        for (size_t pos = start; pos < start + 2; pos++) {
+          const bool isq = k < j && q[k] == pos;
+          if (isq) k++;
+          positions.push_back(pos);
+          d.is_query.push_back(isq);
+          d.value_slot.push_back(g.add_word(c4[0] + pos));
+          for (int c = 1; c < 4; c++) g.add_word(c4[c] + pos);
+        }
+        i = j;
+      }
+      for (auto& nd : witness_nodes(positions, t.L)) d.node_slot.push_back(g.add_hash(t.layer(nd.first) + nd.second * 32));
+      return d;
+    };
+    std::vector<LayerPlan> plans;
+    plans.push_back(plan(d_coords, trees[0], queries));
+    std::vector<size_t> lq;
+    for (size_t q : queries)
+      if (lq.empty() || lq.back() != (q >> 1)) lq.push_back(q >> 1);
+    for (uint32_t k = 1; k < n; k++) {
+      auto cur = cols4(line[k - 1], n - k);
+      plans.push_back(plan(cur.data(), trees[k], lq));
+      std::vector<size_t> nq;
+      for (size_t q : lq)
+        if (nq.empty() || nq.back() != (q >> 1)) nq.push_back(q >> 1);
+      lq = nq;
+    }
+    const size_t last_slot = g.add_word(line[n - 1]);
+    for (int c = 1; c < 4; c++) g.add_word(line[n - 1] + c);
+    std::vector<size_t> root_slot(n);
+    for (uint32_t k = 0; k < n; k++) root_slot[k] = g.add_hash(trees[k].layer(0));
+    const size_t total = g.addrs.size();
+    if (total > gather_cap) {
+      const size_t cap = std::max<size_t>(total, 4096);
+      if ((rc = alloc((void**)&d_gather_addr, cap * 8, err, err_len))) return rc;
+      if ((rc = alloc((void**)&d_gather_out, cap * 4, err, err_len))) return rc;
+      gather_cap = cap;
+    }
+    STWO_CUDA_TRY(cudaMemcpyAsync(d_gather_addr, g.addrs.data(), total * 8, cudaMemcpyHostToDevice, s));
+    gather_kernel<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(d_gather_addr, (uint32_t)total, d_gather_out);
+    STWO_CHECK_LAUNCH();
+    std::vector<uint32_t> words(total);
+    STWO_CUDA_TRY(cudaMemcpyAsync(words.data(), d_gather_out, total * 4, cudaMemcpyDeviceToHost, s));
+    STWO_CUDA_TRY(cudaStreamSynchronize(s));
+    // ---- serialize: FriLayerProof order of core/fri.rs:361-395 ----
+    auto layer = [&](const LayerPlan& d, size_t rs) {
+      size_t n_w = 0;
+      for (bool b : d.is_query) n_w += b ? 0 : 1;
+      out.u64(n_w);
+      for (size_t i = 0; i < d.is_query.size(); i++)
+        if (!d.is_query[i]) {
+          const size_t sl = d.value_slot[i];
+          out.q({words[sl], words[sl + 1], words[sl + 2], words[sl + 3]});
+        }
+      out.u64(d.node_slot.size());
+      for (size_t sl : d.node_slot) out.h(reinterpret_cast<const uint8_t*>(words.data() + sl));
+      out.h(reinterpret_cast<const uint8_t*>(words.data() + rs));
+    };
+    layer(plans[0], root_slot[0]);
+    out.u64(n - 1);
+    for (uint32_t k = 1; k < n; k++) layer(plans[k], root_slot[k]);
+    out.u64(1);
+    out.q({words[last_slot], words[last_slot + 1], words[last_slot + 2], words[last_slot + 3]});
+    cudaEventRecord(ev_out, s);
+    cudaStreamWaitEvent(user_s, ev_out, 0);
+    return 0;
+  }
+};
+
 }  // namespace stwo_b200
 
 using namespace stwo_b200;
@@ -2000,6 +2175,45 @@ extern "C" int stwo_b200_prove_wide_fib(stwo_b200_prover* p, const uint32_t* d_a
   STWO_ARG_CHECK(p && d_a && d_b && proof_len, "null argument");
   ProofOut out;
   int rc = p->impl->prove(d_a, d_b, out, err, err_len);
+  if (rc) return rc;
+  *proof_len = out.bytes.size();
+  if (proof_out) {
+    STWO_ARG_CHECK(proof_cap >= out.bytes.size(), "proof buffer too small (%zu < %zu)", proof_cap, out.bytes.size());
+    std::memcpy(proof_out, out.bytes.data(), out.bytes.size());
+  }
+  return ok(err, err_len);
+}
+
+struct stwo_b200_fri_prover {
+  std::unique_ptr<SeededFriProver> impl;
+};
+
+extern "C" int stwo_b200_fri_prover_create(uint32_t log_size, int m31_output, const uint32_t* d_itwiddles,
+                                           uint32_t tree_log_size, void* stream, stwo_b200_fri_prover** out,
+                                           char* err, size_t err_len) {
+  STWO_ARG_CHECK(out, "null argument");
+  *out = nullptr;
+  auto p = std::make_unique<stwo_b200_fri_prover>();
+  p->impl = std::make_unique<SeededFriProver>();
+  int rc = p->impl->init(log_size, m31_output, d_itwiddles, tree_log_size, as_stream(stream), err, err_len);
+  if (rc) return rc;
+  *out = p.release();
+  return ok(err, err_len);
+}
+
+extern "C" int stwo_b200_fri_prover_destroy(stwo_b200_fri_prover* p, char* err, size_t err_len) {
+  delete p;
+  return ok(err, err_len);
+}
+
+extern "C" int stwo_b200_fri_prove_seeded(stwo_b200_fri_prover* p, const uint32_t* const* d_coords4,
+                                          const uint32_t* alphas, const uint64_t* queries, uint32_t n_queries,
+                                          uint8_t* proof_out, size_t proof_cap, size_t* proof_len, char* err,
+                                          size_t err_len) {
+  STWO_ARG_CHECK(p && d_coords4 && alphas && proof_len && (queries || n_queries == 0), "null argument");
+  STWO_ARG_CHECK(n_queries >= 1, "at least one query");
+  ProofOut out;
+  int rc = p->impl->prove(d_coords4, alphas, queries, n_queries, out, err, err_len);
   if (rc) return rc;
   *proof_len = out.bytes.size();
   if (proof_out) {

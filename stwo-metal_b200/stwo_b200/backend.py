@@ -287,6 +287,7 @@ class Committer:
                  graph: bool = False, stream=None):
         ffi.init()
         self.stream = as_stream(stream)
+        self._tree = tree  # the library keeps its device pointers: keep the buffers alive
         self.log_sizes = [int(x) for x in log_sizes]
         flags = (1 if per_column else 0) | (2 if graph else 0)
         h = C.c_void_p()

@@ -4,6 +4,8 @@ from __future__ import annotations
 
 import ctypes as C
 
+import numpy as np
+
 from . import ffi
 from .backend import DeviceColumn, as_stream
 
@@ -50,6 +52,44 @@ class WideFibProver:
         if getattr(self, "handle", None):
             ffi.call("stwo_b200_prover_destroy", self.handle)
             self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class SeededFriProver:
+    """FriProver commit + decommit of one secure column with supplied alphas
+    (crates/stwo/src/prover/fri.rs:133-350): every layer folded by 2 down to one
+    value, a Blake2s tree per layer, the queried decommitments.  ``prove``
+    returns the FriProof bytes in the proof's canonical layout."""
+
+    def __init__(self, log_size: int, tree, m31: bool = False, stream=None):
+        ffi.init()
+        self.log_size = log_size
+        self.stream = as_stream(stream)
+        self._tree = tree  # the library keeps its device pointers: keep the buffers alive
+        h = C.c_void_p()
+        ffi.call("stwo_b200_fri_prover_create", C.c_uint32(log_size), C.c_int(1 if m31 else 0),
+                 C.c_void_p(tree.itwiddles.ptr), C.c_uint32(tree.log_size), self.stream, C.byref(h))
+        self._h = h
+
+    def prove(self, coords, alphas, queries, cap: int = 1 << 24) -> bytes:
+        a = np.ascontiguousarray(alphas, dtype=np.uint32).reshape(-1)
+        q = np.ascontiguousarray(queries, dtype=np.uint64)
+        ptrs = (C.c_void_p * 4)(*[c.ptr for c in coords])
+        buf = (C.c_uint8 * cap)()
+        n = C.c_size_t()
+        ffi.call("stwo_b200_fri_prove_seeded", self._h, ptrs, a.ctypes.data_as(C.POINTER(C.c_uint32)),
+                 q.ctypes.data_as(C.POINTER(C.c_uint64)), C.c_uint32(q.size), buf, C.c_size_t(cap), C.byref(n))
+        return bytes(buf[:n.value])
+
+    def close(self):
+        if self._h:
+            ffi.call("stwo_b200_fri_prover_destroy", self._h)
+            self._h = None
 
     def __del__(self):
         try:
