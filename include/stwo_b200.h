@@ -273,6 +273,18 @@ int stwo_b200_prover_destroy(stwo_b200_prover* prover, char* err, size_t err_len
 int stwo_b200_prove_wide_fib(stwo_b200_prover* prover, const uint32_t* d_a, const uint32_t* d_b,
                              uint8_t* proof_out, size_t proof_cap, size_t* proof_len, char* err, size_t err_len);
 
+/* The same proof with n_cols (3..the prover's n_cols) trace columns: the
+ * buffers are sized for the prover's n_cols and any narrower trace of the
+ * same log_n_rows reuses them.  No reference counterpart (a resident prover
+ * of the serving loop). */
+int stwo_b200_prove_wide_fib_cols(stwo_b200_prover* prover, uint32_t n_cols, const uint32_t* d_a,
+                                  const uint32_t* d_b, uint8_t* proof_out, size_t proof_cap, size_t* proof_len,
+                                  char* err, size_t err_len);
+/* Device bytes a prover of this configuration allocates (computed, nothing is
+ * allocated; host-only, needs no GPU).  For HBM admission. */
+int stwo_b200_prover_footprint(const stwo_b200_wide_fib_config* cfg, size_t* device_bytes, char* err,
+                               size_t err_len);
+
 /* Per-phase device time (CUDA events on the prover's stream), accumulated over
  * the proofs made since timing was enabled.  Phases, in order: 0 trace
  * generation, 1 trace interpolate, 2 trace evaluate, 3 trace Merkle,
@@ -284,6 +296,37 @@ int stwo_b200_prove_wide_fib(stwo_b200_prover* prover, const uint32_t* d_a, cons
 int stwo_b200_prover_set_timing(stwo_b200_prover* prover, int enable, char* err, size_t err_len);
 int stwo_b200_prover_phase_times(stwo_b200_prover* prover, double* ms_out, uint32_t n, uint32_t* proofs, char* err,
                                  size_t err_len);
+
+/* ---------------------------------------------------------- serving ------ */
+/* Continuous batching of Wide-Fibonacci prove requests on the current GPU
+ * (no reference counterpart: the reference proves one request at a time).
+ * `slots` requests run at once, each on its own resident prover and stream;
+ * provers (buffers, twiddles, captured FRI graph) stay resident per (log_n,
+ * width class = n_cols rounded up to a multiple of 64, PCS config) and are
+ * evicted least recently used when a new one must fit hbm_budget_bytes.  A
+ * request waits until a slot is free and its prover is idle or fits; the
+ * queue is scanned in arrival order.  A proof is the same as when the request
+ * is proved alone. */
+typedef struct stwo_b200_server stwo_b200_server;
+typedef struct stwo_b200_server_stats {
+  uint64_t completed, provers_created, provers_reused, provers_evicted;
+  uint64_t resident_bytes;
+  uint32_t residents, max_running, queued, pad;
+} stwo_b200_server_stats;
+int stwo_b200_server_create(size_t hbm_budget_bytes, uint32_t slots, stwo_b200_server** out, char* err,
+                            size_t err_len);
+/* Finishes every submitted request, then frees the resident provers. */
+int stwo_b200_server_destroy(stwo_b200_server* server, char* err, size_t err_len);
+/* Copies the two input columns (host, 2^log_n_rows words each) and queues the
+ * request; fails at once when its prover could never fit the budget. */
+int stwo_b200_server_submit(stwo_b200_server* server, const stwo_b200_wide_fib_config* cfg, const uint32_t* a,
+                            const uint32_t* b, uint64_t* ticket, char* err, size_t err_len);
+/* Blocks until the request is done; writes its proof and, when times_ms is
+ * non-NULL, [queued, on a prover, latency] in milliseconds.  Returns the
+ * request's own status. */
+int stwo_b200_server_wait(stwo_b200_server* server, uint64_t ticket, uint8_t* proof_out, size_t proof_cap,
+                          size_t* proof_len, double* times_ms, char* err, size_t err_len);
+int stwo_b200_server_get_stats(stwo_b200_server* server, stwo_b200_server_stats* out, char* err, size_t err_len);
 
 /* ------------------------------------------------ FRI commit + decommit -- */
 /* FriProver::commit + decommit (crates/stwo/src/prover/fri.rs:133-350) of one

@@ -1100,8 +1100,8 @@ class WideFibProver {
     proofs_timed++;
   }
   stwo_b200_wide_fib_config cfg;
-  uint32_t log_n, N, blowup, eval_log, L1, L2, lift, tree_log;
-  cudaStream_t s;
+  uint32_t log_n = 0, N = 0, blowup = 0, eval_log = 0, L1 = 0, L2 = 0, lift = 0, tree_log = 0;
+  cudaStream_t s = nullptr;  // the prover's own stream (none in measure mode)
 
   uint32_t *d_tw = nullptr, *d_itw = nullptr;
   uint32_t* d_coeffs = nullptr;   // N x 2^log_n (trace, then coefficients)
@@ -1149,13 +1149,24 @@ class WideFibProver {
     if (ev_in) cudaEventDestroy(ev_in);
     if (ev_out) cudaEventDestroy(ev_out);
     for (cudaEvent_t e : ev_pool) cudaEventDestroy(e);
-    for (void* p : allocs) cudaFree(p);
+    for (void* p : allocs) cudaFree(p);  // empty in measure mode
     if (h_pinned) cudaFreeHost(h_pinned);
     if (h_chan) cudaFreeHost(h_chan);
     if (s) cudaStreamDestroy(s);
   }
 
+  // measure: run init's allocation arithmetic only (no device work), for the
+  // footprint query; allocated_bytes sums every device allocation.
+  bool measure = false;
+  size_t allocated_bytes = 0;
+  uint32_t N_cap = 0;  // columns the buffers hold; a proof may use 3..N_cap
+
   int alloc(void** p, size_t bytes, char* err, size_t err_len) {
+    allocated_bytes += std::max<size_t>(bytes, 16);
+    if (measure) {
+      *p = reinterpret_cast<void*>(uintptr_t{256});  // never dereferenced
+      return 0;
+    }
     STWO_CUDA_TRY(cudaMalloc(p, std::max<size_t>(bytes, 16)));
     allocs.push_back(*p);
     return 0;
@@ -1164,18 +1175,21 @@ class WideFibProver {
   int init(const stwo_b200_wide_fib_config& c, cudaStream_t stream, char* err, size_t err_len) {
     cfg = c;
     user_s = stream;
-    STWO_CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
-    STWO_CUDA_TRY(cudaEventCreateWithFlags(&ev_in, cudaEventDisableTiming));
-    STWO_CUDA_TRY(cudaEventCreateWithFlags(&ev_out, cudaEventDisableTiming));
-    STWO_CUDA_TRY(cudaFuncSetAttribute(fri_tail_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFriTailSmem));
-    STWO_CUDA_TRY(
-        cudaFuncSetAttribute(tree_top_channel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFriTailSmem));
-    STWO_CUDA_TRY(
-        cudaFuncSetAttribute(composition_tma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kStreamSmem));
-    STWO_CUDA_TRY(
-        cudaFuncSetAttribute(quotient_tma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kStreamSmem));
+    if (!measure) {
+      STWO_CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+      STWO_CUDA_TRY(cudaEventCreateWithFlags(&ev_in, cudaEventDisableTiming));
+      STWO_CUDA_TRY(cudaEventCreateWithFlags(&ev_out, cudaEventDisableTiming));
+      STWO_CUDA_TRY(
+          cudaFuncSetAttribute(fri_tail_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFriTailSmem));
+      STWO_CUDA_TRY(cudaFuncSetAttribute(tree_top_channel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)kFriTailSmem));
+      STWO_CUDA_TRY(
+          cudaFuncSetAttribute(composition_tma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kStreamSmem));
+      STWO_CUDA_TRY(
+          cudaFuncSetAttribute(quotient_tma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kStreamSmem));
+    }
     log_n = c.log_n_rows;
-    N = c.n_cols;
+    N = N_cap = c.n_cols;
     blowup = c.log_blowup;
     STWO_ARG_CHECK(N >= 3 && N <= kMaxPolys - 8, "n_cols %u out of range [3, %d]", N, kMaxPolys - 8);
     STWO_ARG_CHECK(log_n >= 4 && log_n + blowup <= 28, "log_n_rows %u / log_blowup %u out of range", log_n, blowup);
@@ -1195,8 +1209,10 @@ class WideFibProver {
     if ((rc = alloc((void**)&d_tw, 4ull << tree_log, err, err_len))) return rc;
     if ((rc = alloc((void**)&d_itw, 4ull << tree_log, err, err_len))) return rc;
     // CanonicCoset(tree_log + 1).half_coset = half_odds(tree_log): initial index 2^(31 - (tree_log + 2)).
-    rc = stwo_b200_precompute_twiddles(1ull << (31 - (tree_log + 2)), tree_log, d_tw, d_itw, s, err, err_len);
-    if (rc) return rc;
+    if (!measure) {
+      rc = stwo_b200_precompute_twiddles(1ull << (31 - (tree_log + 2)), tree_log, d_tw, d_itw, s, err, err_len);
+      if (rc) return rc;
+    }
     if ((rc = alloc((void**)&d_coeffs, (4ull * N) << log_n, err, err_len))) return rc;
     if ((rc = alloc((void**)&d_evals, (4ull * N) << L1, err, err_len))) return rc;
     if (eval_log != L1 && (rc = alloc((void**)&d_ext, (4ull * N) << eval_log, err, err_len))) return rc;
@@ -1237,6 +1253,7 @@ class WideFibProver {
     if ((rc = alloc((void**)&d_chan, sizeof(DevChannel), err, err_len))) return rc;
     if ((rc = alloc((void**)&d_alphas, (fri.size() + 2) * sizeof(qm31), err, err_len))) return rc;
     h_pinned_bytes = std::max<size_t>(small_q * sizeof(qm31), 16ull << last_log);
+    if (measure) return 0;
     STWO_CUDA_TRY(cudaMallocHost((void**)&h_pinned, h_pinned_bytes));
     STWO_CUDA_TRY(cudaMallocHost((void**)&h_chan, sizeof(DevChannel)));
     STWO_CUDA_TRY(cudaStreamSynchronize(s));
@@ -1387,7 +1404,10 @@ class WideFibProver {
                                          t.L, cfg.m31_channel, layers.data(), s, err, err_len);
   }
 
-  int prove(const uint32_t* d_a, const uint32_t* d_b, ProofOut& out, char* err, size_t err_len) {
+  int prove(const uint32_t* d_a, const uint32_t* d_b, ProofOut& out, char* err, size_t err_len,
+            uint32_t n_cols = 0) {
+    STWO_ARG_CHECK(n_cols == 0 || (n_cols >= 3 && n_cols <= N_cap), "n_cols %u out of range [3, %u]", n_cols, N_cap);
+    N = n_cols ? n_cols : N_cap;
     STWO_CUDA_TRY(cudaEventRecord(ev_in, user_s));
     STWO_CUDA_TRY(cudaStreamWaitEvent(s, ev_in, 0));
     const int rc = prove_body(d_a, d_b, out, err, err_len);
@@ -2166,6 +2186,33 @@ extern "C" int stwo_b200_prover_phase_times(stwo_b200_prover* p, double* ms_out,
   STWO_ARG_CHECK(p && ms_out, "null argument");
   for (uint32_t i = 0; i < n && i < (uint32_t)kNumPhases; i++) ms_out[i] = p->impl->phase_ms[i];
   if (proofs) *proofs = p->impl->proofs_timed;
+  return ok(err, err_len);
+}
+
+extern "C" int stwo_b200_prover_footprint(const stwo_b200_wide_fib_config* cfg, size_t* device_bytes, char* err,
+                                          size_t err_len) {
+  STWO_ARG_CHECK(cfg && device_bytes, "null argument");
+  WideFibProver m;
+  m.measure = true;
+  int rc = m.init(*cfg, nullptr, err, err_len);
+  if (rc) return rc;
+  // + the decommitment gather buffers sized at the first proof
+  *device_bytes = m.allocated_bytes + ((size_t)4 << 20);
+  return ok(err, err_len);
+}
+
+extern "C" int stwo_b200_prove_wide_fib_cols(stwo_b200_prover* p, uint32_t n_cols, const uint32_t* d_a,
+                                             const uint32_t* d_b, uint8_t* proof_out, size_t proof_cap,
+                                             size_t* proof_len, char* err, size_t err_len) {
+  STWO_ARG_CHECK(p && d_a && d_b && proof_len, "null argument");
+  ProofOut out;
+  int rc = p->impl->prove(d_a, d_b, out, err, err_len, n_cols);
+  if (rc) return rc;
+  *proof_len = out.bytes.size();
+  if (proof_out) {
+    STWO_ARG_CHECK(proof_cap >= out.bytes.size(), "proof buffer too small (%zu < %zu)", proof_cap, out.bytes.size());
+    std::memcpy(proof_out, out.bytes.data(), out.bytes.size());
+  }
   return ok(err, err_len);
 }
 

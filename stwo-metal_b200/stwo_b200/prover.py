@@ -42,6 +42,14 @@ class WideFibProver:
                  C.c_size_t(cap), C.byref(n))
         return bytes(buf[:n.value])
 
+    def prove_cols(self, a: DeviceColumn, b: DeviceColumn, n_cols: int, cap: int = 1 << 22) -> bytes:
+        """The proof of an n_cols-wide trace (3 <= n_cols <= the prover's width)."""
+        buf = (C.c_uint8 * cap)()
+        n = C.c_size_t()
+        ffi.call("stwo_b200_prove_wide_fib_cols", self.handle, C.c_uint32(n_cols), C.c_void_p(a.ptr),
+                 C.c_void_p(b.ptr), buf, C.c_size_t(cap), C.byref(n))
+        return bytes(buf[:n.value])
+
     def prove_into(self, a_ptr: int, b_ptr: int, out_buf, cap: int) -> int:
         n = C.c_size_t()
         ffi.call("stwo_b200_prove_wide_fib", self.handle, C.c_void_p(a_ptr), C.c_void_p(b_ptr), out_buf,
@@ -89,6 +97,65 @@ class SeededFriProver:
     def close(self):
         if self._h:
             ffi.call("stwo_b200_fri_prover_destroy", self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def prover_footprint(cfg: WideFibConfig) -> int:
+    """Device bytes a prover of this configuration allocates (host-only query)."""
+    n = C.c_size_t()
+    ffi.call("stwo_b200_prover_footprint", C.byref(cfg), C.byref(n))
+    return n.value
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("completed", C.c_uint64), ("provers_created", C.c_uint64), ("provers_reused", C.c_uint64),
+                ("provers_evicted", C.c_uint64), ("resident_bytes", C.c_uint64), ("residents", C.c_uint32),
+                ("max_running", C.c_uint32), ("queued", C.c_uint32), ("pad", C.c_uint32)]
+
+
+class ProveServer:
+    """Continuous batching of Wide-Fibonacci prove requests on the current GPU:
+    ``slots`` requests run at once on resident provers (kept per log size and
+    width class), admitted under an HBM budget with LRU eviction of idle
+    provers.  ``submit`` copies the inputs and returns a ticket; ``wait``
+    returns (proof bytes, {queued_ms, service_ms, latency_ms})."""
+
+    def __init__(self, hbm_budget_bytes: int, slots: int = 3):
+        ffi.init()
+        h = C.c_void_p()
+        ffi.call("stwo_b200_server_create", C.c_size_t(hbm_budget_bytes), C.c_uint32(slots), C.byref(h))
+        self._h = h
+
+    def submit(self, cfg: WideFibConfig, a, b) -> int:
+        a = np.ascontiguousarray(a, dtype=np.uint32)
+        b = np.ascontiguousarray(b, dtype=np.uint32)
+        assert a.size == b.size == 1 << cfg.log_n_rows
+        t = C.c_uint64()
+        ffi.call("stwo_b200_server_submit", self._h, C.byref(cfg), a.ctypes.data_as(C.POINTER(C.c_uint32)),
+                 b.ctypes.data_as(C.POINTER(C.c_uint32)), C.byref(t))
+        return t.value
+
+    def wait(self, ticket: int, cap: int = 1 << 24):
+        buf = (C.c_uint8 * cap)()
+        n = C.c_size_t()
+        times = (C.c_double * 3)()
+        ffi.call("stwo_b200_server_wait", self._h, C.c_uint64(ticket), buf, C.c_size_t(cap), C.byref(n), times)
+        return bytes(buf[:n.value]), {"queued_ms": times[0], "service_ms": times[1], "latency_ms": times[2]}
+
+    def stats(self) -> dict:
+        st = ServerStats()
+        ffi.call("stwo_b200_server_get_stats", self._h, C.byref(st))
+        return {k: getattr(st, k) for k, _ in ServerStats._fields_ if k != "pad"}
+
+    def close(self):
+        if self._h:
+            ffi.call("stwo_b200_server_destroy", self._h)
             self._h = None
 
     def __del__(self):
