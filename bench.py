@@ -877,6 +877,130 @@ def run_fri_b200(args, world, rank, local):
     print(json.dumps(line), flush=True)
 
 
+# --------------------------------------------------------------- serving -----
+SERVE_SEED, SERVE_SLOTS, SERVE_BUDGET = 5, 3, 120 << 30
+
+
+def serving_requests(n):
+    """Seeded prove requests: width U{64..256}, log_n_rows U{14..22}; inputs are
+    generated per request from the request's own seed."""
+    r = np.random.default_rng(SERVE_SEED)
+    return [(int(r.integers(14, 23)), int(r.integers(64, 257)), 10_000 + i) for i in range(n)]
+
+
+def serving_inputs(log_n, seed):
+    r = np.random.default_rng(seed)
+    n = 1 << log_n
+    return r.integers(0, P, n, dtype=np.uint32), r.integers(0, P, n, dtype=np.uint32)
+
+
+def run_stream(srv, reqs, inputs, arrivals):
+    """Submits reqs at the given arrival offsets (seconds) to the server and
+    collects every proof and its latency; returns (proofs, times, makespan_s, stats)."""
+    from stwo_b200 import wide_fib_config
+    tickets = [None] * len(reqs)
+    t0 = time.perf_counter()
+    for i, (ln, nc, _) in enumerate(reqs):
+        delay = arrivals[i] - (time.perf_counter() - t0)
+        if delay > 0:
+            time.sleep(delay)
+        a, b = inputs[i]
+        tickets[i] = srv.submit(wide_fib_config(ln, nc), a, b)
+    out = [srv.wait(t) for t in tickets]
+    makespan = time.perf_counter() - t0
+    return [o[0] for o in out], [o[1] for o in out], makespan, srv.stats()
+
+
+def run_serving_b200(args, world, rank, local):
+    import torch
+    from oracle import ffi as oracle
+    from stwo_b200 import ffi
+
+    torch.cuda.set_device(local)
+    ffi.init(local)
+    n_req = max(24, 8 * args.steps)
+    reqs = serving_requests(n_req)
+    inputs = [serving_inputs(ln, sd) for ln, _, sd in reqs]
+    cells = sum(nc << ln for ln, nc, _ in reqs)
+    from stwo_b200 import ProveServer
+    batched = ProveServer(SERVE_BUDGET, slots=SERVE_SLOTS)
+    serial = ProveServer(SERVE_BUDGET, slots=1)
+    # warm-up: the whole request list once through each server (resident
+    # provers built up to the budget, kernels loaded, FRI graphs captured)
+    for _ in range(max(1, min(args.warmup, 2))):
+        run_stream(batched, reqs, inputs, [0.0] * n_req)
+        run_stream(serial, reqs, inputs, [0.0] * n_req)
+    # capacity: everything submitted at once, serial (1 slot) and batched
+    barrier(world)
+    torch.cuda.synchronize()
+    p_ser, t_ser_sat, mk_ser, _ = run_stream(serial, reqs, inputs, [0.0] * n_req)
+    p_sat, t_sat, mk_sat, st_sat = run_stream(batched, reqs, inputs, [0.0] * n_req)
+    cap_batched = n_req / mk_sat
+    # Poisson arrivals at 70% of the batched capacity, the same schedule for
+    # the batched server and for serial proving.
+    rate = 0.7 * cap_batched
+    gaps = np.random.default_rng(SERVE_SEED + 1).exponential(1.0 / rate, n_req)
+    arrivals = np.cumsum(gaps) - gaps[0]
+    sampler = ClockSampler(local)
+    sampler.start()
+    p_srv, t_srv, mk_srv, st_srv = run_stream(batched, reqs, inputs, arrivals)
+    clocks = sampler.stop()
+    p_ser2, t_ser2, mk_ser2, _ = run_stream(serial, reqs, inputs, arrivals)
+    batched.close()
+    serial.close()
+    barrier(world)
+    exact_mix = all(a == b for a, b in zip(p_srv, p_ser)) and all(a == b for a, b in zip(p_sat, p_ser))
+    exact_serial = all(a == b for a, b in zip(p_ser2, p_ser))
+    rejected = [i for i, (ln, nc, _) in enumerate(reqs)
+                if oracle.verify_wide_fib(p_srv[i], ln, nc) is not None]
+
+    def pct(xs, q):
+        xs = sorted(xs)
+        return xs[min(len(xs) - 1, int(q * len(xs)))]
+
+    lat = [t["latency_ms"] for t in t_srv]
+    lat_ser = [t["latency_ms"] for t in t_ser2]
+    if rank != 0:
+        return
+    # CPU baseline: the oracle proving the smallest request of the stream
+    small = min(range(n_req), key=lambda i: reqs[i][1] << reqs[i][0])
+    ln, nc, _ = reqs[small]
+    a, b = inputs[small]
+    n_threads = oracle.set_threads(os.cpu_count() or 1)
+    t0 = time.perf_counter()
+    cpu_proof = oracle.prove_wide_fib(oracle.wide_fib_config(ln, nc), a, b)
+    cpu_s = time.perf_counter() - t0
+    line = {
+        "metric": METRIC, "value": cells / mk_srv * world, "unit": "proved trace cells/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * mk_srv,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32 (M31/QM31)",
+        "data": "synthetic (seeded numpy PCG64)",
+        "config": {"workload": "serving", "requests": n_req, "widths": "U{64..256}", "log_n_rows": "U{14..22}",
+                   "seed": SERVE_SEED, "arrivals": "Poisson at 70% of the measured batched capacity",
+                   "slots": SERVE_SLOTS, "hbm_budget_bytes": SERVE_BUDGET,
+                   "step": f"one stream of {n_req} requests (host steady clock, submit to proof bytes)",
+                   "parallelism": f"replicas x{world}"},
+        "p50_latency_ms": pct(lat, 0.5), "p99_latency_ms": pct(lat, 0.99),
+        "proofs_per_s": n_req / mk_srv,
+        "serial": {"p50_latency_ms": pct(lat_ser, 0.5), "p99_latency_ms": pct(lat_ser, 0.99),
+                   "proofs_per_s": n_req / mk_ser2, "saturated_proofs_per_s": n_req / mk_ser},
+        "capacity_proofs_per_s": {"batched": cap_batched, "serial": n_req / mk_ser},
+        "server_stats": st_srv,
+        "clocks": clocks,
+        "gpu_launches": None,
+        "e2e": {"value": cells / mk_srv * world, "unit": "proved trace cells/s",
+                "h2d_bytes_per_step": int(sum(8 << ln for ln, _, _ in reqs)),
+                "d2h_bytes_per_step": int(sum(len(p) for p in p_srv)), "ms_per_step": 1000 * mk_srv},
+        "bit_exact_mix_vs_alone": exact_mix and exact_serial,
+        "verifier_rejected": rejected,
+        "bit_exact_vs_oracle_sample": cpu_proof == p_srv[small],
+        "cpu_baseline": {"value": (nc << ln) / cpu_s, "unit": "proved trace cells/s", "cores": n_threads,
+                         "kind": "port", "sample": f"the stream's smallest request ({nc} x 2^{ln}) proved by the "
+                                                   "SimdBackend restatement (C++ oracle, OpenMP)"},
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -884,7 +1008,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="wide_fib_prove",
-                    choices=["wide_fib_prove", "commit_uneven", "commit_plain", "fri_heavy"])
+                    choices=["wide_fib_prove", "commit_uneven", "commit_plain", "fri_heavy", "serving"])
     ap.add_argument("--log-n-rows", type=int, default=20, help="wide_fib_prove: log2 of the trace rows")
     ap.add_argument("--n-cols", type=int, default=100, help="wide_fib_prove: trace columns")
     args = ap.parse_args()
@@ -896,6 +1020,13 @@ def main():
                 run_prove_reference(args, world, rank)
             else:
                 run_prove_b200(args, world, rank, local)
+        elif args.workload == "serving":
+            if args.impl == "reference":
+                if rank == 0:
+                    print(json.dumps({"impl": "reference", "unavailable": "the reference has no serving loop; "
+                                      "the oracle's per-proof rate is reported as cpu_baseline by the b200 arm"}))
+            else:
+                run_serving_b200(args, world, rank, local)
         elif args.workload == "fri_heavy":
             if args.impl == "reference":
                 run_fri_reference(args, world, rank)
