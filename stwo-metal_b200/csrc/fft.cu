@@ -475,33 +475,41 @@ __global__ void __launch_bounds__(256, 4) fft_warp_contig_kernel(FftPass p, FftC
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   uint32_t* col = smem + 1024 + warp * (32 * 33);
   const uint64_t hi = blockIdx.x;
+  const uint32_t c = blockIdx.y * kWarpCols + warp;
+  const bool active = c < p.n_cols;
+  const uint64_t base = hi << 10;
+  // The column tile's loads go out before the twiddle staging, so the two
+  // latencies overlap.
+  uint32_t v[32];
+  if (active) {
+    const uint32_t* __restrict__ src = cols.src[c];
+    if (INV) {
+      const uint4* s4 = reinterpret_cast<const uint4*>(src + base + lane * 32);
+#pragma unroll
+      for (int q = 0; q < 8; q++) {
+        const uint4 w = __ldg(s4 + q);
+        v[4 * q] = w.x;
+        v[4 * q + 1] = w.y;
+        v[4 * q + 2] = w.z;
+        v[4 * q + 3] = w.w;
+      }
+    } else {
+#pragma unroll
+      for (int j = 0; j < 32; j++) v[j] = __ldg(src + base + j * 32 + lane);
+    }
+  }
   stage_tws10(p, hi, tws);
   __syncthreads();
-  const uint32_t c = blockIdx.y * kWarpCols + warp;
-  if (c >= p.n_cols) return;  // no block barrier follows
-  const uint32_t* __restrict__ src = cols.src[c];
+  if (!active) return;  // no block barrier follows
   uint32_t* __restrict__ dst = cols.dst[c];
-  const uint64_t base = hi << 10;
   const uint32_t scale = p.scale;
-  uint32_t v[32];
   if (INV) {
-    const uint4* s4 = reinterpret_cast<const uint4*>(src + base + lane * 32);
-#pragma unroll
-    for (int q = 0; q < 8; q++) {
-      const uint4 w = __ldg(s4 + q);
-      v[4 * q] = w.x;
-      v[4 * q + 1] = w.y;
-      v[4 * q + 2] = w.z;
-      v[4 * q + 3] = w.w;
-    }
     warp_phase_lo<true>(v, tws, lane);
     warp_lo_to_hi(v, col, lane);
     warp_phase_hi<true>(v, tws);
 #pragma unroll
     for (int j = 0; j < 32; j++) dst[base + j * 32 + lane] = scale != 1u ? m31_mul(v[j], scale) : v[j];
   } else {
-#pragma unroll
-    for (int j = 0; j < 32; j++) v[j] = __ldg(src + base + j * 32 + lane);
     warp_phase_hi<false>(v, tws);
     warp_hi_to_lo(v, col, lane);
     warp_phase_lo<false>(v, tws, lane);

@@ -611,6 +611,15 @@ __global__ void gather_kernel(const uint64_t* __restrict__ addrs, uint32_t n, ui
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) out[i] = *reinterpret_cast<const uint32_t*>(addrs[i]);
 }
+// 32-byte hashes at 32-byte aligned addresses (Merkle tree nodes).
+__global__ void gather_hashes_kernel(const uint64_t* __restrict__ addrs, uint32_t n, uint4* __restrict__ out) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) {
+    const uint4* p = reinterpret_cast<const uint4*>(addrs[i]);
+    out[2 * i] = p[0];
+    out[2 * i + 1] = p[1];
+  }
+}
 
 // ---- device-side Fiat-Shamir steps of the FRI commit ----
 // The channel state lives in device memory so the FRI layer loop (commit a
@@ -744,20 +753,21 @@ __global__ void fold_line_dev_kernel(const uint32_t* __restrict__ in, uint32_t l
 
 // First FRI layer: dst = 0 * alpha^2 + fold(src) = fold(src) (prover/fri.rs:74-85
 // with a zero line evaluation), alpha from device memory; log_n > 4.
-__global__ void fold_circle_first_dev_kernel(const uint32_t* __restrict__ src, uint32_t log_n,
-                                             const qm31* __restrict__ d_alpha, const uint32_t* __restrict__ itw,
-                                             uint64_t tw_len, uint32_t* __restrict__ dst,
-                                             uint8_t* __restrict__ leaves, int m31) {
+struct Src4 {
+  const uint32_t* c[4];  // the four coordinate columns
+};
+__global__ void fold_circle_first_dev_kernel(Src4 src, uint32_t log_n, const qm31* __restrict__ d_alpha,
+                                             const uint32_t* __restrict__ itw, uint64_t tw_len,
+                                             uint32_t* __restrict__ dst, uint8_t* __restrict__ leaves, int m31) {
   const uint64_t n_in = 1ull << log_n, n_out = n_in >> 1;
   const uint32_t* lt0 = itw + (tw_len - (1ull << (log_n - 1)));
   qm31 alpha = *d_alpha;
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n_out; i += (uint64_t)gridDim.x * blockDim.x) {
     uint32_t b = __ldg(lt0 + ((i >> 1) ^ 1));
     uint32_t yinv = ((i ^ (i >> 1)) & 1) ? m31_neg(b) : b;
-    qm31 fp = {__ldg(src + 2 * i), __ldg(src + n_in + 2 * i), __ldg(src + 2 * n_in + 2 * i),
-               __ldg(src + 3 * n_in + 2 * i)};
-    qm31 fnp = {__ldg(src + 2 * i + 1), __ldg(src + n_in + 2 * i + 1), __ldg(src + 2 * n_in + 2 * i + 1),
-                __ldg(src + 3 * n_in + 2 * i + 1)};
+    qm31 fp = {__ldg(src.c[0] + 2 * i), __ldg(src.c[1] + 2 * i), __ldg(src.c[2] + 2 * i), __ldg(src.c[3] + 2 * i)};
+    qm31 fnp = {__ldg(src.c[0] + 2 * i + 1), __ldg(src.c[1] + 2 * i + 1), __ldg(src.c[2] + 2 * i + 1),
+                __ldg(src.c[3] + 2 * i + 1)};
     qm31 f0 = qm31_add(fp, fnp);
     qm31 f1 = qm31_mul_m31(qm31_sub(fp, fnp), yinv);
     qm31 v = qm31_add(qm31_zero(), qm31_add(f0, qm31_mul(alpha, f1)));
@@ -1311,8 +1321,9 @@ class WideFibProver {
       uint32_t* dst = fri.empty() ? d_last : fri[0].coords;
       uint8_t* leaves = tail0 > 0 ? fri[0].tree.layer(fri[0].log_size) : nullptr;
       if (lift <= 4) return set_err(err, err_len, STWO_B200_EARG, "lifting domain too small");
+      const Src4 q4{{d_quot, d_quot + (1ull << lift), d_quot + (2ull << lift), d_quot + (3ull << lift)}};
       fold_circle_first_dev_kernel<<<grid1d(1ull << (lift - 1), 256), 256, 0, s>>>(
-          d_quot, lift, d_alphas, d_itw, 1ull << tree_log, dst, leaves, m31 ? 1 : 0);
+          q4, lift, d_alphas, d_itw, 1ull << tree_log, dst, leaves, m31 ? 1 : 0);
       STWO_CHECK_LAUNCH();
     }
     for (size_t li = 0; li < tail0; li++) {
@@ -1986,12 +1997,22 @@ struct SeededFriProver {
   std::vector<uint32_t*> line;   // line[k]: 4 x 2^(n-1-k) words, k = 0..n-1 (line[n-1]: the last value)
   std::vector<MerkleTree> trees;  // trees[0]: circle layer (L = n); trees[k]: line[k-1] (L = n-k)
   std::vector<void*> allocs;
+  qm31* d_alphas = nullptr;  // the folding alphas (uploaded per call; read by the fold kernels)
+  qm31* h_alphas = nullptr;  // pinned staging of the alphas
   uint64_t* d_gather_addr = nullptr;
-  uint32_t* d_gather_out = nullptr;
-  size_t gather_cap = 0;
+  uint8_t* d_gather_out = nullptr;
+  size_t gather_cap = 0;     // entries (words or hashes)
+  uint8_t* h_stage = nullptr;  // pinned: addresses (8 B / entry), then gathered bytes (32 B / entry)
+  // the commit sequence, captured once per input column set
+  cudaGraphExec_t exec = nullptr;
+  const void* key[4] = {nullptr, nullptr, nullptr, nullptr};
+  uint64_t graph_launches = 0;
 
   ~SeededFriProver() {
     if (s) cudaStreamSynchronize(s);
+    if (exec) cudaGraphExecDestroy(exec);
+    if (h_stage) cudaFreeHost(h_stage);
+    if (h_alphas) cudaFreeHost(h_alphas);
     for (void* p : allocs) cudaFree(p);
     if (ev_in) cudaEventDestroy(ev_in);
     if (ev_out) cudaEventDestroy(ev_out);
@@ -2023,6 +2044,8 @@ struct SeededFriProver {
       trees[k].L = n - k;
       if ((rc = alloc((void**)&trees[k].base, MerkleTree::bytes_for(n - k), err, err_len))) return rc;
     }
+    if ((rc = alloc((void**)&d_alphas, n * sizeof(qm31), err, err_len))) return rc;
+    STWO_CUDA_TRY(cudaMallocHost((void**)&h_alphas, n * sizeof(qm31)));
     return 0;
   }
   static std::vector<uint32_t*> cols4(uint32_t* base, uint32_t log_size) {
@@ -2030,11 +2053,62 @@ struct SeededFriProver {
     for (int k = 0; k < 4; k++) c[k] = base + ((uint64_t)k << log_size);
     return c;
   }
-  int commit_layer(const uint32_t* const* c4, const MerkleTree& t, char* err, size_t err_len) {
-    std::vector<uint8_t*> layers(t.L + 1);
-    for (uint32_t k = 0; k <= t.L; k++) layers[k] = t.layer(k);
-    const uint32_t lg[4] = {t.L, t.L, t.L, t.L};
-    return stwo_b200_merkle_build_layers(c4, lg, 4, t.L, m31, layers.data(), s, err, err_len);
+  std::vector<uint8_t*> layer_ptrs(const MerkleTree& t) const {
+    std::vector<uint8_t*> l(t.L + 1);
+    for (uint32_t k = 0; k <= t.L; k++) l[k] = t.layer(k);
+    return l;
+  }
+
+  // Commit with the fused device kernels (log size >= 5): leaves of the circle
+  // layer, then per layer the node levels and a fold that reads its alpha from
+  // device memory and hashes the next layer's leaves.
+  int enqueue_commit(const uint32_t* const* d_coords, char* err, size_t err_len) {
+    int rc;
+    const uint32_t lg[4] = {n, n, n, n};
+    if ((rc = build_leaves_impl(d_coords, lg, 4, n, m31, trees[0].layer(n), s, err, err_len))) return rc;
+    auto l0 = layer_ptrs(trees[0]);
+    if ((rc = build_node_layers_impl(trees[0].layer(n), n, 0, m31, l0.data(), s, err, err_len))) return rc;
+    const Src4 src{{d_coords[0], d_coords[1], d_coords[2], d_coords[3]}};
+    fold_circle_first_dev_kernel<<<grid1d(1ull << (n - 1), 256), 256, 0, s>>>(
+        src, n, d_alphas, itw, 1ull << tree_log, line[0], trees[1].layer(n - 1), m31);
+    STWO_CHECK_LAUNCH();
+    for (uint32_t k = 1; k < n; k++) {
+      const uint32_t L = n - k;  // log size of line[k-1]
+      auto lk = layer_ptrs(trees[k]);
+      if ((rc = build_node_layers_impl(trees[k].layer(L), L, 0, m31, lk.data(), s, err, err_len))) return rc;
+      uint8_t* next_leaves = k + 1 < n ? trees[k + 1].layer(L - 1) : nullptr;
+      fold_line_dev_kernel<<<grid1d(1ull << (L - 1), 256), 256, 0, s>>>(line[k - 1], L, 1, d_alphas + k, itw,
+                                                                         1ull << tree_log, line[k], next_leaves, m31);
+      STWO_CHECK_LAUNCH();
+    }
+    return 0;
+  }
+
+  // Small columns: the stand-alone FriOps and Merkle entry points.
+  int enqueue_commit_small(const uint32_t* const* d_coords, const uint32_t* alphas, char* err, size_t err_len) {
+    int rc;
+    const uint32_t lg[4] = {n, n, n, n};
+    auto l0 = layer_ptrs(trees[0]);
+    if ((rc = stwo_b200_merkle_build_layers(d_coords, lg, 4, n, m31, l0.data(), s, err, err_len))) return rc;
+    STWO_CUDA_TRY(cudaMemsetAsync(line[0], 0, 16ull << (n - 1), s));  // fold_circle_into_line accumulates
+    auto c0 = cols4(line[0], n - 1);
+    if ((rc = stwo_b200_fold_circle_into_line(c0.data(), d_coords, n, 1ull << (31 - (n + 1)), alphas, itw, tree_log,
+                                              s, err, err_len)))
+      return rc;
+    for (uint32_t k = 1; k < n; k++) {
+      const uint32_t L = n - k;
+      auto cur = cols4(line[k - 1], L);
+      auto nxt = cols4(line[k], L - 1);
+      const uint32_t ll[4] = {L, L, L, L};
+      auto lk = layer_ptrs(trees[k]);
+      if ((rc = stwo_b200_merkle_build_layers(const_cast<const uint32_t* const*>(cur.data()), ll, 4, L, m31,
+                                              lk.data(), s, err, err_len)))
+        return rc;
+      if ((rc = stwo_b200_fold_line(const_cast<const uint32_t* const*>(cur.data()), L, alphas + 4 * k, 1, itw,
+                                    tree_log, nxt.data(), s, err, err_len)))
+        return rc;
+    }
+    return 0;
   }
 
   int prove(const uint32_t* const* d_coords, const uint32_t* alphas, const uint64_t* queries_in, uint32_t n_q,
@@ -2048,23 +2122,46 @@ struct SeededFriProver {
     STWO_CUDA_TRY(cudaStreamWaitEvent(s, ev_in, 0));
     int rc;
     // ---- commit (prover/fri.rs:133-291) ----
-    if ((rc = commit_layer(d_coords, trees[0], err, err_len))) return rc;
-    STWO_CUDA_TRY(cudaMemsetAsync(line[0], 0, 16ull << (n - 1), s));  // fold_circle_into_line accumulates
-    auto l0 = cols4(line[0], n - 1);
-    if ((rc = stwo_b200_fold_circle_into_line(l0.data(), d_coords, n, 1ull << (31 - (n + 1)), alphas, itw, tree_log,
-                                              s, err, err_len)))
+    if (n >= 5) {
+      std::memcpy(h_alphas, alphas, n * sizeof(qm31));
+      STWO_CUDA_TRY(cudaMemcpyAsync(d_alphas, h_alphas, n * sizeof(qm31), cudaMemcpyHostToDevice, s));
+      const bool same = exec && std::equal(d_coords, d_coords + 4, key);
+      if (!same) {
+        if (exec) cudaGraphExecDestroy(exec);
+        exec = nullptr;
+        const uint64_t before = g_kernel_launches.load();
+        STWO_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        rc = enqueue_commit(d_coords, err, err_len);
+        cudaGraph_t g = nullptr;
+        const cudaError_t ce = cudaStreamEndCapture(s, &g);
+        const uint64_t launched = g_kernel_launches.load() - before;
+        g_kernel_launches.fetch_sub(launched);  // nothing ran during capture
+        if (rc) {
+          if (g) cudaGraphDestroy(g);
+          return rc;
+        }
+        if (ce != cudaSuccess)
+          return set_err(err, err_len, STWO_B200_ECUDA, "FRI graph capture: %s", cudaGetErrorString(ce));
+        const cudaError_t ie = cudaGraphInstantiate(&exec, g, 0);
+        cudaGraphDestroy(g);
+        if (ie != cudaSuccess) {
+          exec = nullptr;
+          return set_err(err, err_len, STWO_B200_ECUDA, "FRI graph instantiate: %s", cudaGetErrorString(ie));
+        }
+        std::copy(d_coords, d_coords + 4, key);
+        graph_launches = launched;
+      }
+      STWO_CUDA_TRY(cudaGraphLaunch(exec, s));
+      g_kernel_launches.fetch_add(graph_launches);
+    } else if ((rc = enqueue_commit_small(d_coords, alphas, err, err_len))) {
       return rc;
-    for (uint32_t k = 1; k < n; k++) {
-      const uint32_t L = n - k;  // log size of line[k-1]
-      auto cur = cols4(line[k - 1], L);
-      auto nxt = cols4(line[k], L - 1);
-      if ((rc = commit_layer(cur.data(), trees[k], err, err_len))) return rc;
-      if ((rc = stwo_b200_fold_line(const_cast<const uint32_t* const*>(cur.data()), L, alphas + 4 * k, 1, itw,
-                                    tree_log, nxt.data(), s, err, err_len)))
-        return rc;
     }
     // ---- decommit (prover/fri.rs:294-350, 459-488): one gather ----
-    GatherPlan g;
+    // word entries (queried-pair values, 4 coordinates each) first, then hash
+    // entries (Merkle witness nodes and roots).
+    std::vector<uint64_t> word_addr, hash_addr;
+    word_addr.reserve((size_t)n * 4 * 2 * n_q + 4);
+    hash_addr.reserve((size_t)n * (n + 2) * n_q + n);
     struct LayerPlan {
       std::vector<bool> is_query;
       std::vector<size_t> value_slot, node_slot;
@@ -2082,12 +2179,15 @@ struct SeededFriProver {
           if (isq) k++;
           positions.push_back(pos);
           d.is_query.push_back(isq);
-          d.value_slot.push_back(g.add_word(c4[0] + pos));
-          for (int c = 1; c < 4; c++) g.add_word(c4[c] + pos);
+          d.value_slot.push_back(word_addr.size());
+          for (int c = 0; c < 4; c++) word_addr.push_back(reinterpret_cast<uint64_t>(c4[c] + pos));
         }
         i = j;
       }
-      for (auto& nd : witness_nodes(positions, t.L)) d.node_slot.push_back(g.add_hash(t.layer(nd.first) + nd.second * 32));
+      for (auto& nd : witness_nodes(positions, t.L)) {
+        d.node_slot.push_back(hash_addr.size());
+        hash_addr.push_back(reinterpret_cast<uint64_t>(t.layer(nd.first) + nd.second * 32));
+      }
       return d;
     };
     std::vector<LayerPlan> plans;
@@ -2103,24 +2203,41 @@ struct SeededFriProver {
         if (nq.empty() || nq.back() != (q >> 1)) nq.push_back(q >> 1);
       lq = nq;
     }
-    const size_t last_slot = g.add_word(line[n - 1]);
-    for (int c = 1; c < 4; c++) g.add_word(line[n - 1] + c);
+    const size_t last_slot = word_addr.size();
+    for (int c = 0; c < 4; c++) word_addr.push_back(reinterpret_cast<uint64_t>(line[n - 1] + c));
     std::vector<size_t> root_slot(n);
-    for (uint32_t k = 0; k < n; k++) root_slot[k] = g.add_hash(trees[k].layer(0));
-    const size_t total = g.addrs.size();
+    for (uint32_t k = 0; k < n; k++) {
+      root_slot[k] = hash_addr.size();
+      hash_addr.push_back(reinterpret_cast<uint64_t>(trees[k].layer(0)));
+    }
+    const size_t nw = word_addr.size(), nh = hash_addr.size(), total = nw + nh;
     if (total > gather_cap) {
-      const size_t cap = std::max<size_t>(total, 4096);
+      const size_t cap = std::max<size_t>(total * 2, 4096);
       if ((rc = alloc((void**)&d_gather_addr, cap * 8, err, err_len))) return rc;
-      if ((rc = alloc((void**)&d_gather_out, cap * 4, err, err_len))) return rc;
+      if ((rc = alloc((void**)&d_gather_out, cap * 32, err, err_len))) return rc;
+      if (h_stage) cudaFreeHost(h_stage);
+      h_stage = nullptr;
+      STWO_CUDA_TRY(cudaMallocHost((void**)&h_stage, cap * 40));
       gather_cap = cap;
     }
-    STWO_CUDA_TRY(cudaMemcpyAsync(d_gather_addr, g.addrs.data(), total * 8, cudaMemcpyHostToDevice, s));
-    gather_kernel<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(d_gather_addr, (uint32_t)total, d_gather_out);
+    uint64_t* h_addr = reinterpret_cast<uint64_t*>(h_stage);
+    std::memcpy(h_addr, word_addr.data(), nw * 8);
+    std::memcpy(h_addr + nw, hash_addr.data(), nh * 8);
+    STWO_CUDA_TRY(cudaMemcpyAsync(d_gather_addr, h_addr, total * 8, cudaMemcpyHostToDevice, s));
+    uint32_t* d_words = reinterpret_cast<uint32_t*>(d_gather_out);
+    uint4* d_hashes = reinterpret_cast<uint4*>(d_gather_out + ((nw * 4 + 31) / 32) * 32);
+    gather_kernel<<<(unsigned)((nw + 255) / 256), 256, 0, s>>>(d_gather_addr, (uint32_t)nw, d_words);
     STWO_CHECK_LAUNCH();
-    std::vector<uint32_t> words(total);
-    STWO_CUDA_TRY(cudaMemcpyAsync(words.data(), d_gather_out, total * 4, cudaMemcpyDeviceToHost, s));
+    gather_hashes_kernel<<<(unsigned)((nh + 255) / 256), 256, 0, s>>>(d_gather_addr + nw, (uint32_t)nh, d_hashes);
+    STWO_CHECK_LAUNCH();
+    uint8_t* h_out = h_stage + gather_cap * 8;
+    const size_t out_bytes = ((nw * 4 + 31) / 32) * 32 + nh * 32;
+    STWO_CUDA_TRY(cudaMemcpyAsync(h_out, d_gather_out, out_bytes, cudaMemcpyDeviceToHost, s));
     STWO_CUDA_TRY(cudaStreamSynchronize(s));
+    const uint32_t* words = reinterpret_cast<const uint32_t*>(h_out);
+    const uint8_t* hashes = h_out + ((nw * 4 + 31) / 32) * 32;
     // ---- serialize: FriLayerProof order of core/fri.rs:361-395 ----
+    out.bytes.reserve(out.bytes.size() + nw * 4 + nh * 32 + 64 * n);
     auto layer = [&](const LayerPlan& d, size_t rs) {
       size_t n_w = 0;
       for (bool b : d.is_query) n_w += b ? 0 : 1;
@@ -2131,8 +2248,8 @@ struct SeededFriProver {
           out.q({words[sl], words[sl + 1], words[sl + 2], words[sl + 3]});
         }
       out.u64(d.node_slot.size());
-      for (size_t sl : d.node_slot) out.h(reinterpret_cast<const uint8_t*>(words.data() + sl));
-      out.h(reinterpret_cast<const uint8_t*>(words.data() + rs));
+      for (size_t sl : d.node_slot) out.h(hashes + 32 * sl);
+      out.h(hashes + 32 * rs);
     };
     layer(plans[0], root_slot[0]);
     out.u64(n - 1);

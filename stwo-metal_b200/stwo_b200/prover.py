@@ -40,7 +40,7 @@ class WideFibProver:
         n = C.c_size_t()
         ffi.call("stwo_b200_prove_wide_fib", self.handle, C.c_void_p(a.ptr), C.c_void_p(b.ptr), buf,
                  C.c_size_t(cap), C.byref(n))
-        return bytes(buf[:n.value])
+        return C.string_at(buf, n.value)
 
     def prove_cols(self, a: DeviceColumn, b: DeviceColumn, n_cols: int, cap: int = 1 << 22) -> bytes:
         """The proof of an n_cols-wide trace (3 <= n_cols <= the prover's width)."""
@@ -48,7 +48,7 @@ class WideFibProver:
         n = C.c_size_t()
         ffi.call("stwo_b200_prove_wide_fib_cols", self.handle, C.c_uint32(n_cols), C.c_void_p(a.ptr),
                  C.c_void_p(b.ptr), buf, C.c_size_t(cap), C.byref(n))
-        return bytes(buf[:n.value])
+        return C.string_at(buf, n.value)
 
     def prove_into(self, a_ptr: int, b_ptr: int, out_buf, cap: int) -> int:
         n = C.c_size_t()
@@ -84,15 +84,18 @@ class SeededFriProver:
                  C.c_void_p(tree.itwiddles.ptr), C.c_uint32(tree.log_size), self.stream, C.byref(h))
         self._h = h
 
-    def prove(self, coords, alphas, queries, cap: int = 1 << 24) -> bytes:
+    def prove(self, coords, alphas, queries, cap: int = 1 << 22) -> bytes:
         a = np.ascontiguousarray(alphas, dtype=np.uint32).reshape(-1)
         q = np.ascontiguousarray(queries, dtype=np.uint64)
         ptrs = (C.c_void_p * 4)(*[c.ptr for c in coords])
-        buf = (C.c_uint8 * cap)()
+        if getattr(self, "_buf", None) is None or len(self._buf) < cap:
+            self._buf = (C.c_uint8 * cap)()  # reused across calls (a fresh one is zero-filled)
+        buf = self._buf
         n = C.c_size_t()
         ffi.call("stwo_b200_fri_prove_seeded", self._h, ptrs, a.ctypes.data_as(C.POINTER(C.c_uint32)),
-                 q.ctypes.data_as(C.POINTER(C.c_uint64)), C.c_uint32(q.size), buf, C.c_size_t(cap), C.byref(n))
-        return bytes(buf[:n.value])
+                 q.ctypes.data_as(C.POINTER(C.c_uint64)), C.c_uint32(q.size), buf, C.c_size_t(len(buf)),
+                 C.byref(n))
+        return C.string_at(buf, n.value)
 
     def close(self):
         if self._h:
@@ -141,12 +144,12 @@ class ProveServer:
                  b.ctypes.data_as(C.POINTER(C.c_uint32)), C.byref(t))
         return t.value
 
-    def wait(self, ticket: int, cap: int = 1 << 24):
-        buf = (C.c_uint8 * cap)()
+    def wait(self, ticket: int, cap: int = 1 << 22):
+        buf = C.create_string_buffer(cap)
         n = C.c_size_t()
         times = (C.c_double * 3)()
         ffi.call("stwo_b200_server_wait", self._h, C.c_uint64(ticket), buf, C.c_size_t(cap), C.byref(n), times)
-        return bytes(buf[:n.value]), {"queued_ms": times[0], "service_ms": times[1], "latency_ms": times[2]}
+        return C.string_at(buf, n.value), {"queued_ms": times[0], "service_ms": times[1], "latency_ms": times[2]}
 
     def stats(self) -> dict:
         st = ServerStats()
