@@ -469,61 +469,73 @@ __device__ __forceinline__ void stage_tws10(const FftPass& p, uint64_t hi, uint3
 // warp, straight between global memory and registers.  Needs 16-byte aligned
 // columns and no source masking.
 template <bool INV>
+__device__ __forceinline__ void warp_contig_load(const uint32_t* __restrict__ src, uint64_t base, uint32_t lane,
+                                                 uint32_t (&v)[32]) {
+  if (INV) {  // lane-major: rows lane*32 .. +31
+    const uint4* s4 = reinterpret_cast<const uint4*>(src + base + lane * 32);
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+      const uint4 w = __ldg(s4 + q);
+      v[4 * q] = w.x;
+      v[4 * q + 1] = w.y;
+      v[4 * q + 2] = w.z;
+      v[4 * q + 3] = w.w;
+    }
+  } else {  // row-major: rows j*32 + lane
+#pragma unroll
+    for (int j = 0; j < 32; j++) v[j] = __ldg(src + base + j * 32 + lane);
+  }
+}
+
+// Contiguous pass (layer0 = 0, C = 0): 1024 consecutive words of a column per
+// warp, straight between global memory and registers.  A block stages the
+// twiddles of its tile position once and walks p.cpb groups of kWarpCols
+// columns (warp w takes column g * kWarpCols + w), the warps independently:
+// no block barrier after the staging.  Needs 16-byte aligned columns and no
+// source masking.
+template <bool INV>
 __global__ void __launch_bounds__(256, 4) fft_warp_contig_kernel(FftPass p, FftCols cols) {
   extern __shared__ uint32_t smem[];
   uint32_t* tws = smem;
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   uint32_t* col = smem + 1024 + warp * (32 * 33);
   const uint64_t hi = blockIdx.x;
-  const uint32_t c = blockIdx.y * kWarpCols + warp;
-  const bool active = c < p.n_cols;
   const uint64_t base = hi << 10;
-  // The column tile's loads go out before the twiddle staging, so the two
-  // latencies overlap.
+  const uint32_t g0 = blockIdx.y * p.cpb;
+  // The first column tile's loads go out before the twiddle staging, so the
+  // two latencies overlap.
+  uint32_t c = g0 * kWarpCols + warp;
   uint32_t v[32];
-  if (active) {
-    const uint32_t* __restrict__ src = cols.src[c];
-    if (INV) {
-      const uint4* s4 = reinterpret_cast<const uint4*>(src + base + lane * 32);
-#pragma unroll
-      for (int q = 0; q < 8; q++) {
-        const uint4 w = __ldg(s4 + q);
-        v[4 * q] = w.x;
-        v[4 * q + 1] = w.y;
-        v[4 * q + 2] = w.z;
-        v[4 * q + 3] = w.w;
-      }
-    } else {
-#pragma unroll
-      for (int j = 0; j < 32; j++) v[j] = __ldg(src + base + j * 32 + lane);
-    }
-  }
+  if (c < p.n_cols) warp_contig_load<INV>(cols.src[c], base, lane, v);
   stage_tws10(p, hi, tws);
   __syncthreads();
-  if (!active) return;  // no block barrier follows
-  uint32_t* __restrict__ dst = cols.dst[c];
   const uint32_t scale = p.scale;
-  if (INV) {
-    warp_phase_lo<true>(v, tws, lane);
-    warp_lo_to_hi(v, col, lane);
-    warp_phase_hi<true>(v, tws);
+  for (uint32_t g = 0; g < p.cpb; g++, c += kWarpCols) {
+    if (c >= p.n_cols) return;  // no block barrier follows
+    if (g > 0) warp_contig_load<INV>(cols.src[c], base, lane, v);
+    uint32_t* __restrict__ dst = cols.dst[c];
+    if (INV) {
+      warp_phase_lo<true>(v, tws, lane);
+      warp_lo_to_hi(v, col, lane);
+      warp_phase_hi<true>(v, tws);
 #pragma unroll
-    for (int j = 0; j < 32; j++) dst[base + j * 32 + lane] = scale != 1u ? m31_mul(v[j], scale) : v[j];
-  } else {
-    warp_phase_hi<false>(v, tws);
-    warp_hi_to_lo(v, col, lane);
-    warp_phase_lo<false>(v, tws, lane);
-    uint4* d4 = reinterpret_cast<uint4*>(dst + base + lane * 32);
+      for (int j = 0; j < 32; j++) dst[base + j * 32 + lane] = scale != 1u ? m31_mul(v[j], scale) : v[j];
+    } else {
+      warp_phase_hi<false>(v, tws);
+      warp_hi_to_lo(v, col, lane);
+      warp_phase_lo<false>(v, tws, lane);
+      uint4* d4 = reinterpret_cast<uint4*>(dst + base + lane * 32);
 #pragma unroll
-    for (int q = 0; q < 8; q++) {
-      uint4 w = make_uint4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
-      if (scale != 1u) {
-        w.x = m31_mul(w.x, scale);
-        w.y = m31_mul(w.y, scale);
-        w.z = m31_mul(w.z, scale);
-        w.w = m31_mul(w.w, scale);
+      for (int q = 0; q < 8; q++) {
+        uint4 w = make_uint4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+        if (scale != 1u) {
+          w.x = m31_mul(w.x, scale);
+          w.y = m31_mul(w.y, scale);
+          w.z = m31_mul(w.z, scale);
+          w.w = m31_mul(w.w, scale);
+        }
+        d4[q] = w;
       }
-      d4[q] = w;
     }
   }
 }
@@ -621,8 +633,13 @@ static int launch_warp_pass(const FftPass& q, const FftCols& cols, uint64_t tile
                                          (int)smem));
       attr = true;
     }
-    dim3 grid((unsigned)tiles, (unsigned)((nc + kWarpCols - 1) / kWarpCols));
-    fft_warp_contig_kernel<INV><<<grid, 32 * kWarpCols, smem, s>>>(q, cols);
+    // up to 4 column groups per block: fewer twiddle stagings while the grid
+    // still has several waves of blocks
+    const uint32_t groups = (uint32_t)((nc + kWarpCols - 1) / kWarpCols);
+    FftPass qq = q;
+    qq.cpb = std::max<uint32_t>(1, std::min<uint32_t>(4, (uint32_t)((tiles * groups) / (148 * 4 * 6))));
+    dim3 grid((unsigned)tiles, (unsigned)((groups + qq.cpb - 1) / qq.cpb));
+    fft_warp_contig_kernel<INV><<<grid, 32 * kWarpCols, smem, s>>>(qq, cols);
   } else {
     constexpr size_t smem = (1024 + 8 * kColWords) * sizeof(uint32_t);
     static bool attr = false;
