@@ -69,16 +69,63 @@ def make_columns(spec):
 
 # ---------------------------------------------------------- clock sampling --
 class ClockSampler:
+    """SM clocks and clock-event reasons of this rank's GPU, sampled during the
+    timed region.  Reads NVML every 10 ms from a thread (the same counters as
+    `nvidia-smi --query-gpu=clocks.sm,clocks.max.sm,clocks_event_reasons.*`),
+    so that a region of tens of milliseconds still gets several samples; falls
+    back to an `nvidia-smi -lms 100` subprocess when NVML is not importable.
+    Reads only: no clock or power setting is touched."""
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    # nvmlClocksEventReason bits
+    REASON_BITS = {"sw_power_cap": 0x4, "hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20,
+                   "hw_thermal_slowdown": 0x40}
 
     def __init__(self, device: int):
         self.device = device
         self.proc = None
         self.lines = []
+        self.samples = []
+        self.nvml = None
+        self.stop_flag = threading.Event()
+
+    def _nvml_handle(self):
+        import pynvml
+        pynvml.nvmlInit()
+        try:
+            import torch
+            uuid = str(torch.cuda.get_device_properties(self.device).uuid)
+            h = pynvml.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+        except Exception:
+            h = pynvml.nvmlDeviceGetHandleByIndex(self.device)
+        return pynvml, h
+
+    def _poll(self):
+        nv, h = self.nvml
+        get_reasons = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+            nv.nvmlDeviceGetCurrentClocksThrottleReasons
+        while not self.stop_flag.is_set():
+            try:
+                self.samples.append((nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM),
+                                     nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM), int(get_reasons(h))))
+            except Exception:
+                pass
+            self.stop_flag.wait(0.01)
 
     def start(self):
+        try:
+            self.nvml = self._nvml_handle()
+        except Exception:
+            self.nvml = None
+        if self.nvml is not None:
+            self.t = threading.Thread(target=self._poll, daemon=True)
+            self.t.start()
+            t0 = time.perf_counter()
+            while not self.samples and time.perf_counter() - t0 < 1.0:
+                time.sleep(0.001)
+            self.samples.clear()  # keep only samples taken from here on
+            return
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
@@ -93,6 +140,14 @@ class ClockSampler:
             self.lines.append(line.strip())
 
     def stop(self):
+        if self.nvml is not None:
+            self.stop_flag.set()
+            self.t.join(timeout=1.0)
+            got = list(self.samples)
+            reasons = sorted(nm for nm, bit in self.REASON_BITS.items() if any(r & bit for _, _, r in got))
+            return {"sm_mhz": statistics.median(c for c, _, _ in got) if got else None,
+                    "sm_max_mhz": max(m for _, m, _ in got) if got else None,
+                    "reasons": reasons, "samples": len(got), "source": "nvml, 10 ms"}
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.proc.terminate()
@@ -115,7 +170,7 @@ class ClockSampler:
                 if v.lower().startswith("active"):
                     reasons.add(nm)
         return {"sm_mhz": statistics.median(sms) if sms else None, "sm_max_mhz": max(maxes) if maxes else None,
-                "reasons": sorted(reasons), "samples": len(sms)}
+                "reasons": sorted(reasons), "samples": len(sms), "source": "nvidia-smi, 100 ms"}
 
 
 # ------------------------------------------------------------ dist helpers --
