@@ -21,9 +21,13 @@
 namespace stwo_b200 {
 
 constexpr int kLeafMaxCols = 1024;
+constexpr uint8_t kMixedShift = 0xFF;
 struct LeafCols {
   const uint32_t* col[kLeafMaxCols];
   uint8_t shift[kLeafMaxCols];  // L - log_size
+  // shift shared by the 16 columns [16g, 16g + 16) of one compression, or
+  // kMixedShift when they differ or the group is partial
+  uint8_t group_shift[kLeafMaxCols / 16];
 };
 
 __device__ __forceinline__ void store_hash(uint8_t* out, uint64_t i, const uint32_t h[8], bool m31) {
@@ -35,7 +39,7 @@ __device__ __forceinline__ void store_hash(uint8_t* out, uint64_t i, const uint3
   o[1] = make_uint4(w[4], w[5], w[6], w[7]);
 }
 
-__device__ __forceinline__ uint64_t lift_index(uint64_t i, uint32_t r) {
+__device__ __forceinline__ uint32_t lift_index(uint32_t i, uint32_t r) {
   return r == 0 ? i : (((i >> (r + 1)) << 1) + (i & 1));
 }
 
@@ -45,14 +49,14 @@ __device__ __forceinline__ uint64_t lift_index(uint64_t i, uint32_t r) {
 __global__ void __launch_bounds__(256) lifted_leaves_kernel(LeafCols t, uint32_t n_cols, uint32_t L, int m31,
                                                            uint32_t bytes_before, uint32_t total_bytes,
                                                            uint32_t* state, int is_first, int is_last, uint8_t* out) {
-  uint64_t n = 1ull << L;
-  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+  const uint32_t n = 1u << L;  // L <= 30
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     uint32_t h[8];
     if (is_first) {
       blake2s_init(h);
     } else {
 #pragma unroll
-      for (int k = 0; k < 8; k++) h[k] = state[k * n + i];
+      for (int k = 0; k < 8; k++) h[k] = state[(uint64_t)k * n + i];
     }
     uint32_t m[16];
     uint32_t done = bytes_before;
@@ -62,10 +66,18 @@ __global__ void __launch_bounds__(256) lifted_leaves_kernel(LeafCols t, uint32_t
       blake2s_compress(h, m, done, true);
     }
     for (uint32_t c0 = 0; c0 < n_cols; c0 += 16) {
+      const uint32_t gs = t.group_shift[c0 >> 4];
+      if (gs != kMixedShift) {
+        // one lifted row index for the whole group: no per-column index work
+        const uint32_t li = lift_index(i, gs);
 #pragma unroll
-      for (int k = 0; k < 16; k++) {
-        uint32_t c = c0 + k;
-        m[k] = c < n_cols ? __ldg(t.col[c] + lift_index(i, t.shift[c])) : 0u;
+        for (int k = 0; k < 16; k++) m[k] = __ldg(t.col[c0 + k] + li);
+      } else {
+#pragma unroll
+        for (int k = 0; k < 16; k++) {
+          uint32_t c = c0 + k;
+          m[k] = c < n_cols ? __ldg(t.col[c] + lift_index(i, t.shift[c])) : 0u;
+        }
       }
       uint32_t nb = min(16u, n_cols - c0) * 4;
       done += nb;
@@ -75,7 +87,7 @@ __global__ void __launch_bounds__(256) lifted_leaves_kernel(LeafCols t, uint32_t
       store_hash(out, i, h, m31 != 0);
     } else {
 #pragma unroll
-      for (int k = 0; k < 8; k++) state[k * n + i] = h[k];
+      for (int k = 0; k < 8; k++) state[(uint64_t)k * n + i] = h[k];
     }
   }
 }
@@ -147,6 +159,62 @@ __global__ void __launch_bounds__(256) node_layers_kernel(const uint8_t* in, uin
     }
     cur ^= 1;
     __syncthreads();
+  }
+}
+
+// Parent hash of the 64-byte child pair in m (throughput form), reduced to
+// M31 words when the tree stores M31 hashes.
+__device__ __forceinline__ void hash_children(const uint32_t m[16], bool m31, uint32_t h[8]) {
+  blake2s_init(h);
+  blake2s_compress(h, m, 64, true);
+  if (m31) {
+#pragma unroll
+    for (int k = 0; k < 8; k++) h[k] = m31_reduce_u32(h[k]);
+  }
+}
+
+__device__ __forceinline__ void load_children(const uint4* src, uint32_t m[16]) {
+  const uint4 a = __ldg(src), b = __ldg(src + 1), c = __ldg(src + 2), d = __ldg(src + 3);
+  m[0] = a.x; m[1] = a.y; m[2] = a.z; m[3] = a.w;
+  m[4] = b.x; m[5] = b.y; m[6] = b.z; m[7] = b.w;
+  m[8] = c.x; m[9] = c.y; m[10] = c.z; m[11] = c.w;
+  m[12] = d.x; m[13] = d.y; m[14] = d.z; m[15] = d.w;
+}
+
+// Three node layers per thread, for layers wide enough to fill the GPU:
+// thread t reads child hashes 8t..8t+7 of `in` and writes parents 4t..4t+3
+// (out0), 2t, 2t+1 (out1) and t (out2).  Every thread does 7 compressions
+// with no barrier and no idle lanes; the block-cooperative kernel above idles
+// half its threads at each level it climbs.
+__global__ void __launch_bounds__(256) node_subtree3_kernel(const uint8_t* in, uint64_t n, int m31, uint8_t* out0,
+                                                           uint8_t* out1, uint8_t* out2) {
+  for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < n; t += (uint64_t)gridDim.x * blockDim.x) {
+    const uint4* src = reinterpret_cast<const uint4*>(in + t * 256);
+    uint32_t m[16], g0[8], h[8];
+#pragma unroll
+    for (int half = 0; half < 2; half++) {
+      uint32_t a[8];
+      load_children(src + 8 * half, m);
+      hash_children(m, m31 != 0, a);
+      store_hash(out0, 4 * t + 2 * half, a, false);
+      load_children(src + 8 * half + 4, m);
+      hash_children(m, m31 != 0, h);
+      store_hash(out0, 4 * t + 2 * half + 1, h, false);
+#pragma unroll
+      for (int k = 0; k < 8; k++) {
+        m[k] = a[k];
+        m[k + 8] = h[k];
+      }
+      hash_children(m, m31 != 0, half ? h : g0);
+      store_hash(out1, 2 * t + half, half ? h : g0, false);
+    }
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      m[k] = g0[k];
+      m[k + 8] = h[k];
+    }
+    hash_children(m, m31 != 0, h);
+    store_hash(out2, t, h, false);
   }
 }
 
@@ -241,6 +309,12 @@ int build_leaves_impl(const uint32_t* const* d_cols, const uint32_t* log_sizes, 
       t.col[k] = d_cols[c0 + k];
       t.shift[k] = (uint8_t)(L - log_sizes[c0 + k]);
     }
+    for (uint32_t g = 0; g < kLeafMaxCols / 16; g++) {
+      const uint32_t k0 = 16 * g;
+      bool uniform = k0 + 16 <= nc;
+      for (uint32_t k = k0 + 1; uniform && k < k0 + 16; k++) uniform = t.shift[k] == t.shift[k0];
+      t.group_shift[g] = uniform ? t.shift[k0] : kMixedShift;
+    }
     lifted_leaves_kernel<<<grid_for(n, 256), 256, 0, s>>>(t, nc, L, m31, 4u * c0, total_bytes, state, ch == 0,
                                                           ch + 1 == chunks, d_leaves);
     STWO_CHECK_LAUNCH();
@@ -249,6 +323,8 @@ int build_leaves_impl(const uint32_t* const* d_cols, const uint32_t* log_sizes, 
   return STWO_B200_OK;
 }
 
+constexpr uint32_t kSubtree3MinLog = 19;
+
 // Builds layers [in_log - 1 .. stop_log] from layer `in` (2^in_log hashes);
 // outs_by_log[k] is the destination of layer log k.
 int build_node_layers_impl(const uint8_t* in, uint32_t in_log, uint32_t stop_log, int m31,
@@ -256,6 +332,17 @@ int build_node_layers_impl(const uint8_t* in, uint32_t in_log, uint32_t stop_log
   uint32_t cur_log = in_log;
   const uint8_t* cur = in;
   while (cur_log > stop_log) {
+    // Wide layers: three levels per thread while the third level still has
+    // 2^16 parents (256 blocks of 256 threads).
+    if (cur_log - stop_log >= 3 && cur_log >= kSubtree3MinLog) {
+      const uint64_t n = 1ull << (cur_log - 3);
+      node_subtree3_kernel<<<grid_for(n, 256), 256, 0, s>>>(cur, n, m31, outs_by_log[cur_log - 1],
+                                                            outs_by_log[cur_log - 2], outs_by_log[cur_log - 3]);
+      STWO_CHECK_LAUNCH();
+      cur = outs_by_log[cur_log - 3];
+      cur_log -= 3;
+      continue;
+    }
     uint32_t levels = std::min<uint32_t>(8, cur_log - stop_log);
     uint64_t parents0 = 1ull << (cur_log - 1);
     uint32_t width = (uint32_t)std::min<uint64_t>(256, parents0);

@@ -119,6 +119,13 @@ def test_merkle_layers(be, oracle, logs, L, m31):
         assert (layer_to_host(layers[k]) == ref[k]).all(), k
 
 
+@pytest.mark.parametrize("logs,L", [([19, 17], 19), ([20, 22], 22)])
+@pytest.mark.parametrize("m31", [False, True])
+def test_merkle_layers_wide(be, oracle, logs, L, m31):
+    # lifting sizes >= 19 take the three-levels-per-thread node kernel (twice at 22)
+    test_merkle_layers(be, oracle, logs, L, m31)
+
+
 def test_merkle_empty(be, oracle):
     layers = be.build_merkle_layers([], 0)
     assert (layer_to_host(layers[0]) == oracle.merkle_build_layers([], 0)[0]).all()
