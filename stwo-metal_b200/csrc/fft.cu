@@ -62,6 +62,25 @@ __device__ __forceinline__ void bfly(uint32_t& a, uint32_t& b, uint32_t t) {
   a = m31_add(a, m);
 }
 
+// Butterflies with the twiddle stored doubled (t2 = 2t < 2^32): the 64-bit
+// product b * t2 has (b t) >> 31 as its high word and 2 (b t mod 2^31) as its
+// low word, so the reduction needs one shift instead of a mask and a funnel
+// shift.  Same (lo, hi) pair, hence the same result, as m31_mul(b, t).
+__device__ __forceinline__ uint32_t m31_mul_tw2(uint32_t b, uint32_t t2) {
+  const uint64_t x = (uint64_t)b * t2;
+  return m31_add((uint32_t)x >> 1, (uint32_t)(x >> 32));
+}
+__device__ __forceinline__ void ibfly2(uint32_t& a, uint32_t& b, uint32_t t2) {
+  uint32_t s = m31_add(a, b);
+  b = m31_mul_tw2(m31_sub(a, b), t2);
+  a = s;
+}
+__device__ __forceinline__ void bfly2(uint32_t& a, uint32_t& b, uint32_t t2) {
+  uint32_t m = m31_mul_tw2(b, t2);
+  b = m31_sub(a, m);
+  a = m31_add(a, m);
+}
+
 __host__ __device__ constexpr uint32_t tile_stride_words(uint32_t e) { return e + (e >> 4) + 1; }
 __host__ __device__ constexpr uint32_t smem_off(uint32_t e) { return e + (e >> 4); }
 
@@ -401,9 +420,9 @@ __device__ __forceinline__ void warp_phase_lo(uint32_t (&v)[32], const uint32_t*
     for (int j = 0; j < 32; j++) {
       if (j & (1 << lam)) continue;
       if (INV)
-        ibfly(v[j], v[j | (1 << lam)], t[j >> (lam + 1)]);
+        ibfly2(v[j], v[j | (1 << lam)], t[j >> (lam + 1)]);
       else
-        bfly(v[j], v[j | (1 << lam)], t[j >> (lam + 1)]);
+        bfly2(v[j], v[j | (1 << lam)], t[j >> (lam + 1)]);
     }
   }
 }
@@ -423,9 +442,9 @@ __device__ __forceinline__ void warp_phase_hi(uint32_t (&v)[32], const uint32_t*
     for (int j = 0; j < 32; j++) {
       if (j & (1 << k)) continue;
       if (INV)
-        ibfly(v[j], v[j | (1 << k)], t[j >> (k + 1)]);
+        ibfly2(v[j], v[j | (1 << k)], t[j >> (k + 1)]);
       else
-        bfly(v[j], v[j | (1 << k)], t[j >> (k + 1)]);
+        bfly2(v[j], v[j | (1 << k)], t[j >> (k + 1)]);
     }
   }
 }
@@ -447,21 +466,32 @@ __device__ __forceinline__ void warp_hi_to_lo(uint32_t (&v)[32], uint32_t* col, 
   __syncwarp();
 }
 
-// Stages the 1023 twiddles of a 10-layer tile position (as fft_pass_kernel).
+// Stages the 1023 twiddles of a 10-layer tile position (as fft_pass_kernel),
+// doubled for bfly2 / ibfly2: slot s of the table holds layer
+// lam = clz(1023 - s) - 22, entry s - (1024 - 2^(10 - lam)).  Each of the 256 threads loads its 4 slots
+// before storing any, so the block waits for one memory round trip instead
+// of one per layer.
 __device__ __forceinline__ void stage_tws10(const FftPass& p, uint64_t hi, uint32_t* tws) {
+  uint32_t val[4];
 #pragma unroll
-  for (int lam = 0; lam < 10; lam++) {
-    const uint32_t cnt = 1u << (9 - lam);
-    const uint32_t off = 1024u - (1024u >> lam);
-    const uint64_t h0 = hi << (9 - lam);
-    const uint32_t layer = p.layer0 + lam;
-    if (layer == 0) {
-      const uint32_t* lt0 = p.tree + (p.tree_len - (1ull << (p.log_domain - 1)));
-      for (uint32_t i = threadIdx.x; i < cnt; i += blockDim.x) tws[off + i] = circle_tw(lt0, h0 + i);
-    } else {
-      const uint32_t* lt = p.tree + (p.tree_len - (1ull << (p.log_domain - layer))) + h0;
-      for (uint32_t i = threadIdx.x; i < cnt; i += blockDim.x) tws[off + i] = __ldg(lt + i);
+  for (int k = 0; k < 4; k++) {
+    const uint32_t s = threadIdx.x + 256u * k;
+    const uint32_t u = 1023u - s;
+    val[k] = 0;
+    if (u != 0) {
+      const uint32_t lam = __clz(u) - 22;
+      const uint64_t h = (hi << (9 - lam)) + (s - (1024u - (1024u >> lam)));
+      const uint32_t layer = p.layer0 + lam;
+      if (layer == 0)
+        val[k] = circle_tw(p.tree + (p.tree_len - (1ull << (p.log_domain - 1))), h);
+      else
+        val[k] = __ldg(p.tree + (p.tree_len - (1ull << (p.log_domain - layer))) + h);
     }
+  }
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    const uint32_t s = threadIdx.x + 256u * k;
+    if (s < 1023u) tws[s] = val[k] << 1;
   }
 }
 
@@ -557,7 +587,26 @@ __global__ void __launch_bounds__(256, 4) fft_warp_strided_kernel(FftPass p, Fft
   const uint32_t* __restrict__ src = cols.src[blockIdx.y];
   uint32_t* __restrict__ dst = cols.dst[blockIdx.y];
   stage_tws10(p, hi, tws);
-  if (p.vec_io) {
+  if (p.vec_io && p.src_mask == ~0ull && p.src_len == ~0ull) {
+    // all 8 loads in flight before the first shared-memory store
+    const uint32_t* __restrict__ sb = src + base;
+    uint4 w[8];
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+      const uint32_t e = threadIdx.x * 4 + 1024u * q;
+      w[q] = __ldg(reinterpret_cast<const uint4*>(sb + ((size_t)(e >> 3) << L0) + (e & 7)));
+    }
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+      const uint32_t e = threadIdx.x * 4 + 1024u * q;
+      const uint32_t row = e >> 3, c0 = e & 7;
+      const uint32_t r = row + (row >> 5);
+      tile[c0 * kColWords + r] = w[q].x;
+      tile[(c0 + 1) * kColWords + r] = w[q].y;
+      tile[(c0 + 2) * kColWords + r] = w[q].z;
+      tile[(c0 + 3) * kColWords + r] = w[q].w;
+    }
+  } else if (p.vec_io) {
 #pragma unroll 4
     for (uint32_t e = threadIdx.x * 4; e < 8192; e += 1024) {
       const uint32_t row = e >> 3, c0 = e & 7;
