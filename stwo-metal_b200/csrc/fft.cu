@@ -21,6 +21,7 @@
 
 #include "common.cuh"
 #include "field.cuh"
+#include "stream.cuh"
 
 namespace stwo_b200 {
 
@@ -495,64 +496,101 @@ __device__ __forceinline__ void stage_tws10(const FftPass& p, uint64_t hi, uint3
   }
 }
 
-// Contiguous pass (layer0 = 0, C = 0): 1024 consecutive words of a column per
-// warp, straight between global memory and registers.  Needs 16-byte aligned
-// columns and no source masking.
-template <bool INV>
-__device__ __forceinline__ void warp_contig_load(const uint32_t* __restrict__ src, uint64_t base, uint32_t lane,
-                                                 uint32_t (&v)[32]) {
-  if (INV) {  // lane-major: rows lane*32 .. +31
-    const uint4* s4 = reinterpret_cast<const uint4*>(src + base + lane * 32);
-#pragma unroll
-    for (int q = 0; q < 8; q++) {
-      const uint4 w = __ldg(s4 + q);
-      v[4 * q] = w.x;
-      v[4 * q + 1] = w.y;
-      v[4 * q + 2] = w.z;
-      v[4 * q + 3] = w.w;
-    }
-  } else {  // row-major: rows j*32 + lane
-#pragma unroll
-    for (int j = 0; j < 32; j++) v[j] = __ldg(src + base + j * 32 + lane);
-  }
+// Staged column tile of the contiguous pass: word e of the 1024 at
+// (e >> 5) * kTileStride + (e & 31).  Lines of 36 words keep every 16-byte
+// chunk aligned for cp.async, and both register layouts read conflict-free:
+// lane-major (lane l takes words 32l..32l+31 as 8 x 16 bytes; 8 lanes of a
+// quarter-warp cover banks 4l + 4q .. +3, all distinct) and row-major (lane l
+// takes word 32j + l: 32 consecutive words).
+constexpr uint32_t kTileStride = 36;
+constexpr uint32_t kTileWords = 32 * kTileStride;
+
+__device__ __forceinline__ void cp_async16(uint32_t* dst, const uint32_t* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(smem_addr(dst)), "l"(src) : "memory");
 }
 
-// Contiguous pass (layer0 = 0, C = 0): 1024 consecutive words of a column per
-// warp, straight between global memory and registers.  A block stages the
-// twiddles of its tile position once and walks p.cpb groups of kWarpCols
-// columns (warp w takes column g * kWarpCols + w), the warps independently:
-// no block barrier after the staging.  Needs 16-byte aligned columns and no
-// source masking.
+// Copies the 1024 words at src (16-byte aligned) into a staged tile; one
+// commit group per tile.
+__device__ __forceinline__ void tile_prefetch(const uint32_t* __restrict__ src, uint32_t* buf, uint32_t lane) {
+#pragma unroll
+  for (int i = 0; i < 8; i++) {
+    const uint32_t k = lane + 32u * i;  // 16-byte chunk
+    cp_async16(buf + (k >> 3) * kTileStride + (k & 7) * 4, src + 4 * k);
+  }
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+__device__ __forceinline__ void tile_wait() {
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+  __syncwarp();
+}
+__device__ __forceinline__ void tile_to_lane_major(const uint32_t* buf, uint32_t lane, uint32_t (&v)[32]) {
+#pragma unroll
+  for (int q = 0; q < 8; q++) {
+    const uint4 w = *reinterpret_cast<const uint4*>(buf + lane * kTileStride + 4 * q);
+    v[4 * q] = w.x;
+    v[4 * q + 1] = w.y;
+    v[4 * q + 2] = w.z;
+    v[4 * q + 3] = w.w;
+  }
+}
+__device__ __forceinline__ void lane_major_to_tile(uint32_t* buf, uint32_t lane, const uint32_t (&v)[32]) {
+#pragma unroll
+  for (int q = 0; q < 8; q++)
+    *reinterpret_cast<uint4*>(buf + lane * kTileStride + 4 * q) =
+        make_uint4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+}
+
+// Contiguous pass (layer0 = 0, C = 0): warp w transforms 1024 consecutive
+// words of column g * kWarpCols + w for p.cpb column groups g of one tile
+// position, whose twiddles the block stages once.  Each warp streams its
+// tiles through its own staged tile with cp.async: the next tile's copy is
+// issued as soon as the transpose has freed the buffer, so it lands during
+// the second half of the butterflies and the stores.  No block barrier after
+// the staging.  Needs 16-byte aligned columns and no source masking.
 template <bool INV>
 __global__ void __launch_bounds__(256, 4) fft_warp_contig_kernel(FftPass p, FftCols cols) {
-  extern __shared__ uint32_t smem[];
+  extern __shared__ __align__(16) uint32_t smem[];
   uint32_t* tws = smem;
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  uint32_t* col = smem + 1024 + warp * (32 * 33);
+  uint32_t* buf = smem + 1024 + warp * kTileWords;
   const uint64_t hi = blockIdx.x;
   const uint64_t base = hi << 10;
   const uint32_t g0 = blockIdx.y * p.cpb;
-  // The first column tile's loads go out before the twiddle staging, so the
-  // two latencies overlap.
   uint32_t c = g0 * kWarpCols + warp;
-  uint32_t v[32];
-  if (c < p.n_cols) warp_contig_load<INV>(cols.src[c], base, lane, v);
+  if (c < p.n_cols) tile_prefetch(cols.src[c] + base, buf, lane);
   stage_tws10(p, hi, tws);
   __syncthreads();
   const uint32_t scale = p.scale;
   for (uint32_t g = 0; g < p.cpb; g++, c += kWarpCols) {
     if (c >= p.n_cols) return;  // no block barrier follows
-    if (g > 0) warp_contig_load<INV>(cols.src[c], base, lane, v);
+    const uint32_t cn = c + kWarpCols;
+    const bool more = g + 1 < p.cpb && cn < p.n_cols;
     uint32_t* __restrict__ dst = cols.dst[c];
+    uint32_t v[32];
+    tile_wait();
     if (INV) {
+      tile_to_lane_major(buf, lane, v);
       warp_phase_lo<true>(v, tws, lane);
-      warp_lo_to_hi(v, col, lane);
+      lane_major_to_tile(buf, lane, v);
+      __syncwarp();
+#pragma unroll
+      for (int j = 0; j < 32; j++) v[j] = buf[j * kTileStride + lane];
+      __syncwarp();
+      if (more) tile_prefetch(cols.src[cn] + base, buf, lane);
       warp_phase_hi<true>(v, tws);
 #pragma unroll
       for (int j = 0; j < 32; j++) dst[base + j * 32 + lane] = scale != 1u ? m31_mul(v[j], scale) : v[j];
     } else {
+#pragma unroll
+      for (int j = 0; j < 32; j++) v[j] = buf[j * kTileStride + lane];
       warp_phase_hi<false>(v, tws);
-      warp_hi_to_lo(v, col, lane);
+      __syncwarp();
+#pragma unroll
+      for (int j = 0; j < 32; j++) buf[j * kTileStride + lane] = v[j];
+      __syncwarp();
+      tile_to_lane_major(buf, lane, v);
+      __syncwarp();
+      if (more) tile_prefetch(cols.src[cn] + base, buf, lane);
       warp_phase_lo<false>(v, tws, lane);
       uint4* d4 = reinterpret_cast<uint4*>(dst + base + lane * 32);
 #pragma unroll
@@ -587,9 +625,15 @@ __global__ void __launch_bounds__(256, 4) fft_warp_strided_kernel(FftPass p, Fft
   const uint32_t* __restrict__ src = cols.src[blockIdx.y];
   uint32_t* __restrict__ dst = cols.dst[blockIdx.y];
   stage_tws10(p, hi, tws);
-  if (p.vec_io && p.src_mask == ~0ull && p.src_len == ~0ull) {
+  // A power-of-two source mask that covers every row and column bit of the
+  // tile (the duplicated coefficients of a blowup evaluation) only changes
+  // the tile base.
+  const bool mask_on_base = (p.src_mask == ~0ull && p.src_len == ~0ull) ||
+                            (p.src_mask != ~0ull && ((p.src_mask + 1) & p.src_mask) == 0 &&
+                             p.src_mask + 1 >= (1ull << (L0 + 10)) && p.src_len > p.src_mask);
+  if (p.vec_io && mask_on_base) {
     // all 8 loads in flight before the first shared-memory store
-    const uint32_t* __restrict__ sb = src + base;
+    const uint32_t* __restrict__ sb = src + (base & p.src_mask);
     uint4 w[8];
 #pragma unroll
     for (int q = 0; q < 8; q++) {
@@ -675,7 +719,7 @@ template <bool INV>
 static int launch_warp_pass(const FftPass& q, const FftCols& cols, uint64_t tiles, size_t nc, cudaStream_t s,
                             char* err, size_t err_len) {
   if (q.C == 0) {
-    constexpr size_t smem = (1024 + kWarpCols * 32 * 33) * sizeof(uint32_t);
+    constexpr size_t smem = (1024 + kWarpCols * kTileWords) * sizeof(uint32_t);
     static bool attr = false;
     if (!attr) {
       STWO_CUDA_TRY(cudaFuncSetAttribute(fft_warp_contig_kernel<INV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
