@@ -107,6 +107,11 @@ class HostChannel {
  public:
   explicit HostChannel(bool m31_output) : m31_(m31_output) { digest_.fill(0); }
   const Hash32& digest() const { return digest_; }
+  // Adopts a channel state computed elsewhere (the device channel).
+  void set_state(const uint32_t digest[8], uint32_t n_draws) {
+    std::memcpy(digest_.data(), digest, 32);
+    n_draws_ = n_draws;
+  }
   uint32_t n_draws() const { return n_draws_; }
   bool m31() const { return m31_; }
 

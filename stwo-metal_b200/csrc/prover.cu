@@ -251,6 +251,30 @@ __global__ void __launch_bounds__(256) oods_eval_kernel(PolyTable t, uint32_t n_
   }
 }
 
+// OODS fold weights: w_lo[t] = prod of f[b] over the set bits b of t
+// (t < 2^h) and w_hi[t] = prod of f[h + b] (t < 2^hi_bits), the tables of
+// oods_eval_kernel.  Field products are exact, so the order of the factors
+// does not matter.
+struct OodsFolds {
+  qm31 f[32];
+};
+__global__ void oods_weights_kernel(OodsFolds f, uint32_t h, uint32_t hi_bits, qm31* __restrict__ w_lo,
+                                    qm31* __restrict__ w_hi) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < (1u << h)) {
+    qm31 w = qm31_one();
+    for (uint32_t b = 0; b < h; b++)
+      if ((t >> b) & 1) w = qm31_mul(w, f.f[b]);
+    w_lo[t] = w;
+  }
+  if (t < (1u << hi_bits)) {
+    qm31 w = qm31_one();
+    for (uint32_t b = 0; b < hi_bits; b++)
+      if ((t >> b) & 1) w = qm31_mul(w, f.f[h + b]);
+    w_hi[t] = w;
+  }
+}
+
 // out[p] = sum of partial[p][0 .. n_chunks); one block per polynomial.
 __global__ void __launch_bounds__(256) oods_reduce_kernel(const qm31* __restrict__ partial, uint32_t n_chunks,
                                                          qm31* __restrict__ out) {
@@ -1262,7 +1286,7 @@ class WideFibProver {
     if ((rc = alloc((void**)&d_found, 64, err, err_len))) return rc;
     if ((rc = alloc((void**)&d_chan, sizeof(DevChannel), err, err_len))) return rc;
     if ((rc = alloc((void**)&d_alphas, (fri.size() + 2) * sizeof(qm31), err, err_len))) return rc;
-    h_pinned_bytes = std::max<size_t>(small_q * sizeof(qm31), 16ull << last_log);
+    h_pinned_bytes = std::max<size_t>(small_q * sizeof(qm31), (16ull << last_log) + 65536);
     if (measure) return 0;
     STWO_CUDA_TRY(cudaMallocHost((void**)&h_pinned, h_pinned_bytes));
     STWO_CUDA_TRY(cudaMallocHost((void**)&h_chan, sizeof(DevChannel)));
@@ -1563,22 +1587,20 @@ int WideFibProver::prove_body(const uint32_t* d_a, const uint32_t* d_b, ProofOut
     // (log_n coefficients each) are sampled at the OODS point itself.
     STWO_ARG_CHECK(L1 == lift && eval_log - 1 == log_n, "sampling assumes one column size");
     const uint32_t lg = log_n, h = lg / 2;
-    qm31 f[32];
-    f[0] = oods.y;
+    OodsFolds f{};
+    f.f[0] = oods.y;
     qm31 x = oods.x;
     for (uint32_t b = 1; b < lg; b++) {
-      f[b] = x;
+      f.f[b] = x;
       x = qm31_double_x(x);
     }
-    qm31* w_lo = h_pinned;
-    qm31* w_hi = h_pinned + (1u << h);
-    w_lo[0] = qm31_one();
-    for (uint32_t t = 1; t < (1u << h); t++) w_lo[t] = qm31_mul(w_lo[t & (t - 1)], f[__builtin_ctz(t)]);
-    w_hi[0] = qm31_one();
-    for (uint32_t t = 1; t < (1u << (lg - h)); t++) w_hi[t] = qm31_mul(w_hi[t & (t - 1)], f[h + __builtin_ctz(t)]);
     size_t n_w = (1u << h) + (1u << (lg - h));
     phase(kOodsSampling);
-    STWO_CUDA_TRY(cudaMemcpyAsync(d_small, h_pinned, n_w * sizeof(qm31), cudaMemcpyHostToDevice, s));
+    {
+      const uint32_t nt = 1u << std::max(h, lg - h);
+      oods_weights_kernel<<<(nt + 255) / 256, 256, 0, s>>>(f, h, lg - h, d_small, d_small + (1u << h));
+      STWO_CHECK_LAUNCH();
+    }
     PolyTable pt;
     uint32_t np = N + 8;
     for (uint32_t c = 0; c < N; c++) pt.p[c] = coeff_ptrs[c];
@@ -1594,34 +1616,6 @@ int WideFibProver::prove_body(const uint32_t* d_a, const uint32_t* d_b, ProofOut
     std::memcpy(sampled.data(), h_pinned, np * sizeof(qm31));
   }
   ch.mix_felts(sampled.data(), sampled.size());
-
-  // Sanity check (prover/mod.rs:123-138): the composition value rebuilt from
-  // the split halves equals the constraint quotient at the OODS point.
-  {
-    const qm31 basis[4] = {qm31_one(), {0, 1, 0, 0}, {0, 0, 1, 0}, {0, 0, 0, 1}};
-    qm31 left = qm31_zero(), right = qm31_zero();
-    for (int k = 0; k < 4; k++) {
-      left = qm31_add(left, qm31_mul(sampled[N + k], basis[k]));
-      right = qm31_add(right, qm31_mul(sampled[N + 4 + k], basis[k]));
-    }
-    qm31 comp = qm31_add(left, qm31_mul(spoint_repeated_double(oods, max_log_degree_bound - 1).x, right));
-    // coset_vanishing(CanonicCoset(max_log_degree_bound).coset, oods)
-    uint64_t cinit = 1ull << (31 - (max_log_degree_bound + 1)), cstep = 1ull << (31 - max_log_degree_bound);
-    cpoint ci = index_to_cpoint(cinit), hs = index_to_cpoint(cstep >> 1);
-    spoint sp = spoint_add(spoint_add(oods, {qm31_from_m31(ci.x), qm31_from_m31(m31_neg(ci.y))}),
-                           {qm31_from_m31(hs.x), qm31_from_m31(hs.y)});
-    qm31 vx = sp.x;
-    for (uint32_t i = 1; i < max_log_degree_bound; i++) vx = qm31_double_x(vx);
-    qm31 dinv = qm31_inv(vx);
-    qm31 acc = qm31_zero();
-    for (uint32_t k = 0; k < n_cons; k++) {
-      qm31 a = sampled[k], b = sampled[k + 1], c = sampled[k + 2];
-      qm31 cons = qm31_sub(c, qm31_add(qm31_mul(a, a), qm31_mul(b, b)));
-      acc = qm31_add(qm31_mul(acc, random_coeff), qm31_mul(cons, dinv));
-    }
-    if (!qm31_eq(acc, comp))
-      return set_err(err, err_len, STWO_B200_ESTATE, "ConstraintsNotSatisfied: composition OODS mismatch");
-  }
 
   // ---- FRI quotients (pcs/mod.rs:112-118, quotient_ops.rs:134-233) ----
   const qm31 qcoeff = ch.draw_secure_felt();
@@ -1694,45 +1688,76 @@ int WideFibProver::prove_body(const uint32_t* d_a, const uint32_t* d_b, ProofOut
     STWO_CUDA_TRY(cudaMemcpyAsync(d_chan, hc, sizeof(DevChannel), cudaMemcpyHostToDevice, s));
   }
   if ((rc = run_fri(err, err_len))) return rc;
+  // Sanity check (prover/mod.rs:123-138): the composition value rebuilt from
+  // the split halves equals the constraint quotient at the OODS point.  Host
+  // only, so it runs while the device works through the FRI commit.
   {
-    // one download: roots, device alphas, channel state; then the host replay
-    uint8_t* hp = reinterpret_cast<uint8_t*>(h_pinned);
+    const qm31 basis[4] = {qm31_one(), {0, 1, 0, 0}, {0, 0, 1, 0}, {0, 0, 0, 1}};
+    qm31 left = qm31_zero(), right = qm31_zero();
+    for (int k = 0; k < 4; k++) {
+      left = qm31_add(left, qm31_mul(sampled[N + k], basis[k]));
+      right = qm31_add(right, qm31_mul(sampled[N + 4 + k], basis[k]));
+    }
+    qm31 comp = qm31_add(left, qm31_mul(spoint_repeated_double(oods, max_log_degree_bound - 1).x, right));
+    // coset_vanishing(CanonicCoset(max_log_degree_bound).coset, oods)
+    uint64_t cinit = 1ull << (31 - (max_log_degree_bound + 1)), cstep = 1ull << (31 - max_log_degree_bound);
+    cpoint ci = index_to_cpoint(cinit), hs = index_to_cpoint(cstep >> 1);
+    spoint sp = spoint_add(spoint_add(oods, {qm31_from_m31(ci.x), qm31_from_m31(m31_neg(ci.y))}),
+                           {qm31_from_m31(hs.x), qm31_from_m31(hs.y)});
+    qm31 vx = sp.x;
+    for (uint32_t i = 1; i < max_log_degree_bound; i++) vx = qm31_double_x(vx);
+    qm31 dinv = qm31_inv(vx);
+    qm31 acc = qm31_zero();
+    for (uint32_t k = 0; k < n_cons; k++) {
+      qm31 a = sampled[k], b = sampled[k + 1], c = sampled[k + 2];
+      qm31 cons = qm31_sub(c, qm31_add(qm31_mul(a, a), qm31_mul(b, b)));
+      acc = qm31_add(qm31_mul(acc, random_coeff), qm31_mul(cons, dinv));
+    }
+    if (!qm31_eq(acc, comp))
+      return set_err(err, err_len, STWO_B200_ESTATE, "ConstraintsNotSatisfied: composition OODS mismatch");
+  }
+
+  // One download after the FRI commit: roots, device alphas, channel state,
+  // error flags and the last layer.  The host continues from the device
+  // channel's state (last layer, proof of work) and replays the transcript
+  // to check the device alphas while the first grind batch runs.
+  const uint64_t n_last = 1ull << last_log;
+  HostChannel dev_ch(m31);
+  const uint8_t* hp = reinterpret_cast<const uint8_t*>(h_pinned);
+  size_t alpha_off = 0, chan_off = 0, flag_off = 0, last_off = 0;
+  {
+    uint8_t* hpw = reinterpret_cast<uint8_t*>(h_pinned);
     size_t off = 0;
-    STWO_CUDA_TRY(cudaMemcpyAsync(hp + off, tq.layer(0), 32, cudaMemcpyDeviceToHost, s));
+    STWO_CUDA_TRY(cudaMemcpyAsync(hpw + off, tq.layer(0), 32, cudaMemcpyDeviceToHost, s));
     off += 32;
     for (auto& l : fri) {
-      STWO_CUDA_TRY(cudaMemcpyAsync(hp + off, l.tree.layer(0), 32, cudaMemcpyDeviceToHost, s));
+      STWO_CUDA_TRY(cudaMemcpyAsync(hpw + off, l.tree.layer(0), 32, cudaMemcpyDeviceToHost, s));
       off += 32;
     }
-    size_t alpha_off = off;
-    STWO_CUDA_TRY(cudaMemcpyAsync(hp + off, d_alphas, (fri.size() + 1) * sizeof(qm31), cudaMemcpyDeviceToHost, s));
+    alpha_off = off;
+    STWO_CUDA_TRY(cudaMemcpyAsync(hpw + off, d_alphas, (fri.size() + 1) * sizeof(qm31), cudaMemcpyDeviceToHost, s));
     off += (fri.size() + 1) * sizeof(qm31);
-    size_t chan_off = off;
-    STWO_CUDA_TRY(cudaMemcpyAsync(hp + off, d_chan, sizeof(DevChannel), cudaMemcpyDeviceToHost, s));
+    chan_off = off;
+    STWO_CUDA_TRY(cudaMemcpyAsync(hpw + off, d_chan, sizeof(DevChannel), cudaMemcpyDeviceToHost, s));
     off += sizeof(DevChannel);
-    const size_t flag_off = off;
-    STWO_CUDA_TRY(cudaMemcpyAsync(hp + off, d_found + kStreamErrWord, 4, cudaMemcpyDeviceToHost, s));
+    flag_off = off;
+    STWO_CUDA_TRY(cudaMemcpyAsync(hpw + off, d_found + kStreamErrWord, 4, cudaMemcpyDeviceToHost, s));
+    off += 16;
+    last_off = off;
+    STWO_ARG_CHECK(off + 16 * n_last <= h_pinned_bytes, "pinned staging too small for the last layer");
+    STWO_CUDA_TRY(cudaMemcpyAsync(hpw + off, d_last, 16 * n_last, cudaMemcpyDeviceToHost, s));
     STWO_CUDA_TRY(cudaStreamSynchronize(s));
     const DevChannel* dc = reinterpret_cast<const DevChannel*>(hp + chan_off);
     if (dc->error) return set_err(err, err_len, STWO_B200_ESTATE, "device channel: draw retry bound exhausted");
     if (*reinterpret_cast<const uint32_t*>(hp + flag_off))
       return set_err(err, err_len, STWO_B200_ETIMEOUT, "column stream: a bulk copy did not complete in time");
-    const qm31* dev_alpha = reinterpret_cast<const qm31*>(hp + alpha_off);
-    for (size_t i = 0; i < fri_roots.size(); i++) {
-      std::memcpy(fri_roots[i].data(), hp + 32 * i, 32);
-      ch.mix_root(fri_roots[i]);
-      qm31 a = ch.draw_secure_felt();
-      if (!qm31_eq(a, dev_alpha[i]))
-        return set_err(err, err_len, STWO_B200_ESTATE, "device and host channels diverged at FRI layer %zu", i);
-    }
+    dev_ch.set_state(dc->digest, dc->n_draws);
+    for (size_t i = 0; i < fri_roots.size(); i++) std::memcpy(fri_roots[i].data(), hp + 32 * i, 32);
   }
   // Last layer (prover/fri.rs:274-291).
   std::vector<qm31> last_coeffs;
   {
-    const uint64_t n_last = 1ull << last_log;
-    STWO_CUDA_TRY(cudaMemcpyAsync(h_pinned, d_last, 16 * n_last, cudaMemcpyDeviceToHost, s));
-    STWO_CUDA_TRY(cudaStreamSynchronize(s));
-    const uint32_t* hv = reinterpret_cast<const uint32_t*>(h_pinned);
+    const uint32_t* hv = reinterpret_cast<const uint32_t*>(hp + last_off);
     std::vector<qm31> v(n_last);
     for (uint64_t i = 0; i < n_last; i++) v[i] = {hv[i], hv[n_last + i], hv[2 * n_last + i], hv[3 * n_last + i]};
     // LineEvaluation::interpolate (prover/line.rs:54-99): bit-reverse, line IFFT, 1/n.
@@ -1766,25 +1791,45 @@ int WideFibProver::prove_body(const uint32_t* d_a, const uint32_t* d_b, ProofOut
       if (!qm31_eq(v[i], qm31_zero())) return set_err(err, err_len, STWO_B200_ESTATE, "invalid degree");
     v.resize(bound);
     last_coeffs = v;
-    ch.mix_felts(last_coeffs.data(), last_coeffs.size());
+    dev_ch.mix_felts(last_coeffs.data(), last_coeffs.size());
   }
 
   // ---- proof of work (pcs/mod.rs:140-142) ----
   uint64_t nonce = 0;
   phase(kGrind);
   {
-    Hash32 pre = ch.pow_prefixed(cfg.pow_bits);
+    Hash32 pre = dev_ch.pow_prefixed(cfg.pow_bits);
     Digest8 d;
     std::memcpy(d.w, pre.data(), 32);
     bool found = false;
+    bool replayed = false;
     for (uint32_t hi = 0; !found; hi++) {
       for (uint32_t base = 0; base < (1u << 20) && !found; base += 1u << 16) {
-        uint32_t init = 0xFFFFFFFFu;
-        STWO_CUDA_TRY(cudaMemcpyAsync(d_found, &init, 4, cudaMemcpyHostToDevice, s));
+        STWO_CUDA_TRY(cudaMemsetAsync(d_found, 0xFF, 4, s));
         grind_kernel<<<(1u << 16) / 256, 256, 0, s>>>(d, hi, base, cfg.pow_bits, m31, d_found);
         STWO_CHECK_LAUNCH();
-        uint32_t* hf = reinterpret_cast<uint32_t*>(h_pinned);
+        uint32_t* hf = reinterpret_cast<uint32_t*>(h_pinned) + (h_pinned_bytes / 4 - 1);
         STWO_CUDA_TRY(cudaMemcpyAsync(hf, d_found, 4, cudaMemcpyDeviceToHost, s));
+        if (!replayed) {
+          // host replay of the FRI transcript while the batch runs
+          replayed = true;
+          const qm31* dev_alpha = reinterpret_cast<const qm31*>(hp + alpha_off);
+          for (size_t i = 0; i < fri_roots.size(); i++) {
+            ch.mix_root(fri_roots[i]);
+            qm31 a = ch.draw_secure_felt();
+            if (!qm31_eq(a, dev_alpha[i])) {
+              cudaStreamSynchronize(s);
+              return set_err(err, err_len, STWO_B200_ESTATE, "device and host channels diverged at FRI layer %zu",
+                             i);
+            }
+          }
+          const DevChannel* dc = reinterpret_cast<const DevChannel*>(hp + chan_off);
+          if (std::memcmp(ch.digest().data(), dc->digest, 32) != 0 || ch.n_draws() != dc->n_draws) {
+            cudaStreamSynchronize(s);
+            return set_err(err, err_len, STWO_B200_ESTATE, "device and host channel states differ after FRI");
+          }
+          ch.mix_felts(last_coeffs.data(), last_coeffs.size());
+        }
         STWO_CUDA_TRY(cudaStreamSynchronize(s));
         if (*hf != 0xFFFFFFFFu) {
           nonce = ((uint64_t)hi << 32) | *hf;
@@ -1889,7 +1934,9 @@ int WideFibProver::prove_body(const uint32_t* d_a, const uint32_t* d_b, ProofOut
       size_t m = std::min(chunk, n - off);
       std::memcpy(h_pinned, g.addrs.data() + off, m * 8);
       STWO_CUDA_TRY(cudaMemcpyAsync(d_gather_addr + off, h_pinned, m * 8, cudaMemcpyHostToDevice, s));
-      STWO_CUDA_TRY(cudaStreamSynchronize(s));
+      // the staging buffer is reused by the next chunk only; the gather and
+      // the download below are ordered after the upload on the stream
+      if (off + m < n) STWO_CUDA_TRY(cudaStreamSynchronize(s));
     }
     gather_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(d_gather_addr, (uint32_t)n, d_gather_out);
     STWO_CHECK_LAUNCH();
