@@ -296,9 +296,13 @@ __global__ void __launch_bounds__(256) oods_reduce_kernel(const qm31* __restrict
 // (Re z.x - p.x) Im z.y - (Re z.y - p.y) Im z.x in CM31.  Equal, value for
 // value, to the line-coefficient form of prover/backend/simd/quotients.rs:34-164
 // with core/constraints.rs:119-134 coefficients.
-struct QuotientParams {
+// Per-proof constants of the quotient rows (they depend on the OODS point
+// and the sampled values): written in device memory by fs_quotient_kernel.
+struct QuotientDyn {
   qm31 c, A, B;
   cm31 prx, pix, pry, piy;
+};
+struct QuotientParams {
   cpoint init;           // first point of the half coset
   cpoint step_pow[31];   // step * 2^b
   uint32_t log_size;     // lifting domain
@@ -306,7 +310,10 @@ struct QuotientParams {
 };
 
 __global__ void __launch_bounds__(256) quotient_kernel(QuotientParams q, PolyTable cols, uint32_t n_cols,
-                                                      const qm31* __restrict__ alpha_pows, uint32_t* __restrict__ out) {
+                                                      const qm31* __restrict__ alpha_pows,
+                                                      const QuotientDyn* __restrict__ dyn,
+                                                      uint32_t* __restrict__ out) {
+  const QuotientDyn qd = *dyn;
   const uint64_t n = 1ull << q.log_size;
   const uint64_t half = n >> 1;
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
@@ -334,10 +341,10 @@ __global__ void __launch_bounds__(256) quotient_kernel(QuotientParams q, PolyTab
     for (uint32_t b = 0; b + 1 < q.log_size; b++)
       if ((jj >> b) & 1) pt = cpoint_add(pt, q.step_pow[b]);
     if (j >= half) pt.y = m31_neg(pt.y);  // -index is the conjugate point
-    qm31 num = qm31_sub(qm31_mul(q.c, acc), q.B);
-    qm31 full = qm31_sub(num, qm31_mul_m31(q.A, pt.y));
-    cm31 den = cm31_sub(cm31_mul(cm31_sub(q.prx, cm31{pt.x, 0}), q.piy),
-                        cm31_mul(cm31_sub(q.pry, cm31{pt.y, 0}), q.pix));
+    qm31 num = qm31_sub(qm31_mul(qd.c, acc), qd.B);
+    qm31 full = qm31_sub(num, qm31_mul_m31(qd.A, pt.y));
+    cm31 den = cm31_sub(cm31_mul(cm31_sub(qd.prx, cm31{pt.x, 0}), qd.piy),
+                        cm31_mul(cm31_sub(qd.pry, cm31{pt.y, 0}), qd.pix));
     qm31 v = qm31_mul_cm31(full, cm31_inv(den));
     out[i] = v.a;
     out[n + i] = v.b;
@@ -362,7 +369,10 @@ __device__ __forceinline__ cpoint quotient_point(const QuotientParams& q, uint64
 }
 
 __global__ void __launch_bounds__(256) quotient4_kernel(QuotientParams q, PolyTable cols, uint32_t n_cols,
-                                                       const qm31* __restrict__ alpha_pows, uint32_t* __restrict__ out) {
+                                                       const qm31* __restrict__ alpha_pows,
+                                                       const QuotientDyn* __restrict__ dyn,
+                                                       uint32_t* __restrict__ out) {
+  const QuotientDyn qd = *dyn;
   const uint64_t n = 1ull << q.log_size;
   const uint64_t n4 = n >> 2;
   for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < n4; t += (uint64_t)gridDim.x * blockDim.x) {
@@ -401,10 +411,10 @@ __global__ void __launch_bounds__(256) quotient4_kernel(QuotientParams q, PolyTa
 #pragma unroll
     for (int r = 0; r < 4; r++) {
       const cpoint pt = quotient_point(q, i + r);
-      const qm31 num = qm31_sub(qm31_mul(q.c, acc4_reduce(s4[r])), q.B);
-      full[r] = qm31_sub(num, qm31_mul_m31(q.A, pt.y));
-      den[r] = cm31_sub(cm31_mul(cm31_sub(q.prx, cm31{pt.x, 0}), q.piy),
-                        cm31_mul(cm31_sub(q.pry, cm31{pt.y, 0}), q.pix));
+      const qm31 num = qm31_sub(qm31_mul(qd.c, acc4_reduce(s4[r])), qd.B);
+      full[r] = qm31_sub(num, qm31_mul_m31(qd.A, pt.y));
+      den[r] = cm31_sub(cm31_mul(cm31_sub(qd.prx, cm31{pt.x, 0}), qd.piy),
+                        cm31_mul(cm31_sub(qd.pry, cm31{pt.y, 0}), qd.pix));
       norm[r] = m31_add(m31_sqr(den[r].a), m31_sqr(den[r].b));
     }
     // Montgomery batch inversion of the four norms.
@@ -522,7 +532,9 @@ __global__ void __launch_bounds__(kStreamThreads) composition_tma_kernel(
 __global__ void __launch_bounds__(kStreamThreads) quotient_tma_kernel(QuotientParams q, PolyTable cols,
                                                                      uint32_t n_cols,
                                                                      const qm31* __restrict__ alpha_pows,
+                                                                     const QuotientDyn* __restrict__ dyn,
                                                                      uint32_t* __restrict__ out, uint32_t* err) {
+  const QuotientDyn qd = *dyn;
   extern __shared__ __align__(128) uint32_t smem[];
   __shared__ uint64_t bars[kStreamS];
   __shared__ cpoint s_base;
@@ -577,10 +589,10 @@ __global__ void __launch_bounds__(kStreamThreads) quotient_tma_kernel(QuotientPa
     uint32_t norm[4];
 #pragma unroll
     for (int r = 0; r < 4; r++) {
-      const qm31 num = qm31_sub(qm31_mul(q.c, acc4_reduce(s4[r])), q.B);
-      full[r] = qm31_sub(num, qm31_mul_m31(q.A, ys[r]));
-      den[r] = cm31_sub(cm31_mul(cm31_sub(q.prx, cm31{xs[r], 0}), q.piy),
-                        cm31_mul(cm31_sub(q.pry, cm31{ys[r], 0}), q.pix));
+      const qm31 num = qm31_sub(qm31_mul(qd.c, acc4_reduce(s4[r])), qd.B);
+      full[r] = qm31_sub(num, qm31_mul_m31(qd.A, ys[r]));
+      den[r] = cm31_sub(cm31_mul(cm31_sub(qd.prx, cm31{xs[r], 0}), qd.piy),
+                        cm31_mul(cm31_sub(qd.pry, cm31{ys[r], 0}), qd.pix));
       norm[r] = m31_add(m31_sqr(den[r].a), m31_sqr(den[r].b));
     }
     // Montgomery batch inversion of the four norms.
@@ -662,9 +674,8 @@ __device__ void dev_finalize(uint32_t h[8], bool m31) {
     for (int k = 0; k < 8; k++) h[k] = m31_reduce_u32(h[k]);
 }
 
-// mix_root (digest <- H(digest || root)), then draw_secure_felt into *alpha;
-// one thread.
-__device__ void dev_mix_root_draw(DevChannel* ch, const uint32_t* root, qm31* alpha) {
+// digest <- H(digest || root) (core/vcs_lifted/blake2_merkle.rs:49-56); one thread.
+__device__ void dev_chan_mix_root(DevChannel* ch, const uint32_t* root) {
   uint32_t m[16];
   for (int k = 0; k < 8; k++) m[k] = ch->digest[k];
   for (int k = 0; k < 8; k++) m[8 + k] = root[k];
@@ -673,9 +684,15 @@ __device__ void dev_mix_root_draw(DevChannel* ch, const uint32_t* root, qm31* al
   blake2s_compress_lat(h, m, 64, true);
   dev_finalize(h, ch->m31 != 0);
   for (int k = 0; k < 8; k++) ch->digest[k] = h[k];
-  uint32_t n_draws = 0;
-  // draw_base_felts: retry until all 8 words are below 2P (probability of a
-  // retry ~2^-28 per draw); bounded, with an error flag instead of a hang.
+  ch->n_draws = 0;
+}
+
+// draw_secure_felt (core/channel/blake2s.rs:72-120): draw_base_felts retries
+// until all 8 words are below 2P (probability of a retry ~2^-28 per draw);
+// bounded, with an error flag instead of a hang.  One thread.
+__device__ qm31 dev_chan_draw_felt(DevChannel* ch) {
+  uint32_t m[16], h[8];
+  uint32_t n_draws = ch->n_draws;
   for (int attempt = 0; attempt < 64; attempt++) {
     for (int k = 0; k < 8; k++) m[k] = ch->digest[k];
     m[8] = n_draws;
@@ -687,14 +704,174 @@ __device__ void dev_mix_root_draw(DevChannel* ch, const uint32_t* root, qm31* al
     bool okw = true;
     for (int k = 0; k < 8; k++) okw = okw && h[k] < 2 * M31_P;
     if (okw) {
-      *alpha = {m31_reduce_u32(h[0]), m31_reduce_u32(h[1]), m31_reduce_u32(h[2]), m31_reduce_u32(h[3])};
       ch->n_draws = n_draws;
-      return;
+      return {m31_reduce_u32(h[0]), m31_reduce_u32(h[1]), m31_reduce_u32(h[2]), m31_reduce_u32(h[3])};
     }
   }
   ch->error = 1;
   ch->n_draws = n_draws;
-  *alpha = qm31_zero();
+  return qm31_zero();
+}
+
+// digest <- H(digest || LE32 coordinates of f[0..n)) (core/channel/blake2s.rs:54-64);
+// one thread streams the 32 + 16 n bytes through 64-byte blocks.
+__device__ void dev_chan_mix_felts(DevChannel* ch, const qm31* __restrict__ f, uint32_t n) {
+  const uint32_t total_words = 8 + 4 * n;
+  const uint32_t blocks = (total_words + 15) / 16;
+  uint32_t h[8], m[16];
+  blake2s_init(h);
+  for (uint32_t bk = 0; bk < blocks; bk++) {
+    for (int k = 0; k < 16; k++) {
+      const uint32_t w = bk * 16 + k;
+      uint32_t v = 0;
+      if (w < 8) {
+        v = ch->digest[w];
+      } else if (w < total_words) {
+        const qm31 x = f[(w - 8) >> 2];
+        const uint32_t c = (w - 8) & 3;
+        v = c == 0 ? x.a : c == 1 ? x.b : c == 2 ? x.c : x.d;
+      }
+      m[k] = v;
+    }
+    const bool last = bk + 1 == blocks;
+    blake2s_compress_lat(h, m, last ? 4 * total_words : 64 * (bk + 1), last);
+  }
+  dev_finalize(h, ch->m31 != 0);
+  for (int k = 0; k < 8; k++) ch->digest[k] = h[k];
+  ch->n_draws = 0;
+}
+
+// mix_root, then draw_secure_felt into *alpha; one thread.
+__device__ void dev_mix_root_draw(DevChannel* ch, const uint32_t* root, qm31* alpha) {
+  dev_chan_mix_root(ch, root);
+  *alpha = dev_chan_draw_felt(ch);
+}
+
+__device__ qm31 qm31_pow_u32(qm31 x, uint32_t e) {
+  qm31 r = qm31_one();
+  while (e) {
+    if (e & 1) r = qm31_mul(r, x);
+    x = qm31_mul(x, x);
+    e >>= 1;
+  }
+  return r;
+}
+
+// ---- device-side Fiat-Shamir steps before the FRI commit ----
+// Each mixes one commitment into the device channel, draws the next random
+// value and derives what the following kernels read, so the prover enqueues
+// the whole commit-to-FRI sequence without a host round trip.  The host
+// replays the transcript from the downloaded roots and values afterwards.
+// FsOut holds the drawn values for that replay.
+struct FsOut {
+  qm31 random_coeff;  // composition (prover/mod.rs:57-63)
+  qm31 oods_t;        // OODS point parameter (core/circle.rs get_random_point)
+  qm31 oods_x, oods_y;
+  qm31 quotient_coeff;  // pcs/mod.rs:112
+};
+
+// Trace root -> composition random coefficient and its reversed powers
+// pw[n_cons - 1 - k] = coeff^k.
+__global__ void fs_composition_kernel(DevChannel* ch, const uint8_t* root, uint32_t n_cons, qm31* __restrict__ pw,
+                                      FsOut* out) {
+  __shared__ qm31 s_rc;
+  if (threadIdx.x == 0) {
+    dev_chan_mix_root(ch, reinterpret_cast<const uint32_t*>(root));
+    s_rc = dev_chan_draw_felt(ch);
+    out->random_coeff = s_rc;
+  }
+  __syncthreads();
+  for (uint32_t k = threadIdx.x; k < n_cons; k += blockDim.x) pw[n_cons - 1 - k] = qm31_pow_u32(s_rc, k);
+}
+
+// Composition root -> OODS point ((1 - t^2) / (1 + t^2), 2t / (1 + t^2)), its
+// fold factors f = [y, x, pi(x), ...] and the weight tables of
+// oods_eval_kernel (w_lo over f[0..h), w_hi over f[h..lg)).
+__global__ void fs_oods_kernel(DevChannel* ch, const uint8_t* root, uint32_t lg, uint32_t h, qm31* __restrict__ w_lo,
+                               qm31* __restrict__ w_hi, FsOut* out) {
+  __shared__ qm31 f[32];
+  if (threadIdx.x == 0) {
+    dev_chan_mix_root(ch, reinterpret_cast<const uint32_t*>(root));
+    const qm31 t = dev_chan_draw_felt(ch);
+    const qm31 t2s = qm31_mul(t, t);
+    const qm31 inv1 = qm31_inv(qm31_add(t2s, qm31_one()));
+    const qm31 x = qm31_mul(qm31_add(qm31_one(), qm31_neg(t2s)), inv1);
+    const qm31 y = qm31_mul(qm31_add(t, t), inv1);
+    out->oods_t = t;
+    out->oods_x = x;
+    out->oods_y = y;
+    f[0] = y;
+    qm31 xx = x;
+    for (uint32_t b = 1; b < lg; b++) {
+      f[b] = xx;
+      xx = qm31_double_x(xx);
+    }
+  }
+  __syncthreads();
+  const uint32_t hi_bits = lg - h;
+  for (uint32_t t = threadIdx.x; t < (1u << h); t += blockDim.x) {
+    qm31 w = qm31_one();
+    for (uint32_t b = 0; b < h; b++)
+      if ((t >> b) & 1) w = qm31_mul(w, f[b]);
+    w_lo[t] = w;
+  }
+  for (uint32_t t = threadIdx.x; t < (1u << hi_bits); t += blockDim.x) {
+    qm31 w = qm31_one();
+    for (uint32_t b = 0; b < hi_bits; b++)
+      if ((t >> b) & 1) w = qm31_mul(w, f[h + b]);
+    w_hi[t] = w;
+  }
+}
+
+// Sampled values -> quotient random coefficient q, its powers ap[k] = q^k and
+// the row constants (pcs/quotient_ops.rs:134-233 in the form of
+// quotient_kernel): c = conj(y) - y, A = sum q^k (conj(v_k) - v_k),
+// B = sum q^k (v_k c - (conj(v_k) - v_k) y) over the nq sampled values.
+constexpr int kFsThreads = 256;
+__global__ void __launch_bounds__(kFsThreads) fs_quotient_kernel(DevChannel* ch, const qm31* __restrict__ vals,
+                                                                 uint32_t nq, qm31* __restrict__ ap, QuotientDyn* dyn,
+                                                                 FsOut* out) {
+  __shared__ qm31 s_q;
+  __shared__ qm31 sa[kFsThreads], sb[kFsThreads];
+  if (threadIdx.x == 0) {
+    dev_chan_mix_felts(ch, vals, nq);
+    s_q = dev_chan_draw_felt(ch);
+    out->quotient_coeff = s_q;
+  }
+  __syncthreads();
+  const qm31 x = out->oods_x, y = out->oods_y;
+  const qm31 cz = qm31_sub(qm31_conj(y), y);
+  qm31 A = qm31_zero(), B = qm31_zero();
+  for (uint32_t k = threadIdx.x; k < nq; k += blockDim.x) {
+    const qm31 pk = qm31_pow_u32(s_q, k);
+    const qm31 v = vals[k];
+    const qm31 a = qm31_sub(qm31_conj(v), v);
+    const qm31 b = qm31_sub(qm31_mul(v, cz), qm31_mul(a, y));
+    A = qm31_add(A, qm31_mul(pk, a));
+    B = qm31_add(B, qm31_mul(pk, b));
+    ap[k] = pk;
+  }
+  sa[threadIdx.x] = A;
+  sb[threadIdx.x] = B;
+  __syncthreads();
+  for (uint32_t o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) {
+      sa[threadIdx.x] = qm31_add(sa[threadIdx.x], sa[threadIdx.x + o]);
+      sb[threadIdx.x] = qm31_add(sb[threadIdx.x], sb[threadIdx.x + o]);
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    QuotientDyn d;
+    d.c = cz;
+    d.A = sa[0];
+    d.B = sb[0];
+    d.prx = {x.a, x.b};
+    d.pix = {x.c, x.d};
+    d.pry = {y.a, y.b};
+    d.piy = {y.c, y.d};
+    *dyn = d;
+  }
 }
 
 __global__ void channel_mix_root_draw_kernel(DevChannel* ch, const uint8_t* root, qm31* alpha) {
@@ -1149,6 +1326,8 @@ class WideFibProver {
   uint32_t* d_last = nullptr;     // 4 x 2^last_log
   qm31* d_small = nullptr;        // powers / weights / partials / alpha powers
   uint32_t* d_denom = nullptr;
+  FsOut* d_fs = nullptr;         // values drawn by the device Fiat-Shamir steps
+  QuotientDyn* d_qdyn = nullptr;  // per-proof quotient row constants
   uint32_t* d_found = nullptr;
   DevChannel* d_chan = nullptr;
   qm31* d_alphas = nullptr;       // folding alphas of the FRI layers
@@ -1160,6 +1339,9 @@ class WideFibProver {
   DevChannel* h_chan = nullptr;   // staging of the device channel state (own region: the
                                   // quotient upload from h_pinned may still be in flight)
   size_t h_pinned_bytes = 0;
+  uint8_t* h_tx = nullptr;          // pre-FRI transcript download: roots 1-2, FsOut, sampled values
+  size_t h_tx_bytes = 0;
+  cudaEvent_t ev_tx = nullptr;      // recorded after that download
   std::vector<void*> allocs;
 
   // The prover enqueues on its own non-blocking stream `s` (so the FRI commit
@@ -1182,9 +1364,11 @@ class WideFibProver {
     for (cudaEvent_t e : graph_events) cudaEventDestroy(e);
     if (ev_in) cudaEventDestroy(ev_in);
     if (ev_out) cudaEventDestroy(ev_out);
+    if (ev_tx) cudaEventDestroy(ev_tx);
     for (cudaEvent_t e : ev_pool) cudaEventDestroy(e);
     for (void* p : allocs) cudaFree(p);  // empty in measure mode
     if (h_pinned) cudaFreeHost(h_pinned);
+    if (h_tx) cudaFreeHost(h_tx);
     if (h_chan) cudaFreeHost(h_chan);
     if (s) cudaStreamDestroy(s);
   }
@@ -1213,6 +1397,7 @@ class WideFibProver {
       STWO_CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
       STWO_CUDA_TRY(cudaEventCreateWithFlags(&ev_in, cudaEventDisableTiming));
       STWO_CUDA_TRY(cudaEventCreateWithFlags(&ev_out, cudaEventDisableTiming));
+      STWO_CUDA_TRY(cudaEventCreateWithFlags(&ev_tx, cudaEventDisableTiming));
       STWO_CUDA_TRY(
           cudaFuncSetAttribute(fri_tail_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFriTailSmem));
       STWO_CUDA_TRY(cudaFuncSetAttribute(tree_top_channel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1286,10 +1471,36 @@ class WideFibProver {
     if ((rc = alloc((void**)&d_found, 64, err, err_len))) return rc;
     if ((rc = alloc((void**)&d_chan, sizeof(DevChannel), err, err_len))) return rc;
     if ((rc = alloc((void**)&d_alphas, (fri.size() + 2) * sizeof(qm31), err, err_len))) return rc;
+    if ((rc = alloc((void**)&d_fs, sizeof(FsOut), err, err_len))) return rc;
+    if ((rc = alloc((void**)&d_qdyn, sizeof(QuotientDyn), err, err_len))) return rc;
     h_pinned_bytes = std::max<size_t>(small_q * sizeof(qm31), (16ull << last_log) + 65536);
     if (measure) return 0;
     STWO_CUDA_TRY(cudaMallocHost((void**)&h_pinned, h_pinned_bytes));
     STWO_CUDA_TRY(cudaMallocHost((void**)&h_chan, sizeof(DevChannel)));
+    h_tx_bytes = 64 + sizeof(FsOut) + (size_t)(N + 8) * sizeof(qm31);
+    STWO_CUDA_TRY(cudaMallocHost((void**)&h_tx, h_tx_bytes));
+    {
+      // Vanishing inverses of the 2^(eval_log - log_n) trace-coset classes,
+      // bit-reversed (a function of the sizes only).
+      const uint32_t log_expand = eval_log - log_n;
+      uint32_t* dn = reinterpret_cast<uint32_t*>(h_pinned);
+      for (uint32_t j = 0; j < (1u << log_expand); j++) {
+        // eval_domain.at(j): half coset of CanonicCoset(eval_log)
+        uint64_t init = 1ull << (31 - (eval_log + 1)), step = 1ull << (31 - (eval_log - 1));
+        uint64_t half = 1ull << (eval_log - 1);
+        uint64_t idx =
+            j < half ? (init + step * j) : ((1ull << 31) - ((init + step * (j - half)) & ((1ull << 31) - 1)));
+        cpoint p = index_to_cpoint(idx);
+        // coset_vanishing(CanonicCoset(log_n).coset, p) (core/constraints.rs:12-34)
+        uint64_t cinit = 1ull << (31 - (log_n + 1)), cstep = 1ull << (31 - log_n);
+        cpoint ci = index_to_cpoint(cinit);
+        cpoint sh = cpoint_add(cpoint_add(p, cpoint{ci.x, m31_neg(ci.y)}), index_to_cpoint(cstep >> 1));
+        uint32_t x = sh.x;
+        for (uint32_t i = 1; i < log_n; i++) x = m31_sub(m31_add(m31_sqr(x), m31_sqr(x)), 1);
+        dn[bitrev32(j, log_expand)] = m31_inv(x);
+      }
+      STWO_CUDA_TRY(cudaMemcpyAsync(d_denom, dn, 4ull << log_expand, cudaMemcpyHostToDevice, s));
+    }
     STWO_CUDA_TRY(cudaStreamSynchronize(s));
     return 0;
   }
@@ -1466,6 +1677,16 @@ int WideFibProver::prove_body(const uint32_t* d_a, const uint32_t* d_b, ProofOut
     root0 = e.finalize(m31);
   }
   ch.mix_root(root0);
+  // The device channel carries the transcript from here to the end of the
+  // FRI commit; the host replays it after one download.
+  {
+    DevChannel* hc = h_chan;
+    std::memset(hc, 0, sizeof(DevChannel));
+    std::memcpy(hc->digest, ch.digest().data(), 32);
+    hc->n_draws = ch.n_draws();
+    hc->m31 = m31 ? 1 : 0;
+    STWO_CUDA_TRY(cudaMemcpyAsync(d_chan, hc, sizeof(DevChannel), cudaMemcpyHostToDevice, s));
+  }
 
   // ---- tree 1: trace ----
   phase(kTraceGen);
@@ -1487,41 +1708,11 @@ int WideFibProver::prove_body(const uint32_t* d_a, const uint32_t* d_b, ProofOut
     return rc;
   phase(kTraceMerkle);
   if ((rc = commit_columns(eval_ptrs.data(), logs_1, t1, err, err_len))) return rc;
-  Hash32 root1;
-  if ((rc = download_root(t1, root1, err, err_len))) return rc;
-  ch.mix_root(root1);
-
   // ---- composition (prover/mod.rs:57-77) ----
-  const qm31 random_coeff = ch.draw_secure_felt();
   const uint32_t n_cons = N - 2;
   phase(kComposition);
-  {
-    qm31* pw = h_pinned;
-    qm31 acc = qm31_one();
-    for (uint32_t k = 0; k < n_cons; k++) {
-      pw[n_cons - 1 - k] = acc;  // reversed powers
-      acc = qm31_mul(acc, random_coeff);
-    }
-    STWO_CUDA_TRY(cudaMemcpyAsync(d_small, pw, n_cons * sizeof(qm31), cudaMemcpyHostToDevice, s));
-    // vanishing inverses of the 2^(eval_log - log_n) trace-coset classes, bit-reversed
-    uint32_t log_expand = eval_log - log_n;
-    uint32_t* dn = reinterpret_cast<uint32_t*>(h_pinned + n_cons + 1);
-    for (uint32_t j = 0; j < (1u << log_expand); j++) {
-      // eval_domain.at(j): half coset of CanonicCoset(eval_log)
-      uint64_t init = 1ull << (31 - (eval_log + 1)), step = 1ull << (31 - (eval_log - 1));
-      uint64_t half = 1ull << (eval_log - 1);
-      uint64_t idx = j < half ? (init + step * j) : ((1ull << 31) - ((init + step * (j - half)) & ((1ull << 31) - 1)));
-      cpoint p = index_to_cpoint(idx);
-      // coset_vanishing(CanonicCoset(log_n).coset, p) (core/constraints.rs:12-34)
-      uint64_t cinit = 1ull << (31 - (log_n + 1)), cstep = 1ull << (31 - log_n);
-      cpoint ci = index_to_cpoint(cinit);
-      cpoint sh = cpoint_add(cpoint_add(p, cpoint{ci.x, m31_neg(ci.y)}), index_to_cpoint(cstep >> 1));
-      uint32_t x = sh.x;
-      for (uint32_t i = 1; i < log_n; i++) x = m31_sub(m31_add(m31_sqr(x), m31_sqr(x)), 1);
-      dn[bitrev32(j, log_expand)] = m31_inv(x);
-    }
-    STWO_CUDA_TRY(cudaMemcpyAsync(d_denom, dn, 4ull << log_expand, cudaMemcpyHostToDevice, s));
-  }
+  fs_composition_kernel<<<1, 128, 0, s>>>(d_chan, t1.layer(0), n_cons, d_small, d_fs);
+  STWO_CHECK_LAUNCH();
   const uint32_t* comp_src = d_evals;
   uint64_t comp_stride = 1ull << L1;
   if (eval_log != L1) {
@@ -1568,80 +1759,40 @@ int WideFibProver::prove_body(const uint32_t* d_a, const uint32_t* d_b, ProofOut
     return rc;
   phase(kCompMerkle);
   if ((rc = commit_columns(lde.data(), logs_2, t2, err, err_len))) return rc;
-  Hash32 root2;
-  if ((rc = download_root(t2, root2, err, err_len))) return rc;
-  ch.mix_root(root2);
 
   // ---- OODS point and sampled values (prover/mod.rs:80-119, pcs/mod.rs:512-689) ----
-  spoint oods;
-  {
-    qm31 t = ch.draw_secure_felt();
-    qm31 t2s = qm31_mul(t, t);
-    qm31 inv1 = qm31_inv(qm31_add(t2s, qm31_one()));
-    oods = {qm31_mul(qm31_add(qm31_one(), qm31_neg(t2s)), inv1), qm31_mul(qm31_add(t, t), inv1)};
-  }
   const uint32_t max_log_degree_bound = lift - blowup;
-  std::vector<qm31> sampled(N + 8);
+  const uint32_t np = N + 8;
+  qm31* d_vals = nullptr;
   {
     // Every column is committed at the lifting size, so all 108 polynomials
     // (log_n coefficients each) are sampled at the OODS point itself.
     STWO_ARG_CHECK(L1 == lift && eval_log - 1 == log_n, "sampling assumes one column size");
+    STWO_ARG_CHECK(log_n <= 31, "log size too large for the fold factors");
     const uint32_t lg = log_n, h = lg / 2;
-    OodsFolds f{};
-    f.f[0] = oods.y;
-    qm31 x = oods.x;
-    for (uint32_t b = 1; b < lg; b++) {
-      f.f[b] = x;
-      x = qm31_double_x(x);
-    }
     size_t n_w = (1u << h) + (1u << (lg - h));
     phase(kOodsSampling);
-    {
-      const uint32_t nt = 1u << std::max(h, lg - h);
-      oods_weights_kernel<<<(nt + 255) / 256, 256, 0, s>>>(f, h, lg - h, d_small, d_small + (1u << h));
-      STWO_CHECK_LAUNCH();
-    }
+    fs_oods_kernel<<<1, 1024, 0, s>>>(d_chan, t2.layer(0), lg, h, d_small, d_small + (1u << h), d_fs);
+    STWO_CHECK_LAUNCH();
     PolyTable pt;
-    uint32_t np = N + 8;
     for (uint32_t c = 0; c < N; c++) pt.p[c] = coeff_ptrs[c];
     for (int k = 0; k < 8; k++) pt.p[N + k] = split[k];
     const uint32_t chunks = lg > 10 ? 1u << (lg - 10) : 1u;  // kOodsChunk indices each
-    qm31* d_vals = d_small + n_w;
+    d_vals = d_small + n_w;
     oods_eval_kernel<<<chunks, 256, 0, s>>>(pt, np, lg, h, d_small, d_small + (1u << h), d_oods_partial);
     STWO_CHECK_LAUNCH();
     oods_reduce_kernel<<<np, 256, 0, s>>>(d_oods_partial, chunks, d_vals);
     STWO_CHECK_LAUNCH();
-    STWO_CUDA_TRY(cudaMemcpyAsync(h_pinned, d_vals, np * sizeof(qm31), cudaMemcpyDeviceToHost, s));
-    STWO_CUDA_TRY(cudaStreamSynchronize(s));
-    std::memcpy(sampled.data(), h_pinned, np * sizeof(qm31));
   }
-  ch.mix_felts(sampled.data(), sampled.size());
 
   // ---- FRI quotients (pcs/mod.rs:112-118, quotient_ops.rs:134-233) ----
-  const qm31 qcoeff = ch.draw_secure_felt();
   {
+    const uint32_t nq = np;
     QuotientParams qp;
-    qm31 cz = qm31_sub(qm31_conj(oods.y), oods.y);
-    qm31 A = qm31_zero(), B = qm31_zero();
-    qm31* ap = h_pinned;
-    qm31 pk = qm31_one();
-    const uint32_t nq = N + 8;
-    for (uint32_t k = 0; k < nq; k++) {
-      qm31 v = sampled[k];
-      qm31 a = qm31_sub(qm31_conj(v), v);
-      qm31 b = qm31_sub(qm31_mul(v, cz), qm31_mul(a, oods.y));
-      A = qm31_add(A, qm31_mul(pk, a));
-      B = qm31_add(B, qm31_mul(pk, b));
-      ap[k] = pk;
-      pk = qm31_mul(pk, qcoeff);
-    }
-    qp.c = cz;
-    qp.A = A;
-    qp.B = B;
-    qp.prx = {oods.x.a, oods.x.b};
-    qp.pix = {oods.x.c, oods.x.d};
-    qp.pry = {oods.y.a, oods.y.b};
-    qp.piy = {oods.y.c, oods.y.d};
+    phase(kQuotients);
+    qm31* d_ap = d_vals + np;  // after the sampled values, which the host downloads later
+    fs_quotient_kernel<<<1, kFsThreads, 0, s>>>(d_chan, d_vals, nq, d_ap, d_qdyn, d_fs);
+    STWO_CHECK_LAUNCH();
     qp.log_size = lift;
     qp.init = index_to_cpoint(1ull << (31 - (lift + 1)));
     cpoint st = index_to_cpoint(1ull << (31 - (lift - 1)));
@@ -1649,8 +1800,6 @@ int WideFibProver::prove_body(const uint32_t* d_a, const uint32_t* d_b, ProofOut
       qp.step_pow[b] = st;
       st = cpoint_add(st, st);
     }
-    phase(kQuotients);
-    STWO_CUDA_TRY(cudaMemcpyAsync(d_small, ap, nq * sizeof(qm31), cudaMemcpyHostToDevice, s));
     PolyTable cols;
     for (uint32_t c = 0; c < N; c++) cols.p[c] = eval_ptrs[c];
     for (int k = 0; k < 8; k++) cols.p[N + k] = lde[k];
@@ -1665,11 +1814,11 @@ int WideFibProver::prove_body(const uint32_t* d_a, const uint32_t* d_b, ProofOut
       quotient_tma_kernel<<<stream_grid(quotient_tma_kernel, kStreamRing + nq * sizeof(uint4),
                                         (uint32_t)((1ull << lift) / kStreamRows)),
                             kStreamThreads, kStreamRing + nq * sizeof(uint4), s>>>(
-          qp, cols, nq, d_small, d_quot, d_found + kStreamErrWord);
+          qp, cols, nq, d_ap, d_qdyn, d_quot, d_found + kStreamErrWord);
     } else if (aligned)
-      quotient4_kernel<<<grid1d(1ull << (lift - 2), 256), 256, 0, s>>>(qp, cols, nq, d_small, d_quot);
+      quotient4_kernel<<<grid1d(1ull << (lift - 2), 256), 256, 0, s>>>(qp, cols, nq, d_ap, d_qdyn, d_quot);
     else
-      quotient_kernel<<<grid1d(1ull << lift, 256), 256, 0, s>>>(qp, cols, nq, d_small, d_quot);
+      quotient_kernel<<<grid1d(1ull << lift, 256), 256, 0, s>>>(qp, cols, nq, d_ap, d_qdyn, d_quot);
     STWO_CHECK_LAUNCH();
   }
 
@@ -1679,44 +1828,72 @@ int WideFibProver::prove_body(const uint32_t* d_a, const uint32_t* d_b, ProofOut
   // downloaded roots and checks the device alphas against its own.
   std::vector<Hash32> fri_roots(1 + fri.size());
   const uint32_t last_log = cfg.log_last_layer_degree_bound + blowup;
-  {
-    DevChannel* hc = h_chan;
-    std::memset(hc, 0, sizeof(DevChannel));
-    std::memcpy(hc->digest, ch.digest().data(), 32);
-    hc->n_draws = ch.n_draws();
-    hc->m31 = m31 ? 1 : 0;
-    STWO_CUDA_TRY(cudaMemcpyAsync(d_chan, hc, sizeof(DevChannel), cudaMemcpyHostToDevice, s));
-  }
+  // Download of the pre-FRI transcript values, so that the host replays
+  // them while the device runs the FRI commit.
+  STWO_CUDA_TRY(cudaMemcpyAsync(h_tx, t1.layer(0), 32, cudaMemcpyDeviceToHost, s));
+  STWO_CUDA_TRY(cudaMemcpyAsync(h_tx + 32, t2.layer(0), 32, cudaMemcpyDeviceToHost, s));
+  STWO_CUDA_TRY(cudaMemcpyAsync(h_tx + 64, d_fs, sizeof(FsOut), cudaMemcpyDeviceToHost, s));
+  STWO_CUDA_TRY(cudaMemcpyAsync(h_tx + 64 + sizeof(FsOut), d_vals, np * sizeof(qm31), cudaMemcpyDeviceToHost, s));
+  STWO_CUDA_TRY(cudaEventRecord(ev_tx, s));
   if ((rc = run_fri(err, err_len))) return rc;
-  // Sanity check (prover/mod.rs:123-138): the composition value rebuilt from
-  // the split halves equals the constraint quotient at the OODS point.  Host
-  // only, so it runs while the device works through the FRI commit.
+  Hash32 root1, root2;
+  std::vector<qm31> sampled(np);
   {
-    const qm31 basis[4] = {qm31_one(), {0, 1, 0, 0}, {0, 0, 1, 0}, {0, 0, 0, 1}};
-    qm31 left = qm31_zero(), right = qm31_zero();
-    for (int k = 0; k < 4; k++) {
-      left = qm31_add(left, qm31_mul(sampled[N + k], basis[k]));
-      right = qm31_add(right, qm31_mul(sampled[N + 4 + k], basis[k]));
+    STWO_CUDA_TRY(cudaEventSynchronize(ev_tx));
+    FsOut fs;
+    std::memcpy(root1.data(), h_tx, 32);
+    std::memcpy(root2.data(), h_tx + 32, 32);
+    std::memcpy(&fs, h_tx + 64, sizeof(FsOut));
+    std::memcpy(sampled.data(), h_tx + 64 + sizeof(FsOut), np * sizeof(qm31));
+    auto fail = [&](int code, const char* what) {
+      cudaStreamSynchronize(s);
+      return set_err(err, err_len, code, "%s", what);
+    };
+    ch.mix_root(root1);
+    const qm31 random_coeff = ch.draw_secure_felt();
+    if (!qm31_eq(random_coeff, fs.random_coeff))
+      return fail(STWO_B200_ESTATE, "device and host channels diverged at the composition coefficient");
+    ch.mix_root(root2);
+    spoint oods;
+    {
+      const qm31 t = ch.draw_secure_felt();
+      const qm31 t2s = qm31_mul(t, t);
+      const qm31 inv1 = qm31_inv(qm31_add(t2s, qm31_one()));
+      oods = {qm31_mul(qm31_add(qm31_one(), qm31_neg(t2s)), inv1), qm31_mul(qm31_add(t, t), inv1)};
+      if (!qm31_eq(t, fs.oods_t) || !qm31_eq(oods.x, fs.oods_x) || !qm31_eq(oods.y, fs.oods_y))
+        return fail(STWO_B200_ESTATE, "device and host channels diverged at the OODS point");
     }
-    qm31 comp = qm31_add(left, qm31_mul(spoint_repeated_double(oods, max_log_degree_bound - 1).x, right));
-    // coset_vanishing(CanonicCoset(max_log_degree_bound).coset, oods)
-    uint64_t cinit = 1ull << (31 - (max_log_degree_bound + 1)), cstep = 1ull << (31 - max_log_degree_bound);
-    cpoint ci = index_to_cpoint(cinit), hs = index_to_cpoint(cstep >> 1);
-    spoint sp = spoint_add(spoint_add(oods, {qm31_from_m31(ci.x), qm31_from_m31(m31_neg(ci.y))}),
-                           {qm31_from_m31(hs.x), qm31_from_m31(hs.y)});
-    qm31 vx = sp.x;
-    for (uint32_t i = 1; i < max_log_degree_bound; i++) vx = qm31_double_x(vx);
-    qm31 dinv = qm31_inv(vx);
-    qm31 acc = qm31_zero();
-    for (uint32_t k = 0; k < n_cons; k++) {
-      qm31 a = sampled[k], b = sampled[k + 1], c = sampled[k + 2];
-      qm31 cons = qm31_sub(c, qm31_add(qm31_mul(a, a), qm31_mul(b, b)));
-      acc = qm31_add(qm31_mul(acc, random_coeff), qm31_mul(cons, dinv));
+    ch.mix_felts(sampled.data(), sampled.size());
+    if (!qm31_eq(ch.draw_secure_felt(), fs.quotient_coeff))
+      return fail(STWO_B200_ESTATE, "device and host channels diverged at the quotient coefficient");
+    // Sanity check (prover/mod.rs:123-138): the composition value rebuilt
+    // from the split halves equals the constraint quotient at the OODS point.
+    {
+      const qm31 basis[4] = {qm31_one(), {0, 1, 0, 0}, {0, 0, 1, 0}, {0, 0, 0, 1}};
+      qm31 left = qm31_zero(), right = qm31_zero();
+      for (int k = 0; k < 4; k++) {
+        left = qm31_add(left, qm31_mul(sampled[N + k], basis[k]));
+        right = qm31_add(right, qm31_mul(sampled[N + 4 + k], basis[k]));
+      }
+      qm31 comp = qm31_add(left, qm31_mul(spoint_repeated_double(oods, max_log_degree_bound - 1).x, right));
+      // coset_vanishing(CanonicCoset(max_log_degree_bound).coset, oods)
+      uint64_t cinit = 1ull << (31 - (max_log_degree_bound + 1)), cstep = 1ull << (31 - max_log_degree_bound);
+      cpoint ci = index_to_cpoint(cinit), hs = index_to_cpoint(cstep >> 1);
+      spoint sp = spoint_add(spoint_add(oods, {qm31_from_m31(ci.x), qm31_from_m31(m31_neg(ci.y))}),
+                             {qm31_from_m31(hs.x), qm31_from_m31(hs.y)});
+      qm31 vx = sp.x;
+      for (uint32_t i = 1; i < max_log_degree_bound; i++) vx = qm31_double_x(vx);
+      qm31 dinv = qm31_inv(vx);
+      qm31 acc = qm31_zero();
+      for (uint32_t k = 0; k < n_cons; k++) {
+        qm31 a = sampled[k], b = sampled[k + 1], c = sampled[k + 2];
+        qm31 cons = qm31_sub(c, qm31_add(qm31_mul(a, a), qm31_mul(b, b)));
+        acc = qm31_add(qm31_mul(acc, random_coeff), qm31_mul(cons, dinv));
+      }
+      if (!qm31_eq(acc, comp))
+        return fail(STWO_B200_ESTATE, "ConstraintsNotSatisfied: composition OODS mismatch");
     }
-    if (!qm31_eq(acc, comp))
-      return set_err(err, err_len, STWO_B200_ESTATE, "ConstraintsNotSatisfied: composition OODS mismatch");
   }
-
   // One download after the FRI commit: roots, device alphas, channel state,
   // error flags and the last layer.  The host continues from the device
   // channel's state (last layer, proof of work) and replays the transcript
@@ -1725,6 +1902,9 @@ int WideFibProver::prove_body(const uint32_t* d_a, const uint32_t* d_b, ProofOut
   HostChannel dev_ch(m31);
   const uint8_t* hp = reinterpret_cast<const uint8_t*>(h_pinned);
   size_t alpha_off = 0, chan_off = 0, flag_off = 0, last_off = 0;
+  uint32_t fri_end_digest[8];
+  uint32_t fri_end_draws = 0;
+  std::vector<qm31> dev_alphas;
   {
     uint8_t* hpw = reinterpret_cast<uint8_t*>(h_pinned);
     size_t off = 0;
@@ -1752,7 +1932,11 @@ int WideFibProver::prove_body(const uint32_t* d_a, const uint32_t* d_b, ProofOut
     if (*reinterpret_cast<const uint32_t*>(hp + flag_off))
       return set_err(err, err_len, STWO_B200_ETIMEOUT, "column stream: a bulk copy did not complete in time");
     dev_ch.set_state(dc->digest, dc->n_draws);
+    std::memcpy(fri_end_digest, dc->digest, 32);
+    fri_end_draws = dc->n_draws;
     for (size_t i = 0; i < fri_roots.size(); i++) std::memcpy(fri_roots[i].data(), hp + 32 * i, 32);
+    dev_alphas.resize(fri_roots.size());
+    std::memcpy(dev_alphas.data(), hp + alpha_off, fri_roots.size() * sizeof(qm31));
   }
   // Last layer (prover/fri.rs:274-291).
   std::vector<qm31> last_coeffs;
@@ -1802,7 +1986,6 @@ int WideFibProver::prove_body(const uint32_t* d_a, const uint32_t* d_b, ProofOut
     Digest8 d;
     std::memcpy(d.w, pre.data(), 32);
     bool found = false;
-    bool replayed = false;
     for (uint32_t hi = 0; !found; hi++) {
       for (uint32_t base = 0; base < (1u << 20) && !found; base += 1u << 16) {
         STWO_CUDA_TRY(cudaMemsetAsync(d_found, 0xFF, 4, s));
@@ -1810,26 +1993,6 @@ int WideFibProver::prove_body(const uint32_t* d_a, const uint32_t* d_b, ProofOut
         STWO_CHECK_LAUNCH();
         uint32_t* hf = reinterpret_cast<uint32_t*>(h_pinned) + (h_pinned_bytes / 4 - 1);
         STWO_CUDA_TRY(cudaMemcpyAsync(hf, d_found, 4, cudaMemcpyDeviceToHost, s));
-        if (!replayed) {
-          // host replay of the FRI transcript while the batch runs
-          replayed = true;
-          const qm31* dev_alpha = reinterpret_cast<const qm31*>(hp + alpha_off);
-          for (size_t i = 0; i < fri_roots.size(); i++) {
-            ch.mix_root(fri_roots[i]);
-            qm31 a = ch.draw_secure_felt();
-            if (!qm31_eq(a, dev_alpha[i])) {
-              cudaStreamSynchronize(s);
-              return set_err(err, err_len, STWO_B200_ESTATE, "device and host channels diverged at FRI layer %zu",
-                             i);
-            }
-          }
-          const DevChannel* dc = reinterpret_cast<const DevChannel*>(hp + chan_off);
-          if (std::memcmp(ch.digest().data(), dc->digest, 32) != 0 || ch.n_draws() != dc->n_draws) {
-            cudaStreamSynchronize(s);
-            return set_err(err, err_len, STWO_B200_ESTATE, "device and host channel states differ after FRI");
-          }
-          ch.mix_felts(last_coeffs.data(), last_coeffs.size());
-        }
         STWO_CUDA_TRY(cudaStreamSynchronize(s));
         if (*hf != 0xFFFFFFFFu) {
           nonce = ((uint64_t)hi << 32) | *hf;
@@ -1839,14 +2002,14 @@ int WideFibProver::prove_body(const uint32_t* d_a, const uint32_t* d_b, ProofOut
       if (hi == 0x7ffffffeu && !found) return set_err(err, err_len, STWO_B200_ESTATE, "grind found no nonce");
     }
   }
-  ch.mix_u64(nonce);
+  dev_ch.mix_u64(nonce);
 
   // ---- queries (core/queries.rs:11-58) ----
   std::vector<size_t> queries;
   {
     size_t mask = ((size_t)1 << lift) - 1;
     while (queries.size() < cfg.n_queries) {
-      auto w = ch.draw_u32s();
+      auto w = dev_ch.draw_u32s();
       for (uint32_t x : w)
         if (queries.size() < cfg.n_queries) queries.push_back(x & mask);
     }
@@ -1940,6 +2103,19 @@ int WideFibProver::prove_body(const uint32_t* d_a, const uint32_t* d_b, ProofOut
     }
     gather_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(d_gather_addr, (uint32_t)n, d_gather_out);
     STWO_CHECK_LAUNCH();
+    // host replay of the FRI transcript while the gather runs: every device
+    // alpha and the channel state at the end of the commit
+    for (size_t i = 0; i < fri_roots.size(); i++) {
+      ch.mix_root(fri_roots[i]);
+      if (!qm31_eq(ch.draw_secure_felt(), dev_alphas[i])) {
+        cudaStreamSynchronize(s);
+        return set_err(err, err_len, STWO_B200_ESTATE, "device and host channels diverged at FRI layer %zu", i);
+      }
+    }
+    if (std::memcmp(ch.digest().data(), fri_end_digest, 32) != 0 || ch.n_draws() != fri_end_draws) {
+      cudaStreamSynchronize(s);
+      return set_err(err, err_len, STWO_B200_ESTATE, "device and host channel states differ after FRI");
+    }
     size_t wchunk = h_pinned_bytes / 4;
     for (size_t off = 0; off < n; off += wchunk) {
       size_t m = std::min(wchunk, n - off);
