@@ -741,6 +741,61 @@ __device__ void dev_chan_mix_felts(DevChannel* ch, const qm31* __restrict__ f, u
   ch->n_draws = 0;
 }
 
+// The channel state in registers, for the one-CTA kernels that run several
+// Fiat-Shamir steps: loaded once, where its latency overlaps the tree work,
+// and stored once.  Same steps as dev_chan_mix_root / dev_chan_draw_felt.
+struct ChanRegs {
+  uint32_t digest[8];
+  uint32_t n_draws, m31, error;
+};
+__device__ __forceinline__ void chan_load(const DevChannel* ch, ChanRegs& c) {
+#pragma unroll
+  for (int k = 0; k < 8; k++) c.digest[k] = ch->digest[k];
+  c.n_draws = ch->n_draws;
+  c.m31 = ch->m31;
+  c.error = ch->error;
+}
+__device__ __forceinline__ void chan_store(DevChannel* ch, const ChanRegs& c) {
+#pragma unroll
+  for (int k = 0; k < 8; k++) ch->digest[k] = c.digest[k];
+  ch->n_draws = c.n_draws;
+  ch->error = c.error;
+}
+__device__ __forceinline__ void chan_mix_root(ChanRegs& c, const uint32_t root[8]) {
+  uint32_t m[16], h[8];
+#pragma unroll
+  for (int k = 0; k < 8; k++) {
+    m[k] = c.digest[k];
+    m[8 + k] = root[k];
+  }
+  blake2s_init(h);
+  blake2s_compress_lat(h, m, 64, true);
+  dev_finalize(h, c.m31 != 0);
+#pragma unroll
+  for (int k = 0; k < 8; k++) c.digest[k] = h[k];
+  c.n_draws = 0;
+}
+__device__ __forceinline__ qm31 chan_draw_felt(ChanRegs& c) {
+  uint32_t m[16], h[8];
+  for (int attempt = 0; attempt < 64; attempt++) {
+#pragma unroll
+    for (int k = 0; k < 8; k++) m[k] = c.digest[k];
+    m[8] = c.n_draws;
+#pragma unroll
+    for (int k = 9; k < 16; k++) m[k] = 0;
+    c.n_draws++;
+    blake2s_init(h);
+    blake2s_compress_lat(h, m, 37, true);
+    dev_finalize(h, c.m31 != 0);
+    bool okw = true;
+#pragma unroll
+    for (int k = 0; k < 8; k++) okw = okw && h[k] < 2 * M31_P;
+    if (okw) return {m31_reduce_u32(h[0]), m31_reduce_u32(h[1]), m31_reduce_u32(h[2]), m31_reduce_u32(h[3])};
+  }
+  c.error = 1;
+  return qm31_zero();
+}
+
 // mix_root, then draw_secure_felt into *alpha; one thread.
 __device__ void dev_mix_root_draw(DevChannel* ch, const uint32_t* root, qm31* alpha) {
   dev_chan_mix_root(ch, root);
@@ -1055,6 +1110,8 @@ __global__ void __launch_bounds__(kFriTailThreads, 1) tree_top_channel_kernel(ui
   uint4* pong = tail_smem + (2u << kFriTailLog);
   const bool m31b = m31 != 0;
   const uint4* src = ping;
+  ChanRegs cr;
+  if (threadIdx.x == 0) chan_load(ch, cr);  // used after the tree levels
   if (top_log == 0) {
     if (threadIdx.x == 0) {
       const uint4* r = reinterpret_cast<const uint4*>(base);
@@ -1087,7 +1144,9 @@ __global__ void __launch_bounds__(kFriTailThreads, 1) tree_top_channel_kernel(ui
   if (threadIdx.x == 0) {
     const uint4 a = src[0], b = src[1];
     const uint32_t root[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
-    dev_mix_root_draw(ch, root, alpha);
+    chan_mix_root(cr, root);
+    *alpha = chan_draw_felt(cr);
+    chan_store(ch, cr);
   }
 }
 
@@ -1100,6 +1159,8 @@ __global__ void __launch_bounds__(kFriTailThreads, 1) fri_tail_kernel(FriTail t,
   uint4* pong = tail_smem + (2u << kFriTailLog);
   const uint32_t tid = threadIdx.x;
   const bool m31 = t.m31 != 0;
+  ChanRegs cr;
+  if (tid == 0) chan_load(ch, cr);
   for (uint32_t li = 0; li < t.n_layers; li++) {
     const uint32_t L = t.log_size[li];
     const uint32_t n = 1u << L;
@@ -1124,8 +1185,11 @@ __global__ void __launch_bounds__(kFriTailThreads, 1) fri_tail_kernel(FriTail t,
     if (tid == 0) {
       const uint4 a = src[0], b = src[1];
       const uint32_t root[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
-      dev_mix_root_draw(ch, root, alphas + li);
-      s_alpha = alphas[li];
+      chan_mix_root(cr, root);
+      const qm31 alpha = chan_draw_felt(cr);
+      alphas[li] = alpha;
+      s_alpha = alpha;
+      if (li + 1 == t.n_layers) chan_store(ch, cr);
     }
     __syncthreads();
     const qm31 a0 = s_alpha;
