@@ -209,11 +209,16 @@ __global__ void __launch_bounds__(256) oods_eval_kernel(PolyTable t, uint32_t n_
   const uint32_t chunk = n < kOodsChunk ? (uint32_t)n : kOodsChunk;
   const uint64_t j0 = (uint64_t)blockIdx.x * chunk;
   const uint64_t lo_mask = (1ull << h) - 1;
+  // A chunk inside one w_hi bucket (chunk <= 2^h, both powers of two): the
+  // inner sums take w_lo alone and each partial is multiplied by the bucket's
+  // w_hi once, an exact rewrite of the same sum.
+  const bool one_bucket = chunk <= (1ull << h);
   for (uint32_t k = threadIdx.x; k < chunk; k += blockDim.x) {
     const uint64_t j = j0 + k;
-    const qm31 w = qm31_mul(w_hi[j >> h], w_lo[j & lo_mask]);
+    const qm31 w = one_bucket ? w_lo[j & lo_mask] : qm31_mul(w_hi[j >> h], w_lo[j & lo_mask]);
     ws[k] = make_uint4(w.a, w.b, w.c, w.d);
   }
+  const qm31 wh = one_bucket ? w_hi[j0 >> h] : qm31_one();
   __syncthreads();
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint32_t n_warps = blockDim.x >> 5;
@@ -222,15 +227,15 @@ __global__ void __launch_bounds__(256) oods_eval_kernel(PolyTable t, uint32_t n_
     acc4 s{0, 0, 0, 0};
     if (chunk == kOodsChunk) {
 #pragma unroll 1
-      for (uint32_t b = 0; b < kOodsChunk; b += 256) {
-        uint32_t v[8];
+      for (uint32_t b = 0; b < kOodsChunk; b += 512) {
+        uint32_t v[16];  // 16 loads in flight per lane
 #pragma unroll
-        for (int u = 0; u < 8; u++) v[u] = __ldg(col + b + u * 32 + lane);
+        for (int u = 0; u < 16; u++) v[u] = __ldg(col + b + u * 32 + lane);
 #pragma unroll
-        for (int u = 0; u < 8; u++) {
+        for (int u = 0; u < 16; u++) {
           const uint4 w = ws[b + u * 32 + lane];
           acc4_mad(s, qm31{w.x, w.y, w.z, w.w}, v[u]);
-          if (u == 2 || u == 5 || u == 7) acc4_fold(s);
+          if (u % 8 == 2 || u % 8 == 5 || u % 8 == 7) acc4_fold(s);
         }
       }
     } else {
@@ -247,7 +252,7 @@ __global__ void __launch_bounds__(256) oods_eval_kernel(PolyTable t, uint32_t n_
                       __shfl_xor_sync(0xffffffffu, v.c, o), __shfl_xor_sync(0xffffffffu, v.d, o)};
       v = qm31_add(v, u);
     }
-    if (lane == 0) partial[(uint64_t)p * gridDim.x + blockIdx.x] = v;
+    if (lane == 0) partial[(uint64_t)p * gridDim.x + blockIdx.x] = one_bucket ? qm31_mul(v, wh) : v;
   }
 }
 
@@ -313,7 +318,7 @@ __global__ void __launch_bounds__(256) quotient_kernel(QuotientParams q, PolyTab
                                                       const qm31* __restrict__ alpha_pows,
                                                       const QuotientDyn* __restrict__ dyn,
                                                       uint32_t* __restrict__ out) {
-  const QuotientDyn qd = *dyn;
+  const QuotientDyn& qd = *dyn;  // read at the epilogue, through the read-only cache
   const uint64_t n = 1ull << q.log_size;
   const uint64_t half = n >> 1;
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
@@ -372,7 +377,7 @@ __global__ void __launch_bounds__(256) quotient4_kernel(QuotientParams q, PolyTa
                                                        const qm31* __restrict__ alpha_pows,
                                                        const QuotientDyn* __restrict__ dyn,
                                                        uint32_t* __restrict__ out) {
-  const QuotientDyn qd = *dyn;
+  const QuotientDyn& qd = *dyn;  // read at the epilogue, through the read-only cache
   const uint64_t n = 1ull << q.log_size;
   const uint64_t n4 = n >> 2;
   for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < n4; t += (uint64_t)gridDim.x * blockDim.x) {
@@ -534,7 +539,7 @@ __global__ void __launch_bounds__(kStreamThreads) quotient_tma_kernel(QuotientPa
                                                                      const qm31* __restrict__ alpha_pows,
                                                                      const QuotientDyn* __restrict__ dyn,
                                                                      uint32_t* __restrict__ out, uint32_t* err) {
-  const QuotientDyn qd = *dyn;
+  const QuotientDyn& qd = *dyn;  // read at the epilogue, through the read-only cache
   extern __shared__ __align__(128) uint32_t smem[];
   __shared__ uint64_t bars[kStreamS];
   __shared__ cpoint s_base;
