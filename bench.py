@@ -144,6 +144,15 @@ class ClockSampler:
             self.stop_flag.set()
             self.t.join(timeout=1.0)
             got = list(self.samples)
+            if not got:  # a region shorter than the period: one reading right at its end
+                nv, h = self.nvml
+                try:
+                    get_reasons = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+                        nv.nvmlDeviceGetCurrentClocksThrottleReasons
+                    got = [(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM),
+                            nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM), int(get_reasons(h)))]
+                except Exception:
+                    got = []
             reasons = sorted(nm for nm, bit in self.REASON_BITS.items() if any(r & bit for _, _, r in got))
             return {"sm_mhz": statistics.median(c for c, _, _ in got) if got else None,
                     "sm_max_mhz": max(m for _, m, _ in got) if got else None,
@@ -315,9 +324,7 @@ def run_b200(args, spec, world, rank, local):
         if spec["bitrev"]:
             # bit-reverse the natural-order trace into the coefficient buffers,
             # then interpolate in place.
-            for s_, d_ in zip(inputs, coeffs):
-                ffi.call("stwo_b200_memcpy_d2d", ffi_ptr(d_), ffi_ptr(s_), size_t(s_.nbytes), be.stream)
-                be.bit_reverse_column(d_)
+            be.bit_reverse_columns(inputs, coeffs)
             rec(evs, 0)
             be.interpolate_columns(coeffs, tree)
         else:

@@ -77,6 +77,12 @@ int stwo_b200_host_free(void* h_ptr, char* err, size_t err_len);
  * SimdBackend prover/backend/simd/bit_reverse.rs:22-33), in place.  Replaces
  * bit_reverse_base_field (raw.rs:77). */
 int stwo_b200_bit_reverse_column(uint32_t* d_col, uint32_t log_size, void* stream, char* err, size_t err_len);
+/* bit_reverse_column over many columns in one launch per run of equal sizes
+ * (the loop over columns that callers of prover/backend/mod.rs:37-39 write):
+ * out of place (d_dst[i] <- bit-reversed d_src[i]) or in place where
+ * d_dst[i] == d_src[i].  Columns of one run must not overlap. */
+int stwo_b200_bit_reverse_columns(const uint32_t* const* d_src, uint32_t* const* d_dst, const uint32_t* log_sizes,
+                                  uint32_t n_cols, void* stream, char* err, size_t err_len);
 
 /* -------------------------------------------------------------- PolyOps -- */
 /* PolyOps::precompute_twiddles (prover/poly/circle/ops.rs:144; SimdBackend

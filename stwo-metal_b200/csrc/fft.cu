@@ -1027,6 +1027,57 @@ extern "C" int stwo_b200_fft_get_plan(uint32_t log_size, uint32_t* pass_layers, 
   return ok(err, err_len);
 }
 
+// Bit reversal of up to kFftMaxCols columns of one size in one launch
+// (blockIdx.y = column): out of place (dst[brev(i)] = src[i], coalesced
+// reads), or in place by pairwise swaps when dst == src.
+__global__ void bit_reverse_cols_kernel(FftCols t, uint32_t log_n) {
+  const uint64_t n = 1ull << log_n;
+  const uint32_t* __restrict__ src = t.src[blockIdx.y];
+  uint32_t* dst = t.dst[blockIdx.y];
+  const bool in_place = src == dst;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t j = __brevll(i) >> (64 - log_n);
+    if (!in_place) {
+      dst[j] = src[i];
+    } else if (i < j) {
+      const uint32_t a = dst[i], b = dst[j];
+      dst[i] = b;
+      dst[j] = a;
+    }
+  }
+}
+
+extern "C" int stwo_b200_bit_reverse_columns(const uint32_t* const* d_src, uint32_t* const* d_dst,
+                                             const uint32_t* log_sizes, uint32_t n_cols, void* stream, char* err,
+                                             size_t err_len) {
+  STWO_ARG_CHECK(n_cols == 0 || (d_src && d_dst && log_sizes), "null argument");
+  cudaStream_t s = as_stream(stream);
+  // one launch per run of equal sizes (at most kFftMaxCols columns each)
+  for (uint32_t a = 0; a < n_cols;) {
+    const uint32_t lg = log_sizes[a];
+    STWO_ARG_CHECK(lg <= 31, "log size %u too large", lg);
+    uint32_t b = a;
+    FftCols t;
+    while (b < n_cols && log_sizes[b] == lg && b - a < (uint32_t)kFftMaxCols) {
+      STWO_ARG_CHECK(d_src[b] && d_dst[b], "null column %u", b);
+      t.src[b - a] = d_src[b];
+      t.dst[b - a] = d_dst[b];
+      b++;
+    }
+    if (lg > 0) {
+      const uint64_t n = 1ull << lg;
+      const unsigned bx = (unsigned)std::min<uint64_t>((n + 255) / 256, std::max<uint64_t>(1, 148 * 32 / (b - a)));
+      bit_reverse_cols_kernel<<<dim3(bx, b - a), 256, 0, s>>>(t, lg);
+      STWO_CHECK_LAUNCH();
+    } else {
+      for (uint32_t k = a; k < b; k++)
+        if (d_src[k] != d_dst[k]) STWO_CUDA_TRY(cudaMemcpyAsync(d_dst[k], d_src[k], 4, cudaMemcpyDeviceToDevice, s));
+    }
+    a = b;
+  }
+  return ok(err, err_len);
+}
+
 extern "C" int stwo_b200_bit_reverse_column(uint32_t* d_col, uint32_t log_size, void* stream, char* err,
                                             size_t err_len) {
   STWO_ARG_CHECK(log_size <= 31, "log size %u too large", log_size);

@@ -158,6 +158,15 @@ class B200Backend:
     def bit_reverse_column(self, col: DeviceColumn):
         ffi.call("stwo_b200_bit_reverse_column", C.c_void_p(col.ptr), C.c_uint32(col.log_size), self.stream)
 
+    def bit_reverse_columns(self, srcs, dsts=None):
+        """bit_reverse_column over many columns in one call: into ``dsts``
+        (same sizes), or in place when ``dsts`` is None."""
+        dsts = srcs if dsts is None else dsts
+        if len(dsts) != len(srcs) or any(d.log_size != s_.log_size for s_, d in zip(srcs, dsts)):
+            raise ValueError("source and destination columns differ in number or size")
+        ffi.call("stwo_b200_bit_reverse_columns", _ptr_array(srcs), _ptr_array(dsts),
+                 _u32_array([c.log_size for c in srcs]), C.c_uint32(len(srcs)), self.stream)
+
     # ---- PolyOps::interpolate_columns (in place) ------------------------------
     def interpolate_columns(self, cols, tree: TwiddleTree, half_initial_indices=None):
         his = None

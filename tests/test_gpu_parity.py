@@ -42,6 +42,23 @@ def test_bit_reverse(be, oracle, log_n):
     assert (c.to_host() == oracle.bit_reverse(v)).all()
 
 
+@pytest.mark.parametrize("in_place", [False, True])
+def test_bit_reverse_columns(be, oracle, in_place):
+    # a batch with runs of equal sizes, including log 0 and a run longer than
+    # one launch's column table
+    logs = [0, 3, 3, 7, 7, 7, 12] + [5] * 300 + [16]
+    r = rng(77)
+    vals = [rand_col(r, l) for l in logs]
+    srcs = [DeviceColumn.from_host(v) for v in vals]
+    dsts = None if in_place else [DeviceColumn(1 << l) for l in logs]
+    be.bit_reverse_columns(srcs, dsts)
+    for v, c in zip(vals, srcs if in_place else dsts):
+        assert (c.to_host() == oracle.bit_reverse(v)).all()
+    if not in_place:  # sources untouched
+        for v, c in zip(vals, srcs):
+            assert (c.to_host() == v).all()
+
+
 LOGS = [1, 2, 3, 4, 5, 6, 8, 11, 12, 13, 16, 17, 20, 22]
 
 
