@@ -595,6 +595,11 @@ def run_prove_reference(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
+# DRAM bytes of one trace evaluate (100 columns, 2^20 -> 2^21) measured by ncu:
+# strided pass 419.6 MB read + 791.5 MB written, contiguous pass 855.1 + 785.9 MB.
+EVALUATE_TRAFFIC_100x2e20 = (419.6 + 791.5 + 855.1 + 785.9) * 1e6
+
+
 def run_prove_b200(args, world, rank, local):
     import ctypes
     import torch
@@ -727,6 +732,12 @@ def run_prove_b200(args, world, rank, local):
         roof = {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                 "frac": achieved / hbm_peak, "peak_kind": peak_kind, "traffic": None,
                 "alg_bytes_per_step": amount}
+        if dominant == "trace_evaluate" and (n, nc, lb) == (20, 100, 1):
+            # dram__bytes_read.sum + dram__bytes_write.sum of the two evaluate
+            # passes (fft_warp_strided_kernel<0>, fft_warp_contig_kernel<0>),
+            # one ncu capture at this shape
+            roof["traffic"] = EVALUATE_TRAFFIC_100x2e20
+            roof["traffic_source"] = "ncu capture of fft_bench.py 20 100 (profiles/fft_warp_kernels_100x2e20_full_capture.md)"
     phase_frac = {}
     for k, (kd, amt) in alg.items():
         if phase_ms.get(k, 0) > 0:
