@@ -404,7 +404,13 @@ static void index_point(uint64_t idx, uint32_t& x, uint32_t& y) {
 // block's twiddles are staged.  Butterflies, twiddle indices (row >> (lam+1)
 // of tree layer layer0 + lam) and layer order are those of fft_stage.
 constexpr int kWarpCols = 8;                  // warps (columns) per block
-constexpr uint32_t kColWords = 1024 + 32 + 1;  // padded column region
+// Column region of the strided pass: row r at (r >> 5) * kTileStride + (r & 31)
+// (the staged-tile layout of the contiguous pass), regions kColStride words
+// apart.  kColStride = 4 (mod 32) keeps the 4-word scatter and gather of the
+// staging conflict-free; the 16-byte aligned lines let the lane-major side
+// of a column move as 8 x 16 bytes per lane.
+constexpr uint32_t kColStride = 32 * 36 + 4;
+__device__ __forceinline__ uint32_t colpos(uint32_t r) { return (r >> 5) * 36 + (r & 31); }
 
 // Layers 0..4 on v[j] = row lane*32 + j.
 template <bool INV>
@@ -448,23 +454,6 @@ __device__ __forceinline__ void warp_phase_hi(uint32_t (&v)[32], const uint32_t*
         bfly2(v[j], v[j | (1 << k)], t[j >> (k + 1)]);
     }
   }
-}
-
-__device__ __forceinline__ void warp_lo_to_hi(uint32_t (&v)[32], uint32_t* col, uint32_t lane) {
-#pragma unroll
-  for (int j = 0; j < 32; j++) col[lane * 33 + j] = v[j];
-  __syncwarp();
-#pragma unroll
-  for (int j = 0; j < 32; j++) v[j] = col[j * 33 + lane];
-  __syncwarp();
-}
-__device__ __forceinline__ void warp_hi_to_lo(uint32_t (&v)[32], uint32_t* col, uint32_t lane) {
-#pragma unroll
-  for (int j = 0; j < 32; j++) col[j * 33 + lane] = v[j];
-  __syncwarp();
-#pragma unroll
-  for (int j = 0; j < 32; j++) v[j] = col[lane * 33 + j];
-  __syncwarp();
 }
 
 // Stages the 1023 twiddles of a 10-layer tile position (as fft_pass_kernel),
@@ -612,9 +601,9 @@ __global__ void __launch_bounds__(256, 4) fft_warp_contig_kernel(FftPass p, FftC
 // column; warp w transforms tile column w.
 template <bool INV>
 __global__ void __launch_bounds__(256, 4) fft_warp_strided_kernel(FftPass p, FftCols cols) {
-  extern __shared__ uint32_t smem[];
+  extern __shared__ __align__(16) uint32_t smem[];
   uint32_t* tws = smem;
-  uint32_t* tile = smem + 1024;  // 8 column regions of kColWords
+  uint32_t* tile = smem + 1024;  // 8 column regions of kColStride words
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint32_t L0 = p.layer0;
   const uint64_t t = blockIdx.x;
@@ -644,11 +633,11 @@ __global__ void __launch_bounds__(256, 4) fft_warp_strided_kernel(FftPass p, Fft
     for (int q = 0; q < 8; q++) {
       const uint32_t e = threadIdx.x * 4 + 1024u * q;
       const uint32_t row = e >> 3, c0 = e & 7;
-      const uint32_t r = row + (row >> 5);
-      tile[c0 * kColWords + r] = w[q].x;
-      tile[(c0 + 1) * kColWords + r] = w[q].y;
-      tile[(c0 + 2) * kColWords + r] = w[q].z;
-      tile[(c0 + 3) * kColWords + r] = w[q].w;
+      const uint32_t r = colpos(row);
+      tile[c0 * kColStride + r] = w[q].x;
+      tile[(c0 + 1) * kColStride + r] = w[q].y;
+      tile[(c0 + 2) * kColStride + r] = w[q].z;
+      tile[(c0 + 3) * kColStride + r] = w[q].w;
     }
   } else if (p.vec_io) {
 #pragma unroll 4
@@ -656,38 +645,45 @@ __global__ void __launch_bounds__(256, 4) fft_warp_strided_kernel(FftPass p, Fft
       const uint32_t row = e >> 3, c0 = e & 7;
       const uint64_t gi = (base + ((uint64_t)row << L0) + c0) & p.src_mask;
       const uint4 w = gi < p.src_len ? __ldg(reinterpret_cast<const uint4*>(src + gi)) : make_uint4(0, 0, 0, 0);
-      const uint32_t r = row + (row >> 5);
-      tile[c0 * kColWords + r] = w.x;
-      tile[(c0 + 1) * kColWords + r] = w.y;
-      tile[(c0 + 2) * kColWords + r] = w.z;
-      tile[(c0 + 3) * kColWords + r] = w.w;
+      const uint32_t r = colpos(row);
+      tile[c0 * kColStride + r] = w.x;
+      tile[(c0 + 1) * kColStride + r] = w.y;
+      tile[(c0 + 2) * kColStride + r] = w.z;
+      tile[(c0 + 3) * kColStride + r] = w.w;
     }
   } else {
     for (uint32_t e = threadIdx.x; e < 8192; e += 256) {
       const uint32_t row = e >> 3, c0 = e & 7;
       const uint64_t gi = (base + ((uint64_t)row << L0) + c0) & p.src_mask;
-      tile[c0 * kColWords + row + (row >> 5)] = gi < p.src_len ? __ldg(src + gi) : 0u;
+      tile[c0 * kColStride + colpos(row)] = gi < p.src_len ? __ldg(src + gi) : 0u;
     }
   }
   __syncthreads();
-  uint32_t* cw = tile + warp * kColWords;
+  // Each warp's column stays in its region: lane-major accesses (a lane's
+  // own line, 8 x 16 bytes) and row-major ones (word 36 j + lane); the
+  // __syncwarp separates writes and reads of other lanes' lines.
+  uint32_t* cw = tile + warp * kColStride;
   uint32_t v[32];
   if (INV) {
-#pragma unroll
-    for (int j = 0; j < 32; j++) v[j] = cw[lane * 33 + j];
+    tile_to_lane_major(cw, lane, v);
     warp_phase_lo<true>(v, tws, lane);
-    warp_lo_to_hi(v, cw, lane);
+    lane_major_to_tile(cw, lane, v);
+    __syncwarp();
+#pragma unroll
+    for (int j = 0; j < 32; j++) v[j] = cw[j * kTileStride + lane];
     warp_phase_hi<true>(v, tws);
 #pragma unroll
-    for (int j = 0; j < 32; j++) cw[j * 33 + lane] = v[j];
+    for (int j = 0; j < 32; j++) cw[j * kTileStride + lane] = v[j];
   } else {
 #pragma unroll
-    for (int j = 0; j < 32; j++) v[j] = cw[j * 33 + lane];
+    for (int j = 0; j < 32; j++) v[j] = cw[j * kTileStride + lane];
     warp_phase_hi<false>(v, tws);
-    warp_hi_to_lo(v, cw, lane);
-    warp_phase_lo<false>(v, tws, lane);
 #pragma unroll
-    for (int j = 0; j < 32; j++) cw[lane * 33 + j] = v[j];
+    for (int j = 0; j < 32; j++) cw[j * kTileStride + lane] = v[j];
+    __syncwarp();
+    tile_to_lane_major(cw, lane, v);
+    warp_phase_lo<false>(v, tws, lane);
+    lane_major_to_tile(cw, lane, v);
   }
   __syncthreads();
   const uint32_t scale = p.scale;
@@ -695,9 +691,9 @@ __global__ void __launch_bounds__(256, 4) fft_warp_strided_kernel(FftPass p, Fft
 #pragma unroll 4
     for (uint32_t e = threadIdx.x * 4; e < 8192; e += 1024) {
       const uint32_t row = e >> 3, c0 = e & 7;
-      const uint32_t r = row + (row >> 5);
-      uint4 w = make_uint4(tile[c0 * kColWords + r], tile[(c0 + 1) * kColWords + r], tile[(c0 + 2) * kColWords + r],
-                           tile[(c0 + 3) * kColWords + r]);
+      const uint32_t r = colpos(row);
+      uint4 w = make_uint4(tile[c0 * kColStride + r], tile[(c0 + 1) * kColStride + r],
+                           tile[(c0 + 2) * kColStride + r], tile[(c0 + 3) * kColStride + r]);
       if (scale != 1u) {
         w.x = m31_mul(w.x, scale);
         w.y = m31_mul(w.y, scale);
@@ -709,7 +705,7 @@ __global__ void __launch_bounds__(256, 4) fft_warp_strided_kernel(FftPass p, Fft
   } else {
     for (uint32_t e = threadIdx.x; e < 8192; e += 256) {
       const uint32_t row = e >> 3, c0 = e & 7;
-      const uint32_t v1 = tile[c0 * kColWords + row + (row >> 5)];
+      const uint32_t v1 = tile[c0 * kColStride + colpos(row)];
       dst[base + ((uint64_t)row << L0) + c0] = scale != 1u ? m31_mul(v1, scale) : v1;
     }
   }
@@ -734,7 +730,7 @@ static int launch_warp_pass(const FftPass& q, const FftCols& cols, uint64_t tile
     dim3 grid((unsigned)tiles, (unsigned)((groups + qq.cpb - 1) / qq.cpb));
     fft_warp_contig_kernel<INV><<<grid, 32 * kWarpCols, smem, s>>>(qq, cols);
   } else {
-    constexpr size_t smem = (1024 + 8 * kColWords) * sizeof(uint32_t);
+    constexpr size_t smem = (1024 + 8 * kColStride) * sizeof(uint32_t);
     static bool attr = false;
     if (!attr) {
       STWO_CUDA_TRY(cudaFuncSetAttribute(fft_warp_strided_kernel<INV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
