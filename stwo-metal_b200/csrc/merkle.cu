@@ -188,25 +188,31 @@ __device__ __forceinline__ void load_children(const uint4* src, uint32_t m[16]) 
 // half its threads at each level it climbs.
 __global__ void __launch_bounds__(256) node_subtree3_kernel(const uint8_t* in, uint64_t n, int m31, uint8_t* out0,
                                                            uint8_t* out1, uint8_t* out2) {
+  // Rolled loops keep three copies of the compression in the code instead of
+  // seven, so the instruction cache holds the kernel's working set.
   for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < n; t += (uint64_t)gridDim.x * blockDim.x) {
     const uint4* src = reinterpret_cast<const uint4*>(in + t * 256);
-    uint32_t m[16], g0[8], h[8];
-#pragma unroll
+    uint32_t m[16], h[8], g0[8];
+#pragma unroll 1
     for (int half = 0; half < 2; half++) {
       uint32_t a[8];
-      load_children(src + 8 * half, m);
-      hash_children(m, m31 != 0, a);
-      store_hash(out0, 4 * t + 2 * half, a, false);
-      load_children(src + 8 * half + 4, m);
-      hash_children(m, m31 != 0, h);
-      store_hash(out0, 4 * t + 2 * half + 1, h, false);
+#pragma unroll 1
+      for (int e = 0; e < 2; e++) {
+        load_children(src + 8 * half + 4 * e, m);
+        hash_children(m, m31 != 0, h);
+        store_hash(out0, 4 * t + 2 * half + e, h, false);
+#pragma unroll
+        for (int k = 0; k < 8; k++) a[k] = e == 0 ? h[k] : a[k];
+      }
 #pragma unroll
       for (int k = 0; k < 8; k++) {
         m[k] = a[k];
         m[k + 8] = h[k];
       }
-      hash_children(m, m31 != 0, half ? h : g0);
-      store_hash(out1, 2 * t + half, half ? h : g0, false);
+      hash_children(m, m31 != 0, h);
+      store_hash(out1, 2 * t + half, h, false);
+#pragma unroll
+      for (int k = 0; k < 8; k++) g0[k] = half == 0 ? h[k] : g0[k];
     }
 #pragma unroll
     for (int k = 0; k < 8; k++) {
