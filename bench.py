@@ -183,6 +183,16 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------ dist helpers --
+# Replicas only: every rank proves (or commits) its own copy of the workload,
+# with no collective on the data path.  The only collectives are the barriers
+# around the timed region and one all-reduce of the timing scalar; they run
+# over NCCL when the ranks have GPUs, and over gloo otherwise (the CPU tests
+# of this plumbing).
+def dist_backend() -> str:
+    import torch
+    return "nccl" if torch.cuda.is_available() else "gloo"
+
+
 def dist_setup():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -191,8 +201,10 @@ def dist_setup():
         import torch
         import torch.distributed as dist
         from datetime import timedelta
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+        backend = dist_backend()
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=timedelta(seconds=120))
     return world, rank, local
 
 
@@ -201,9 +213,16 @@ def max_over_ranks(x: float, world: int) -> float:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def replica_rate(units_per_rank: float, ms_max: float, world: int) -> float:
+    """Whole-job throughput of `world` replicas: all units over the slowest
+    rank's time (weak scaling)."""
+    return units_per_rank * world / (ms_max * 1e-3)
 
 
 def barrier(world):
@@ -494,7 +513,7 @@ def run_b200(args, spec, world, rank, local):
     cpu_rate, cpu_sample, cpu_cores = cpu_commit_rate(spec, host_cols, budget_s=10.0)
     line = {
         "metric": METRIC,
-        "value": cells / (ms * 1e-3),
+        "value": replica_rate(cells, ms, world),
         "unit": "committed trace cells/s",
         "n_gpus": world,
         "steps": args.steps,
@@ -511,7 +530,7 @@ def run_b200(args, spec, world, rank, local):
                    "l2": "inputs larger than L2 (no flush)", "parallelism": f"replicas x{world}"},
         "clocks": clocks,
         "gpu_launches": launches,
-        "e2e": {"value": cells / (e2e_ms * 1e-3), "unit": "committed trace cells/s", "h2d_bytes_per_step": h2d,
+        "e2e": {"value": replica_rate(cells, e2e_ms, world), "unit": "committed trace cells/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": 32, "ms_per_step": e2e_ms},
         "roofline": roof,
         "phase_roofline": {p: (alg_bytes[p] / (phase_ms[p] * 1e-3) / 1e9 / hbm_peak) if phase_ms[p] > 0 else None
@@ -747,7 +766,7 @@ def run_prove_b200(args, world, rank, local):
     srt = sorted(step_ms)
     line = {
         "metric": METRIC,
-        "value": cells / (ms_max * 1e-3) * world,
+        "value": replica_rate(cells, ms_max, world),
         "unit": "proved trace cells/s",
         "n_gpus": world,
         "steps": args.steps,
@@ -763,7 +782,7 @@ def run_prove_b200(args, world, rank, local):
         "p99_prove_ms": srt[min(len(srt) - 1, int(0.99 * len(srt)))],
         "clocks": clocks,
         "gpu_launches": launches,
-        "e2e": {"value": cells / (e2e_ms * 1e-3) * world, "unit": "proved trace cells/s",
+        "e2e": {"value": replica_rate(cells, e2e_ms, world), "unit": "proved trace cells/s",
                 "h2d_bytes_per_step": int(a.nbytes + b.nbytes), "d2h_bytes_per_step": int(n_e2e),
                 "ms_per_step": e2e_ms},
         "roofline": roof,
@@ -935,13 +954,13 @@ def run_fri_b200(args, world, rank, local):
     units = fri_units()
     srt = sorted(step_ms)
     line = {
-        "metric": METRIC, "value": units / (ms * 1e-3) * world, "unit": "folded QM31 elements/s",
+        "metric": METRIC, "value": replica_rate(units, ms, world), "unit": "folded QM31 elements/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32 (M31/QM31)",
         "data": "synthetic (seeded numpy PCG64)", "config": fri_config_json(world),
         "p50_ms": srt[len(srt) // 2], "p99_ms": srt[min(len(srt) - 1, int(0.99 * len(srt)))],
         "clocks": clocks, "gpu_launches": launches,
-        "e2e": {"value": units / (e2e_ms * 1e-3) * world, "unit": "folded QM31 elements/s",
+        "e2e": {"value": replica_rate(units, e2e_ms, world), "unit": "folded QM31 elements/s",
                 "h2d_bytes_per_step": int(sum(d.nbytes for d in dev)), "d2h_bytes_per_step": len(proof),
                 "ms_per_step": e2e_ms},
         "roofline": roof,
