@@ -2286,6 +2286,12 @@ struct SeededFriProver {
   const uint32_t* itw = nullptr;
   cudaStream_t user_s = nullptr, s = nullptr;
   cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+  // The alphas are given, so no layer waits for another layer's root: the
+  // node levels of each tree run on side streams, forked from the fold chain
+  // when the tree's leaves are written and joined at the end of the commit.
+  static constexpr int kSide = 4;
+  cudaStream_t side[kSide] = {nullptr, nullptr, nullptr, nullptr};
+  std::vector<cudaEvent_t> ev_fork;  // one per tree, plus one per side stream for the join
   std::vector<uint32_t*> line;   // line[k]: 4 x 2^(n-1-k) words, k = 0..n-1 (line[n-1]: the last value)
   std::vector<MerkleTree> trees;  // trees[0]: circle layer (L = n); trees[k]: line[k-1] (L = n-k)
   std::vector<void*> allocs;
@@ -2308,6 +2314,9 @@ struct SeededFriProver {
     for (void* p : allocs) cudaFree(p);
     if (ev_in) cudaEventDestroy(ev_in);
     if (ev_out) cudaEventDestroy(ev_out);
+    for (cudaEvent_t e : ev_fork) cudaEventDestroy(e);
+    for (cudaStream_t x : side)
+      if (x) cudaStreamDestroy(x);
     if (s) cudaStreamDestroy(s);
   }
   int alloc(void** p, size_t bytes, char* err, size_t err_len) {
@@ -2327,6 +2336,9 @@ struct SeededFriProver {
     STWO_CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
     STWO_CUDA_TRY(cudaEventCreateWithFlags(&ev_in, cudaEventDisableTiming));
     STWO_CUDA_TRY(cudaEventCreateWithFlags(&ev_out, cudaEventDisableTiming));
+    for (cudaStream_t& x : side) STWO_CUDA_TRY(cudaStreamCreateWithFlags(&x, cudaStreamNonBlocking));
+    ev_fork.resize(n + kSide);
+    for (cudaEvent_t& e : ev_fork) STWO_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     int rc;
     line.resize(n);
     for (uint32_t k = 0; k < n; k++)
@@ -2357,21 +2369,39 @@ struct SeededFriProver {
   int enqueue_commit(const uint32_t* const* d_coords, char* err, size_t err_len) {
     int rc;
     const uint32_t lg[4] = {n, n, n, n};
-    if ((rc = build_leaves_impl(d_coords, lg, 4, n, m31, trees[0].layer(n), s, err, err_len))) return rc;
-    auto l0 = layer_ptrs(trees[0]);
-    if ((rc = build_node_layers_impl(trees[0].layer(n), n, 0, m31, l0.data(), s, err, err_len))) return rc;
+    // node levels of tree k (leaves at level L, written on `s`) on a side stream
+    auto nodes_on_side = [&](uint32_t k, uint32_t L) -> int {
+      cudaStream_t x = side[1 + (k - 1) % (kSide - 1)];  // side[0] carries the circle layer's tree
+      STWO_CUDA_TRY(cudaEventRecord(ev_fork[k], s));
+      STWO_CUDA_TRY(cudaStreamWaitEvent(x, ev_fork[k], 0));
+      auto lk = layer_ptrs(trees[k]);
+      return build_node_layers_impl(trees[k].layer(L), L, 0, m31, lk.data(), x, err, err_len);
+    };
+    {
+      // the circle layer's whole tree reads only the input columns: it runs
+      // beside the fold chain from the start
+      cudaStream_t x = side[0];
+      STWO_CUDA_TRY(cudaEventRecord(ev_fork[0], s));
+      STWO_CUDA_TRY(cudaStreamWaitEvent(x, ev_fork[0], 0));
+      if ((rc = build_leaves_impl(d_coords, lg, 4, n, m31, trees[0].layer(n), x, err, err_len))) return rc;
+      auto l0 = layer_ptrs(trees[0]);
+      if ((rc = build_node_layers_impl(trees[0].layer(n), n, 0, m31, l0.data(), x, err, err_len))) return rc;
+    }
     const Src4 src{{d_coords[0], d_coords[1], d_coords[2], d_coords[3]}};
     fold_circle_first_dev_kernel<<<grid1d(1ull << (n - 1), 256), 256, 0, s>>>(
         src, n, d_alphas, itw, 1ull << tree_log, line[0], trees[1].layer(n - 1), m31);
     STWO_CHECK_LAUNCH();
     for (uint32_t k = 1; k < n; k++) {
       const uint32_t L = n - k;  // log size of line[k-1]
-      auto lk = layer_ptrs(trees[k]);
-      if ((rc = build_node_layers_impl(trees[k].layer(L), L, 0, m31, lk.data(), s, err, err_len))) return rc;
+      if ((rc = nodes_on_side(k, L))) return rc;
       uint8_t* next_leaves = k + 1 < n ? trees[k + 1].layer(L - 1) : nullptr;
       fold_line_dev_kernel<<<grid1d(1ull << (L - 1), 256), 256, 0, s>>>(line[k - 1], L, 1, d_alphas + k, itw,
                                                                          1ull << tree_log, line[k], next_leaves, m31);
       STWO_CHECK_LAUNCH();
+    }
+    for (int j = 0; j < kSide; j++) {  // join
+      STWO_CUDA_TRY(cudaEventRecord(ev_fork[n + j], side[j]));
+      STWO_CUDA_TRY(cudaStreamWaitEvent(s, ev_fork[n + j], 0));
     }
     return 0;
   }
