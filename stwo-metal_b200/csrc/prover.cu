@@ -30,9 +30,10 @@ int build_node_layers_impl(const uint8_t* in, uint32_t in_log, uint32_t stop_log
 
 // ----------------------------------------------------------------- kernels --
 
-// Exact M31 dot products: products of canonical words (< 2^62) are summed in
-// 64 bits and folded with 2^31 = 1 (mod P) every three terms, then reduced
-// once to the canonical value.  The residue is exact, so the result equals the
+// Exact M31 dot products: products of words <= P with canonical weights
+// (<= P (P - 1)) are summed in 64 bits and folded with 2^31 = 1 (mod P) every
+// four terms (a folded value is < 2^33 + 2^31, and that plus four products
+// stays below 2^64), then reduced once to the canonical value.  The residue is exact, so the result equals the
 // canonical value SimdBackend's reduced-per-operation arithmetic produces.
 __device__ __forceinline__ uint64_t fold64(uint64_t x) { return (x & M31_P) + (x >> 31); }  // < 2^34
 __device__ __forceinline__ uint32_t reduce_acc(uint64_t x) {
@@ -235,7 +236,7 @@ __global__ void __launch_bounds__(256) oods_eval_kernel(PolyTable t, uint32_t n_
         for (int u = 0; u < 16; u++) {
           const uint4 w = ws[b + u * 32 + lane];
           acc4_mad(s, qm31{w.x, w.y, w.z, w.w}, v[u]);
-          if (u % 8 == 2 || u % 8 == 5 || u % 8 == 7) acc4_fold(s);
+          if (u % 4 == 3) acc4_fold(s);
         }
       }
     } else {
@@ -453,6 +454,7 @@ __global__ void __launch_bounds__(256) quotient4_kernel(QuotientParams q, PolyTa
 // next groups overlap the arithmetic of the current one.  Same arithmetic
 // per point as composition_kernel / quotient_kernel.
 constexpr int kStreamTileBits = 9, kStreamRows = 1 << kStreamTileBits, kStreamG = 6, kStreamS = 3;
+static_assert(kStreamG == 6, "the fold positions of the streaming kernels assume 6-column groups");
 constexpr int kStreamThreads = kStreamRows / 4;  // four rows per thread
 constexpr uint32_t kStreamErrWord = 8;  // word of the prover's flag buffer set by a timed-out stage
 constexpr size_t kStreamRing = (size_t)kStreamS * kStreamG * kStreamRows * sizeof(uint32_t);
@@ -481,8 +483,9 @@ __global__ void __launch_bounds__(kStreamThreads) composition_tma_kernel(
     acc4 row[4];
 #pragma unroll
     for (int r = 0; r < 4; r++) row[r] = {0, 0, 0, 0};
-    // Constraint k = c - 2 of column c = 6g + j: folding after j = 1 and
-    // j = 4 leaves at most three products between folds.
+    // Constraint k = c - 2 of column c = 6g + j: folding after j = 3 in even
+    // groups and after j = 1 and j = 5 in odd ones leaves at most four
+    // products between folds.
     for (uint32_t g = 0; g < ring.n_groups; g++) {
       const uint32_t gg = t * ring.n_groups + g;
       if (!ring.wait(gg, err)) return;
@@ -510,7 +513,7 @@ __global__ void __launch_bounds__(kStreamThreads) composition_tma_kernel(
             }
           }
         }
-        if (j == 1 || j == 4) {
+        if ((g & 1) ? (j == 1 || j == 5) : (j == 3)) {
 #pragma unroll
           for (int r = 0; r < 4; r++) acc4_fold(row[r]);
         }
@@ -578,7 +581,7 @@ __global__ void __launch_bounds__(kStreamThreads) quotient_tma_kernel(QuotientPa
 #pragma unroll
           for (int r = 0; r < 4; r++) acc4_mad(s4[r], ap, u4get(v, r));
         }
-        if (j == 2 || j == 5) {
+        if ((g & 1) ? (j == 1 || j == 5) : (j == 3)) {  // at most four products between folds
 #pragma unroll
           for (int r = 0; r < 4; r++) acc4_fold(s4[r]);
         }
