@@ -25,8 +25,8 @@ constexpr uint8_t kMixedShift = 0xFF;
 struct LeafCols {
   const uint32_t* col[kLeafMaxCols];
   uint8_t shift[kLeafMaxCols];  // L - log_size
-  // shift shared by the 16 columns [16g, 16g + 16) of one compression, or
-  // kMixedShift when they differ or the group is partial
+  // shift shared by the columns [16g, min(16g + 16, n)) of one compression,
+  // or kMixedShift when they differ
   uint8_t group_shift[kLeafMaxCols / 16];
 };
 
@@ -68,10 +68,16 @@ __global__ void __launch_bounds__(256) lifted_leaves_kernel(LeafCols t, uint32_t
     for (uint32_t c0 = 0; c0 < n_cols; c0 += 16) {
       const uint32_t gs = t.group_shift[c0 >> 4];
       if (gs != kMixedShift) {
-        // one lifted row index for the whole group: no per-column index work
+        // one lifted row index for the whole group (full or the last, partial
+        // one): no per-column index work
         const uint32_t li = lift_index(i, gs);
+        if (c0 + 16 <= n_cols) {
 #pragma unroll
-        for (int k = 0; k < 16; k++) m[k] = __ldg(t.col[c0 + k] + li);
+          for (int k = 0; k < 16; k++) m[k] = __ldg(t.col[c0 + k] + li);
+        } else {
+#pragma unroll
+          for (int k = 0; k < 16; k++) m[k] = c0 + k < n_cols ? __ldg(t.col[c0 + k] + li) : 0u;
+        }
       } else {
 #pragma unroll
         for (int k = 0; k < 16; k++) {
@@ -317,8 +323,8 @@ int build_leaves_impl(const uint32_t* const* d_cols, const uint32_t* log_sizes, 
     }
     for (uint32_t g = 0; g < kLeafMaxCols / 16; g++) {
       const uint32_t k0 = 16 * g;
-      bool uniform = k0 + 16 <= nc;
-      for (uint32_t k = k0 + 1; uniform && k < k0 + 16; k++) uniform = t.shift[k] == t.shift[k0];
+      bool uniform = k0 < nc;
+      for (uint32_t k = k0 + 1; uniform && k < std::min<uint32_t>(k0 + 16, nc); k++) uniform = t.shift[k] == t.shift[k0];
       t.group_shift[g] = uniform ? t.shift[k0] : kMixedShift;
     }
     lifted_leaves_kernel<<<grid_for(n, 256), 256, 0, s>>>(t, nc, L, m31, 4u * c0, total_bytes, state, ch == 0,
