@@ -236,6 +236,16 @@ int stwo_b200_committer_lifting_log_size(const stwo_b200_committer* committer, u
 int stwo_b200_committer_commit(stwo_b200_committer* committer, const uint32_t* const* d_evals,
                                uint32_t* const* d_coeffs, uint32_t* const* d_ldes, uint8_t* const* d_layers,
                                void* stream, char* err, size_t err_len);
+/* committer_commit with the columns in host memory (h_evals[i], 2^log_sizes[i]
+ * words; pinned memory for asynchronous copies): copies them into d_evals one
+ * log-size group at a time, largest first, on the committer's copy stream, and
+ * transforms each group as soon as its copies land, so the transforms overlap
+ * the remaining copies.  The same outputs as committer_commit on the same
+ * columns.  Ordered after the work already on `stream`, and the work on
+ * `stream` after it. */
+int stwo_b200_committer_commit_from_host(stwo_b200_committer* committer, const uint32_t* const* h_evals,
+                                         uint32_t* const* d_evals, uint32_t* const* d_coeffs, uint32_t* const* d_ldes,
+                                         uint8_t* const* d_layers, void* stream, char* err, size_t err_len);
 /* Times every candidate pass plan of each (log_size, column count) group of
  * the committer on these buffers (reps timed runs each) and keeps the fastest
  * as the process-wide plan; cache_path (optional) is read first and written

@@ -18,6 +18,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cstdio>
+#include <functional>
 #include <map>
 #include <string>
 #include <vector>
@@ -39,12 +40,63 @@ struct Committer {
   cudaGraphExec_t exec = nullptr;
   uint64_t graph_launches = 0;
 
+  // host-streamed commits: the H2D copies run on `cs`, one size group at a
+  // time, and each group's transforms wait only for that group's copies
+  cudaStream_t cs = nullptr;
+  std::vector<cudaEvent_t> ev_group;
+
   ~Committer() {
     if (s) cudaStreamSynchronize(s);
+    if (cs) cudaStreamSynchronize(cs);
     if (exec) cudaGraphExecDestroy(exec);
     if (ev_in) cudaEventDestroy(ev_in);
     if (ev_out) cudaEventDestroy(ev_out);
+    for (cudaEvent_t e : ev_group) cudaEventDestroy(e);
+    if (cs) cudaStreamDestroy(cs);
     if (s) cudaStreamDestroy(s);
+  }
+
+  // commit() with the columns still in host memory: copies them into d_evals
+  // size group by size group, largest first, on a copy stream, so the
+  // transforms of the groups already on the device overlap the copies of the
+  // rest; the tree follows once every group is transformed.  Host columns in
+  // pinned memory make the copies asynchronous.
+  int commit_from_host(const uint32_t* const* h_evals, uint32_t* const* d_evals, uint32_t* const* coeffs,
+                       uint32_t* const* ldes, uint8_t* const* layers, cudaStream_t user, char* err, size_t err_len) {
+    std::map<uint32_t, std::vector<uint32_t>, std::greater<uint32_t>> groups;
+    for (uint32_t i = 0; i < logs.size(); i++) groups[logs[i]].push_back(i);
+    if (!cs) STWO_CUDA_TRY(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    while (ev_group.size() < groups.size()) {
+      cudaEvent_t e;
+      STWO_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+      ev_group.push_back(e);
+    }
+    STWO_CUDA_TRY(cudaEventRecord(ev_in, user));
+    STWO_CUDA_TRY(cudaStreamWaitEvent(s, ev_in, 0));
+    STWO_CUDA_TRY(cudaStreamWaitEvent(cs, ev_in, 0));
+    int rc = 0;
+    size_t g = 0;
+    for (const auto& kv : groups) {
+      for (uint32_t i : kv.second)
+        STWO_CUDA_TRY(cudaMemcpyAsync(d_evals[i], h_evals[i], sizeof(uint32_t) << logs[i], cudaMemcpyHostToDevice, cs));
+      STWO_CUDA_TRY(cudaEventRecord(ev_group[g], cs));
+      STWO_CUDA_TRY(cudaStreamWaitEvent(s, ev_group[g], 0));
+      g++;
+      if (flags & STWO_B200_COMMIT_PER_COLUMN) {
+        for (uint32_t i : kv.second)
+          if ((rc = interpolate_evaluate(d_evals, coeffs, ldes, {i}, err, err_len))) return rc;
+      } else if ((rc = interpolate_evaluate(d_evals, coeffs, ldes, kv.second, err, err_len))) {
+        return rc;
+      }
+    }
+    const uint32_t n = (uint32_t)logs.size();
+    std::vector<uint32_t> lde_logs(n);
+    for (uint32_t i = 0; i < n; i++) lde_logs[i] = logs[i] + blowup;
+    rc = stwo_b200_merkle_build_layers(const_cast<const uint32_t* const*>(ldes), lde_logs.data(), n, L, m31, layers, s,
+                                       err, err_len);
+    cudaEventRecord(ev_out, s);
+    cudaStreamWaitEvent(user, ev_out, 0);
+    return rc;
   }
 
   int interpolate_evaluate(const uint32_t* const* evals, uint32_t* const* coeffs, uint32_t* const* ldes,
@@ -223,6 +275,15 @@ extern "C" int stwo_b200_committer_commit(stwo_b200_committer* c, const uint32_t
                                           uint8_t* const* d_layers, void* stream, char* err, size_t err_len) {
   STWO_ARG_CHECK(c && d_evals && d_coeffs && d_ldes && d_layers, "null argument");
   int rc = c->c.commit(d_evals, d_coeffs, d_ldes, d_layers, as_stream(stream), err, err_len);
+  return rc ? rc : ok(err, err_len);
+}
+
+extern "C" int stwo_b200_committer_commit_from_host(stwo_b200_committer* c, const uint32_t* const* h_evals,
+                                                    uint32_t* const* d_evals, uint32_t* const* d_coeffs,
+                                                    uint32_t* const* d_ldes, uint8_t* const* d_layers, void* stream,
+                                                    char* err, size_t err_len) {
+  STWO_ARG_CHECK(c && h_evals && d_evals && d_coeffs && d_ldes && d_layers, "null argument");
+  int rc = c->c.commit_from_host(h_evals, d_evals, d_coeffs, d_ldes, d_layers, as_stream(stream), err, err_len);
   return rc ? rc : ok(err, err_len);
 }
 

@@ -316,6 +316,18 @@ class Committer:
                  _ptr_array(layers), self.stream)
         return layers
 
+    def commit_from_host(self, host_ptrs, evals, coeffs, ldes, layers):
+        """commit() with the columns in host memory: ``host_ptrs[i]`` is the
+        address of column i (pinned for asynchronous copies), copied into
+        ``evals[i]`` one size group at a time while the groups already on the
+        device are transformed."""
+        if len(host_ptrs) != len(self.log_sizes):
+            raise ValueError("one host column per committed column")
+        hp = (C.c_void_p * len(host_ptrs))(*[C.c_void_p(int(p)) for p in host_ptrs])
+        ffi.call("stwo_b200_committer_commit_from_host", self._h, hp, _ptr_array(evals), _ptr_array(coeffs),
+                 _ptr_array(ldes), _ptr_array(layers), self.stream)
+        return layers
+
     def autotune(self, evals, coeffs, ldes, cache_path: str | None = None, reps: int = 3):
         path = cache_path.encode() if cache_path else None
         ffi.call("stwo_b200_committer_autotune", self._h, _ptr_array(evals), _ptr_array(coeffs), _ptr_array(ldes),

@@ -64,6 +64,31 @@ def test_commit_forms(setup, per_column, graph):
     cm.close()
 
 
+@pytest.mark.parametrize("per_column", [False, True])
+def test_commit_from_host(setup, per_column):
+    # the columns start in (pinned) host memory and are copied size group by
+    # size group while earlier groups are transformed; same bytes as commit()
+    import torch
+
+    s = setup
+    cm = Committer(s["logs"], s["blowup"], s["tree"], per_column=per_column)
+    pinned = []
+    for v in s["vals"]:
+        t = torch.empty(v.size, dtype=torch.int32).pin_memory()
+        t.numpy().view(np.uint32)[:] = v
+        pinned.append(t)
+    evals = [DeviceColumn(v.size) for v in s["vals"]]
+    coeffs = [DeviceColumn(v.size) for v in s["vals"]]
+    ldes = [DeviceColumn(v.size << s["blowup"]) for v in s["vals"]]
+    layers = cm.new_layers()
+    for _ in range(2):  # the second call reuses the copy stream and events
+        cm.commit_from_host([t.data_ptr() for t in pinned], evals, coeffs, ldes, layers)
+        for e, v in zip(evals, s["vals"]):
+            assert (e.to_host() == v).all()
+        check(s, coeffs, ldes, layers)
+    cm.close()
+
+
 def test_autotune_and_cache(setup, tmp_path):
     s = setup
     cm = Committer(s["logs"], s["blowup"], s["tree"], graph=True)
