@@ -640,8 +640,8 @@ def run_prove_reference(args, world, rank):
 
 
 # DRAM bytes of one trace evaluate (100 columns, 2^20 -> 2^21) measured by ncu:
-# strided pass 419.6 MB read + 791.5 MB written, contiguous pass 855.1 + 785.9 MB.
-EVALUATE_TRAFFIC_100x2e20 = (419.6 + 791.5 + 855.1 + 785.9) * 1e6
+# strided pass 419.5 MB read + 791.1 MB written, contiguous pass 855.0 + 786.3 MB.
+EVALUATE_TRAFFIC_100x2e20 = (419.5 + 791.1 + 855.0 + 786.3) * 1e6
 
 
 def run_prove_b200(args, world, rank, local):
