@@ -782,8 +782,8 @@ def run_prove_b200(args, world, rank, local):
             # one ncu capture at this shape
             roof["traffic"] = EVALUATE_TRAFFIC_100x2e20
             roof["traffic_source"] = "ncu capture of fft_bench.py 20 100 (profiles/fft_warp_kernels_100x2e20_full_capture.md)"
-            roof["note"] = ("bound by integer issue, not HBM: in that capture the ALU pipe is 56-70% busy and "
-                            "55-69% of issue slots are active, at about 9-12 instructions per M31 butterfly")
+            roof["note"] = ("bound by integer issue, not HBM: in that capture the ALU pipe is 57-70% busy and "
+                            "56-69% of issue slots are active, at about 9-12 instructions per M31 butterfly")
     phase_frac = {}
     for k, (kd, amt) in alg.items():
         if phase_ms.get(k, 0) > 0:
