@@ -29,6 +29,22 @@ inline int ok(char* err, size_t err_len) {
 
 inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
 
+// Raises a kernel's dynamic shared-memory limit on the current device the
+// first time it is launched there.  The attribute is per device, so `done`
+// keeps one bit per device; threads that race to set it both set the same
+// value, which is harmless.
+template <typename Kernel>
+inline cudaError_t ensure_smem_limit(Kernel* kernel, int bytes, std::atomic<uint32_t>& done) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  const uint32_t bit = dev >= 0 && dev < 32 ? 1u << dev : 0u;
+  if (bit && (done.load(std::memory_order_acquire) & bit)) return cudaSuccess;
+  e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e == cudaSuccess && bit) done.fetch_or(bit, std::memory_order_release);
+  return e;
+}
+
 // Number of kernels this library has launched (read by stwo_b200_launch_count).
 extern std::atomic<uint64_t> g_kernel_launches;
 

@@ -716,12 +716,8 @@ static int launch_warp_pass(const FftPass& q, const FftCols& cols, uint64_t tile
                             char* err, size_t err_len) {
   if (q.C == 0) {
     constexpr size_t smem = (1024 + kWarpCols * kTileWords) * sizeof(uint32_t);
-    static bool attr = false;
-    if (!attr) {
-      STWO_CUDA_TRY(cudaFuncSetAttribute(fft_warp_contig_kernel<INV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem));
-      attr = true;
-    }
+    static std::atomic<uint32_t> attr{0};
+    STWO_CUDA_TRY(ensure_smem_limit(fft_warp_contig_kernel<INV>, (int)smem, attr));
     // up to 4 column groups per block: fewer twiddle stagings while the grid
     // still has several waves of blocks
     const uint32_t groups = (uint32_t)((nc + kWarpCols - 1) / kWarpCols);
@@ -731,12 +727,8 @@ static int launch_warp_pass(const FftPass& q, const FftCols& cols, uint64_t tile
     fft_warp_contig_kernel<INV><<<grid, 32 * kWarpCols, smem, s>>>(qq, cols);
   } else {
     constexpr size_t smem = (1024 + 8 * kColStride) * sizeof(uint32_t);
-    static bool attr = false;
-    if (!attr) {
-      STWO_CUDA_TRY(cudaFuncSetAttribute(fft_warp_strided_kernel<INV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem));
-      attr = true;
-    }
+    static std::atomic<uint32_t> attr{0};
+    STWO_CUDA_TRY(ensure_smem_limit(fft_warp_strided_kernel<INV>, (int)smem, attr));
     dim3 grid((unsigned)tiles, (unsigned)nc);
     fft_warp_strided_kernel<INV><<<grid, 256, smem, s>>>(q, cols);
   }
@@ -750,12 +742,8 @@ static int launch_tile(const FftPass& q, const FftCols& cols, dim3 grid, cudaStr
   constexpr size_t E = (size_t)1 << (T + C);
   constexpr size_t smem = ((size_t)CPB * tile_stride_words(E) + ((size_t)1 << T)) * sizeof(uint32_t);
   static_assert(smem <= 200 * 1024, "FFT tile exceeds shared memory");
-  static bool attr_set = false;
-  if (!attr_set) {
-    STWO_CUDA_TRY(cudaFuncSetAttribute(fft_pass_kernel<INV, T, C, CPB, NT>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    attr_set = true;
-  }
+  static std::atomic<uint32_t> attr{0};
+  STWO_CUDA_TRY(ensure_smem_limit(fft_pass_kernel<INV, T, C, CPB, NT>, (int)smem, attr));
   fft_pass_kernel<INV, T, C, CPB, NT><<<grid, NT, smem, s>>>(q, cols);
   STWO_CHECK_LAUNCH();
   return STWO_B200_OK;
