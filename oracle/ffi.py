@@ -77,6 +77,18 @@ def index_to_point(index: int):
     return int(xy[0]), int(xy[1])
 
 
+def qm31_mul(a, b) -> tuple:
+    x, y, out = _u32(a), _u32(b), np.zeros(4, np.uint32)
+    _check(lib().oracle_qm31_mul(_p(x), _p(y), _p(out)))
+    return tuple(int(v) for v in out)
+
+
+def qm31_inv(a) -> tuple:
+    x, out = _u32(a), np.zeros(4, np.uint32)
+    _check(lib().oracle_qm31_inv(_p(x), _p(out)))
+    return tuple(int(v) for v in out)
+
+
 def canonic_half_initial_index(log_size: int) -> int:
     """CanonicCoset(log_size).circle_domain().half_coset initial index."""
     return 1 << (31 - (log_size + 1))

@@ -52,6 +52,22 @@ void oracle_index_to_point(uint64_t index, uint32_t* xy) {
 
 void oracle_bit_reverse(uint32_t* v, uint32_t log_n) { bit_reverse(v, log_n); }
 
+// QM31 product and inverse (core/fields/qm31.rs:78-88, 125-133); CM31 values
+// are the QM31 values with the upper half zero.
+int oracle_qm31_mul(const uint32_t* a, const uint32_t* b, uint32_t* out) {
+  return guard([&] {
+    QM31 r = QM31::from(a[0], a[1], a[2], a[3]) * QM31::from(b[0], b[1], b[2], b[3]);
+    out[0] = r.x.a; out[1] = r.x.b; out[2] = r.y.a; out[3] = r.y.b;
+  });
+}
+
+int oracle_qm31_inv(const uint32_t* a, uint32_t* out) {
+  return guard([&] {
+    QM31 r = qinv(QM31::from(a[0], a[1], a[2], a[3]));
+    out[0] = r.x.a; out[1] = r.x.b; out[2] = r.y.a; out[3] = r.y.b;
+  });
+}
+
 // Twiddle tree of the coset (initial_index, log_size): 2^log_size words each.
 int oracle_precompute_twiddles(uint64_t initial_index, uint32_t log_size, uint32_t* tw, uint32_t* itw) {
   return guard([&] {
