@@ -448,14 +448,18 @@ __global__ void __launch_bounds__(256) quotient4_kernel(QuotientParams q, PolyTa
 }
 
 // ---- TMA column-streaming versions ----
-// A block owns kStreamRows consecutive rows; thread t owns rows 4t .. 4t+3.
-// Columns arrive kStreamG at a time through the shared-memory ring of
-// ColumnRing (cp.async.bulk, mbarrier completion), so the DRAM reads of the
-// next groups overlap the arithmetic of the current one.  Same arithmetic
-// per point as composition_kernel / quotient_kernel.
+// A block owns kStreamRows consecutive rows; consumer thread t owns rows 4t ..
+// 4t+3.  Columns arrive kStreamG at a time through the shared-memory stages of
+// ColumnPipe (cp.async.bulk issued by a producer warp, full/empty mbarriers),
+// so the DRAM reads of the next groups overlap the arithmetic of the current
+// one and no block barrier is taken per group.  Same arithmetic per point as
+// composition_kernel / quotient_kernel.
 constexpr int kStreamTileBits = 9, kStreamRows = 1 << kStreamTileBits, kStreamG = 6, kStreamS = 3;
 static_assert(kStreamG == 6, "the fold positions of the streaming kernels assume 6-column groups");
-constexpr int kStreamThreads = kStreamRows / 4;  // four rows per thread
+constexpr int kStreamThreads = kStreamRows / 4;      // consumers: four rows per thread
+constexpr int kStreamBlock = kStreamThreads + 32;    // plus the producer warp
+using StreamPipe = ColumnPipe<kStreamG, kStreamS, kStreamRows, kStreamThreads>;
+constexpr int kPipeBarWords = 2 * kStreamS + (kStreamS * kPipeHeaderWords + 1 + 1) / 2;  // uint64 slots
 constexpr uint32_t kStreamErrWord = 8;  // word of the prover's flag buffer set by a timed-out stage
 constexpr size_t kStreamRing = (size_t)kStreamS * kStreamG * kStreamRows * sizeof(uint32_t);
 constexpr uint32_t kStreamMaxW = 1024;  // QM31 weights staged in shared memory
@@ -465,20 +469,23 @@ __device__ __forceinline__ void stage_weights(uint4* sw, const qm31* __restrict_
   for (uint32_t k = threadIdx.x; k < n; k += blockDim.x) sw[k] = make_uint4(w[k].a, w[k].b, w[k].c, w[k].d);
 }
 
-__global__ void __launch_bounds__(kStreamThreads) composition_tma_kernel(
+__global__ void __launch_bounds__(kStreamBlock) composition_tma_kernel(
     const uint32_t* __restrict__ evals, uint64_t col_stride, uint32_t n_cons, const qm31* __restrict__ powers,
     const uint32_t* __restrict__ denom_inv, uint32_t log_n, uint64_t n_points, uint32_t* __restrict__ out,
     uint32_t* err) {
   extern __shared__ __align__(128) uint32_t smem[];
-  __shared__ uint64_t bars[kStreamS];
+  __shared__ uint64_t bars[kPipeBarWords];
   uint4* sw = reinterpret_cast<uint4*>(smem + kStreamRing / sizeof(uint32_t));
   const uint32_t t4 = threadIdx.x * 4;
   auto col = [evals, col_stride](uint32_t c) { return evals + (uint64_t)c * col_stride; };
-  ColumnRing<kStreamG, kStreamS, kStreamRows> ring(smem, bars, n_cons + 2, (uint32_t)(n_points / kStreamRows));
+  StreamPipe pipe(smem, bars, n_cons + 2, (uint32_t)(n_points / kStreamRows));
   stage_weights(sw, powers, n_cons);
-  __syncthreads();
-  ring.start(col);
-  for (uint32_t t = 0; t < ring.my_tiles; t++) {
+  __syncthreads();  // the last block barrier: the producer warp leaves the loop below
+  if (threadIdx.x >= kStreamThreads) {
+    if (threadIdx.x == kStreamThreads) pipe.produce(col, [](uint32_t, uint32_t*) {}, err);
+    return;
+  }
+  for (uint32_t t = 0; t < pipe.my_tiles; t++) {
     uint32_t sa[4] = {0, 0, 0, 0}, sb[4] = {0, 0, 0, 0};
     acc4 row[4];
 #pragma unroll
@@ -486,15 +493,15 @@ __global__ void __launch_bounds__(kStreamThreads) composition_tma_kernel(
     // Constraint k = c - 2 of column c = 6g + j: folding after j = 3 in even
     // groups and after j = 1 and j = 5 in odd ones leaves at most four
     // products between folds.
-    for (uint32_t g = 0; g < ring.n_groups; g++) {
-      const uint32_t gg = t * ring.n_groups + g;
-      if (!ring.wait(gg, err)) return;
-      const uint32_t nc = ring.cols_in(g);
+    for (uint32_t g = 0; g < pipe.n_groups; g++) {
+      const uint32_t gg = t * pipe.n_groups + g;
+      if (!pipe.wait(gg, err)) return;
+      const uint32_t nc = pipe.cols_in(g);
 #pragma unroll
       for (int j = 0; j < kStreamG; j++) {
         if ((uint32_t)j < nc) {
           const uint32_t c = g * kStreamG + j;
-          const uint4 v = *reinterpret_cast<const uint4*>(ring.seg(gg, j) + t4);
+          const uint4 v = *reinterpret_cast<const uint4*>(pipe.seg(gg, j) + t4);
           if (c >= 2) {
             const uint4 pw4 = sw[c - 2];
             const qm31 pw{pw4.x, pw4.y, pw4.z, pw4.w};
@@ -518,9 +525,9 @@ __global__ void __launch_bounds__(kStreamThreads) composition_tma_kernel(
           for (int r = 0; r < 4; r++) acc4_fold(row[r]);
         }
       }
-      ring.release(gg, col);
+      pipe.release(gg);
     }
-    const uint64_t i = ring.tile_row0(t) + t4;
+    const uint64_t i = pipe.tile_row0(t) + t4;
     qm31 v[4];
 #pragma unroll
     for (int r = 0; r < 4; r++) v[r] = qm31_mul_m31(acc4_reduce(row[r]), __ldg(denom_inv + ((i + r) >> log_n)));
@@ -537,45 +544,58 @@ __global__ void __launch_bounds__(kStreamThreads) composition_tma_kernel(
 // bitrev_{b-2}(t) * 2^(log-b) and that + 2^(log-2)); e = 1, 3 are their
 // conjugates in the upper half.  So the two points are B +
 // tile_pts[bitrev_{b-2}(t)] and that + step * 2^(log-2), B = init + J0 * step.
-__global__ void __launch_bounds__(kStreamThreads) quotient_tma_kernel(QuotientParams q, PolyTable cols,
-                                                                     uint32_t n_cols,
-                                                                     const qm31* __restrict__ alpha_pows,
-                                                                     const QuotientDyn* __restrict__ dyn,
-                                                                     uint32_t* __restrict__ out, uint32_t* err) {
+__global__ void __launch_bounds__(kStreamBlock) quotient_tma_kernel(QuotientParams q, PolyTable cols,
+                                                                   uint32_t n_cols,
+                                                                   const qm31* __restrict__ alpha_pows,
+                                                                   const QuotientDyn* __restrict__ dyn,
+                                                                   uint32_t* __restrict__ out, uint32_t* err) {
   const QuotientDyn& qd = *dyn;  // read at the epilogue, through the read-only cache
   extern __shared__ __align__(128) uint32_t smem[];
-  __shared__ uint64_t bars[kStreamS];
-  __shared__ cpoint s_base;
+  __shared__ uint64_t bars[kPipeBarWords];
   uint4* sw = reinterpret_cast<uint4*>(smem + kStreamRing / sizeof(uint32_t));
   const uint64_t n = 1ull << q.log_size;
   const uint32_t t4 = threadIdx.x * 4;
   const PolyTable* tab = &cols;
   auto col = [tab](uint32_t c) { return tab->p[c]; };
-  ColumnRing<kStreamG, kStreamS, kStreamRows> ring(smem, bars, n_cols, (uint32_t)(n / kStreamRows));
+  StreamPipe pipe(smem, bars, n_cols, (uint32_t)(n / kStreamRows));
   stage_weights(sw, alpha_pows, n_cols);
-  __syncthreads();
-  ring.start(col);
-  for (uint32_t t = 0; t < ring.my_tiles; t++) {
-    const uint64_t r0 = ring.tile_row0(t);
-    if (threadIdx.x == 0) {  // read by all threads only after the first release barrier of the tile
-      const uint64_t J0 = __brevll(r0) >> (64 - q.log_size);
-      cpoint b = q.init;
-      for (uint32_t k = 0; k + 1 < q.log_size; k++)
-        if ((J0 >> k) & 1) b = cpoint_add(b, q.step_pow[k]);
-      s_base = b;
+  __syncthreads();  // the last block barrier: the producer warp leaves the loop below
+  if (threadIdx.x >= kStreamThreads) {
+    if (threadIdx.x == kStreamThreads) {
+      // Tile header: B = init + J0 * step, J0 the bit-reversed first row.
+      const QuotientParams* qp = &q;
+      pipe.produce(col,
+                   [qp, &pipe](uint32_t t, uint32_t* h) {
+                     const uint64_t J0 = __brevll(pipe.tile_row0(t)) >> (64 - qp->log_size);
+                     cpoint b = qp->init;
+                     for (uint32_t k = 0; k + 1 < qp->log_size; k++)
+                       if ((J0 >> k) & 1) b = cpoint_add(b, qp->step_pow[k]);
+                     h[0] = b.x;
+                     h[1] = b.y;
+                   },
+                   err);
     }
+    return;
+  }
+  for (uint32_t t = 0; t < pipe.my_tiles; t++) {
+    const uint64_t r0 = pipe.tile_row0(t);
+    cpoint base{0, 0};
     acc4 s4[4];
 #pragma unroll
     for (int r = 0; r < 4; r++) s4[r] = {0, 0, 0, 0};
-    for (uint32_t g = 0; g < ring.n_groups; g++) {
-      const uint32_t gg = t * ring.n_groups + g;
-      if (!ring.wait(gg, err)) return;
-      const uint32_t nc = ring.cols_in(g);
+    for (uint32_t g = 0; g < pipe.n_groups; g++) {
+      const uint32_t gg = t * pipe.n_groups + g;
+      if (!pipe.wait(gg, err)) return;
+      if (g == 0) {  // header of the tile, valid while this stage is held
+        const uint32_t* h = pipe.head(gg);
+        base = cpoint{h[0], h[1]};
+      }
+      const uint32_t nc = pipe.cols_in(g);
 #pragma unroll
       for (int j = 0; j < kStreamG; j++) {
         if ((uint32_t)j < nc) {
           const uint32_t c = g * kStreamG + j;
-          const uint4 v = *reinterpret_cast<const uint4*>(ring.seg(gg, j) + t4);
+          const uint4 v = *reinterpret_cast<const uint4*>(pipe.seg(gg, j) + t4);
           const uint4 a4 = sw[c];
           const qm31 ap{a4.x, a4.y, a4.z, a4.w};
 #pragma unroll
@@ -586,9 +606,9 @@ __global__ void __launch_bounds__(kStreamThreads) quotient_tma_kernel(QuotientPa
           for (int r = 0; r < 4; r++) acc4_fold(s4[r]);
         }
       }
-      ring.release(gg, col);
+      pipe.release(gg);
     }
-    const cpoint p0 = cpoint_add(s_base, q.tile_pts[__brev(threadIdx.x) >> (32 - (kStreamTileBits - 2))]);
+    const cpoint p0 = cpoint_add(base, q.tile_pts[__brev(threadIdx.x) >> (32 - (kStreamTileBits - 2))]);
     const cpoint p2 = cpoint_add(p0, q.step_pow[q.log_size - 2]);
     const uint32_t xs[4] = {p0.x, p0.x, p2.x, p2.x};
     const uint32_t ys[4] = {p0.y, m31_neg(p0.y), p2.y, m31_neg(p2.y)};
@@ -623,7 +643,6 @@ __global__ void __launch_bounds__(kStreamThreads) quotient_tma_kernel(QuotientPa
     *reinterpret_cast<uint4*>(out + n + i) = make_uint4(v[0].b, v[1].b, v[2].b, v[3].b);
     *reinterpret_cast<uint4*>(out + 2 * n + i) = make_uint4(v[0].c, v[1].c, v[2].c, v[3].c);
     *reinterpret_cast<uint4*>(out + 3 * n + i) = make_uint4(v[0].d, v[1].d, v[2].d, v[3].d);
-    __syncthreads();  // s_base of this tile read by every thread before thread 0 rewrites it
   }
 }
 
@@ -1252,7 +1271,7 @@ static unsigned stream_grid(K kernel, size_t smem, uint32_t n_tiles) {
   int dev = 0, sms = 148, per_sm = 1;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kStreamThreads, smem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kStreamBlock, smem);
   const uint32_t resident = (uint32_t)std::max(1, sms) * (uint32_t)std::max(1, per_sm);
   return std::max(1u, std::min(n_tiles, resident));
 }
@@ -1801,7 +1820,7 @@ int WideFibProver::prove_body(const uint32_t* d_a, const uint32_t* d_b, ProofOut
       reinterpret_cast<uintptr_t>(comp_src) % 16 == 0)
     composition_tma_kernel<<<stream_grid(composition_tma_kernel, kStreamRing + n_cons * sizeof(uint4),
                                          (uint32_t)(n_eval / kStreamRows)),
-                             kStreamThreads, kStreamRing + n_cons * sizeof(uint4), s>>>(
+                             kStreamBlock, kStreamRing + n_cons * sizeof(uint4), s>>>(
         comp_src, comp_stride, n_cons, d_small, d_denom, log_n, n_eval, d_comp, d_found + kStreamErrWord);
   else if (n_eval % 4 == 0 && comp_stride % 4 == 0 && reinterpret_cast<uintptr_t>(comp_src) % 16 == 0)
     composition4_kernel<<<grid1d(n_eval / 4, 256), 256, 0, s>>>(comp_src, comp_stride, n_cons, d_small, d_denom,
@@ -1885,7 +1904,7 @@ int WideFibProver::prove_body(const uint32_t* d_a, const uint32_t* d_b, ProofOut
       }
       quotient_tma_kernel<<<stream_grid(quotient_tma_kernel, kStreamRing + nq * sizeof(uint4),
                                         (uint32_t)((1ull << lift) / kStreamRows)),
-                            kStreamThreads, kStreamRing + nq * sizeof(uint4), s>>>(
+                            kStreamBlock, kStreamRing + nq * sizeof(uint4), s>>>(
           qp, cols, nq, d_ap, d_qdyn, d_quot, d_found + kStreamErrWord);
     } else if (aligned)
       quotient4_kernel<<<grid1d(1ull << (lift - 2), 256), 256, 0, s>>>(qp, cols, nq, d_ap, d_qdyn, d_quot);
