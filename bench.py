@@ -11,8 +11,9 @@ Workloads (seeded synthetic M31 data, values uniform in [0, P)):
   commit_uneven  512 columns, log sizes U{12..22}, blowup 2, one lifted
                  Blake2s tree (L = 24): interpolate -> evaluate -> leaves ->
                  nodes.  Unit: committed trace cells / s.
-  commit_plain   32 columns of log 16, blowup 1: bit-reverse -> interpolate ->
-                 evaluate -> Merkle (L = 17).
+  commit_plain   32 columns of log 16, blowup 1, natural-order input:
+                 interpolate (the bit reversal rides on the first IFFT pass's
+                 loads) -> evaluate -> Merkle (L = 17).
 
 A step is one commit of the whole trace.  `value` is device-timed with inputs
 resident in HBM; `e2e` goes through the same public calls with the trace in
@@ -341,11 +342,10 @@ def run_b200(args, spec, world, rank, local):
 
     def step(evs=None):
         if spec["bitrev"]:
-            # bit-reverse the natural-order trace into the coefficient buffers,
-            # then interpolate in place.
-            be.bit_reverse_columns(inputs, coeffs)
+            # natural-order trace: bit reversal + interpolation in one call,
+            # the bit reversal fused into the first IFFT pass (no phase of its own)
             rec(evs, 0)
-            be.interpolate_columns(coeffs, tree)
+            be.interpolate_natural_into(inputs, coeffs, tree)
         else:
             rec(evs, 0)
             be.interpolate_columns_into(inputs, coeffs, tree)
@@ -506,7 +506,7 @@ def run_b200(args, spec, world, rank, local):
     hbm_peak, peak_kind = load_peaks()
     # algorithmic bytes per phase (inputs + outputs once; twiddles excluded)
     alg_bytes = {
-        "bitrev": 8 * cells if spec["bitrev"] else 0,
+        "bitrev": 0,  # fused into the first IFFT pass (natural-order loads)
         "ifft": 8 * cells,
         "rfft": 4 * cells + 4 * eval_cells,
         "leaves": 4 * eval_cells + 32 * (1 << L),

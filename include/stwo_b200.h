@@ -110,6 +110,19 @@ int stwo_b200_interpolate_columns_into(const uint32_t* const* d_evals, uint32_t*
                                        uint32_t n_cols, const uint32_t* d_itwiddles, uint32_t tree_log_size,
                                        void* stream, char* err, size_t err_len);
 
+/* Interpolation of natural-order evaluations: the pair
+ * CircleEvaluation<_, _, NaturalOrder>::bit_reverse (core/poly/circle/
+ * evaluation.rs:61-64, i.e. ColumnOps::bit_reverse_column) + PolyOps::interpolate
+ * in one call.  Reads d_natural[i] (natural order), writes d_coeffs[i].  Where
+ * every column of a size is out of place (d_natural[i] != d_coeffs[i]) and the
+ * size is >= 3, the bit reversal is done by the loads of the first FFT pass;
+ * otherwise by one batched bit-reversal launch into d_coeffs first.  In place
+ * (d_natural[i] == d_coeffs[i]) is allowed. */
+int stwo_b200_interpolate_columns_natural(const uint32_t* const* d_natural, uint32_t* const* d_coeffs,
+                                          const uint32_t* log_sizes, const uint64_t* half_initial_indices,
+                                          uint32_t n_cols, const uint32_t* d_itwiddles, uint32_t tree_log_size,
+                                          void* stream, char* err, size_t err_len);
+
 /* PolyOps::evaluate_polynomials (prover/poly/circle/ops.rs:110-211 ->
  * evaluate_into, simd/circle.rs:388-443): coefficients (2^log_sizes[i]) ->
  * evaluations on CanonicCoset(log_sizes[i] + log_blowup), bit-reversed.

@@ -43,6 +43,7 @@ struct FftPass {
   uint32_t vec_io;     // 16-byte global loads/stores are legal for this launch
   uint32_t cpb;        // columns per block: tiles of the same position share staged twiddles
   uint32_t n_cols;     // columns in this launch
+  uint32_t natural = 0;  // the source is in natural order: the contiguous first pass gathers src[rev_N(i)]
 };
 
 
@@ -201,7 +202,15 @@ __global__ void __launch_bounds__(NT, 1024 / NT) fft_pass_kernel(FftPass p, FftC
   for (uint32_t cc = 0; cc < n_tiles; cc++) {
     const uint32_t* __restrict__ src = cols.src[col0 + cc];
     uint32_t* tsm = sm + cc * STRIDE;
-    if (p.vec_io) {
+    if (C == 0 && p.natural) {
+      // Natural-order source (first pass, L0 = 0): element e of tile position
+      // hi is src[rev_T(e) * 2^(N-T) + rev_{N-T}(hi)], the bit reversal of
+      // ColumnOps::bit_reverse_column done by the loads.
+      const uint32_t sh = p.log_domain - T;
+      const uint64_t rh = sh ? __brevll(hi) >> (64 - sh) : 0;
+      for (uint32_t e = threadIdx.x; e < E; e += NT)
+        tsm[smem_off(e)] = __ldg(src + (((uint64_t)(__brev(e) >> (32 - T)) << sh) | rh));
+    } else if (p.vec_io) {
 #pragma unroll 4
       for (uint32_t e = threadIdx.x * 4; e < E; e += NT * 4) {
         const uint64_t g = base + ((uint64_t)(e >> C) << L0) + (e & CMASK);
@@ -313,6 +322,26 @@ __global__ void bit_reverse_kernel(uint32_t* v, uint32_t log_n) {
       uint32_t a = v[i], b = v[j];
       v[i] = b;
       v[j] = a;
+    }
+  }
+}
+
+// Bit reversal of up to kFftMaxCols columns of one size in one launch
+// (blockIdx.y = column): out of place (dst[brev(i)] = src[i], coalesced
+// reads), or in place by pairwise swaps when dst == src.
+__global__ void bit_reverse_cols_kernel(FftCols t, uint32_t log_n) {
+  const uint64_t n = 1ull << log_n;
+  const uint32_t* __restrict__ src = t.src[blockIdx.y];
+  uint32_t* dst = t.dst[blockIdx.y];
+  const bool in_place = src == dst;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t j = __brevll(i) >> (64 - log_n);
+    if (!in_place) {
+      dst[j] = src[i];
+    } else if (i < j) {
+      const uint32_t a = dst[i], b = dst[j];
+      dst[i] = b;
+      dst[j] = a;
     }
   }
 }
@@ -512,6 +541,26 @@ __device__ __forceinline__ void tile_wait() {
   asm volatile("cp.async.wait_group 0;\n" ::: "memory");
   __syncwarp();
 }
+// Tile position hi of a natural-order column of 2^log_n words (log_n >= 10)
+// staged in bit-reversed order, which fuses ColumnOps::bit_reverse_column
+// (prover/backend/simd/bit_reverse.rs:21-33) into the first pass: word e of
+// the tile is src[rev10(e) * 2^(log_n-10) + rev(hi)].  Lane l copies words
+// 32 i + l with 4-byte cp.async; each 32-byte sector holds one word of 8
+// tile positions, which read it through L2.  One commit group per tile.
+__device__ __forceinline__ void tile_gather_natural(const uint32_t* __restrict__ src, uint32_t log_n, uint64_t hi,
+                                                    uint32_t* buf, uint32_t lane) {
+  const uint32_t sh = log_n - 10;
+  const uint64_t rh = sh ? __brevll(hi) >> (64 - sh) : 0;
+#pragma unroll 8
+  for (int i = 0; i < 32; i++) {
+    const uint32_t e = 32u * i + lane;
+    const uint64_t g = ((uint64_t)(__brev(e) >> 22) << sh) | rh;
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(smem_addr(buf + i * kTileStride + lane)),
+                 "l"(src + g)
+                 : "memory");
+  }
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
 __device__ __forceinline__ void tile_to_lane_major(const uint32_t* buf, uint32_t lane, uint32_t (&v)[32]) {
 #pragma unroll
   for (int q = 0; q < 8; q++) {
@@ -535,7 +584,9 @@ __device__ __forceinline__ void lane_major_to_tile(uint32_t* buf, uint32_t lane,
 // tiles through its own staged tile with cp.async: the next tile's copy is
 // issued as soon as the transpose has freed the buffer, so it lands during
 // the second half of the butterflies and the stores.  No block barrier after
-// the staging.  Needs 16-byte aligned columns and no source masking.
+// the staging.  Needs 16-byte aligned columns and no source masking.  With
+// p.natural (inverse transforms, source distinct from destination) the tiles
+// are gathered from a natural-order source instead.
 template <bool INV>
 __global__ void __launch_bounds__(256, 4) fft_warp_contig_kernel(FftPass p, FftCols cols) {
   extern __shared__ __align__(16) uint32_t smem[];
@@ -546,7 +597,13 @@ __global__ void __launch_bounds__(256, 4) fft_warp_contig_kernel(FftPass p, FftC
   const uint64_t base = hi << 10;
   const uint32_t g0 = blockIdx.y * p.cpb;
   uint32_t c = g0 * kWarpCols + warp;
-  if (c < p.n_cols) tile_prefetch(cols.src[c] + base, buf, lane);
+  const bool natural = p.natural != 0;
+  if (c < p.n_cols) {
+    if (natural)
+      tile_gather_natural(cols.src[c], p.log_domain, hi, buf, lane);
+    else
+      tile_prefetch(cols.src[c] + base, buf, lane);
+  }
   stage_tws10(p, hi, tws);
   __syncthreads();
   const uint32_t scale = p.scale;
@@ -565,7 +622,12 @@ __global__ void __launch_bounds__(256, 4) fft_warp_contig_kernel(FftPass p, FftC
 #pragma unroll
       for (int j = 0; j < 32; j++) v[j] = buf[j * kTileStride + lane];
       __syncwarp();
-      if (more) tile_prefetch(cols.src[cn] + base, buf, lane);
+      if (more) {
+        if (natural)
+          tile_gather_natural(cols.src[cn], p.log_domain, hi, buf, lane);
+        else
+          tile_prefetch(cols.src[cn] + base, buf, lane);
+      }
       warp_phase_hi<true>(v, tws);
 #pragma unroll
       for (int j = 0; j < 32; j++) dst[base + j * 32 + lane] = scale != 1u ? m31_mul(v[j], scale) : v[j];
@@ -793,6 +855,8 @@ static int launch_pass(const FftPass& p, const std::vector<const uint32_t*>& src
     const bool warp_contig = p.T == 10 && p.C == 0 && p.layer0 == 0 && aligned && p.src_mask == ~0ull &&
                              p.src_len == ~0ull;
     const bool warp_strided = p.T == 10 && p.C == 3 && p.layer0 >= 3;
+    STWO_ARG_CHECK(!p.natural || (INV && p.C == 0 && p.layer0 == 0 && p.src_mask == ~0ull && p.src_len == ~0ull),
+                   "natural-order source needs an unmasked first inverse pass");
     if (warp_contig || warp_strided)
       rc = launch_warp_pass<INV>(q, cols, tiles, nc, s, err, err_len);
     else if (p.C == 3)
@@ -810,9 +874,41 @@ static int launch_pass(const FftPass& p, const std::vector<const uint32_t*>& src
 
 using namespace stwo_b200;
 
+// Bit reversal of columns of one log size, kFftMaxCols per launch: into dst
+// (out of place) or in place where dst == src.
+static int bit_reverse_group(const uint32_t* const* src, uint32_t* const* dst, uint32_t n_cols, uint32_t lg,
+                             cudaStream_t s, char* err, size_t err_len) {
+  for (uint32_t a = 0; a < n_cols; a += kFftMaxCols) {
+    const uint32_t nc = std::min<uint32_t>(kFftMaxCols, n_cols - a);
+    FftCols t;
+    for (uint32_t k = 0; k < nc; k++) {
+      STWO_ARG_CHECK(src[a + k] && dst[a + k], "null column %u", a + k);
+      t.src[k] = src[a + k];
+      t.dst[k] = dst[a + k];
+    }
+    if (lg > 0) {
+      const uint64_t n = 1ull << lg;
+      const unsigned bx = (unsigned)std::min<uint64_t>((n + 255) / 256, std::max<uint64_t>(1, 148 * 32 / nc));
+      bit_reverse_cols_kernel<<<dim3(bx, nc), 256, 0, s>>>(t, lg);
+      STWO_CHECK_LAUNCH();
+    } else {
+      for (uint32_t k = 0; k < nc; k++)
+        if (t.src[k] != t.dst[k]) STWO_CUDA_TRY(cudaMemcpyAsync(t.dst[k], t.src[k], 4, cudaMemcpyDeviceToDevice, s));
+    }
+  }
+  return STWO_B200_OK;
+}
+
+// natural: the sources are in natural order (CircleEvaluation<_, _,
+// NaturalOrder>::bit_reverse, core/poly/circle/evaluation.rs:61-64, before
+// the interpolation).  Where every source of a size group is distinct from
+// its destination, the bit reversal happens in the loads of the first pass
+// (warp or tile form); otherwise (in place, or log size <= 2) one batched
+// bit-reversal launch into the destinations precedes the transform.
 static int interpolate_impl(const uint32_t* const* d_src, uint32_t* const* d_cols, const uint32_t* log_sizes,
                             const uint64_t* half_initial_indices, uint32_t n_cols, const uint32_t* d_itwiddles,
-                            uint32_t tree_log_size, cudaStream_t s, char* err, size_t err_len) {
+                            uint32_t tree_log_size, cudaStream_t s, char* err, size_t err_len,
+                            bool natural = false) {
   STWO_ARG_CHECK(n_cols == 0 || (d_src && d_cols && log_sizes), "null column arrays");
   // Group columns by log size: one launch per (size, pass).
   std::vector<uint32_t> order(n_cols);
@@ -830,6 +926,16 @@ static int interpolate_impl(const uint32_t* const* d_src, uint32_t* const* d_col
       continue;
     }
     if (n <= 2) {
+      if (natural) {
+        std::vector<const uint32_t*> gs;
+        std::vector<uint32_t*> gd;
+        for (size_t i = a; i < b; i++) {
+          gs.push_back(d_src[order[i]]);
+          gd.push_back(d_cols[order[i]]);
+        }
+        int rc = bit_reverse_group(gs.data(), gd.data(), (uint32_t)gs.size(), n, s, err, err_len);
+        if (rc) return rc;
+      }
       for (size_t i = a; i < b; i++) {
         uint32_t c = order[i];
         uint64_t hi = half_initial_indices ? half_initial_indices[c] : (1ull << (31 - (n + 1)));
@@ -838,7 +944,7 @@ static int interpolate_impl(const uint32_t* const* d_src, uint32_t* const* d_col
           STWO_CHECK_LAUNCH();
           n_small = 0;
         }
-        small.src[n_small] = d_src[c];
+        small.src[n_small] = natural ? d_cols[c] : d_src[c];
         small.dst[n_small] = d_cols[c];
         index_point(hi, small.x[n_small], small.y[n_small]);
         small.log_src[n_small] = n;
@@ -858,6 +964,13 @@ static int interpolate_impl(const uint32_t* const* d_src, uint32_t* const* d_col
     }
     std::vector<const uint32_t*> inplace(dsts.begin(), dsts.end());
     auto plan = plan_passes(n);
+    bool fuse = natural;  // the first pass (C = 0, layer 0) gathers, when it does not overwrite its source
+    for (size_t i = 0; fuse && i < srcs.size(); i++) fuse = srcs[i] != dsts[i];
+    if (natural && !fuse) {
+      int rc = bit_reverse_group(srcs.data(), dsts.data(), (uint32_t)srcs.size(), n, s, err, err_len);
+      if (rc) return rc;
+      srcs = inplace;
+    }
     for (size_t pi = 0; pi < plan.size(); pi++) {
       FftPass p;
       p.tree = d_itwiddles;
@@ -869,6 +982,7 @@ static int interpolate_impl(const uint32_t* const* d_src, uint32_t* const* d_col
       p.T = plan[pi].T;
       p.C = plan[pi].C;
       p.scale = (pi + 1 == plan.size()) ? host_pow2_inv(n) : 1u;
+      p.natural = (pi == 0 && fuse) ? 1u : 0u;
       int rc = launch_pass<true>(p, pi == 0 ? srcs : inplace, dsts, n, s, err, err_len);
       if (rc) return rc;
     }
@@ -896,6 +1010,15 @@ extern "C" int stwo_b200_interpolate_columns_into(const uint32_t* const* d_evals
                                                   uint32_t tree_log_size, void* stream, char* err, size_t err_len) {
   int rc = interpolate_impl(d_evals, d_coeffs, log_sizes, half_initial_indices, n_cols, d_itwiddles, tree_log_size,
                             as_stream(stream), err, err_len);
+  return rc ? rc : ok(err, err_len);
+}
+
+extern "C" int stwo_b200_interpolate_columns_natural(const uint32_t* const* d_natural, uint32_t* const* d_coeffs,
+                                                     const uint32_t* log_sizes, const uint64_t* half_initial_indices,
+                                                     uint32_t n_cols, const uint32_t* d_itwiddles,
+                                                     uint32_t tree_log_size, void* stream, char* err, size_t err_len) {
+  int rc = interpolate_impl(d_natural, d_coeffs, log_sizes, half_initial_indices, n_cols, d_itwiddles, tree_log_size,
+                            as_stream(stream), err, err_len, true);
   return rc ? rc : ok(err, err_len);
 }
 
@@ -1011,52 +1134,18 @@ extern "C" int stwo_b200_fft_get_plan(uint32_t log_size, uint32_t* pass_layers, 
   return ok(err, err_len);
 }
 
-// Bit reversal of up to kFftMaxCols columns of one size in one launch
-// (blockIdx.y = column): out of place (dst[brev(i)] = src[i], coalesced
-// reads), or in place by pairwise swaps when dst == src.
-__global__ void bit_reverse_cols_kernel(FftCols t, uint32_t log_n) {
-  const uint64_t n = 1ull << log_n;
-  const uint32_t* __restrict__ src = t.src[blockIdx.y];
-  uint32_t* dst = t.dst[blockIdx.y];
-  const bool in_place = src == dst;
-  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
-    const uint64_t j = __brevll(i) >> (64 - log_n);
-    if (!in_place) {
-      dst[j] = src[i];
-    } else if (i < j) {
-      const uint32_t a = dst[i], b = dst[j];
-      dst[i] = b;
-      dst[j] = a;
-    }
-  }
-}
-
 extern "C" int stwo_b200_bit_reverse_columns(const uint32_t* const* d_src, uint32_t* const* d_dst,
                                              const uint32_t* log_sizes, uint32_t n_cols, void* stream, char* err,
                                              size_t err_len) {
   STWO_ARG_CHECK(n_cols == 0 || (d_src && d_dst && log_sizes), "null argument");
-  cudaStream_t s = as_stream(stream);
   // one launch per run of equal sizes (at most kFftMaxCols columns each)
   for (uint32_t a = 0; a < n_cols;) {
     const uint32_t lg = log_sizes[a];
     STWO_ARG_CHECK(lg <= 31, "log size %u too large", lg);
     uint32_t b = a;
-    FftCols t;
-    while (b < n_cols && log_sizes[b] == lg && b - a < (uint32_t)kFftMaxCols) {
-      STWO_ARG_CHECK(d_src[b] && d_dst[b], "null column %u", b);
-      t.src[b - a] = d_src[b];
-      t.dst[b - a] = d_dst[b];
-      b++;
-    }
-    if (lg > 0) {
-      const uint64_t n = 1ull << lg;
-      const unsigned bx = (unsigned)std::min<uint64_t>((n + 255) / 256, std::max<uint64_t>(1, 148 * 32 / (b - a)));
-      bit_reverse_cols_kernel<<<dim3(bx, b - a), 256, 0, s>>>(t, lg);
-      STWO_CHECK_LAUNCH();
-    } else {
-      for (uint32_t k = a; k < b; k++)
-        if (d_src[k] != d_dst[k]) STWO_CUDA_TRY(cudaMemcpyAsync(d_dst[k], d_src[k], 4, cudaMemcpyDeviceToDevice, s));
-    }
+    while (b < n_cols && log_sizes[b] == lg) b++;
+    int rc = bit_reverse_group(d_src + a, d_dst + a, b - a, lg, as_stream(stream), err, err_len);
+    if (rc) return rc;
     a = b;
   }
   return ok(err, err_len);

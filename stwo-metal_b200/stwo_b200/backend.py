@@ -183,6 +183,17 @@ class B200Backend:
                  C.c_void_p(tree.itwiddles.ptr), C.c_uint32(tree.log_size), self.stream)
         return coeffs
 
+    def interpolate_natural_into(self, naturals, coeffs, tree: TwiddleTree):
+        """CircleEvaluation<NaturalOrder>::bit_reverse + interpolate in one call:
+        natural-order evaluations in, coefficients out (the bit reversal rides
+        on the first FFT pass where it can)."""
+        if len(naturals) != len(coeffs) or any(a.log_size != b.log_size for a, b in zip(naturals, coeffs)):
+            raise ValueError("source and destination columns differ in number or size")
+        ffi.call("stwo_b200_interpolate_columns_natural", _ptr_array(naturals), _ptr_array(coeffs),
+                 _u32_array([c.log_size for c in naturals]), None, C.c_uint32(len(naturals)),
+                 C.c_void_p(tree.itwiddles.ptr), C.c_uint32(tree.log_size), self.stream)
+        return coeffs
+
     def evaluate_polynomials_into(self, coeffs, log_blowup: int, tree: TwiddleTree, outs):
         ffi.call("stwo_b200_evaluate_polynomials", _ptr_array(coeffs), _u32_array([c.log_size for c in coeffs]),
                  C.c_uint32(len(coeffs)), C.c_uint32(log_blowup), _ptr_array(outs), C.c_void_p(tree.twiddles.ptr),

@@ -79,6 +79,47 @@ def test_interpolate(be, oracle, big_tree, log_n):
         assert (c.to_host() == oracle.interpolate(v, itw)).all()
 
 
+@pytest.mark.parametrize("log_n", [1, 2, 3, 9, 10, 11, 12, 16, 17, 20, 22])
+@pytest.mark.parametrize("in_place", [False, True])
+def test_interpolate_natural(be, oracle, big_tree, log_n, in_place):
+    # natural-order evaluations: bit reversal + interpolation in one call (the
+    # bit reversal fused into the first pass from log 3 up, out of place);
+    # 11 columns leave a partial group of 8; P-valued words included
+    tree, tw, itw = big_tree
+    r = rng(3000 + log_n)
+    vals = [rand_col(r, log_n) for _ in range(11 if log_n <= 17 else 2)]
+    vals[0][:: max(1, len(vals[0]) // 7)] = P
+    srcs = [DeviceColumn.from_host(v) for v in vals]
+    dsts = srcs if in_place else [DeviceColumn(1 << log_n) for _ in vals]
+    be.interpolate_natural_into(srcs, dsts, tree)
+    for v, d in zip(vals, dsts):
+        assert (d.to_host() == oracle.interpolate(oracle.bit_reverse(v), itw)).all()
+    if not in_place:
+        for v, c in zip(vals, srcs):
+            assert (c.to_host() == v).all()
+
+
+def test_interpolate_natural_mixed_sizes_and_plans(be, oracle, big_tree):
+    # uneven sizes in one call, under the default plans and with log 12 as
+    # 6 + 6 layers (a tile first pass instead of the single 12-layer one)
+    from stwo_b200 import fft_get_plan, fft_set_plan
+    tree, tw, itw = big_tree
+    r = rng(31)
+    logs = [12, 3, 14, 12, 10, 1, 14, 18, 12]
+    vals = [rand_col(r, l) for l in logs]
+    old = fft_get_plan(12)
+    try:
+        for plan in ([], [6, 6]):
+            fft_set_plan(12, plan)
+            srcs = [DeviceColumn.from_host(v) for v in vals]
+            dsts = [DeviceColumn(1 << l) for l in logs]
+            be.interpolate_natural_into(srcs, dsts, tree)
+            for v, d in zip(vals, dsts):
+                assert (d.to_host() == oracle.interpolate(oracle.bit_reverse(v), itw)).all(), (plan, v.size)
+    finally:
+        fft_set_plan(12, old)
+
+
 @pytest.mark.parametrize("log_n", LOGS)
 @pytest.mark.parametrize("log_blowup", [0, 1, 2])
 def test_evaluate(be, oracle, big_tree, log_n, log_blowup):
