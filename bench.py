@@ -1074,7 +1074,9 @@ def run_serving_b200(args, world, rank, local):
     arrivals = np.cumsum(gaps) - gaps[0]
     sampler = ClockSampler(local)
     sampler.start()
+    launches0 = ffi.launch_count()
     p_srv, t_srv, mk_srv, st_srv = run_stream(batched, reqs, inputs, arrivals)
+    launches = ffi.launch_count() - launches0
     clocks = sampler.stop()
     p_ser2, t_ser2, mk_ser2, _ = run_stream(serial, reqs, inputs, arrivals)
     batched.close()
@@ -1118,7 +1120,7 @@ def run_serving_b200(args, world, rank, local):
         "capacity_proofs_per_s": {"batched": cap_batched, "serial": n_req / mk_ser},
         "server_stats": st_srv,
         "clocks": clocks,
-        "gpu_launches": None,
+        "gpu_launches": launches,
         "e2e": {"value": cells / mk_srv * world, "unit": "proved trace cells/s",
                 "h2d_bytes_per_step": int(sum(8 << ln for ln, _, _ in reqs)),
                 "d2h_bytes_per_step": int(sum(len(p) for p in p_srv)), "ms_per_step": 1000 * mk_srv},
