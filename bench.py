@@ -713,11 +713,9 @@ def run_prove_b200(args, world, rank, local):
     sp = ctypes.c_void_p(stream.cuda_stream)
 
     def e2e_step():
-        ffi.call("stwo_b200_memcpy_h2d", ctypes.c_void_p(a.ptr), ctypes.c_void_p(pa.data_ptr()),
-                 ctypes.c_size_t(a.nbytes), sp)
-        ffi.call("stwo_b200_memcpy_h2d", ctypes.c_void_p(b.ptr), ctypes.c_void_p(pb.data_ptr()),
-                 ctypes.c_size_t(b.nbytes), sp)
-        return prover.prove_into(a.ptr, b.ptr, buf, cap)
+        # the prover copies the pinned columns itself, chunk by chunk, and
+        # generates each chunk's trace rows as it lands
+        return prover.prove_host_into(pa.data_ptr(), pb.data_ptr(), buf, cap)
 
     with torch.cuda.stream(stream):
         e2e_step()

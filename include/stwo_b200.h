@@ -302,6 +302,15 @@ int stwo_b200_prover_destroy(stwo_b200_prover* prover, char* err, size_t err_len
 int stwo_b200_prove_wide_fib(stwo_b200_prover* prover, const uint32_t* d_a, const uint32_t* d_b,
                              uint8_t* proof_out, size_t proof_cap, size_t* proof_len, char* err, size_t err_len);
 
+/* stwo_b200_prove_wide_fib with the two input columns in HOST memory (the
+ * same bytes out).  The prover copies them in 4 row chunks on its own copy
+ * stream and generates each chunk's trace rows as soon as the chunk lands, so
+ * with pinned (page-locked) inputs the host-to-device copy overlaps the trace
+ * generation; pageable inputs are copied synchronously.  The first call
+ * allocates a 2 x 2^log_n_rows-word input buffer and the copy stream. */
+int stwo_b200_prove_wide_fib_host(stwo_b200_prover* prover, const uint32_t* h_a, const uint32_t* h_b,
+                                  uint8_t* proof_out, size_t proof_cap, size_t* proof_len, char* err, size_t err_len);
+
 /* The same proof with n_cols (3..the prover's n_cols) trace columns: the
  * buffers are sized for the prover's n_cols and any narrower trace of the
  * same log_n_rows reuses them.  No reference counterpart (a resident prover

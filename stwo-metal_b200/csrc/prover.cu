@@ -61,15 +61,16 @@ __device__ __forceinline__ qm31 acc4_reduce(const acc4& s) {
 }
 
 // One thread per row: col[i+2] = col[i]^2 + col[i+1]^2 (wide_fibonacci/mod.rs:27-50).
+// `rows` rows from a/b; column c of the trace at cols + c * stride.
 __global__ void wide_fib_trace_kernel(const uint32_t* __restrict__ a, const uint32_t* __restrict__ b,
-                                      uint32_t* __restrict__ cols, uint32_t n_cols, uint64_t rows) {
+                                      uint32_t* __restrict__ cols, uint32_t n_cols, uint64_t rows, uint64_t stride) {
   for (uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; r < rows; r += (uint64_t)gridDim.x * blockDim.x) {
     uint32_t x = __ldg(a + r), y = __ldg(b + r);
     cols[r] = x;
-    cols[rows + r] = y;
+    cols[stride + r] = y;
     for (uint32_t c = 2; c < n_cols; c++) {
       uint32_t z = m31_add(m31_sqr(x), m31_sqr(y));
-      cols[(uint64_t)c * rows + r] = z;
+      cols[(uint64_t)c * stride + r] = z;
       x = y;
       y = z;
     }
@@ -1440,6 +1441,16 @@ class WideFibProver {
   // stream `user_s` with events.
   cudaStream_t user_s = nullptr;
   cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+  // Host-input proofs: the two input columns are copied in kHostChunks row
+  // chunks on the copy stream `cs` into d_in (allocated on first use), and
+  // each chunk's trace rows are generated as soon as it lands.  Four chunks:
+  // with sixteen the per-copy overhead outweighed the overlap.
+  static constexpr uint32_t kHostChunks = 4;
+  uint32_t* d_in = nullptr;
+  cudaStream_t cs = nullptr;
+  cudaEvent_t ev_chunk[kHostChunks] = {};
+  const uint32_t* h_src_a = nullptr;  // set for the duration of a host-input proof
+  const uint32_t* h_src_b = nullptr;
   // FRI commit graphs, [timing off, timing on], captured on first use.
   cudaGraphExec_t fri_exec[2] = {nullptr, nullptr};
   uint64_t fri_graph_launches[2] = {0, 0};
@@ -1456,6 +1467,12 @@ class WideFibProver {
     if (ev_in) cudaEventDestroy(ev_in);
     if (ev_out) cudaEventDestroy(ev_out);
     if (ev_tx) cudaEventDestroy(ev_tx);
+    for (cudaEvent_t e : ev_chunk)
+      if (e) cudaEventDestroy(e);
+    if (cs) {
+      cudaStreamSynchronize(cs);
+      cudaStreamDestroy(cs);
+    }
     for (cudaEvent_t e : ev_pool) cudaEventDestroy(e);
     for (void* p : allocs) cudaFree(p);  // empty in measure mode
     if (h_pinned) cudaFreeHost(h_pinned);
@@ -1752,6 +1769,22 @@ class WideFibProver {
     cudaStreamWaitEvent(user_s, ev_out, 0);
     return rc;
   }
+  // The same proof from host input columns (pinned memory overlaps the copy
+  // with the trace generation; pageable memory works, copied synchronously).
+  int prove_host(const uint32_t* h_a, const uint32_t* h_b, ProofOut& out, char* err, size_t err_len) {
+    const uint64_t rows = 1ull << log_n;
+    if (!d_in) {
+      int rc;
+      if ((rc = alloc((void**)&d_in, 8ull << log_n, err, err_len))) return rc;
+      STWO_CUDA_TRY(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+      for (cudaEvent_t& e : ev_chunk) STWO_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    }
+    h_src_a = h_a;
+    h_src_b = h_b;
+    const int rc = prove(d_in, d_in + rows, out, err, err_len);
+    h_src_a = h_src_b = nullptr;
+    return rc;
+  }
   int prove_body(const uint32_t* d_a, const uint32_t* d_b, ProofOut& out, char* err, size_t err_len);
 };
 
@@ -1781,8 +1814,26 @@ int WideFibProver::prove_body(const uint32_t* d_a, const uint32_t* d_b, ProofOut
 
   // ---- tree 1: trace ----
   phase(kTraceGen);
-  wide_fib_trace_kernel<<<grid1d(rows, 256), 256, 0, s>>>(d_a, d_b, d_coeffs, N, rows);
-  STWO_CHECK_LAUNCH();
+  if (h_src_a) {
+    // Host inputs: chunk k's copies (copy stream, ordered after the caller's
+    // stream) gate chunk k's trace rows on the prover's stream.
+    const uint64_t chunk = rows / kHostChunks;  // rows >= 16
+    STWO_CUDA_TRY(cudaStreamWaitEvent(cs, ev_in, 0));
+    for (uint32_t k = 0; k < kHostChunks; k++) {
+      const uint64_t off = k * chunk;
+      STWO_CUDA_TRY(cudaMemcpyAsync(const_cast<uint32_t*>(d_a) + off, h_src_a + off, 4 * chunk, cudaMemcpyHostToDevice,
+                                    cs));
+      STWO_CUDA_TRY(cudaMemcpyAsync(const_cast<uint32_t*>(d_b) + off, h_src_b + off, 4 * chunk, cudaMemcpyHostToDevice,
+                                    cs));
+      STWO_CUDA_TRY(cudaEventRecord(ev_chunk[k], cs));
+      STWO_CUDA_TRY(cudaStreamWaitEvent(s, ev_chunk[k], 0));
+      wide_fib_trace_kernel<<<grid1d(chunk, 256), 256, 0, s>>>(d_a + off, d_b + off, d_coeffs + off, N, chunk, rows);
+      STWO_CHECK_LAUNCH();
+    }
+  } else {
+    wide_fib_trace_kernel<<<grid1d(rows, 256), 256, 0, s>>>(d_a, d_b, d_coeffs, N, rows, rows);
+    STWO_CHECK_LAUNCH();
+  }
   std::vector<uint32_t*> coeff_ptrs(N), eval_ptrs(N);
   std::vector<uint32_t> logs_n(N, log_n), logs_1(N, L1);
   for (uint32_t c = 0; c < N; c++) {
@@ -2683,6 +2734,21 @@ extern "C" int stwo_b200_prove_wide_fib(stwo_b200_prover* p, const uint32_t* d_a
   STWO_ARG_CHECK(p && d_a && d_b && proof_len, "null argument");
   ProofOut out;
   int rc = p->impl->prove(d_a, d_b, out, err, err_len);
+  if (rc) return rc;
+  *proof_len = out.bytes.size();
+  if (proof_out) {
+    STWO_ARG_CHECK(proof_cap >= out.bytes.size(), "proof buffer too small (%zu < %zu)", proof_cap, out.bytes.size());
+    std::memcpy(proof_out, out.bytes.data(), out.bytes.size());
+  }
+  return ok(err, err_len);
+}
+
+extern "C" int stwo_b200_prove_wide_fib_host(stwo_b200_prover* p, const uint32_t* h_a, const uint32_t* h_b,
+                                             uint8_t* proof_out, size_t proof_cap, size_t* proof_len, char* err,
+                                             size_t err_len) {
+  STWO_ARG_CHECK(p && h_a && h_b && proof_len, "null argument");
+  ProofOut out;
+  int rc = p->impl->prove_host(h_a, h_b, out, err, err_len);
   if (rc) return rc;
   *proof_len = out.bytes.size();
   if (proof_out) {

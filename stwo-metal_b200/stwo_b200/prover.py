@@ -50,6 +50,24 @@ class WideFibProver:
                  C.c_void_p(b.ptr), buf, C.c_size_t(cap), C.byref(n))
         return C.string_at(buf, n.value)
 
+    def prove_host(self, a: np.ndarray, b: np.ndarray, cap: int = 1 << 22) -> bytes:
+        """The proof from host columns (numpy, uint32); copied by the prover,
+        overlapped with the trace generation when the memory is pinned."""
+        a = np.ascontiguousarray(a, dtype=np.uint32)
+        b = np.ascontiguousarray(b, dtype=np.uint32)
+        buf = (C.c_uint8 * cap)()
+        n = C.c_size_t()
+        ffi.call("stwo_b200_prove_wide_fib_host", self.handle, C.c_void_p(a.ctypes.data), C.c_void_p(b.ctypes.data),
+                 buf, C.c_size_t(cap), C.byref(n))
+        return C.string_at(buf, n.value)
+
+    def prove_host_into(self, a_ptr: int, b_ptr: int, out_buf, cap: int) -> int:
+        """prove_host from raw host pointers (e.g. pinned buffers) into out_buf."""
+        n = C.c_size_t()
+        ffi.call("stwo_b200_prove_wide_fib_host", self.handle, C.c_void_p(a_ptr), C.c_void_p(b_ptr), out_buf,
+                 C.c_size_t(cap), C.byref(n))
+        return n.value
+
     def prove_into(self, a_ptr: int, b_ptr: int, out_buf, cap: int) -> int:
         n = C.c_size_t()
         ffi.call("stwo_b200_prove_wide_fib", self.handle, C.c_void_p(a_ptr), C.c_void_p(b_ptr), out_buf,

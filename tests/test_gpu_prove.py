@@ -76,3 +76,32 @@ def test_phase_timing_does_not_change_proofs(oracle):
     ffi.call("stwo_b200_prover_phase_times", prover.handle, ms, C.c_uint32(14), C.byref(n))
     assert n.value == 4
     assert all(x > 0 for x in ms)
+
+
+@pytest.mark.parametrize("pinned", [False, True])
+def test_prove_from_host_columns(oracle, pinned):
+    # host inputs (pageable numpy, or page-locked memory from the library):
+    # copied chunk by chunk by the prover, the same proof bytes
+    import ctypes as C
+    from stwo_b200 import ffi
+    log_n, cols = 12, 24
+    a, b = oracle.wide_fib_inputs(log_n, 55)
+    ref = oracle.prove_wide_fib(oracle.wide_fib_config(log_n, cols), a, b)
+    prover = WideFibProver(wide_fib_config(log_n, cols))
+    if not pinned:
+        assert prover.prove_host(a, b) == ref
+        assert prover.prove(DeviceColumn.from_host(a), DeviceColumn.from_host(b)) == ref  # device path after
+        assert prover.prove_host(a, b) == ref
+        return
+    hp = C.c_void_p()
+    ffi.call("stwo_b200_host_alloc", C.c_size_t(8 << log_n), C.byref(hp))
+    try:
+        host = np.ctypeslib.as_array((C.c_uint32 * (2 << log_n)).from_address(hp.value))
+        host[: 1 << log_n] = a
+        host[1 << log_n:] = b
+        buf = (C.c_uint8 * (1 << 22))()
+        for _ in range(2):
+            n = prover.prove_host_into(hp.value, hp.value + (4 << log_n), buf, len(buf))
+            assert C.string_at(buf, n) == ref
+    finally:
+        ffi.call("stwo_b200_host_free", hp)
