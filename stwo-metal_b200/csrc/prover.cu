@@ -258,30 +258,6 @@ __global__ void __launch_bounds__(256) oods_eval_kernel(PolyTable t, uint32_t n_
   }
 }
 
-// OODS fold weights: w_lo[t] = prod of f[b] over the set bits b of t
-// (t < 2^h) and w_hi[t] = prod of f[h + b] (t < 2^hi_bits), the tables of
-// oods_eval_kernel.  Field products are exact, so the order of the factors
-// does not matter.
-struct OodsFolds {
-  qm31 f[32];
-};
-__global__ void oods_weights_kernel(OodsFolds f, uint32_t h, uint32_t hi_bits, qm31* __restrict__ w_lo,
-                                    qm31* __restrict__ w_hi) {
-  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t < (1u << h)) {
-    qm31 w = qm31_one();
-    for (uint32_t b = 0; b < h; b++)
-      if ((t >> b) & 1) w = qm31_mul(w, f.f[b]);
-    w_lo[t] = w;
-  }
-  if (t < (1u << hi_bits)) {
-    qm31 w = qm31_one();
-    for (uint32_t b = 0; b < hi_bits; b++)
-      if ((t >> b) & 1) w = qm31_mul(w, f.f[h + b]);
-    w_hi[t] = w;
-  }
-}
-
 // out[p] = sum of partial[p][0 .. n_chunks); one block per polynomial.
 __global__ void __launch_bounds__(256) oods_reduce_kernel(const qm31* __restrict__ partial, uint32_t n_chunks,
                                                          qm31* __restrict__ out) {
@@ -824,12 +800,6 @@ __device__ __forceinline__ qm31 chan_draw_felt(ChanRegs& c) {
   return qm31_zero();
 }
 
-// mix_root, then draw_secure_felt into *alpha; one thread.
-__device__ void dev_mix_root_draw(DevChannel* ch, const uint32_t* root, qm31* alpha) {
-  dev_chan_mix_root(ch, root);
-  *alpha = dev_chan_draw_felt(ch);
-}
-
 __device__ qm31 qm31_pow_u32(qm31 x, uint32_t e) {
   qm31 r = qm31_one();
   while (e) {
@@ -957,12 +927,6 @@ __global__ void __launch_bounds__(kFsThreads) fs_quotient_kernel(DevChannel* ch,
   }
 }
 
-__global__ void channel_mix_root_draw_kernel(DevChannel* ch, const uint8_t* root, qm31* alpha) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  dev_mix_root_draw(ch, reinterpret_cast<const uint32_t*>(root), alpha);
-}
-
-// fold_line with alpha read from device memory (prover/backend/cpu/fri.rs:67-92).
 // Lifted leaf of one FRI layer element: Blake2s of its 4 coordinates (16
 // bytes), the leaf of a tree over 4 equal-length columns
 // (prover/backend/cpu/merkle_lifted.rs:44-78).
@@ -983,6 +947,7 @@ __device__ __forceinline__ void fri_leaf_store(uint8_t* leaves, uint64_t i, cons
   g[1] = make_uint4(h[4], h[5], h[6], h[7]);
 }
 
+// fold_line with alpha read from device memory (prover/backend/cpu/fri.rs:67-92).
 // When `leaves` is not null the fold also writes the leaf hashes of the next
 // layer's tree (its Merkle leaf layer), saving a launch and a re-read.
 __global__ void fold_line_dev_kernel(const uint32_t* __restrict__ in, uint32_t log_m, uint32_t fold_step,
