@@ -746,6 +746,19 @@ def run_prove_b200(args, world, rank, local):
         p1.record(stream)
     torch.cuda.synchronize()
     probe_rate = 148 * 8 * 256 * 256 / (p0.elapsed_time(p1) * 1e-3)
+    # Integer-issue ceiling of the M31 butterfly (register-only bfly2 chains,
+    # 80 butterflies per thread and round, all SMs).
+    bf_blocks, bf_iters = 148 * 8, 512
+    for _ in range(2):
+        ffi.call("stwo_b200_butterfly_probe", ctypes.c_uint32(bf_blocks), ctypes.c_uint32(bf_iters),
+                 ctypes.c_void_p(probe_out.ptr), sp)
+    with torch.cuda.stream(stream):
+        p0.record(stream)
+        ffi.call("stwo_b200_butterfly_probe", ctypes.c_uint32(bf_blocks), ctypes.c_uint32(bf_iters),
+                 ctypes.c_void_p(probe_out.ptr), sp)
+        p1.record(stream)
+    torch.cuda.synchronize()
+    bfly_rate = bf_blocks * 256 * bf_iters * 80 / (p0.elapsed_time(p1) * 1e-3)
 
     if rank != 0:
         return
@@ -785,6 +798,19 @@ def run_prove_b200(args, world, rank, local):
             roof["traffic_source"] = "ncu capture of fft_bench.py 20 100 (profiles/fft_warp_kernels_100x2e20_full_capture.md)"
             roof["note"] = ("bound by integer issue, not HBM: in that capture the ALU pipe is 57-70% busy and "
                             "56-69% of issue slots are active, at about 9-12 instructions per M31 butterfly")
+    # The trace FFTs against the butterfly ceiling: the interpolation runs n
+    # layers of 2^(n-1) butterflies per column; the evaluation n layers of
+    # 2^(n+lb-1) (its top lb layers only copy the zero-padded coefficients).
+    fft_bflies = nc * n * ((1 << (n - 1)) + (1 << (n + lb - 1)))
+    fft_ms = phase_ms.get("trace_interpolate", 0) + phase_ms.get("trace_evaluate", 0)
+    fft_issue = None
+    if fft_ms > 0:
+        fft_rate = fft_bflies / (fft_ms * 1e-3)
+        fft_issue = {"bound": "int32 issue", "kernel": "trace interpolate + evaluate (fft_warp_contig_kernel, "
+                     "fft_warp_strided_kernel)", "achieved": fft_rate / 1e9, "peak": bfly_rate / 1e9,
+                     "unit": "G M31 butterflies/s", "frac": fft_rate / bfly_rate,
+                     "peak_kind": "measured in this run (register-only butterfly chains, all SMs)",
+                     "alg_butterflies_per_step": fft_bflies}
     phase_frac = {}
     for k, (kd, amt) in alg.items():
         if phase_ms.get(k, 0) > 0:
@@ -815,9 +841,11 @@ def run_prove_b200(args, world, rank, local):
                 "h2d_bytes_per_step": int(a.nbytes + b.nbytes), "d2h_bytes_per_step": int(n_e2e),
                 "ms_per_step": e2e_ms},
         "roofline": roof,
+        "fft_issue_roofline": fft_issue,
         "phase_ms": phase_ms,
         "phase_roofline_frac": phase_frac,
         "blake2s_probe_compressions_per_s": probe_rate,
+        "butterfly_probe_per_s": bfly_rate,
         "proof_bytes": len(proof),
         "verifier": "accepted" if verdict is None else f"REJECTED: {verdict}",
         "bit_exact_vs_oracle": proof == cpu_proof if world == 1 else "checked at N=1",

@@ -165,6 +165,13 @@ int stwo_b200_merkle_build_nodes(uint8_t* const* d_layers, uint32_t lifting_log_
 int stwo_b200_blake2s_probe(uint32_t blocks, uint32_t iters, uint32_t* d_out, void* stream, char* err,
                             size_t err_len);
 
+/* Throughput probe (no reference counterpart): `blocks` x 256 threads each
+ * apply `iters` rounds of 80 M31 butterflies (the FFT passes' arithmetic) to
+ * 32 register-held values.  80 * iters * threads / elapsed time is the
+ * integer-issue ceiling the FFT passes are measured against. */
+int stwo_b200_butterfly_probe(uint32_t blocks, uint32_t iters, uint32_t* d_out, void* stream, char* err,
+                              size_t err_len);
+
 /* ------------------------------------------------------------ MerkleOps -- */
 /* MerkleOps<Blake2sMerkleHasherGeneric<m31_output>>::commit_on_layer
  * (prover/vcs/ops.rs:24-28; cpu/blake2s.rs:13-26): node i = Blake2s(

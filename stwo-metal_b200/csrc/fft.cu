@@ -326,6 +326,33 @@ __global__ void bit_reverse_kernel(uint32_t* v, uint32_t log_n) {
   }
 }
 
+// Integer-issue ceiling of the butterfly (no reference counterpart): every
+// thread applies `iters` rounds of 5 layers x 16 forward butterflies (bfly2,
+// the pass kernels' arithmetic) to 32 values held in registers, with one
+// doubled twiddle per layer.  butterflies / elapsed time is the rate the FFT
+// passes are measured against; no memory traffic, no twiddle loads.
+__global__ void __launch_bounds__(256) butterfly_probe_kernel(uint32_t iters, uint32_t* out) {
+  const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
+  uint32_t v[32];
+#pragma unroll
+  for (int j = 0; j < 32; j++) v[j] = (tid * 32u + (uint32_t)j) & M31_P;  // < 2^31, so <= P
+  uint32_t t2[5];
+#pragma unroll
+  for (int k = 0; k < 5; k++) t2[k] = ((tid * 5u + (uint32_t)k + 1u) % M31_P) << 1;  // 2t with t < P
+  for (uint32_t it = 0; it < iters; it++) {
+#pragma unroll
+    for (int k = 0; k < 5; k++) {
+#pragma unroll
+      for (int j = 0; j < 32; j++)
+        if (!(j & (1 << k))) bfly2(v[j], v[j | (1 << k)], t2[k]);
+    }
+  }
+  uint32_t x = 0;
+#pragma unroll
+  for (int j = 0; j < 32; j++) x ^= v[j];
+  if (x == 0x12345678u) out[0] = x;  // keeps the chain live
+}
+
 // Bit reversal of up to kFftMaxCols columns of one size in one launch
 // (blockIdx.y = column): out of place (dst[brev(i)] = src[i], coalesced
 // reads), or in place by pairwise swaps when dst == src.
@@ -1148,6 +1175,14 @@ extern "C" int stwo_b200_bit_reverse_columns(const uint32_t* const* d_src, uint3
     if (rc) return rc;
     a = b;
   }
+  return ok(err, err_len);
+}
+
+extern "C" int stwo_b200_butterfly_probe(uint32_t blocks, uint32_t iters, uint32_t* d_out, void* stream, char* err,
+                                         size_t err_len) {
+  STWO_ARG_CHECK(d_out && blocks >= 1 && blocks <= (1u << 20), "bad probe arguments");
+  butterfly_probe_kernel<<<blocks, 256, 0, as_stream(stream)>>>(iters, d_out);
+  STWO_CHECK_LAUNCH();
   return ok(err, err_len);
 }
 

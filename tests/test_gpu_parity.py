@@ -280,3 +280,16 @@ def test_decompose(be, oracle, log_n):
     assert (lam == lr).all()
     for a, b in zip(g.to_host(), gr):
         assert (a == b).all()
+
+
+def test_throughput_probes_run(be):
+    # the register-only ceilings the bench divides by: both launch and finish
+    import ctypes as C
+    from stwo_b200 import DeviceBuffer, ffi, sync
+    out = DeviceBuffer(64)
+    ffi.call("stwo_b200_butterfly_probe", C.c_uint32(148), C.c_uint32(4), C.c_void_p(out.ptr), be.stream)
+    ffi.call("stwo_b200_blake2s_probe", C.c_uint32(148), C.c_uint32(4), C.c_void_p(out.ptr), be.stream)
+    sync(be.stream)
+    from stwo_b200.ffi import B200Error
+    with pytest.raises(B200Error):
+        ffi.call("stwo_b200_butterfly_probe", C.c_uint32(0), C.c_uint32(4), C.c_void_p(out.ptr), be.stream)
