@@ -1037,10 +1037,12 @@ __global__ void fold_circle_first_dev_kernel(Src4 src, uint32_t log_n, const qm3
 // tree buffer, for decommitment), mixes the root and draws alpha on the device
 // channel, and folds into the next layer (prover/backend/cpu/fri.rs:67-92).
 // Data written inside the kernel is read back with plain loads, never through
-// the read-only path.
-constexpr uint32_t kFriTailLog = 8;
+// the read-only path.  Layers up to log 9 (512 threads): one SM's hash
+// throughput still keeps up there, while a log-10 layer already cost more in
+// the one CTA than its separate grid launches.
+constexpr uint32_t kFriTailLog = 9;
 constexpr int kFriTailMaxLayers = 32;
-constexpr int kFriTailThreads = 256;  // one thread per leaf of the largest tail layer
+constexpr int kFriTailThreads = 1 << kFriTailLog;  // one thread per leaf of the largest tail layer
 constexpr size_t kFriTailSmem = (size_t)3 << (kFriTailLog + 4);  // 2^L + 2^(L-1) hashes of 32 bytes
 struct FriTail {
   uint32_t* coords[kFriTailMaxLayers];  // 4 x 2^log_size
