@@ -717,26 +717,25 @@ __device__ qm31 dev_chan_draw_felt(DevChannel* ch) {
   return qm31_zero();
 }
 
-// digest <- H(digest || LE32 coordinates of f[0..n)) (core/channel/blake2s.rs:54-64);
-// one thread streams the 32 + 16 n bytes through 64-byte blocks.
-__device__ void dev_chan_mix_felts(DevChannel* ch, const qm31* __restrict__ f, uint32_t n) {
+// digest <- H(digest || LE32 coordinates of n QM31 values) (core/channel/
+// blake2s.rs:54-64).  The digest and the values are staged by the block as
+// 16-word message blocks in s_words (zero padded, 8 + 4 n words); thread 0
+// then chains the compressions, reading each block from shared memory.
+constexpr uint32_t kMixWordsCap = (8 + 4 * kMaxPolys + 15) & ~15u;
+__device__ void stage_mix_words(const DevChannel* ch, const qm31* __restrict__ f, uint32_t n, uint32_t* s_words) {
+  const uint32_t total = 8 + 4 * n, padded = (total + 15) & ~15u;
+  const uint32_t* fw = reinterpret_cast<const uint32_t*>(f);  // a, b, c, d of each value in order
+  for (uint32_t w = threadIdx.x; w < padded; w += blockDim.x)
+    s_words[w] = w < 8 ? ch->digest[w] : (w < total ? fw[w - 8] : 0u);
+}
+__device__ void dev_chan_mix_staged(DevChannel* ch, const uint32_t* s_words, uint32_t n) {
   const uint32_t total_words = 8 + 4 * n;
   const uint32_t blocks = (total_words + 15) / 16;
   uint32_t h[8], m[16];
   blake2s_init(h);
   for (uint32_t bk = 0; bk < blocks; bk++) {
-    for (int k = 0; k < 16; k++) {
-      const uint32_t w = bk * 16 + k;
-      uint32_t v = 0;
-      if (w < 8) {
-        v = ch->digest[w];
-      } else if (w < total_words) {
-        const qm31 x = f[(w - 8) >> 2];
-        const uint32_t c = (w - 8) & 3;
-        v = c == 0 ? x.a : c == 1 ? x.b : c == 2 ? x.c : x.d;
-      }
-      m[k] = v;
-    }
+#pragma unroll
+    for (int k = 0; k < 16; k++) m[k] = s_words[bk * 16 + k];
     const bool last = bk + 1 == blocks;
     blake2s_compress_lat(h, m, last ? 4 * total_words : 64 * (bk + 1), last);
   }
@@ -886,8 +885,11 @@ __global__ void __launch_bounds__(kFsThreads) fs_quotient_kernel(DevChannel* ch,
                                                                  FsOut* out) {
   __shared__ qm31 s_q;
   __shared__ qm31 sa[kFsThreads], sb[kFsThreads];
+  __shared__ __align__(16) uint32_t s_words[kMixWordsCap];
+  stage_mix_words(ch, vals, nq, s_words);
+  __syncthreads();
   if (threadIdx.x == 0) {
-    dev_chan_mix_felts(ch, vals, nq);
+    dev_chan_mix_staged(ch, s_words, nq);
     s_q = dev_chan_draw_felt(ch);
     out->quotient_coeff = s_q;
   }
