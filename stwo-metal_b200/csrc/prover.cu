@@ -224,7 +224,11 @@ __global__ void __launch_bounds__(256) oods_eval_kernel(PolyTable t, uint32_t n_
   __syncthreads();
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint32_t n_warps = blockDim.x >> 5;
-  for (uint32_t p = warp; p < n_polys; p += n_warps) {
+  // blockIdx.y picks a group of polynomials: smaller blocks, so that the grid
+  // spans several waves instead of one full wave and a nearly empty second.
+  const uint32_t per_group = (n_polys + gridDim.y - 1) / gridDim.y;
+  const uint32_t p_end = min(n_polys, (blockIdx.y + 1) * per_group);
+  for (uint32_t p = blockIdx.y * per_group + warp; p < p_end; p += n_warps) {
     const uint32_t* __restrict__ col = t.p[p] + j0;
     acc4 s{0, 0, 0, 0};
     if (chunk == kOodsChunk) {
@@ -1890,7 +1894,10 @@ int WideFibProver::prove_body(const uint32_t* d_a, const uint32_t* d_b, ProofOut
     for (int k = 0; k < 8; k++) pt.p[N + k] = split[k];
     const uint32_t chunks = lg > 10 ? 1u << (lg - 10) : 1u;  // kOodsChunk indices each
     d_vals = d_small + n_w;
-    oods_eval_kernel<<<chunks, 256, 0, s>>>(pt, np, lg, h, d_small, d_small + (1u << h), d_oods_partial);
+    // about 4 waves of 148 SMs x 6 resident blocks, at least 8 polynomials (one per warp) per group
+    const uint32_t groups = std::max(1u, std::min({8u, (4u * 148u * 6u + chunks - 1) / chunks, np / 8u}));
+    oods_eval_kernel<<<dim3(chunks, groups), 256, 0, s>>>(pt, np, lg, h, d_small, d_small + (1u << h),
+                                                          d_oods_partial);
     STWO_CHECK_LAUNCH();
     oods_reduce_kernel<<<np, 256, 0, s>>>(d_oods_partial, chunks, d_vals);
     STWO_CHECK_LAUNCH();
