@@ -14,6 +14,15 @@ Workloads (seeded synthetic M31 data, values uniform in [0, P)):
   commit_plain   32 columns of log 16, blowup 1, natural-order input:
                  interpolate (the bit reversal rides on the first IFFT pass's
                  loads) -> evaluate -> Merkle (L = 17).
+  fri_heavy      one QM31 column of log 24: FRI commit + 70-query decommit.
+  serving        Poisson stream of Wide-Fibonacci requests (p50/p99 latency).
+  trace_fft      the prover's trace transforms alone (--n-cols x 2^--log-n-rows,
+                 interpolate, then evaluate at blowup 1): the kernels' profile
+                 target.
+
+The default line also carries, measured in the same run at N = 1, the uneven
+commit's per-column / batched / graph forms and the FRI-heavy commit with the
+stand-alone folds against HBM (skip with --no-extras).
 
 A step is one commit of the whole trace.  `value` is device-timed with inputs
 resident in HBM; `e2e` goes through the same public calls with the trace in
@@ -600,6 +609,10 @@ def prove_config_json(spec, world):
             "fri": "circle fold + line folds by 2 to last layer log degree 0",
             "channel": "Blake2sMerkleChannel", "inputs": "col0/col1 uniform [0, 2^31-1) per row, seed 2",
             "l2": prove_l2_note(spec),
+            "twiddles": "resident on the device from prover creation (outside the timed region; the "
+                        "reference harness precomputes them inside every sample)",
+            "e2e_inputs": "the two seed columns (2 x 2^log_n_rows words) are copied per proof; the other "
+                          "columns are generated on the device, as the Wide-Fibonacci trace is defined",
             "parallelism": f"replicas x{world}"}
 
 
@@ -759,10 +772,20 @@ def run_prove_b200(args, world, rank, local):
         p1.record(stream)
     torch.cuda.synchronize()
     bfly_rate = bf_blocks * 256 * bf_iters * 80 / (p0.elapsed_time(p1) * 1e-3)
+    hbm_peak, peak_kind = load_peaks()
+
+    # The rest of the metric, in the same run (N = 1 only; replica runs skip
+    # it): the uneven commit's forms and the FRI-heavy commit.
+    extras = {}
+    if world == 1 and args.extras:
+        prover.close()
+        a.close()
+        b.close()
+        extras["commit_uneven"] = extra_commit_uneven(args, stream, world, hbm_peak, probe_rate)
+        extras["fri_heavy"] = extra_fri_heavy(args, stream, world, hbm_peak, probe_rate)
 
     if rank != 0:
         return
-    hbm_peak, peak_kind = load_peaks()
     n, nc, lb = spec["log_n"], spec["n_cols"], spec["log_blowup"]
     rows, ev = 1 << n, 1 << (n + lb)
     # algorithmic bytes / compressions per phase (inputs + outputs once)
@@ -795,7 +818,7 @@ def run_prove_b200(args, world, rank, local):
             # passes (fft_warp_strided_kernel<0>, fft_warp_contig_kernel<0>),
             # one ncu capture at this shape
             roof["traffic"] = EVALUATE_TRAFFIC_100x2e20
-            roof["traffic_source"] = "ncu capture of fft_bench.py 20 100 (profiles/fft_warp_kernels_100x2e20_full_capture.md)"
+            roof["traffic_source"] = "ncu capture (dram__bytes_read.sum + dram__bytes_write.sum) of the two evaluate passes at this shape"
             roof["note"] = ("bound by integer issue, not HBM: in that capture the ALU pipe is 57-70% busy and "
                             "56-69% of issue slots are active, at about 9-12 instructions per M31 butterfly")
     # The trace FFTs against the butterfly ceiling: the interpolation runs n
@@ -855,6 +878,7 @@ def run_prove_b200(args, world, rank, local):
                                     "OpenMP), same inputs; its proof bytes are compared with the GPU's"}
                          if world == 1 else None),
     }
+    line.update(extras)
     print(json.dumps(line), flush=True)
 
 
@@ -1034,6 +1058,304 @@ def run_fri_b200(args, world, rank, local):
     print(json.dumps(line), flush=True)
 
 
+# ------------------------------------------------- default-line extras -----
+# The default run reports, beside the Wide-Fibonacci headline, the rest of the
+# metric: the uneven 512-column commit in its batched, CUDA-graph and
+# per-column forms (the "batched vs per-column" ratio), the FRI-heavy commit,
+# and the FRI folds against HBM.  Bit-exactness at these sizes is checked
+# against oracle digests committed in tests/golden/full_size_digests.json
+# (made by tests/golden/make_full_size_digests.py; tests/test_gpu_full_size.py
+# re-runs the oracle itself).
+DIGESTS_PATH = os.path.join(ROOT, "tests", "golden", "full_size_digests.json")
+
+
+def load_digests():
+    if os.path.exists(DIGESTS_PATH):
+        with open(DIGESTS_PATH) as f:
+            return json.load(f)
+    return {}
+
+
+def fri_heavy_inputs(log_n=FRI_LOG, seed=FRI_SEED, n_queries=FRI_QUERIES):
+    """The FRI-heavy inputs (numpy PCG64): 4 coordinate columns uniform in
+    [0, P), one QM31 alpha per fold, sorted distinct query positions."""
+    r = np.random.default_rng(seed)
+    n = 1 << log_n
+    coords = [r.integers(0, P, n, dtype=np.uint32) for _ in range(4)]
+    alphas = r.integers(0, P, (log_n, 4), dtype=np.uint32)
+    queries = np.unique(r.integers(0, n, n_queries, dtype=np.uint64))
+    return coords, alphas, queries
+
+
+def time_region(stream, fn, steps):
+    """Mean device ms of `fn` over `steps` calls (CUDA events on `stream`)."""
+    import torch
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+def extra_commit_uneven(args, stream, world, hbm_peak, probe_rate):
+    """512 uneven columns (log 12..22, blowup 2, L = 24): per-column, batched
+    and batched + graph committer forms, and the batched phases."""
+    import torch
+    from stwo_b200 import B200Backend, Committer, DeviceBuffer, DeviceColumn, fft_get_plan, ffi, layer_to_host
+    from stwo_b200.backend import canonic_half_coset
+    spec = workload_spec("commit_uneven")
+    logs, blowup = spec["logs"], spec["blowup"]
+    host_cols = make_columns(spec)
+    be = B200Backend(stream.cuda_stream)
+    L = max(logs) + blowup
+    init, lg = canonic_half_coset(L + 1)
+    tree = be.precompute_twiddles(init, lg)
+    inputs = [DeviceColumn.from_host(c, stream.cuda_stream) for c in host_cols]
+    coeffs = [DeviceColumn(c.size, stream.cuda_stream) for c in host_cols]
+    evals = [DeviceColumn(c.size << blowup, stream.cuda_stream) for c in host_cols]
+    layers = [DeviceBuffer(32 << k, stream.cuda_stream) for k in range(L + 1)]
+    order = sorted(range(len(logs)), key=lambda i: logs[i])
+    evals_sorted = [evals[i] for i in order]
+    cells = sum(c.size for c in host_cols)
+    eval_cells = cells << blowup
+    del host_cols
+    cms = {"per_column": Committer(logs, blowup, tree, per_column=True, stream=stream.cuda_stream),
+           "batched": Committer(logs, blowup, tree, stream=stream.cuda_stream),
+           "batched_graph": Committer(logs, blowup, tree, graph=True, stream=stream.cuda_stream)}
+    torch.cuda.synchronize()
+    t_tune = time.perf_counter()
+    cms["batched_graph"].autotune(inputs, coeffs, evals, reps=2)
+    torch.cuda.synchronize()
+    tune_s = time.perf_counter() - t_tune
+    steps = max(3, min(args.steps, 10))
+    forms, roots = {}, {}
+    for name, cm in cms.items():
+        with torch.cuda.stream(stream):
+            for _ in range(2):
+                cm.commit(inputs, coeffs, evals, layers)
+        torch.cuda.synchronize()
+        l0 = ffi.launch_count()
+        f_ms = max_over_ranks(time_region(stream, lambda: cm.commit(inputs, coeffs, evals, layers), steps), world)
+        roots[name] = bytes(layer_to_host(layers[0])[0]).hex()
+        forms[name] = {"ms_per_step": f_ms, "committed_cells_per_s": cells / (f_ms * 1e-3),
+                       "launches_per_step": (ffi.launch_count() - l0) / steps}
+        cm.close()
+    # phases of the batched form through the per-op calls (the same launches)
+    marks = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
+    phase_ms = {p: 0.0 for p in ("ifft", "rfft", "leaves", "nodes")}
+    for _ in range(steps):
+        with torch.cuda.stream(stream):
+            marks[0].record(stream)
+            be.interpolate_columns_into(inputs, coeffs, tree)
+            marks[1].record(stream)
+            be.evaluate_polynomials_into(coeffs, blowup, tree, evals)
+            marks[2].record(stream)
+            be.build_leaves_into(evals_sorted, L, layers[L])
+            marks[3].record(stream)
+            be.build_nodes(layers)
+            marks[4].record(stream)
+        torch.cuda.synchronize()
+        for i, ph in enumerate(phase_ms):
+            phase_ms[ph] += marks[i].elapsed_time(marks[i + 1]) / steps
+    root = bytes(layer_to_host(layers[0])[0]).hex()
+    golden = load_digests().get("commit_uneven_root")
+    alg = {"ifft": 8 * cells, "rfft": 4 * cells + 4 * eval_cells}
+    compressions = (1 << L) * ((len(logs) + 15) // 16)
+    out = {
+        "workload": "commit_uneven: 512 columns, log sizes U{12..22} seed 3, blowup 2, lifted Blake2s tree L=24",
+        "committed_cells": cells,
+        "forms": forms,
+        "batched_over_per_column": forms["per_column"]["ms_per_step"] / forms["batched"]["ms_per_step"],
+        "graph_over_per_column": forms["per_column"]["ms_per_step"] / forms["batched_graph"]["ms_per_step"],
+        "phase_ms_batched": phase_ms,
+        "phase_hbm_frac": {p: alg[p] / (phase_ms[p] * 1e-3) / (hbm_peak * 1e9) for p in alg},
+        "leaves_vs_blake2s_ceiling": compressions / (phase_ms["leaves"] * 1e-3) / probe_rate,
+        "autotune": {"seconds": tune_s, "plans": {str(n): fft_get_plan(n) for n in sorted(set(logs))}},
+        "root": root,
+        "roots_equal_across_forms": len(set(roots.values()) | {root}) == 1,
+        "bit_exact_root_vs_oracle": (root == golden) if golden else "no oracle digest",
+    }
+    for x in inputs + coeffs + evals + layers:
+        x.close()
+    tree.twiddles.close()
+    tree.itwiddles.close()
+    return out
+
+
+def extra_fri_heavy(args, stream, world, hbm_peak, probe_rate):
+    """FRI-heavy commit + decommit (log 24, 70 queries) and the stand-alone
+    FriOps folds at log 24 against HBM."""
+    import ctypes
+    import hashlib
+    import torch
+    from stwo_b200 import B200Backend, DeviceColumn, SeededFriProver, ffi
+    from stwo_b200.backend import _ptr_array, _u32_array, canonic_half_coset
+    coords, alphas, queries = fri_heavy_inputs()
+    be = B200Backend(stream.cuda_stream)
+    init, lg = canonic_half_coset(FRI_LOG + 1)
+    tree = be.precompute_twiddles(init, lg)
+    half_init = canonic_half_coset(FRI_LOG)[0]  # the source domain's half coset (read below log 5 only)
+    dev = [DeviceColumn.from_host(c, stream.cuda_stream) for c in coords]
+    del coords
+    fp = SeededFriProver(FRI_LOG, tree, stream=stream.cuda_stream)
+    for _ in range(2):
+        proof = fp.prove(dev, alphas, queries)
+    steps = max(3, min(args.steps, 10))
+    ms = max_over_ranks(time_region(stream, lambda: fp.prove(dev, alphas, queries), steps), world)
+    fp.close()
+    golden = load_digests().get("fri_heavy_sha256")
+    # stand-alone folds: FriOps::fold_circle_into_line (2^24 -> 2^23) and
+    # FriOps::fold_line (2^23 -> 2^22), one thread per output
+    n = 1 << FRI_LOG
+    line = [DeviceColumn(n >> 1, stream.cuda_stream) for _ in range(4)]
+    out = [DeviceColumn(n >> 2, stream.cuda_stream) for _ in range(4)]
+    sp = ctypes.c_void_p(stream.cuda_stream)
+    a0 = _u32_array(alphas[0])
+
+    def circle():
+        ffi.call("stwo_b200_fold_circle_into_line", _ptr_array(line), _ptr_array(dev), ctypes.c_uint32(FRI_LOG),
+                 ctypes.c_uint64(half_init), a0, ctypes.c_void_p(tree.itwiddles.ptr), ctypes.c_uint32(tree.log_size), sp)
+
+    def fold():
+        ffi.call("stwo_b200_fold_line", _ptr_array(line), ctypes.c_uint32(FRI_LOG - 1), a0, ctypes.c_uint32(1),
+                 ctypes.c_void_p(tree.itwiddles.ptr), ctypes.c_uint32(tree.log_size), _ptr_array(out), sp)
+
+    for _ in range(3):
+        circle()
+        fold()
+    c_ms = time_region(stream, circle, 20)
+    f_ms = time_region(stream, fold, 20)
+    # algorithmic bytes: circle fold reads 16 B per input and reads + writes
+    # 16 B per output (dst <- dst * alpha^2 + f'); line fold reads 16 B per
+    # input and writes 16 B per output
+    c_bytes = 16 * n + 32 * (n >> 1)
+    f_bytes = 16 * (n >> 1) + 16 * (n >> 2)
+    for x in dev + line + out:
+        x.close()
+    tree.twiddles.close()
+    tree.itwiddles.close()
+    compressions = sum((1 << (k + 1)) - 1 for k in range(1, FRI_LOG + 1))
+    return {
+        "workload": "fri_heavy: one QM31 column of log 24, circle fold + line folds by 2 to log 0, "
+                    "70 query draws, seeded alphas",
+        "ms_per_step": ms, "folded_elements_per_s": fri_units() / (ms * 1e-3),
+        "trees_vs_blake2s_ceiling": compressions / (ms * 1e-3) / probe_rate,
+        "bit_exact_vs_oracle": (hashlib.sha256(proof).hexdigest() == golden) if golden else "no oracle digest",
+        "fold_roofline": {
+            "fold_circle_into_line_log24": {"ms": c_ms, "alg_bytes": c_bytes,
+                                            "achieved_gbs": c_bytes / (c_ms * 1e-3) / 1e9,
+                                            "frac": c_bytes / (c_ms * 1e-3) / (hbm_peak * 1e9)},
+            "fold_line_log23": {"ms": f_ms, "alg_bytes": f_bytes, "achieved_gbs": f_bytes / (f_ms * 1e-3) / 1e9,
+                                "frac": f_bytes / (f_ms * 1e-3) / (hbm_peak * 1e9)},
+            "peak": hbm_peak, "unit": "GB/s",
+            "kernels": "fold_circle_kernel, fold_line_kernel (the FriOps entry points; the prover's fused "
+                       "fold + next-layer leaf hash kernels are in phase_roofline_frac)"},
+    }
+
+
+# ------------------------------------------------------------- trace FFT ----
+def trace_fft_setup(args):
+    r = np.random.default_rng(1)
+    return r.integers(0, P, 1 << args.log_n_rows, dtype=np.uint32)
+
+
+def run_trace_fft_b200(args, world, rank, local):
+    """The trace transforms of the prover alone: interpolate n_cols columns of
+    2^log_n bit-reversed evaluations into coefficients, then evaluate them on
+    the blowup-1 domain, through the batched C ABI calls the prover makes."""
+    import torch
+    from stwo_b200 import B200Backend, DeviceColumn, ffi
+    from stwo_b200.backend import canonic_half_coset
+    torch.cuda.set_device(local)
+    ffi.init(local)
+    stream = torch.cuda.Stream()
+    be = B200Backend(stream.cuda_stream)
+    log_n, nc = args.log_n_rows, args.n_cols
+    init, lg = canonic_half_coset(log_n + 2)
+    tree = be.precompute_twiddles(init, lg)
+    host = trace_fft_setup(args)
+    evals = [DeviceColumn.from_host(host, stream.cuda_stream) for _ in range(nc)]
+    coeffs = [DeviceColumn(1 << log_n, stream.cuda_stream) for _ in range(nc)]
+    outs = [DeviceColumn(1 << (log_n + 1), stream.cuda_stream) for _ in range(nc)]
+    torch.cuda.synchronize()
+    for _ in range(args.warmup):
+        be.interpolate_columns_into(evals, coeffs, tree)
+        be.evaluate_polynomials_into(coeffs, 1, tree, outs)
+    torch.cuda.synchronize()
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    ti = te = 0.0
+    launches0 = ffi.launch_count()
+    for _ in range(args.steps):
+        with torch.cuda.stream(stream):
+            evs[0].record(stream)
+            be.interpolate_columns_into(evals, coeffs, tree)
+            evs[1].record(stream)
+            be.evaluate_polynomials_into(coeffs, 1, tree, outs)
+            evs[2].record(stream)
+        torch.cuda.synchronize()
+        ti += evs[0].elapsed_time(evs[1])
+        te += evs[1].elapsed_time(evs[2])
+    launches = ffi.launch_count() - launches0
+    ti, te = max_over_ranks(ti / args.steps, world), max_over_ranks(te / args.steps, world)
+    if rank != 0:
+        return
+    hbm_peak, peak_kind = load_peaks()
+    n = 1 << log_n
+    alg_i, alg_e = 8 * nc * n, 4 * nc * n + 8 * nc * n
+    bflies = nc * log_n * (n // 2 + n)
+    cells = nc * n
+    line = {
+        "metric": METRIC, "value": replica_rate(cells, ti + te, world), "unit": "transformed trace cells/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ti + te,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32 (M31)",
+        "data": "synthetic (seeded numpy PCG64)",
+        "config": {"workload": "trace_fft", "n_columns": nc, "log_n_rows": log_n, "log_blowup": 1,
+                   "parallelism": f"replicas x{world}"},
+        "gpu_launches": launches,
+        "interpolate_ms": ti, "evaluate_ms": te,
+        "roofline": {"bound": "hbm", "kernel": "trace interpolate + evaluate", "achieved": (alg_i + alg_e) / ((ti + te) * 1e-3) / 1e9,
+                     "peak": hbm_peak, "unit": "GB/s", "frac": (alg_i + alg_e) / ((ti + te) * 1e-3) / (hbm_peak * 1e9),
+                     "peak_kind": peak_kind, "traffic": None, "alg_bytes_per_step": alg_i + alg_e},
+        "butterflies_per_s": bflies / ((ti + te) * 1e-3),
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_trace_fft_reference(args, world, rank):
+    if rank != 0:
+        return
+    from oracle import ffi as oracle
+    n_threads = oracle.set_threads(os.cpu_count() or 1)
+    log_n = args.log_n_rows
+    init, lg = oracle.canonic_half_coset_root(log_n + 2)
+    tw, itw = oracle.precompute_twiddles(init, lg)
+    host = trace_fft_setup(args)
+    k = max(1, min(args.n_cols, 8))  # a bounded sample of the columns per step
+    secs = []
+    for i in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        co = oracle.interpolate_columns([host] * k, itw)
+        oracle.evaluate_columns(co, 1, tw)
+        if i >= args.warmup:
+            secs.append(time.perf_counter() - t0)
+    med = statistics.median(secs)
+    value = k * (1 << log_n) / med
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "transformed trace cells/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * med * args.n_cols / k,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32 (M31)",
+        "data": "synthetic (seeded numpy PCG64)",
+        "config": {"workload": "trace_fft", "n_columns": args.n_cols, "log_n_rows": log_n, "log_blowup": 1},
+        "cpu_baseline": {"value": value, "unit": "transformed trace cells/s", "cores": n_threads, "kind": "port",
+                         "sample": f"per step {k} of the {args.n_cols} columns (SimdBackend restatement, OpenMP)"},
+        "e2e": {"value": value, "unit": "transformed trace cells/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
 # --------------------------------------------------------------- serving -----
 SERVE_SEED, SERVE_SLOTS, SERVE_BUDGET = 5, 3, 120 << 30
 
@@ -1167,9 +1489,11 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="wide_fib_prove",
-                    choices=["wide_fib_prove", "commit_uneven", "commit_plain", "fri_heavy", "serving"])
+                    choices=["wide_fib_prove", "commit_uneven", "commit_plain", "fri_heavy", "serving", "trace_fft"])
     ap.add_argument("--log-n-rows", type=int, default=20, help="wide_fib_prove: log2 of the trace rows")
     ap.add_argument("--n-cols", type=int, default=100, help="wide_fib_prove: trace columns")
+    ap.add_argument("--no-extras", dest="extras", action="store_false",
+                    help="wide_fib_prove: skip the uneven-commit and FRI-heavy measurements of the default line")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world, rank, local = dist_setup()
@@ -1186,6 +1510,11 @@ def main():
                                       "the oracle's per-proof rate is reported as cpu_baseline by the b200 arm"}))
             else:
                 run_serving_b200(args, world, rank, local)
+        elif args.workload == "trace_fft":
+            if args.impl == "reference":
+                run_trace_fft_reference(args, world, rank)
+            else:
+                run_trace_fft_b200(args, world, rank, local)
         elif args.workload == "fri_heavy":
             if args.impl == "reference":
                 run_fri_reference(args, world, rank)

@@ -215,7 +215,8 @@ int stwo_b200_decompose(const uint32_t* const* d_in4, uint32_t log_size, uint32_
  * (18,960 bytes) is a fixed device array that every GPU loading the library
  * keeps until exit.  Inputs up to 2^30 elements per coordinate; larger sizes
  * are rejected.  The first call on a device looks up the array's device
- * address (make it before any stream capture).  Calls share the array:
+ * address and caches it per device (make it before any stream capture; a
+ * cudaDeviceReset between calls is not supported).  Calls share the array:
  * calls that overlap on the GPU race.  Synchronises `stream`. */
 int stwo_b200_decompose_noalloc(const uint32_t* const* d_in4, uint32_t log_size, uint32_t* const* d_out4,
                                 uint32_t* lambda_out, void* stream, char* err, size_t err_len);
@@ -341,6 +342,17 @@ int stwo_b200_prover_footprint(const stwo_b200_wide_fib_config* cfg, size_t* dev
 int stwo_b200_prover_set_timing(stwo_b200_prover* prover, int enable, char* err, size_t err_len);
 int stwo_b200_prover_phase_times(stwo_b200_prover* prover, double* ms_out, uint32_t n, uint32_t* proofs, char* err,
                                  size_t err_len);
+
+/* Wait bound of the prover's column-streaming kernels (composition,
+ * quotients): a consumer warp polls a stage's mbarrier at most `polls` times
+ * before it gives up, sets the prover's error flag and leaves; the prove then
+ * returns STWO_B200_ETIMEOUT.  0 gives up at the first wait (every such
+ * prove fails); STWO_B200_STREAM_SPIN_DEFAULT restores the default.  The
+ * producer's own waits, including its wait for copies still in flight before
+ * its block exits, keep the default bound.  No reference counterpart: this
+ * exercises the failure path of the bounded device waits. */
+#define STWO_B200_STREAM_SPIN_DEFAULT (1u << 22)
+int stwo_b200_prover_set_stream_spin(stwo_b200_prover* prover, uint32_t polls, char* err, size_t err_len);
 
 /* ---------------------------------------------------------- serving ------ */
 /* Continuous batching of Wide-Fibonacci prove requests on the current GPU

@@ -266,7 +266,9 @@ extern "C" int stwo_b200_decompose(const uint32_t* const* d_in4, uint32_t log_si
 // host code the symbol's name is a host-side stand-in, not a device address,
 // so the address is fetched once per device with cudaGetSymbolAddress (with
 // that device current) and cached; the first call on a device does that
-// set-up, so make it before any stream capture.  All calls on a device share
+// set-up, so make it before any stream capture.  The cache is keyed by device
+// ordinal: a cudaDeviceReset between calls (which recreates the device's
+// context and may move the array) is not supported.  All calls on a device share
 // the array and it keeps the last call's contents: each call overwrites every
 // word it reads, and calls that overlap on the GPU (different streams, or
 // host threads without ordering) race on it.
@@ -274,6 +276,9 @@ namespace stwo_b200 {
 
 constexpr uint32_t kNoAllocBlocks = 148 * 8;                  // reduction blocks (one wave)
 constexpr uint32_t kNoAllocScratchWords = kNoAllocBlocks * 4 + 4;  // partials + lambda: 18,960 bytes
+// A launch of at most kNoAllocBlocks blocks writes 4 partial words per block,
+// and lambda sits after the last block's partials.
+static_assert(kNoAllocScratchWords >= kNoAllocBlocks * 4 + 4, "partials and lambda must fit the fixed array");
 static __device__ __align__(256) uint32_t g_decompose_scratch[kNoAllocScratchWords];
 
 static uint32_t* noalloc_scratch(int device, char* err, size_t err_len, int* rc) {
@@ -313,10 +318,9 @@ extern "C" int stwo_b200_decompose_noalloc(const uint32_t* const* d_in4, uint32_
   uint64_t range = n / 16, half_a = range / 2;
   uint64_t split_sum = 16 * half_a, end_sum = 16 * range;
   uint64_t split_apply = 16 * (((n + 15) / 16) / 2);
+  // At most kNoAllocBlocks blocks, so the partials and lambda fit the array
+  // (static_assert above).
   unsigned blocks = (unsigned)std::min<uint64_t>(std::max<uint64_t>((end_sum + 255) / 256, 1), kNoAllocBlocks);
-  // blocks * 4 partial words + 4 lambda words must fit the fixed array.
-  STWO_ARG_CHECK((uint64_t)blocks * 4 + 4 <= kNoAllocScratchWords, "scratch of %u words exceeds the maximum of %u",
-                 blocks * 4 + 4, kNoAllocScratchWords);
   uint32_t* lam = scratch + blocks * 4;
   Cols4 in{{d_in4[0], d_in4[1], d_in4[2], d_in4[3]}};
   Cols4W out{{d_out4[0], d_out4[1], d_out4[2], d_out4[3]}};

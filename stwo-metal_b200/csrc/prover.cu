@@ -77,57 +77,19 @@ __global__ void wide_fib_trace_kernel(const uint32_t* __restrict__ a, const uint
   }
 }
 
-// Composition evaluation at every point of the evaluation domain
-// (constraint-framework/src/prover/component_prover.rs:91-160): for constraint
-// k (0-based) c_{k+2} - (c_k^2 + c_{k+1}^2) weighted by powers[k] (already
-// reversed), times the vanishing inverse of the point's trace-coset class.
-__global__ void composition_kernel(const uint32_t* __restrict__ evals, uint64_t col_stride, uint32_t n_cons,
-                                   const qm31* __restrict__ powers, const uint32_t* __restrict__ denom_inv,
-                                   uint32_t log_n, uint64_t n_points, uint32_t* __restrict__ out) {
-  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n_points;
-       i += (uint64_t)gridDim.x * blockDim.x) {
-    uint32_t a = __ldg(evals + i), b = __ldg(evals + col_stride + i);
-    uint32_t sa = m31_sqr(a), sb = m31_sqr(b);
-    acc4 row{0, 0, 0, 0};
-    uint32_t k = 0;
-    for (; k + 6 <= n_cons; k += 6) {
-      uint32_t cv[6];  // six independent loads in flight per thread
-#pragma unroll
-      for (int u = 0; u < 6; u++) cv[u] = __ldg(evals + (uint64_t)(k + u + 2) * col_stride + i);
-#pragma unroll
-      for (int u = 0; u < 6; u++) {
-        uint32_t cons = m31_sub(cv[u], m31_add(sa, sb));
-        acc4_mad(row, powers[k + u], cons);
-        sa = sb;
-        sb = m31_sqr(cv[u]);
-        if (u == 2 || u == 5) acc4_fold(row);
-      }
-    }
-    for (; k < n_cons; k++) {  // remainder: fold after every term
-      uint32_t c = __ldg(evals + (uint64_t)(k + 2) * col_stride + i);
-      uint32_t cons = m31_sub(c, m31_add(sa, sb));
-      acc4_mad(row, powers[k], cons);
-      acc4_fold(row);
-      sa = sb;
-      sb = m31_sqr(c);
-    }
-    qm31 v = qm31_mul_m31(acc4_reduce(row), __ldg(denom_inv + (i >> log_n)));
-    out[i] = v.a;
-    out[n_points + i] = v.b;
-    out[2 * n_points + i] = v.c;
-    out[3 * n_points + i] = v.d;
-  }
-}
-
 __device__ __forceinline__ uint4 ldg4(const uint32_t* p) { return __ldg(reinterpret_cast<const uint4*>(p)); }
 __device__ __forceinline__ uint32_t u4get(const uint4& v, int r) {
   return r == 0 ? v.x : r == 1 ? v.y : r == 2 ? v.z : v.w;
 }
 
-// composition_kernel for 4 consecutive points per thread: 16-byte loads keep
-// four times the bytes in flight per load, which this memory-latency-bound
-// loop needs.  Same arithmetic per point.  n_points % 4 == 0, columns
-// 16-byte aligned.
+// Composition evaluation at every point of the evaluation domain
+// (constraint-framework/src/prover/component_prover.rs:91-160): for constraint
+// k (0-based) c_{k+2} - (c_k^2 + c_{k+1}^2) weighted by powers[k] (already
+// reversed), times the vanishing inverse of the point's trace-coset class.
+// Four consecutive points per thread: 16-byte loads keep four times the bytes
+// in flight per load, which this memory-latency-bound loop needs.
+// n_points % 4 == 0, columns 16-byte aligned.  The streaming form
+// composition_tma_kernel takes every domain of at least one 512-row tile.
 __global__ void __launch_bounds__(256) composition4_kernel(const uint32_t* __restrict__ evals, uint64_t col_stride,
                                                           uint32_t n_cons, const qm31* __restrict__ powers,
                                                           const uint32_t* __restrict__ denom_inv, uint32_t log_n,
@@ -296,54 +258,11 @@ struct QuotientParams {
   cpoint tile_pts[256];  // m * step * 2^(log_size - tile bits), m < rows/4 (quotient_tma_kernel)
 };
 
-__global__ void __launch_bounds__(256) quotient_kernel(QuotientParams q, PolyTable cols, uint32_t n_cols,
-                                                      const qm31* __restrict__ alpha_pows,
-                                                      const QuotientDyn* __restrict__ dyn,
-                                                      uint32_t* __restrict__ out) {
-  const QuotientDyn& qd = *dyn;  // read at the epilogue, through the read-only cache
-  const uint64_t n = 1ull << q.log_size;
-  const uint64_t half = n >> 1;
-  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
-    acc4 s4{0, 0, 0, 0};
-    uint32_t k = 0;
-    for (; k + 6 <= n_cols; k += 6) {
-      uint32_t fv[6];  // six independent loads in flight per thread
-#pragma unroll
-      for (int u = 0; u < 6; u++) fv[u] = __ldg(cols.p[k + u] + i);
-#pragma unroll
-      for (int u = 0; u < 6; u++) {
-        acc4_mad(s4, alpha_pows[k + u], fv[u]);
-        if (u == 2 || u == 5) acc4_fold(s4);
-      }
-    }
-    for (; k < n_cols; k++) {  // remainder: fold after every term
-      acc4_mad(s4, alpha_pows[k], __ldg(cols.p[k] + i));
-      acc4_fold(s4);
-    }
-    qm31 acc = acc4_reduce(s4);
-    // domain point at bit-reversed position i (core/poly/circle/domain.rs:56-66)
-    uint64_t j = __brevll(i) >> (64 - q.log_size);
-    uint64_t jj = j < half ? j : j - half;
-    cpoint pt = q.init;
-    for (uint32_t b = 0; b + 1 < q.log_size; b++)
-      if ((jj >> b) & 1) pt = cpoint_add(pt, q.step_pow[b]);
-    if (j >= half) pt.y = m31_neg(pt.y);  // -index is the conjugate point
-    qm31 num = qm31_sub(qm31_mul(qd.c, acc), qd.B);
-    qm31 full = qm31_sub(num, qm31_mul_m31(qd.A, pt.y));
-    cm31 den = cm31_sub(cm31_mul(cm31_sub(qd.prx, cm31{pt.x, 0}), qd.piy),
-                        cm31_mul(cm31_sub(qd.pry, cm31{pt.y, 0}), qd.pix));
-    qm31 v = qm31_mul_cm31(full, cm31_inv(den));
-    out[i] = v.a;
-    out[n + i] = v.b;
-    out[2 * n + i] = v.c;
-    out[3 * n + i] = v.d;
-  }
-}
-
-// quotient_kernel for 4 consecutive rows per thread: 16-byte column loads and
-// one shared inversion for the four denominators (their norms are inverted
+// FRI quotients, 4 consecutive rows per thread: 16-byte column loads and one
+// shared inversion for the four denominators (their norms are inverted
 // together with Montgomery's trick; exact, so equal to four cm31_inv).
-// n % 4 == 0, columns 16-byte aligned.
+// n % 4 == 0, columns 16-byte aligned.  The streaming form quotient_tma_kernel
+// takes every domain of at least two 512-row tiles.
 __device__ __forceinline__ cpoint quotient_point(const QuotientParams& q, uint64_t i) {
   const uint64_t n = 1ull << q.log_size, half = n >> 1;
   const uint64_t j = __brevll(i) >> (64 - q.log_size);
@@ -434,7 +353,7 @@ __global__ void __launch_bounds__(256) quotient4_kernel(QuotientParams q, PolyTa
 // ColumnPipe (cp.async.bulk issued by a producer warp, full/empty mbarriers),
 // so the DRAM reads of the next groups overlap the arithmetic of the current
 // one and no block barrier is taken per group.  Same arithmetic per point as
-// composition_kernel / quotient_kernel.
+// composition4_kernel / quotient4_kernel.
 constexpr int kStreamTileBits = 9, kStreamRows = 1 << kStreamTileBits, kStreamG = 6, kStreamS = 3;
 static_assert(kStreamG == 6, "the fold positions of the streaming kernels assume 6-column groups");
 constexpr int kStreamThreads = kStreamRows / 4;      // consumers: four rows per thread
@@ -453,13 +372,13 @@ __device__ __forceinline__ void stage_weights(uint4* sw, const qm31* __restrict_
 __global__ void __launch_bounds__(kStreamBlock) composition_tma_kernel(
     const uint32_t* __restrict__ evals, uint64_t col_stride, uint32_t n_cons, const qm31* __restrict__ powers,
     const uint32_t* __restrict__ denom_inv, uint32_t log_n, uint64_t n_points, uint32_t* __restrict__ out,
-    uint32_t* err) {
+    uint32_t* err, uint32_t spin) {
   extern __shared__ __align__(128) uint32_t smem[];
   __shared__ uint64_t bars[kPipeBarWords];
   uint4* sw = reinterpret_cast<uint4*>(smem + kStreamRing / sizeof(uint32_t));
   const uint32_t t4 = threadIdx.x * 4;
   auto col = [evals, col_stride](uint32_t c) { return evals + (uint64_t)c * col_stride; };
-  StreamPipe pipe(smem, bars, n_cons + 2, (uint32_t)(n_points / kStreamRows));
+  StreamPipe pipe(smem, bars, n_cons + 2, (uint32_t)(n_points / kStreamRows), spin);
   stage_weights(sw, powers, n_cons);
   __syncthreads();  // the last block barrier: the producer warp leaves the loop below
   if (threadIdx.x >= kStreamThreads) {
@@ -529,7 +448,8 @@ __global__ void __launch_bounds__(kStreamBlock) quotient_tma_kernel(QuotientPara
                                                                    uint32_t n_cols,
                                                                    const qm31* __restrict__ alpha_pows,
                                                                    const QuotientDyn* __restrict__ dyn,
-                                                                   uint32_t* __restrict__ out, uint32_t* err) {
+                                                                   uint32_t* __restrict__ out, uint32_t* err,
+                                                                   uint32_t spin) {
   const QuotientDyn& qd = *dyn;  // read at the epilogue, through the read-only cache
   extern __shared__ __align__(128) uint32_t smem[];
   __shared__ uint64_t bars[kPipeBarWords];
@@ -538,7 +458,7 @@ __global__ void __launch_bounds__(kStreamBlock) quotient_tma_kernel(QuotientPara
   const uint32_t t4 = threadIdx.x * 4;
   const PolyTable* tab = &cols;
   auto col = [tab](uint32_t c) { return tab->p[c]; };
-  StreamPipe pipe(smem, bars, n_cols, (uint32_t)(n / kStreamRows));
+  StreamPipe pipe(smem, bars, n_cols, (uint32_t)(n / kStreamRows), spin);
   stage_weights(sw, alpha_pows, n_cols);
   __syncthreads();  // the last block barrier: the producer warp leaves the loop below
   if (threadIdx.x >= kStreamThreads) {
@@ -881,7 +801,7 @@ __global__ void fs_oods_kernel(DevChannel* ch, const uint8_t* root, uint32_t lg,
 
 // Sampled values -> quotient random coefficient q, its powers ap[k] = q^k and
 // the row constants (pcs/quotient_ops.rs:134-233 in the form of
-// quotient_kernel): c = conj(y) - y, A = sum q^k (conj(v_k) - v_k),
+// quotient4_kernel): c = conj(y) - y, A = sum q^k (conj(v_k) - v_k),
 // B = sum q^k (v_k c - (conj(v_k) - v_k) y) over the nq sampled values.
 constexpr int kFsThreads = 256;
 __global__ void __launch_bounds__(kFsThreads) fs_quotient_kernel(DevChannel* ch, const qm31* __restrict__ vals,
@@ -1327,6 +1247,9 @@ enum Phase {
 class WideFibProver {
  public:
   bool timing = false;
+  // Polls a consumer of the column-streaming kernels makes before a stage
+  // wait gives up (stwo_b200_prover_set_stream_spin).
+  uint32_t stream_spin = kStreamSpin;
   std::vector<cudaEvent_t> ev_pool;
   std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> marks;
   size_t ev_used = 0;
@@ -1558,7 +1481,7 @@ class WideFibProver {
     if (measure) return 0;
     STWO_CUDA_TRY(cudaMallocHost((void**)&h_pinned, h_pinned_bytes));
     STWO_CUDA_TRY(cudaMallocHost((void**)&h_chan, sizeof(DevChannel)));
-    h_tx_bytes = 64 + sizeof(FsOut) + (size_t)(N + 8) * sizeof(qm31);
+    h_tx_bytes = 64 + sizeof(FsOut) + (size_t)(N + 8) * sizeof(qm31) + 16;  // + the stream error word
     STWO_CUDA_TRY(cudaMallocHost((void**)&h_tx, h_tx_bytes));
     {
       // Vanishing inverses of the 2^(eval_log - log_n) trace-coset classes,
@@ -1845,13 +1768,13 @@ int WideFibProver::prove_body(const uint32_t* d_a, const uint32_t* d_b, ProofOut
     composition_tma_kernel<<<stream_grid(composition_tma_kernel, kStreamRing + n_cons * sizeof(uint4),
                                          (uint32_t)(n_eval / kStreamRows)),
                              kStreamBlock, kStreamRing + n_cons * sizeof(uint4), s>>>(
-        comp_src, comp_stride, n_cons, d_small, d_denom, log_n, n_eval, d_comp, d_found + kStreamErrWord);
+        comp_src, comp_stride, n_cons, d_small, d_denom, log_n, n_eval, d_comp, d_found + kStreamErrWord,
+        stream_spin);
   else if (n_eval % 4 == 0 && comp_stride % 4 == 0 && reinterpret_cast<uintptr_t>(comp_src) % 16 == 0)
     composition4_kernel<<<grid1d(n_eval / 4, 256), 256, 0, s>>>(comp_src, comp_stride, n_cons, d_small, d_denom,
                                                                 log_n, n_eval, d_comp);
-  else
-    composition_kernel<<<grid1d(n_eval, 256), 256, 0, s>>>(comp_src, comp_stride, n_cons, d_small, d_denom, log_n,
-                                                           n_eval, d_comp);
+  else  // the prover's own buffers are pool-allocated (256-byte aligned) and log_n >= 4
+    return set_err(err, err_len, STWO_B200_ESTATE, "composition: unaligned evaluation buffer");
   STWO_CHECK_LAUNCH();
   std::vector<uint32_t*> comp_cols(4);
   std::vector<uint32_t> logs_e(4, eval_log);
@@ -1932,11 +1855,12 @@ int WideFibProver::prove_body(const uint32_t* d_a, const uint32_t* d_b, ProofOut
       quotient_tma_kernel<<<stream_grid(quotient_tma_kernel, kStreamRing + nq * sizeof(uint4),
                                         (uint32_t)((1ull << lift) / kStreamRows)),
                             kStreamBlock, kStreamRing + nq * sizeof(uint4), s>>>(
-          qp, cols, nq, d_ap, d_qdyn, d_quot, d_found + kStreamErrWord);
-    } else if (aligned)
+          qp, cols, nq, d_ap, d_qdyn, d_quot, d_found + kStreamErrWord, stream_spin);
+    } else if (aligned) {
       quotient4_kernel<<<grid1d(1ull << (lift - 2), 256), 256, 0, s>>>(qp, cols, nq, d_ap, d_qdyn, d_quot);
-    else
-      quotient_kernel<<<grid1d(1ull << lift, 256), 256, 0, s>>>(qp, cols, nq, d_ap, d_qdyn, d_quot);
+    } else {  // pool-allocated columns are 256-byte aligned and lift >= 5
+      return set_err(err, err_len, STWO_B200_ESTATE, "quotients: unaligned column buffer");
+    }
     STWO_CHECK_LAUNCH();
   }
 
@@ -1952,6 +1876,8 @@ int WideFibProver::prove_body(const uint32_t* d_a, const uint32_t* d_b, ProofOut
   STWO_CUDA_TRY(cudaMemcpyAsync(h_tx + 32, t2.layer(0), 32, cudaMemcpyDeviceToHost, s));
   STWO_CUDA_TRY(cudaMemcpyAsync(h_tx + 64, d_fs, sizeof(FsOut), cudaMemcpyDeviceToHost, s));
   STWO_CUDA_TRY(cudaMemcpyAsync(h_tx + 64 + sizeof(FsOut), d_vals, np * sizeof(qm31), cudaMemcpyDeviceToHost, s));
+  const size_t tx_flag_off = 64 + sizeof(FsOut) + np * sizeof(qm31);
+  STWO_CUDA_TRY(cudaMemcpyAsync(h_tx + tx_flag_off, d_found + kStreamErrWord, 4, cudaMemcpyDeviceToHost, s));
   STWO_CUDA_TRY(cudaEventRecord(ev_tx, s));
   if ((rc = run_fri(err, err_len))) return rc;
   Hash32 root1, root2;
@@ -1967,6 +1893,10 @@ int WideFibProver::prove_body(const uint32_t* d_a, const uint32_t* d_b, ProofOut
       cudaStreamSynchronize(s);
       return set_err(err, err_len, code, "%s", what);
     };
+    // A timed-out composition stream leaves partial rows behind: report it
+    // before any check of the values built on them.
+    if (*reinterpret_cast<const uint32_t*>(h_tx + tx_flag_off))
+      return fail(STWO_B200_ETIMEOUT, "column stream: a bulk copy did not complete in time");
     ch.mix_root(root1);
     const qm31 random_coeff = ch.draw_secure_felt();
     if (!qm31_eq(random_coeff, fs.random_coeff))
@@ -2046,9 +1976,11 @@ int WideFibProver::prove_body(const uint32_t* d_a, const uint32_t* d_b, ProofOut
     STWO_CUDA_TRY(cudaMemcpyAsync(hpw + off, d_last, 16 * n_last, cudaMemcpyDeviceToHost, s));
     STWO_CUDA_TRY(cudaStreamSynchronize(s));
     const DevChannel* dc = reinterpret_cast<const DevChannel*>(hp + chan_off);
-    if (dc->error) return set_err(err, err_len, STWO_B200_ESTATE, "device channel: draw retry bound exhausted");
+    // A timed-out stream leaves the transcript built on partial rows, so its
+    // flag is reported first.
     if (*reinterpret_cast<const uint32_t*>(hp + flag_off))
       return set_err(err, err_len, STWO_B200_ETIMEOUT, "column stream: a bulk copy did not complete in time");
+    if (dc->error) return set_err(err, err_len, STWO_B200_ESTATE, "device channel: draw retry bound exhausted");
     dev_ch.set_state(dc->digest, dc->n_draws);
     std::memcpy(fri_end_digest, dc->digest, 32);
     fri_end_draws = dc->n_draws;
@@ -2666,6 +2598,12 @@ extern "C" int stwo_b200_prover_set_timing(stwo_b200_prover* p, int enable, char
   p->impl->timing = enable != 0;
   for (double& x : p->impl->phase_ms) x = 0;
   p->impl->proofs_timed = 0;
+  return ok(err, err_len);
+}
+
+extern "C" int stwo_b200_prover_set_stream_spin(stwo_b200_prover* p, uint32_t polls, char* err, size_t err_len) {
+  STWO_ARG_CHECK(p, "null prover");
+  p->impl->stream_spin = polls;
   return ok(err, err_len);
 }
 

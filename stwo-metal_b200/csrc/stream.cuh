@@ -10,16 +10,20 @@
 // combined.  No multicast: every copy lands in the issuing CTA's own shared
 // memory.
 //
-// Every wait is bounded (kStreamSpin polls); a wait that runs out sets an
-// error word and the block leaves after its copies in flight have landed.
+// Every wait is bounded: a consumer's wait for a stage by the pipe's `spin`
+// polls (a kernel argument, kStreamSpin by default), every producer wait by
+// kStreamSpin.  A wait that runs out sets an error word and the block leaves
+// after its copies in flight have landed.
 #pragma once
 #include <cuda_runtime.h>
 
 #include <cstdint>
 
+#include "../../include/stwo_b200.h"
+
 namespace stwo_b200 {
 
-constexpr uint32_t kStreamSpin = 1u << 22;  // try_wait polls before giving up
+constexpr uint32_t kStreamSpin = STWO_B200_STREAM_SPIN_DEFAULT;  // try_wait polls before giving up
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -71,7 +75,7 @@ __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
 // producer stops issuing and waits (bounded) for its copies in flight before
 // it exits, so no copy lands after the block's shared memory is released.
 // Usage (block = CONSUMERS + 32 threads, CONSUMERS % 32 == 0):
-//   ColumnPipe<G, S, ROWS, C> pipe(buf, bars, n_cols, n_tiles);   // then one barrier
+//   ColumnPipe<G, S, ROWS, C> pipe(buf, bars, n_cols, n_tiles, spin);   // then one barrier
 //   if (threadIdx.x >= C) { if (threadIdx.x == C) pipe.produce(col, head, err); return; }
 //   for (t ...) for (g ...) { gg = t * n_groups + g;
 //     if (!pipe.wait(gg, err)) return;  ... read pipe.seg(gg, k) ...;  pipe.release(gg); }
@@ -85,10 +89,11 @@ struct ColumnPipe {
   uint32_t* header;  // S * kPipeHeaderWords words
   volatile uint32_t* abort_word;
   uint32_t n_cols, n_groups, my_tiles, total;
+  uint32_t spin;  // polls of a consumer's stage wait before it gives up (0: at once)
   // `bars` holds 2 * S mbarriers followed by S * kPipeHeaderWords + 1 words
   // (8-byte aligned shared memory).
-  __device__ ColumnPipe(uint32_t* b, uint64_t* bars, uint32_t n, uint32_t n_tiles)
-      : buf(b), full(bars), empty(bars + S), n_cols(n), n_groups((n + G - 1) / G) {
+  __device__ ColumnPipe(uint32_t* b, uint64_t* bars, uint32_t n, uint32_t n_tiles, uint32_t consumer_spin)
+      : buf(b), full(bars), empty(bars + S), n_cols(n), n_groups((n + G - 1) / G), spin(consumer_spin) {
     header = reinterpret_cast<uint32_t*>(bars + 2 * S);
     abort_word = header + S * kPipeHeaderWords;
     my_tiles = blockIdx.x < n_tiles ? (n_tiles - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
@@ -115,11 +120,11 @@ struct ColumnPipe {
   __device__ __forceinline__ const uint32_t* head(uint32_t gg) const {
     return header + (gg % S) * kPipeHeaderWords;
   }
-  // Bounded poll of phase `parity` that also gives up when another thread
-  // has aborted.
-  __device__ __forceinline__ bool poll(uint64_t* bar, uint32_t parity) const {
+  // Poll of phase `parity`, at most `limit` times, that also gives up when
+  // another thread has aborted.
+  __device__ __forceinline__ bool poll(uint64_t* bar, uint32_t parity, uint32_t limit) const {
     const uint32_t a = smem_addr(bar);
-    for (uint32_t it = 0; it < kStreamSpin; it++) {
+    for (uint32_t it = 0; it < limit; it++) {
       uint32_t done;
       asm volatile(
           "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
@@ -137,7 +142,7 @@ struct ColumnPipe {
   }
   // Consumer side.
   __device__ __forceinline__ bool wait(uint32_t gg, uint32_t* err) const {
-    if (poll(full + gg % S, (gg / S) & 1)) return true;
+    if (poll(full + gg % S, (gg / S) & 1, spin)) return true;
     fail(err);
     return false;
   }
@@ -149,7 +154,7 @@ struct ColumnPipe {
     uint32_t gg = 0;
     for (; gg < total; gg++) {
       const uint32_t st = gg % S;
-      if (gg >= (uint32_t)S && !poll(empty + st, (gg / S - 1) & 1)) {
+      if (gg >= (uint32_t)S && !poll(empty + st, (gg / S - 1) & 1, kStreamSpin)) {
         fail(err);
         break;
       }

@@ -74,6 +74,14 @@ class WideFibProver:
                  C.c_size_t(cap), C.byref(n))
         return n.value
 
+    STREAM_SPIN_DEFAULT = 1 << 22
+
+    def set_stream_spin(self, polls: int) -> None:
+        """Poll bound of a consumer's stage wait in the column-streaming
+        kernels (composition, quotients); 0 makes every such wait give up at
+        once, so the prove returns STWO_B200_ETIMEOUT."""
+        ffi.call("stwo_b200_prover_set_stream_spin", self.handle, C.c_uint32(polls))
+
     def close(self):
         if getattr(self, "handle", None):
             ffi.call("stwo_b200_prover_destroy", self.handle)

@@ -95,6 +95,25 @@ def test_oracle_reproduces_uneven_commit_fixture(oracle):
     assert bytes(root.reshape(-1)).hex() == spec["root"]
 
 
+def test_oracle_reproduces_full_size_digests(oracle):
+    # full_size_digests.json (make_full_size_digests.py) is what bench.py
+    # compares its full-size results with; the quick entries are re-derived
+    # here, the 512-column commit root on the GPU suite's full-size test.
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("mk", os.path.join(HERE, "make_full_size_digests.py"))
+    mk = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mk)
+    d = json.loads(_read("full_size_digests.json", "r"))
+    logs, cols = mk.commit_plain_columns()
+    assert mk.commit_root(oracle, logs, cols, 1, True) == d["commit_plain_root"]
+    a, b = mk.wide_fib_columns()
+    proof = oracle.prove_wide_fib(oracle.wide_fib_config(20, 100), a, b)
+    assert (hashlib.sha256(proof).hexdigest(), len(proof)) == (d["wide_fib_prove_sha256"], d["wide_fib_prove_bytes"])
+    coords, alphas, queries = oracle.fri_inputs(24, 4, 70)
+    fri = oracle.fri_prove_seeded(coords, 24, alphas, queries)
+    assert (hashlib.sha256(fri).hexdigest(), len(fri)) == (d["fri_heavy_sha256"], d["fri_heavy_bytes"])
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("name,log_n,cols,blowup,step,nq,m31,seed", WIDE_FIB)
 def test_gpu_wide_fib_matches_fixture(oracle, name, log_n, cols, blowup, step, nq, m31, seed):

@@ -5,8 +5,9 @@ allocate device memory while they run (their device memory is divided up
 front, e.g. by a prover service's admission controller, or owned by their own
 runtime).  Its reduction scratch is a fixed device array instead of a pool
 allocation.  This checks, through the C ABI, that it returns exactly what the
-allocating entry point stwo_b200_decompose returns, on two calls in a row: the
-second, smaller call reuses the shared scratch the first one left behind.
+allocating entry point stwo_b200_decompose returns, on calls in a row of
+different sizes: each call reuses the shared scratch the previous one left
+behind.
 Collected last so a stop-at-first-failure run has already run the rest.
 """
 import ctypes as C
@@ -32,7 +33,10 @@ def _decompose_noalloc(ev: SecureColumn):
 def test_decompose_noalloc_matches_allocating_entry_point():
     be = B200Backend()
     rng = np.random.default_rng(2024)
-    for log_n in (20, 12):
+    # large then small (the small call reads only partials it wrote itself),
+    # sizes below 16 elements (no reduction blocks with data, lambda 0), then
+    # small then large again (the large call overwrites every partial it reads)
+    for log_n in (20, 12, 0, 3, 4, 5, 21):
         coords = [rng.integers(0, P, 1 << log_n, dtype=np.uint32) for _ in range(4)]
         ev = SecureColumn.from_host(coords)
         g_ref, lam_ref = be.decompose(ev)
