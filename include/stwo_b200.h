@@ -221,6 +221,109 @@ int stwo_b200_decompose(const uint32_t* const* d_in4, uint32_t log_size, uint32_
 int stwo_b200_decompose_noalloc(const uint32_t* const* d_in4, uint32_t log_size, uint32_t* const* d_out4,
                                 uint32_t* lambda_out, void* stream, char* err, size_t err_len);
 
+/* --------------------------------------------- QuotientOps (PCS quotients) */
+/* One term of a sample batch: column d_cols[column_index] sampled to
+ * sample_value (QM31) with random coefficient random_coeff (QM31): the
+ * NumeratorData of core/pcs/quotients.rs:63-71. */
+typedef struct stwo_b200_numerator_term {
+  uint32_t column_index;
+  uint32_t sample_value[4];
+  uint32_t random_coeff[4];
+} stwo_b200_numerator_term;
+/* ColumnSampleBatch (core/pcs/quotients.rs:55-61): the point
+ * CirclePoint<SecureField> as 8 words (x then y, 4 each) and its terms (host). */
+typedef struct stwo_b200_sample_batch {
+  uint32_t point[8];
+  const stwo_b200_numerator_term* terms;
+  uint32_t n_terms;
+} stwo_b200_sample_batch;
+
+/* QuotientOps::accumulate_numerators (prover/pcs/quotient_ops.rs:22-33;
+ * SimdBackend prover/backend/simd/quotients.rs:34-71, 124-134) for n_cols
+ * device columns of 2^log_size words (bit-reversed evaluations): for batch b,
+ * d_out[4b .. 4b+3] (the 4 coordinate columns of its partial numerator, 2^log_size
+ * words each) receive sum_i (c_i * col_i[p] - b_i) at every row p, and
+ * first_linear_term_out[4b .. 4b+3] (host) receives sum_i a_i, where
+ * (a_i, b_i, c_i) are the complex-conjugate line coefficients of the term
+ * times its random coefficient (core/constraints.rs:119-134).  No reference
+ * CUDA-ABI counterpart (the reference computed quotients on the host). */
+int stwo_b200_accumulate_numerators(const uint32_t* const* d_cols, uint32_t n_cols, uint32_t log_size,
+                                    const stwo_b200_sample_batch* batches, uint32_t n_batches, uint32_t* const* d_out,
+                                    uint32_t* first_linear_term_out, void* stream, char* err, size_t err_len);
+
+/* AccumulatedNumerators (prover/pcs/quotient_ops.rs:48-74) of one sample point:
+ * the partial numerator's 4 device coordinate columns of 2^log_size words and
+ * the first linear term. */
+typedef struct stwo_b200_accumulated_numerators {
+  uint32_t sample_point[8];
+  const uint32_t* d_partial[4];
+  uint32_t log_size;
+  uint32_t first_linear_term[4];
+} stwo_b200_accumulated_numerators;
+
+/* QuotientOps::compute_quotients_and_combine (quotient_ops.rs:35-45;
+ * simd/quotients.rs:73-164): on the bit-reversed CanonicCoset(lifting_log_size)
+ * domain, d_out4 (4 coordinate columns of 2^lifting_log_size words) receives
+ * sum_z (lift(num_z) - A_z * p.y) / den_z(p), each partial numerator lifted
+ * to the lifting size (l(i, r) = ((i >> (r + 1)) << 1) + (i & 1)). */
+int stwo_b200_compute_quotients_and_combine(const stwo_b200_accumulated_numerators* accs, uint32_t n_accs,
+                                            uint32_t lifting_log_size, uint32_t* const* d_out4, void* stream,
+                                            char* err, size_t err_len);
+
+/* ----------------------------------------------------- AccumulationOps -- */
+/* AccumulationOps::accumulate (prover/air/accumulation.rs:127-130;
+ * simd/accumulation.rs:13-18): column += other, coordinate-wise, `len`
+ * elements (4 coordinate columns each). */
+int stwo_b200_accumulate(uint32_t* const* d_col4, const uint32_t* const* d_other4, uint64_t len, void* stream,
+                         char* err, size_t err_len);
+/* AccumulationOps::generate_secure_powers (accumulation.rs:132-133;
+ * simd/accumulation.rs:20-39): d_out (device, 16-byte aligned) receives
+ * felt^0 .. felt^(n_powers-1), 4 words each. */
+int stwo_b200_generate_secure_powers(const uint32_t* felt, uint32_t n_powers, uint32_t* d_out, void* stream,
+                                     char* err, size_t err_len);
+/* AccumulationOps::lift_and_accumulate (accumulation.rs:135-145;
+ * simd/accumulation.rs:45-80): n_cols secure columns (d_cols4[4k .. 4k+3],
+ * 2^log_sizes[k] words each, log sizes strictly increasing) -> d_out4 (the
+ * size of the last; may be the last column itself) = the coordinate-wise sum
+ * of every column lifted to that size.  Columns of fewer than 16 elements
+ * take part in the sum as the trait defines it (SimdBackend's packed loop
+ * would leave such a column out). */
+int stwo_b200_lift_and_accumulate(const uint32_t* const* d_cols4, const uint32_t* log_sizes, uint32_t n_cols,
+                                  uint32_t* const* d_out4, void* stream, char* err, size_t err_len);
+
+/* ------------------------------------------------- PolyOps::eval_at_point */
+/* PolyOps::batch_eval_at_point (prover/poly/circle/ops.rs:44-63;
+ * simd/circle.rs:168-230): n_polys polynomials of 2^log_size natural-order
+ * coefficients (device) at the point (8 words: x, y) -> values_out (host,
+ * 4 words per polynomial).  Synchronises `stream`.  Replaces the reference's
+ * Metal eval_at_point kernels (crates/stwo-metal-sys/metal/eval_at_point.metal). */
+int stwo_b200_batch_eval_at_point(const uint32_t* const* d_coeffs, uint32_t n_polys, uint32_t log_size,
+                                  const uint32_t* point, uint32_t* values_out, void* stream, char* err,
+                                  size_t err_len);
+/* PolyOps::eval_at_point (ops.rs:44-48) of one polynomial. */
+int stwo_b200_eval_at_point(const uint32_t* d_coeffs, uint32_t log_size, const uint32_t* point, uint32_t* value_out,
+                            void* stream, char* err, size_t err_len);
+
+/* ---------------------------------------------------------- GrindOps ----- */
+/* GrindOps<Blake2sChannel(Generic)>::grind (prover/backend/simd/grind.rs:25-96)
+ * from the channel's 32-byte digest: the smallest nonce (hi << 32) | low,
+ * low < 2^20, whose Blake2s hash after the proof-of-work prefix has at least
+ * pow_bits (<= 32) trailing zeros.  m31_channel selects
+ * Blake2sM31Channel.  Synchronises `stream`. */
+int stwo_b200_grind(const uint8_t* digest, uint32_t pow_bits, int m31_channel, uint64_t* nonce_out, void* stream,
+                    char* err, size_t err_len);
+
+/* ------------------------------------------------ ColumnOps<SecureField> */
+/* ColumnOps<SecureField>::bit_reverse_column (prover/backend/mod.rs:37-39) of
+ * a secure column stored as 4 coordinate columns (SecureColumnByCoords), in
+ * place. */
+int stwo_b200_bit_reverse_secure_column(uint32_t* const* d_coords4, uint32_t log_size, void* stream, char* err,
+                                        size_t err_len);
+/* The same for QM31 values stored 4 words each (16-byte aligned), in place.
+ * Replaces bit_reverse_secure_field (raw.rs:86). */
+int stwo_b200_bit_reverse_secure_field(uint32_t* d_values, uint32_t log_size, void* stream, char* err,
+                                       size_t err_len);
+
 /* --------------------------------------------------------- FFT pass plans */
 /* Pass plan of every n-layer circle FFT: n_passes (1-4) layer counts of 1-12,
  * low layers first, summing to n; the first at least 3 when there are several

@@ -280,6 +280,70 @@ def decompose(cols4):
     return outs, lam
 
 
+# ---- QuotientOps / AccumulationOps / eval_at_point (oracle_pcs.cpp) ----
+def accumulate_numerators(cols, log_n: int, point, terms):
+    """One sample batch: terms = [(column index, value (4 words), alpha (4
+    words)), ...]; returns (4 partial-numerator columns, first linear term)."""
+    arrs = [_u32(c) for c in cols]
+    idx = _u32([t[0] for t in terms])
+    vals = _u32(np.asarray([t[1] for t in terms], np.uint32).reshape(-1))
+    alps = _u32(np.asarray([t[2] for t in terms], np.uint32).reshape(-1))
+    outs = [np.zeros(1 << log_n, np.uint32) for _ in range(4)]
+    first = np.zeros(4, np.uint32)
+    pt = _u32(np.asarray(point, np.uint32).reshape(-1))
+    rc = lib().oracle_accumulate_numerators(_ptrs(arrs), C.c_uint32(len(arrs)), C.c_uint32(log_n), _p(pt), _p(idx),
+                                            _p(vals), _p(alps), C.c_uint32(len(terms)), _ptrs(outs), _p(first))
+    if rc != 0:
+        raise RuntimeError("oracle: accumulate_numerators failed")
+    return outs, first
+
+
+def compute_quotients_and_combine(accs, lifting_log: int):
+    """accs = [(point (8 words), 4 partial columns, first linear term (4)), ...]."""
+    pts = _u32(np.asarray([a[0] for a in accs], np.uint32).reshape(-1))
+    parts = [_u32(c) for a in accs for c in a[1]]
+    logs = _u32([int(a[1][0].size).bit_length() - 1 for a in accs])
+    firsts = _u32(np.asarray([a[2] for a in accs], np.uint32).reshape(-1))
+    outs = [np.zeros(1 << lifting_log, np.uint32) for _ in range(4)]
+    rc = lib().oracle_compute_quotients_and_combine(_p(pts), _ptrs(parts), _p(logs), _p(firsts),
+                                                    C.c_uint32(len(accs)), C.c_uint32(lifting_log), _ptrs(outs))
+    if rc != 0:
+        raise RuntimeError("oracle: compute_quotients_and_combine failed")
+    return outs
+
+
+def lift_and_accumulate(cols4_list):
+    """cols4_list: secure columns (4 coordinate arrays each), strictly increasing sizes."""
+    arrs = [_u32(c) for cols4 in cols4_list for c in cols4]
+    logs = _u32([int(c4[0].size).bit_length() - 1 for c4 in cols4_list])
+    outs = [np.zeros(cols4_list[-1][0].size, np.uint32) for _ in range(4)]
+    if lib().oracle_lift_and_accumulate(_ptrs(arrs), _p(logs), C.c_uint32(len(cols4_list)), _ptrs(outs)) != 0:
+        raise RuntimeError("oracle: lift_and_accumulate failed")
+    return outs
+
+
+def accumulate(col4, other4):
+    out = [np.array(c, dtype=np.uint32) for c in col4]
+    oth = [_u32(c) for c in other4]
+    lib().oracle_accumulate(_ptrs(out), _ptrs(oth), C.c_size_t(out[0].size))
+    return out
+
+
+def generate_secure_powers(felt, n: int) -> np.ndarray:
+    f = _u32(np.asarray(felt, np.uint32).reshape(-1))
+    out = np.zeros(4 * n, np.uint32)
+    lib().oracle_generate_secure_powers(_p(f), C.c_uint32(n), _p(out))
+    return out.reshape(n, 4)
+
+
+def eval_at_secure_point(coeffs, point) -> np.ndarray:
+    c = _u32(coeffs)
+    pt = _u32(np.asarray(point, np.uint32).reshape(-1))
+    out = np.zeros(4, np.uint32)
+    lib().oracle_eval_at_secure_point(_p(c), C.c_uint32(int(c.size).bit_length() - 1), _p(pt), _p(out))
+    return out
+
+
 class ChannelState(C.Structure):
     _fields_ = [("digest", C.c_uint8 * 32), ("n_draws", C.c_uint32), ("m31", C.c_int32)]
 

@@ -32,7 +32,8 @@ def _stale(target: str, deps) -> bool:
 def build(verbose: bool = False, jobs: int = 8) -> str:
     os.makedirs(OBJ, exist_ok=True)
     sources = sorted(glob.glob(os.path.join(CSRC, "*.cu")))
-    headers = glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(HERE, "..", "include", "*.h"))
+    headers = (glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(CSRC, "*.hpp")) +
+               glob.glob(os.path.join(HERE, "..", "include", "*.h")))
     objs, procs = [], []
     for src in sources:
         obj = os.path.join(OBJ, os.path.basename(src) + ".o")

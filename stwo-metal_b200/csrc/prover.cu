@@ -19,6 +19,8 @@
 #include "channel.hpp"
 #include "common.cuh"
 #include "field.cuh"
+#include "pcs.hpp"
+#include "rowops.cuh"
 #include "stream.cuh"
 
 namespace stwo_b200 {
@@ -29,36 +31,6 @@ int build_node_layers_impl(const uint8_t* in, uint32_t in_log, uint32_t stop_log
                            uint8_t* const* outs_by_log, cudaStream_t s, char* err, size_t err_len);
 
 // ----------------------------------------------------------------- kernels --
-
-// Exact M31 dot products: products of words <= P with canonical weights
-// (<= P (P - 1)) are summed in 64 bits and folded with 2^31 = 1 (mod P) every
-// four terms (a folded value is < 2^33 + 2^31, and that plus four products
-// stays below 2^64), then reduced once to the canonical value.  The residue is exact, so the result equals the
-// canonical value SimdBackend's reduced-per-operation arithmetic produces.
-__device__ __forceinline__ uint64_t fold64(uint64_t x) { return (x & M31_P) + (x >> 31); }  // < 2^34
-__device__ __forceinline__ uint32_t reduce_acc(uint64_t x) {
-  x = fold64(fold64(x));  // < P + 8
-  uint32_t y = (uint32_t)x;
-  return y >= M31_P ? y - M31_P : y;
-}
-struct acc4 {
-  uint64_t a, b, c, d;
-};
-__device__ __forceinline__ void acc4_mad(acc4& s, const qm31& w, uint32_t v) {
-  s.a += (uint64_t)w.a * v;
-  s.b += (uint64_t)w.b * v;
-  s.c += (uint64_t)w.c * v;
-  s.d += (uint64_t)w.d * v;
-}
-__device__ __forceinline__ void acc4_fold(acc4& s) {
-  s.a = fold64(s.a);
-  s.b = fold64(s.b);
-  s.c = fold64(s.c);
-  s.d = fold64(s.d);
-}
-__device__ __forceinline__ qm31 acc4_reduce(const acc4& s) {
-  return {reduce_acc(s.a), reduce_acc(s.b), reduce_acc(s.c), reduce_acc(s.d)};
-}
 
 // One thread per row: col[i+2] = col[i]^2 + col[i+1]^2 (wide_fibonacci/mod.rs:27-50).
 // `rows` rows from a/b; column c of the trace at cols + c * stride.
@@ -75,11 +47,6 @@ __global__ void wide_fib_trace_kernel(const uint32_t* __restrict__ a, const uint
       y = z;
     }
   }
-}
-
-__device__ __forceinline__ uint4 ldg4(const uint32_t* p) { return __ldg(reinterpret_cast<const uint4*>(p)); }
-__device__ __forceinline__ uint32_t u4get(const uint4& v, int r) {
-  return r == 0 ? v.x : r == 1 ? v.y : r == 2 ? v.z : v.w;
 }
 
 // Composition evaluation at every point of the evaluation domain
@@ -149,15 +116,6 @@ __global__ void __launch_bounds__(256) composition4_kernel(const uint32_t* __res
     *reinterpret_cast<uint4*>(out + 3 * n_points + i) = make_uint4(v[0].d, v[1].d, v[2].d, v[3].d);
   }
 }
-
-// Polynomial values at one secure point: sum_j coeff_j * w_j where
-// w_j = prod over set bits b of j of f_b, f = [y, x, pi(x), pi^2(x), ...]
-// (the coefficient fold of prover/backend/cpu/circle.rs:82-99), w_j =
-// w_hi[j >> h] * w_lo[j & (2^h - 1)]; see oods_eval_kernel.
-constexpr int kMaxPolys = 1024;
-struct PolyTable {
-  const uint32_t* p[kMaxPolys];
-};
 
 // OODS sampling for every polynomial of one size: the block stages the
 // weights w_j of a 1024-index chunk in shared memory, then each warp takes one
@@ -238,6 +196,23 @@ __global__ void __launch_bounds__(256) oods_reduce_kernel(const qm31* __restrict
     __syncthreads();
   }
   if (threadIdx.x == 0) out[p] = red[0];
+}
+
+uint32_t poly_eval_chunks(uint32_t lg) { return lg > 10 ? 1u << (lg - 10) : 1u; }  // kOodsChunk indices each
+
+int launch_poly_eval(const uint32_t* const* polys, uint32_t n_polys, uint32_t lg, const qm31* d_w_lo,
+                     const qm31* d_w_hi, qm31* d_partial, qm31* d_out, cudaStream_t s, char* err, size_t err_len) {
+  STWO_ARG_CHECK(n_polys >= 1 && n_polys <= (uint32_t)kMaxPolys && lg <= 30, "poly eval: bad shape");
+  PolyTable pt;
+  for (uint32_t c = 0; c < n_polys; c++) pt.p[c] = polys[c];
+  const uint32_t chunks = poly_eval_chunks(lg);
+  // about 4 waves of 148 SMs x 6 resident blocks, at least 8 polynomials (one per warp) per group
+  const uint32_t groups = std::max(1u, std::min({8u, (4u * 148u * 6u + chunks - 1) / chunks, n_polys / 8u}));
+  oods_eval_kernel<<<dim3(chunks, groups), 256, 0, s>>>(pt, n_polys, lg, lg / 2, d_w_lo, d_w_hi, d_partial);
+  STWO_CHECK_LAUNCH();
+  oods_reduce_kernel<<<n_polys, 256, 0, s>>>(d_partial, chunks, d_out);
+  STWO_CHECK_LAUNCH();
+  return STWO_B200_OK;
 }
 
 // FRI quotient of one sample batch (all columns sampled at point z, same
@@ -571,6 +546,19 @@ __global__ void grind_kernel(Digest8 pre, uint32_t hi, uint32_t low_base, uint32
   if (tz >= bits) atomicMin(found, low);
 }
 
+// Nonces (hi << 32) | (low_base + t), t < count (a multiple of 256): the
+// smallest hit is atomicMin'ed into *d_found (which the caller sets to
+// 0xFFFFFFFF first).
+int launch_grind(const uint32_t pre[8], uint32_t hi, uint32_t low_base, uint32_t count, uint32_t bits, int m31,
+                 uint32_t* d_found, cudaStream_t s, char* err, size_t err_len) {
+  STWO_ARG_CHECK(count % 256 == 0 && count > 0, "grind batch must be a positive multiple of 256");
+  Digest8 d;
+  for (int k = 0; k < 8; k++) d.w[k] = pre[k];
+  grind_kernel<<<count / 256, 256, 0, s>>>(d, hi, low_base, bits, m31, d_found);
+  STWO_CHECK_LAUNCH();
+  return STWO_B200_OK;
+}
+
 __global__ void gather_kernel(const uint64_t* __restrict__ addrs, uint32_t n, uint32_t* __restrict__ out) {
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) out[i] = *reinterpret_cast<const uint32_t*>(addrs[i]);
@@ -760,6 +748,26 @@ __global__ void fs_composition_kernel(DevChannel* ch, const uint8_t* root, uint3
   for (uint32_t k = threadIdx.x; k < n_cons; k += blockDim.x) pw[n_cons - 1 - k] = qm31_pow_u32(s_rc, k);
 }
 
+// Weight tables of oods_eval_kernel from the fold factors f[0..lg) (shared
+// memory, written before a block barrier): w_lo[t] = prod over set bits b of t
+// of f[b] (t < 2^h), w_hi[t] = prod over set bits b of t of f[h + b].
+__device__ void build_eval_weights(const qm31* f, uint32_t lg, uint32_t h, qm31* __restrict__ w_lo,
+                                   qm31* __restrict__ w_hi) {
+  const uint32_t hi_bits = lg - h;
+  for (uint32_t t = threadIdx.x; t < (1u << h); t += blockDim.x) {
+    qm31 w = qm31_one();
+    for (uint32_t b = 0; b < h; b++)
+      if ((t >> b) & 1) w = qm31_mul(w, f[b]);
+    w_lo[t] = w;
+  }
+  for (uint32_t t = threadIdx.x; t < (1u << hi_bits); t += blockDim.x) {
+    qm31 w = qm31_one();
+    for (uint32_t b = 0; b < hi_bits; b++)
+      if ((t >> b) & 1) w = qm31_mul(w, f[h + b]);
+    w_hi[t] = w;
+  }
+}
+
 // Composition root -> OODS point ((1 - t^2) / (1 + t^2), 2t / (1 + t^2)), its
 // fold factors f = [y, x, pi(x), ...] and the weight tables of
 // oods_eval_kernel (w_lo over f[0..h), w_hi over f[h..lg)).
@@ -784,20 +792,33 @@ __global__ void fs_oods_kernel(DevChannel* ch, const uint8_t* root, uint32_t lg,
     }
   }
   __syncthreads();
-  const uint32_t hi_bits = lg - h;
-  for (uint32_t t = threadIdx.x; t < (1u << h); t += blockDim.x) {
-    qm31 w = qm31_one();
-    for (uint32_t b = 0; b < h; b++)
-      if ((t >> b) & 1) w = qm31_mul(w, f[b]);
-    w_lo[t] = w;
-  }
-  for (uint32_t t = threadIdx.x; t < (1u << hi_bits); t += blockDim.x) {
-    qm31 w = qm31_one();
-    for (uint32_t b = 0; b < hi_bits; b++)
-      if ((t >> b) & 1) w = qm31_mul(w, f[h + b]);
-    w_hi[t] = w;
-  }
+  build_eval_weights(f, lg, h, w_lo, w_hi);
 }
+
+// The weight tables of oods_eval_kernel for an explicit point z
+// (PolyOps::batch_eval_at_point): f = [y, x, pi(x), ...] of z, then as above.
+__global__ void eval_weights_kernel(spoint z, uint32_t lg, uint32_t h, qm31* __restrict__ w_lo,
+                                    qm31* __restrict__ w_hi) {
+  __shared__ qm31 f[32];
+  if (threadIdx.x == 0) {
+    f[0] = z.y;
+    qm31 xx = z.x;
+    for (uint32_t b = 1; b < lg; b++) {
+      f[b] = xx;
+      xx = qm31_double_x(xx);
+    }
+  }
+  __syncthreads();
+  build_eval_weights(f, lg, h, w_lo, w_hi);
+}
+
+int launch_eval_weights(const spoint& z, uint32_t lg, qm31* d_w_lo, qm31* d_w_hi, cudaStream_t s, char* err,
+                        size_t err_len) {
+  eval_weights_kernel<<<1, 1024, 0, s>>>(z, lg, lg / 2, d_w_lo, d_w_hi);
+  STWO_CHECK_LAUNCH();
+  return STWO_B200_OK;
+}
+
 
 // Sampled values -> quotient random coefficient q, its powers ap[k] = q^k and
 // the row constants (pcs/quotient_ops.rs:134-233 in the form of
@@ -1812,18 +1833,12 @@ int WideFibProver::prove_body(const uint32_t* d_a, const uint32_t* d_b, ProofOut
     phase(kOodsSampling);
     fs_oods_kernel<<<1, 1024, 0, s>>>(d_chan, t2.layer(0), lg, h, d_small, d_small + (1u << h), d_fs);
     STWO_CHECK_LAUNCH();
-    PolyTable pt;
-    for (uint32_t c = 0; c < N; c++) pt.p[c] = coeff_ptrs[c];
-    for (int k = 0; k < 8; k++) pt.p[N + k] = split[k];
-    const uint32_t chunks = lg > 10 ? 1u << (lg - 10) : 1u;  // kOodsChunk indices each
+    std::vector<const uint32_t*> polys(coeff_ptrs.begin(), coeff_ptrs.begin() + N);
+    for (int k = 0; k < 8; k++) polys.push_back(split[k]);
     d_vals = d_small + n_w;
-    // about 4 waves of 148 SMs x 6 resident blocks, at least 8 polynomials (one per warp) per group
-    const uint32_t groups = std::max(1u, std::min({8u, (4u * 148u * 6u + chunks - 1) / chunks, np / 8u}));
-    oods_eval_kernel<<<dim3(chunks, groups), 256, 0, s>>>(pt, np, lg, h, d_small, d_small + (1u << h),
-                                                          d_oods_partial);
-    STWO_CHECK_LAUNCH();
-    oods_reduce_kernel<<<np, 256, 0, s>>>(d_oods_partial, chunks, d_vals);
-    STWO_CHECK_LAUNCH();
+    if ((rc = launch_poly_eval(polys.data(), np, lg, d_small, d_small + (1u << h), d_oods_partial, d_vals, s, err,
+                               err_len)))
+      return rc;
   }
 
   // ---- FRI quotients (pcs/mod.rs:112-118, quotient_ops.rs:134-233) ----
@@ -2039,8 +2054,7 @@ int WideFibProver::prove_body(const uint32_t* d_a, const uint32_t* d_b, ProofOut
     for (uint32_t hi = 0; !found; hi++) {
       for (uint32_t base = 0; base < (1u << 20) && !found; base += 1u << 16) {
         STWO_CUDA_TRY(cudaMemsetAsync(d_found, 0xFF, 4, s));
-        grind_kernel<<<(1u << 16) / 256, 256, 0, s>>>(d, hi, base, cfg.pow_bits, m31, d_found);
-        STWO_CHECK_LAUNCH();
+        if ((rc = launch_grind(d.w, hi, base, 1u << 16, cfg.pow_bits, m31, d_found, s, err, err_len))) return rc;
         uint32_t* hf = reinterpret_cast<uint32_t*>(h_pinned) + (h_pinned_bytes / 4 - 1);
         STWO_CUDA_TRY(cudaMemcpyAsync(hf, d_found, 4, cudaMemcpyDeviceToHost, s));
         STWO_CUDA_TRY(cudaStreamSynchronize(s));

@@ -269,12 +269,122 @@ class B200Backend:
                  C.c_uint32(tree.log_size), self.stream)
         return dst
 
+    # ---- QuotientOps ----------------------------------------------------------
+    def accumulate_numerators(self, cols, batches):
+        """QuotientOps::accumulate_numerators over same-size columns; batches =
+        [(point (8 words), [(column index, value (4), random coeff (4)), ...])].
+        Returns [(partial numerator SecureColumn, first linear term (4,))]."""
+        log_n = cols[0].log_size
+        cb = (SampleBatch * max(1, len(batches)))()
+        keep, outs = [], []
+        for b, (point, terms) in enumerate(batches):
+            arr = (NumeratorTerm * max(1, len(terms)))()
+            for k, (idx, val, alpha) in enumerate(terms):
+                arr[k].column_index = int(idx)
+                arr[k].sample_value = _words(val, 4)
+                arr[k].random_coeff = _words(alpha, 4)
+            keep.append(arr)
+            cb[b].point = _words(point, 8)
+            cb[b].terms = C.cast(arr, C.POINTER(NumeratorTerm))
+            cb[b].n_terms = len(terms)
+            outs.append(SecureColumn.empty(1 << log_n, self.stream))
+        first = (C.c_uint32 * (4 * max(1, len(batches))))()
+        ffi.call("stwo_b200_accumulate_numerators", _ptr_array(cols), C.c_uint32(len(cols)), C.c_uint32(log_n), cb,
+                 C.c_uint32(len(batches)), _ptr_array([c for o in outs for c in o.cols]), first, self.stream)
+        return [(o, np.array(first[4 * b:4 * b + 4], np.uint32)) for b, o in enumerate(outs)]
+
+    def compute_quotients_and_combine(self, accs, lifting_log_size: int) -> SecureColumn:
+        """accs = [(point (8 words), partial numerator SecureColumn, first linear term (4))]."""
+        arr = (AccumulatedNumeratorsC * max(1, len(accs)))()
+        for z, (point, col, first) in enumerate(accs):
+            arr[z].sample_point = _words(point, 8)
+            arr[z].d_partial = (C.c_void_p * 4)(*[c.ptr for c in col.cols])
+            arr[z].log_size = col.cols[0].log_size
+            arr[z].first_linear_term = _words(first, 4)
+        out = SecureColumn.empty(1 << lifting_log_size, self.stream)
+        ffi.call("stwo_b200_compute_quotients_and_combine", arr, C.c_uint32(len(accs)), C.c_uint32(lifting_log_size),
+                 _ptr_array(out.cols), self.stream)
+        return out
+
+    # ---- AccumulationOps --------------------------------------------------------
+    def accumulate(self, col: SecureColumn, other: SecureColumn):
+        ffi.call("stwo_b200_accumulate", _ptr_array(col.cols), _ptr_array(other.cols), C.c_uint64(col.length),
+                 self.stream)
+        return col
+
+    def generate_secure_powers(self, felt, n: int) -> np.ndarray:
+        buf = DeviceBuffer(16 * max(1, n), self.stream)
+        ffi.call("stwo_b200_generate_secure_powers", _words(felt, 4), C.c_uint32(n), C.c_void_p(buf.ptr),
+                 self.stream)
+        return buf.download(np.uint32, 4 * n).reshape(n, 4)
+
+    def lift_and_accumulate(self, cols, out: SecureColumn | None = None) -> SecureColumn:
+        out = SecureColumn.empty(cols[-1].length, self.stream) if out is None else out
+        ffi.call("stwo_b200_lift_and_accumulate", _ptr_array([c for sc in cols for c in sc.cols]),
+                 _u32_array([sc.cols[0].log_size for sc in cols]), C.c_uint32(len(cols)), _ptr_array(out.cols),
+                 self.stream)
+        return out
+
+    # ---- PolyOps::eval_at_point -----------------------------------------------
+    def batch_eval_at_point(self, polys, point) -> np.ndarray:
+        out = (C.c_uint32 * (4 * max(1, len(polys))))()
+        ffi.call("stwo_b200_batch_eval_at_point", _ptr_array(polys), C.c_uint32(len(polys)),
+                 C.c_uint32(polys[0].log_size if polys else 0), _words(point, 8), out, self.stream)
+        return np.array(out[:4 * len(polys)], np.uint32).reshape(len(polys), 4)
+
+    def eval_at_point(self, poly: DeviceColumn, point) -> np.ndarray:
+        out = (C.c_uint32 * 4)()
+        ffi.call("stwo_b200_eval_at_point", C.c_void_p(poly.ptr), C.c_uint32(poly.log_size), _words(point, 8), out,
+                 self.stream)
+        return np.array(out[:], np.uint32)
+
+    # ---- GrindOps ---------------------------------------------------------------
+    def grind(self, digest: bytes, pow_bits: int, m31_channel: bool = False) -> int:
+        d = (C.c_uint8 * 32).from_buffer_copy(bytes(digest))
+        nonce = C.c_uint64()
+        ffi.call("stwo_b200_grind", d, C.c_uint32(pow_bits), C.c_int(int(m31_channel)), C.byref(nonce), self.stream)
+        return nonce.value
+
+    # ---- ColumnOps<SecureField> -------------------------------------------------
+    def bit_reverse_secure_column(self, col: SecureColumn):
+        ffi.call("stwo_b200_bit_reverse_secure_column", _ptr_array(col.cols), C.c_uint32(col.cols[0].log_size),
+                 self.stream)
+        return col
+
+    def bit_reverse_secure_field(self, buf: DeviceBuffer, log_size: int):
+        """In place, on QM31 values stored 4 words each."""
+        ffi.call("stwo_b200_bit_reverse_secure_field", C.c_void_p(buf.ptr), C.c_uint32(log_size), self.stream)
+        return buf
+
     def decompose(self, ev: SecureColumn):
         out = SecureColumn.empty(ev.length, self.stream)
         lam = (C.c_uint32 * 4)()
         ffi.call("stwo_b200_decompose", _ptr_array(ev.cols), C.c_uint32(ev.cols[0].log_size), _ptr_array(out.cols),
                  lam, self.stream)
         return out, np.array(list(lam), np.uint32)
+
+
+# ---- C structures of the QuotientOps entry points ---------------------------
+class NumeratorTerm(C.Structure):
+    """stwo_b200_numerator_term (core/pcs/quotients.rs:63-71 NumeratorData)."""
+    _fields_ = [("column_index", C.c_uint32), ("sample_value", C.c_uint32 * 4), ("random_coeff", C.c_uint32 * 4)]
+
+
+class SampleBatch(C.Structure):
+    """stwo_b200_sample_batch (core/pcs/quotients.rs:55-61 ColumnSampleBatch)."""
+    _fields_ = [("point", C.c_uint32 * 8), ("terms", C.POINTER(NumeratorTerm)), ("n_terms", C.c_uint32)]
+
+
+class AccumulatedNumeratorsC(C.Structure):
+    """stwo_b200_accumulated_numerators (prover/pcs/quotient_ops.rs:48-74)."""
+    _fields_ = [("sample_point", C.c_uint32 * 8), ("d_partial", C.c_void_p * 4), ("log_size", C.c_uint32),
+                ("first_linear_term", C.c_uint32 * 4)]
+
+
+def _words(v, n):
+    a = np.asarray(v, dtype=np.uint32).reshape(-1)
+    assert a.size == n
+    return (C.c_uint32 * n)(*[int(x) for x in a])
 
 
 def layer_to_host(buf: DeviceBuffer) -> np.ndarray:
