@@ -26,3 +26,14 @@ def test_init_fails_loudly_without_gpu():
         pytest.skip("GPU present")
     with pytest.raises(ffi.B200Error):
         ffi.call("stwo_b200_init", ctypes.c_int(0))
+
+
+def test_integration_binding_declares_every_entry_point():
+    # the Rust extern block a maintainer adds covers the whole header
+    import os
+    import re
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    text = open(os.path.join(root, "INTEGRATION.md")).read()
+    bound = set(re.findall(r"pub fn (stwo_b200_[a-z0-9_]+)\s*\(", text))
+    missing = [n for n in ffi.declared_symbols() if n not in bound]
+    assert not missing, missing
