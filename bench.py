@@ -17,8 +17,10 @@ Workloads (seeded synthetic M31 data, values uniform in [0, P)):
   fri_heavy      one QM31 column of log 24: FRI commit + 70-query decommit.
   serving        Poisson stream of Wide-Fibonacci requests (p50/p99 latency).
   trace_fft      the prover's trace transforms alone (--n-cols x 2^--log-n-rows,
-                 interpolate, then evaluate at blowup 1): the kernels' profile
-                 target.
+                 interpolate, then evaluate at --log-blowup): the kernels'
+                 profile target.
+  fri_fold       the stand-alone FriOps folds at log 24 (fold_circle_into_line,
+                 fold_line) against HBM: their profile target.
 
 The default line also carries, measured in the same run at N = 1, the uneven
 commit's per-column / batched / graph forms and the FRI-heavy commit with the
@@ -1189,11 +1191,9 @@ def extra_commit_uneven(args, stream, world, hbm_peak, probe_rate):
 def extra_fri_heavy(args, stream, world, hbm_peak, probe_rate):
     """FRI-heavy commit + decommit (log 24, 70 queries) and the stand-alone
     FriOps folds at log 24 against HBM."""
-    import ctypes
     import hashlib
-    import torch
-    from stwo_b200 import B200Backend, DeviceColumn, SeededFriProver, ffi
-    from stwo_b200.backend import _ptr_array, _u32_array, canonic_half_coset
+    from stwo_b200 import B200Backend, DeviceColumn, SeededFriProver
+    from stwo_b200.backend import canonic_half_coset
     coords, alphas, queries = fri_heavy_inputs()
     be = B200Backend(stream.cuda_stream)
     init, lg = canonic_half_coset(FRI_LOG + 1)
@@ -1208,33 +1208,8 @@ def extra_fri_heavy(args, stream, world, hbm_peak, probe_rate):
     ms = max_over_ranks(time_region(stream, lambda: fp.prove(dev, alphas, queries), steps), world)
     fp.close()
     golden = load_digests().get("fri_heavy_sha256")
-    # stand-alone folds: FriOps::fold_circle_into_line (2^24 -> 2^23) and
-    # FriOps::fold_line (2^23 -> 2^22), one thread per output
-    n = 1 << FRI_LOG
-    line = [DeviceColumn(n >> 1, stream.cuda_stream) for _ in range(4)]
-    out = [DeviceColumn(n >> 2, stream.cuda_stream) for _ in range(4)]
-    sp = ctypes.c_void_p(stream.cuda_stream)
-    a0 = _u32_array(alphas[0])
-
-    def circle():
-        ffi.call("stwo_b200_fold_circle_into_line", _ptr_array(line), _ptr_array(dev), ctypes.c_uint32(FRI_LOG),
-                 ctypes.c_uint64(half_init), a0, ctypes.c_void_p(tree.itwiddles.ptr), ctypes.c_uint32(tree.log_size), sp)
-
-    def fold():
-        ffi.call("stwo_b200_fold_line", _ptr_array(line), ctypes.c_uint32(FRI_LOG - 1), a0, ctypes.c_uint32(1),
-                 ctypes.c_void_p(tree.itwiddles.ptr), ctypes.c_uint32(tree.log_size), _ptr_array(out), sp)
-
-    for _ in range(3):
-        circle()
-        fold()
-    c_ms = time_region(stream, circle, 20)
-    f_ms = time_region(stream, fold, 20)
-    # algorithmic bytes: circle fold reads 16 B per input and reads + writes
-    # 16 B per output (dst <- dst * alpha^2 + f'); line fold reads 16 B per
-    # input and writes 16 B per output
-    c_bytes = 16 * n + 32 * (n >> 1)
-    f_bytes = 16 * (n >> 1) + 16 * (n >> 2)
-    for x in dev + line + out:
+    folds = standalone_fold_roofline(stream, tree, dev, alphas[0], half_init, hbm_peak, steps=20)
+    for x in dev:
         x.close()
     tree.twiddles.close()
     tree.itwiddles.close()
@@ -1245,16 +1220,88 @@ def extra_fri_heavy(args, stream, world, hbm_peak, probe_rate):
         "ms_per_step": ms, "folded_elements_per_s": fri_units() / (ms * 1e-3),
         "trees_vs_blake2s_ceiling": compressions / (ms * 1e-3) / probe_rate,
         "bit_exact_vs_oracle": (hashlib.sha256(proof).hexdigest() == golden) if golden else "no oracle digest",
-        "fold_roofline": {
-            "fold_circle_into_line_log24": {"ms": c_ms, "alg_bytes": c_bytes,
-                                            "achieved_gbs": c_bytes / (c_ms * 1e-3) / 1e9,
-                                            "frac": c_bytes / (c_ms * 1e-3) / (hbm_peak * 1e9)},
-            "fold_line_log23": {"ms": f_ms, "alg_bytes": f_bytes, "achieved_gbs": f_bytes / (f_ms * 1e-3) / 1e9,
-                                "frac": f_bytes / (f_ms * 1e-3) / (hbm_peak * 1e9)},
-            "peak": hbm_peak, "unit": "GB/s",
-            "kernels": "fold_circle_kernel, fold_line_kernel (the FriOps entry points; the prover's fused "
-                       "fold + next-layer leaf hash kernels are in phase_roofline_frac)"},
+        "fold_roofline": folds,
     }
+
+
+def standalone_fold_roofline(stream, tree, dev, alpha, half_init, hbm_peak, steps=20):
+    """FriOps::fold_circle_into_line (2^k -> 2^(k-1), k = log size of `dev`)
+    and FriOps::fold_line (2^(k-1) -> 2^(k-2)) through the C ABI, each timed
+    alone with CUDA events, against HBM."""
+    import ctypes
+    from stwo_b200 import DeviceColumn, ffi
+    from stwo_b200.backend import _ptr_array, _u32_array
+    log_n = dev[0].log_size
+    n = 1 << log_n
+    line = [DeviceColumn(n >> 1, stream.cuda_stream) for _ in range(4)]
+    out = [DeviceColumn(n >> 2, stream.cuda_stream) for _ in range(4)]
+    sp = ctypes.c_void_p(stream.cuda_stream)
+    a0 = _u32_array(alpha)
+
+    def circle():
+        ffi.call("stwo_b200_fold_circle_into_line", _ptr_array(line), _ptr_array(dev), ctypes.c_uint32(log_n),
+                 ctypes.c_uint64(half_init), a0, ctypes.c_void_p(tree.itwiddles.ptr), ctypes.c_uint32(tree.log_size), sp)
+
+    def fold():
+        ffi.call("stwo_b200_fold_line", _ptr_array(line), ctypes.c_uint32(log_n - 1), a0, ctypes.c_uint32(1),
+                 ctypes.c_void_p(tree.itwiddles.ptr), ctypes.c_uint32(tree.log_size), _ptr_array(out), sp)
+
+    for _ in range(3):
+        circle()
+        fold()
+    c_ms = time_region(stream, circle, steps)
+    f_ms = time_region(stream, fold, steps)
+    # algorithmic bytes: the circle fold reads 16 B per input and reads and
+    # writes 16 B per output (dst <- dst * alpha^2 + f'); the line fold reads
+    # 16 B per input and writes 16 B per output
+    c_bytes = 16 * n + 32 * (n >> 1)
+    f_bytes = 16 * (n >> 1) + 16 * (n >> 2)
+    for x in line + out:
+        x.close()
+    return {
+        f"fold_circle_into_line_log{log_n}": {"ms": c_ms, "alg_bytes": c_bytes,
+                                              "achieved_gbs": c_bytes / (c_ms * 1e-3) / 1e9,
+                                              "frac": c_bytes / (c_ms * 1e-3) / (hbm_peak * 1e9)},
+        f"fold_line_log{log_n - 1}": {"ms": f_ms, "alg_bytes": f_bytes, "achieved_gbs": f_bytes / (f_ms * 1e-3) / 1e9,
+                                      "frac": f_bytes / (f_ms * 1e-3) / (hbm_peak * 1e9)},
+        "peak": hbm_peak, "unit": "GB/s",
+        "kernels": "fold_circle_kernel, fold_line_kernel (the FriOps entry points; the prover's fused fold + "
+                   "next-layer leaf hash kernels are in phase_roofline_frac)",
+    }
+
+
+def run_fri_fold_b200(args, world, rank, local):
+    """The stand-alone FriOps folds at the FRI-heavy size (one QM31 column of
+    log 24): the HBM-streaming kernels alone, for their roofline and profile."""
+    import torch
+    from stwo_b200 import B200Backend, DeviceColumn, ffi
+    from stwo_b200.backend import canonic_half_coset
+    torch.cuda.set_device(local)
+    ffi.init(local)
+    stream = torch.cuda.Stream()
+    be = B200Backend(stream.cuda_stream)
+    coords, alphas, _ = fri_heavy_inputs()
+    init, lg = canonic_half_coset(FRI_LOG + 1)
+    tree = be.precompute_twiddles(init, lg)
+    dev = [DeviceColumn.from_host(c, stream.cuda_stream) for c in coords]
+    torch.cuda.synchronize()
+    launches0 = ffi.launch_count()
+    r = standalone_fold_roofline(stream, tree, dev, alphas[0], canonic_half_coset(FRI_LOG)[0], load_peaks()[0],
+                                 steps=args.steps)
+    launches = ffi.launch_count() - launches0
+    if rank != 0:
+        return
+    c = r[f"fold_circle_into_line_log{FRI_LOG}"]
+    units = 1 << FRI_LOG
+    print(json.dumps({
+        "metric": METRIC, "value": replica_rate(units, c["ms"], world), "unit": "folded QM31 elements/s",
+        "n_gpus": world, "steps": args.steps, "warmup": 3, "ms_per_step": c["ms"], "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u32 (M31/QM31)", "data": "synthetic (seeded numpy PCG64)",
+        "config": {"workload": "fri_fold", "log_size": FRI_LOG, "parallelism": f"replicas x{world}"},
+        "gpu_launches": launches, "roofline": {"bound": "hbm", "kernel": "fold_circle_kernel",
+                                               "achieved": c["achieved_gbs"], "peak": r["peak"], "unit": "GB/s",
+                                               "frac": c["frac"], "traffic": None, "alg_bytes_per_step": c["alg_bytes"]},
+        "folds": r}), flush=True)
 
 
 # ------------------------------------------------------------- trace FFT ----
@@ -1268,23 +1315,23 @@ def run_trace_fft_b200(args, world, rank, local):
     2^log_n bit-reversed evaluations into coefficients, then evaluate them on
     the blowup-1 domain, through the batched C ABI calls the prover makes."""
     import torch
-    from stwo_b200 import B200Backend, DeviceColumn, ffi
+    from stwo_b200 import B200Backend, DeviceColumn, ffi, fft_get_plan
     from stwo_b200.backend import canonic_half_coset
     torch.cuda.set_device(local)
     ffi.init(local)
     stream = torch.cuda.Stream()
     be = B200Backend(stream.cuda_stream)
-    log_n, nc = args.log_n_rows, args.n_cols
-    init, lg = canonic_half_coset(log_n + 2)
+    log_n, nc, lb = args.log_n_rows, args.n_cols, args.log_blowup
+    init, lg = canonic_half_coset(log_n + lb + 1)
     tree = be.precompute_twiddles(init, lg)
     host = trace_fft_setup(args)
     evals = [DeviceColumn.from_host(host, stream.cuda_stream) for _ in range(nc)]
     coeffs = [DeviceColumn(1 << log_n, stream.cuda_stream) for _ in range(nc)]
-    outs = [DeviceColumn(1 << (log_n + 1), stream.cuda_stream) for _ in range(nc)]
+    outs = [DeviceColumn(1 << (log_n + lb), stream.cuda_stream) for _ in range(nc)]
     torch.cuda.synchronize()
     for _ in range(args.warmup):
         be.interpolate_columns_into(evals, coeffs, tree)
-        be.evaluate_polynomials_into(coeffs, 1, tree, outs)
+        be.evaluate_polynomials_into(coeffs, lb, tree, outs)
     torch.cuda.synchronize()
     evs = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
     ti = te = 0.0
@@ -1294,7 +1341,7 @@ def run_trace_fft_b200(args, world, rank, local):
             evs[0].record(stream)
             be.interpolate_columns_into(evals, coeffs, tree)
             evs[1].record(stream)
-            be.evaluate_polynomials_into(coeffs, 1, tree, outs)
+            be.evaluate_polynomials_into(coeffs, lb, tree, outs)
             evs[2].record(stream)
         torch.cuda.synchronize()
         ti += evs[0].elapsed_time(evs[1])
@@ -1305,18 +1352,21 @@ def run_trace_fft_b200(args, world, rank, local):
         return
     hbm_peak, peak_kind = load_peaks()
     n = 1 << log_n
-    alg_i, alg_e = 8 * nc * n, 4 * nc * n + 8 * nc * n
-    bflies = nc * log_n * (n // 2 + n)
+    alg_i, alg_e = 8 * nc * n, 4 * nc * n + 4 * nc * (n << lb)
+    bflies = nc * log_n * (n // 2 + (n << lb) // 2)
     cells = nc * n
     line = {
         "metric": METRIC, "value": replica_rate(cells, ti + te, world), "unit": "transformed trace cells/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ti + te,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32 (M31)",
         "data": "synthetic (seeded numpy PCG64)",
-        "config": {"workload": "trace_fft", "n_columns": nc, "log_n_rows": log_n, "log_blowup": 1,
+        "config": {"workload": "trace_fft", "n_columns": nc, "log_n_rows": log_n, "log_blowup": lb,
                    "parallelism": f"replicas x{world}"},
         "gpu_launches": launches,
         "interpolate_ms": ti, "evaluate_ms": te,
+        "pass_plan_layers": fft_get_plan(log_n),
+        "phase_hbm_frac": {"interpolate": alg_i / (ti * 1e-3) / (hbm_peak * 1e9),
+                           "evaluate": alg_e / (te * 1e-3) / (hbm_peak * 1e9)},
         "roofline": {"bound": "hbm", "kernel": "trace interpolate + evaluate", "achieved": (alg_i + alg_e) / ((ti + te) * 1e-3) / 1e9,
                      "peak": hbm_peak, "unit": "GB/s", "frac": (alg_i + alg_e) / ((ti + te) * 1e-3) / (hbm_peak * 1e9),
                      "peak_kind": peak_kind, "traffic": None, "alg_bytes_per_step": alg_i + alg_e},
@@ -1331,7 +1381,7 @@ def run_trace_fft_reference(args, world, rank):
     from oracle import ffi as oracle
     n_threads = oracle.set_threads(os.cpu_count() or 1)
     log_n = args.log_n_rows
-    init, lg = oracle.canonic_half_coset_root(log_n + 2)
+    init, lg = oracle.canonic_half_coset_root(log_n + args.log_blowup + 1)
     tw, itw = oracle.precompute_twiddles(init, lg)
     host = trace_fft_setup(args)
     k = max(1, min(args.n_cols, 8))  # a bounded sample of the columns per step
@@ -1339,7 +1389,7 @@ def run_trace_fft_reference(args, world, rank):
     for i in range(args.warmup + args.steps):
         t0 = time.perf_counter()
         co = oracle.interpolate_columns([host] * k, itw)
-        oracle.evaluate_columns(co, 1, tw)
+        oracle.evaluate_columns(co, args.log_blowup, tw)
         if i >= args.warmup:
             secs.append(time.perf_counter() - t0)
     med = statistics.median(secs)
@@ -1489,9 +1539,11 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="wide_fib_prove",
-                    choices=["wide_fib_prove", "commit_uneven", "commit_plain", "fri_heavy", "serving", "trace_fft"])
+                    choices=["wide_fib_prove", "commit_uneven", "commit_plain", "fri_heavy", "serving", "trace_fft",
+                             "fri_fold"])
     ap.add_argument("--log-n-rows", type=int, default=20, help="wide_fib_prove: log2 of the trace rows")
     ap.add_argument("--n-cols", type=int, default=100, help="wide_fib_prove: trace columns")
+    ap.add_argument("--log-blowup", type=int, default=1, help="trace_fft: log blowup of the evaluation")
     ap.add_argument("--no-extras", dest="extras", action="store_false",
                     help="wide_fib_prove: skip the uneven-commit and FRI-heavy measurements of the default line")
     args = ap.parse_args()
@@ -1510,6 +1562,13 @@ def main():
                                       "the oracle's per-proof rate is reported as cpu_baseline by the b200 arm"}))
             else:
                 run_serving_b200(args, world, rank, local)
+        elif args.workload == "fri_fold":
+            if args.impl == "reference":
+                if rank == 0:
+                    print(json.dumps({"impl": "reference", "unavailable": "kernel profile target; the oracle's "
+                                      "FRI rate is the fri_heavy workload's reference arm"}))
+            else:
+                run_fri_fold_b200(args, world, rank, local)
         elif args.workload == "trace_fft":
             if args.impl == "reference":
                 run_trace_fft_reference(args, world, rank)

@@ -69,6 +69,32 @@ __global__ void fold_line_kernel(Cols4 in, uint32_t log_m, uint32_t fold_step, F
   }
 }
 
+// fold_line with fold_step 1, two outputs per thread: the four inputs of
+// outputs 2k, 2k + 1 are one 16-byte load per coordinate, their twiddles one
+// 8-byte load, the outputs one 8-byte store per coordinate.  Same arithmetic
+// per output as fold_line_kernel.  Inputs 16-byte and outputs 8-byte aligned,
+// at least 2 outputs.
+__global__ void __launch_bounds__(256) fold_line2_kernel(Cols4 in, uint32_t log_m, qm31 alpha, const uint32_t* itw,
+                                                         uint64_t tw_len, Cols4W out) {
+  const uint64_t n_pairs = 1ull << (log_m - 2);
+  const uint32_t* lt = itw + (tw_len - (1ull << log_m));
+  for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < n_pairs;
+       k += (uint64_t)gridDim.x * blockDim.x) {
+    uint4 w[4];
+#pragma unroll
+    for (int c = 0; c < 4; c++) w[c] = __ldg(reinterpret_cast<const uint4*>(in.c[c]) + k);
+    const uint2 t = __ldg(reinterpret_cast<const uint2*>(lt) + k);
+    const qm31 f0x{w[0].x, w[1].x, w[2].x, w[3].x}, f0n{w[0].y, w[1].y, w[2].y, w[3].y};
+    const qm31 f1x{w[0].z, w[1].z, w[2].z, w[3].z}, f1n{w[0].w, w[1].w, w[2].w, w[3].w};
+    const qm31 v0 = qm31_add(qm31_add(f0x, f0n), qm31_mul(alpha, qm31_mul_m31(qm31_sub(f0x, f0n), t.x)));
+    const qm31 v1 = qm31_add(qm31_add(f1x, f1n), qm31_mul(alpha, qm31_mul_m31(qm31_sub(f1x, f1n), t.y)));
+    reinterpret_cast<uint2*>(out.c[0])[k] = make_uint2(v0.a, v1.a);
+    reinterpret_cast<uint2*>(out.c[1])[k] = make_uint2(v0.b, v1.b);
+    reinterpret_cast<uint2*>(out.c[2])[k] = make_uint2(v0.c, v1.c);
+    reinterpret_cast<uint2*>(out.c[3])[k] = make_uint2(v0.d, v1.d);
+  }
+}
+
 // Circle-layer inverse twiddle of pair i, derived from line layer 1 of the
 // source domain: [y, -y, -x, x] (simd/fft/mod.rs:61-97).
 __device__ __forceinline__ uint32_t circle_itw(const uint32_t* lt0, uint64_t i) {
@@ -94,6 +120,44 @@ __global__ void fold_circle_kernel(Cols4W dst, Cols4 src, uint32_t log_n, qm31 a
     qm31 d = load_q(dr, i);
     store_q(dst, i, qm31_add(qm31_mul(d, alpha_sq), fprime));
   }
+}
+
+// fold_circle_kernel, two outputs per thread (log_n > 4): the four source
+// values of outputs 2k, 2k + 1 are one 16-byte load per coordinate, dst one
+// 8-byte load and store.  The circle twiddles of outputs 2k, 2k + 1 are
+// [y, -y] or [-x, x] of one line-layer-1 entry (circle_itw).  Same arithmetic
+// per output as fold_circle_kernel.
+__global__ void __launch_bounds__(256) fold_circle2_kernel(Cols4W dst, Cols4 src, uint32_t log_n, qm31 alpha,
+                                                           qm31 alpha_sq, const uint32_t* itw, uint64_t tw_len) {
+  const uint64_t n_pairs = 1ull << (log_n - 2);
+  const uint32_t* lt0 = itw + (tw_len - (1ull << (log_n - 1)));
+  for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < n_pairs;
+       k += (uint64_t)gridDim.x * blockDim.x) {
+    uint4 w[4];
+    uint2 d[4];
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+      w[c] = __ldg(reinterpret_cast<const uint4*>(src.c[c]) + k);
+      d[c] = reinterpret_cast<const uint2*>(dst.c[c])[k];
+    }
+    const uint32_t y0 = circle_itw(lt0, 2 * k), y1 = circle_itw(lt0, 2 * k + 1);
+    const qm31 p0{w[0].x, w[1].x, w[2].x, w[3].x}, n0{w[0].y, w[1].y, w[2].y, w[3].y};
+    const qm31 p1{w[0].z, w[1].z, w[2].z, w[3].z}, n1{w[0].w, w[1].w, w[2].w, w[3].w};
+    const qm31 f0 = qm31_add(qm31_add(p0, n0), qm31_mul(alpha, qm31_mul_m31(qm31_sub(p0, n0), y0)));
+    const qm31 f1 = qm31_add(qm31_add(p1, n1), qm31_mul(alpha, qm31_mul_m31(qm31_sub(p1, n1), y1)));
+    const qm31 v0 = qm31_add(qm31_mul(qm31{d[0].x, d[1].x, d[2].x, d[3].x}, alpha_sq), f0);
+    const qm31 v1 = qm31_add(qm31_mul(qm31{d[0].y, d[1].y, d[2].y, d[3].y}, alpha_sq), f1);
+    reinterpret_cast<uint2*>(dst.c[0])[k] = make_uint2(v0.a, v1.a);
+    reinterpret_cast<uint2*>(dst.c[1])[k] = make_uint2(v0.b, v1.b);
+    reinterpret_cast<uint2*>(dst.c[2])[k] = make_uint2(v0.c, v1.c);
+    reinterpret_cast<uint2*>(dst.c[3])[k] = make_uint2(v0.d, v1.d);
+  }
+}
+
+static bool aligned4(const void* const* p, uintptr_t a) {
+  for (int c = 0; c < 4; c++)
+    if (reinterpret_cast<uintptr_t>(p[c]) % a) return false;
+  return true;
 }
 
 // decompose: per-block signed sums (+ on [0, 16*half_a), - on [16*half_a,
@@ -184,8 +248,13 @@ extern "C" int stwo_b200_fold_line(const uint32_t* const* d_in4, uint32_t log_si
     a = qm31_mul(a, a);
   }
   uint64_t n_out = 1ull << (log_size - fold_step);
-  fold_line_kernel<<<grid_for(n_out, 256), 256, 0, as_stream(stream)>>>(in, log_size, fold_step, al, d_itwiddles,
-                                                                        1ull << tree_log_size, out);
+  if (fold_step == 1 && log_size >= 2 && aligned4(reinterpret_cast<const void* const*>(in.c), 16) &&
+      aligned4(reinterpret_cast<const void* const*>(out.c), 8))
+    fold_line2_kernel<<<grid_for(n_out / 2, 256), 256, 0, as_stream(stream)>>>(in, log_size, al.a[0], d_itwiddles,
+                                                                              1ull << tree_log_size, out);
+  else
+    fold_line_kernel<<<grid_for(n_out, 256), 256, 0, as_stream(stream)>>>(in, log_size, fold_step, al, d_itwiddles,
+                                                                          1ull << tree_log_size, out);
   STWO_CHECK_LAUNCH();
   return ok(err, err_len);
 }
@@ -217,8 +286,13 @@ extern "C" int stwo_b200_fold_circle_into_line(uint32_t* const* d_dst4, const ui
   Cols4 src{{d_src4[0], d_src4[1], d_src4[2], d_src4[3]}};
   qm31 a{alpha[0], alpha[1], alpha[2], alpha[3]};
   uint64_t n_out = 1ull << (log_size - 1);
-  fold_circle_kernel<<<grid_for(n_out, 256), 256, 0, as_stream(stream)>>>(
-      dst, src, log_size, a, qm31_mul(a, a), d_itwiddles, d_itwiddles ? (1ull << tree_log_size) : 0, small);
+  if (log_size > 4 && aligned4(reinterpret_cast<const void* const*>(src.c), 16) &&
+      aligned4(reinterpret_cast<const void* const*>(dst.c), 8))
+    fold_circle2_kernel<<<grid_for(n_out / 2, 256), 256, 0, as_stream(stream)>>>(dst, src, log_size, a, qm31_mul(a, a),
+                                                                                d_itwiddles, 1ull << tree_log_size);
+  else
+    fold_circle_kernel<<<grid_for(n_out, 256), 256, 0, as_stream(stream)>>>(
+        dst, src, log_size, a, qm31_mul(a, a), d_itwiddles, d_itwiddles ? (1ull << tree_log_size) : 0, small);
   STWO_CHECK_LAUNCH();
   return ok(err, err_len);
 }

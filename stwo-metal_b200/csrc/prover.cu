@@ -904,6 +904,32 @@ __global__ void fold_line_dev_kernel(const uint32_t* __restrict__ in, uint32_t l
   const uint64_t n_in = 1ull << log_m;
   const uint64_t n_out = n_in >> fold_step;
   qm31 a0 = *d_alpha;
+  if (fold_step == 1 && log_m >= 2 && reinterpret_cast<uintptr_t>(in) % 16 == 0 &&
+      reinterpret_cast<uintptr_t>(out) % 8 == 0) {
+    // two outputs per thread: one 16-byte load per input coordinate, one
+    // 8-byte twiddle load and one 8-byte store per output coordinate
+    const uint32_t* lt = itw + (tw_len - (1ull << log_m));
+    for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < (n_out >> 1);
+         k += (uint64_t)gridDim.x * blockDim.x) {
+      uint4 w[4];
+#pragma unroll
+      for (int c = 0; c < 4; c++) w[c] = __ldg(reinterpret_cast<const uint4*>(in + c * n_in) + k);
+      const uint2 t = __ldg(reinterpret_cast<const uint2*>(lt) + k);
+      const qm31 f0x{w[0].x, w[1].x, w[2].x, w[3].x}, f0n{w[0].y, w[1].y, w[2].y, w[3].y};
+      const qm31 f1x{w[0].z, w[1].z, w[2].z, w[3].z}, f1n{w[0].w, w[1].w, w[2].w, w[3].w};
+      const qm31 v0 = qm31_add(qm31_add(f0x, f0n), qm31_mul(a0, qm31_mul_m31(qm31_sub(f0x, f0n), t.x)));
+      const qm31 v1 = qm31_add(qm31_add(f1x, f1n), qm31_mul(a0, qm31_mul_m31(qm31_sub(f1x, f1n), t.y)));
+      reinterpret_cast<uint2*>(out)[k] = make_uint2(v0.a, v1.a);
+      reinterpret_cast<uint2*>(out + n_out)[k] = make_uint2(v0.b, v1.b);
+      reinterpret_cast<uint2*>(out + 2 * n_out)[k] = make_uint2(v0.c, v1.c);
+      reinterpret_cast<uint2*>(out + 3 * n_out)[k] = make_uint2(v0.d, v1.d);
+      if (leaves) {
+        fri_leaf_store(leaves, 2 * k, v0, m31 != 0);
+        fri_leaf_store(leaves, 2 * k + 1, v1, m31 != 0);
+      }
+    }
+    return;
+  }
   if (fold_step == 1) {
     const uint32_t* lt = itw + (tw_len - (1ull << log_m));
     for (uint64_t o = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; o < n_out;
@@ -958,6 +984,33 @@ __global__ void fold_circle_first_dev_kernel(Src4 src, uint32_t log_n, const qm3
   const uint64_t n_in = 1ull << log_n, n_out = n_in >> 1;
   const uint32_t* lt0 = itw + (tw_len - (1ull << (log_n - 1)));
   qm31 alpha = *d_alpha;
+  bool vec = log_n >= 3 && reinterpret_cast<uintptr_t>(dst) % 8 == 0;
+  for (int c = 0; c < 4; c++) vec = vec && reinterpret_cast<uintptr_t>(src.c[c]) % 16 == 0;
+  if (vec) {
+    // two outputs per thread: one 16-byte load per source coordinate, one
+    // 8-byte store per output coordinate
+    for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < (n_out >> 1);
+         k += (uint64_t)gridDim.x * blockDim.x) {
+      uint4 w[4];
+#pragma unroll
+      for (int c = 0; c < 4; c++) w[c] = __ldg(reinterpret_cast<const uint4*>(src.c[c]) + k);
+      const uint32_t b = __ldg(lt0 + (k ^ 1));  // circle twiddles of outputs 2k, 2k + 1: [b, -b] or [-b, b]
+      const uint32_t y0 = (k & 1) ? m31_neg(b) : b, y1 = (k & 1) ? b : m31_neg(b);
+      const qm31 p0{w[0].x, w[1].x, w[2].x, w[3].x}, n0{w[0].y, w[1].y, w[2].y, w[3].y};
+      const qm31 p1{w[0].z, w[1].z, w[2].z, w[3].z}, n1{w[0].w, w[1].w, w[2].w, w[3].w};
+      const qm31 v0 = qm31_add(qm31_zero(), qm31_add(qm31_add(p0, n0), qm31_mul(alpha, qm31_mul_m31(qm31_sub(p0, n0), y0))));
+      const qm31 v1 = qm31_add(qm31_zero(), qm31_add(qm31_add(p1, n1), qm31_mul(alpha, qm31_mul_m31(qm31_sub(p1, n1), y1))));
+      reinterpret_cast<uint2*>(dst)[k] = make_uint2(v0.a, v1.a);
+      reinterpret_cast<uint2*>(dst + n_out)[k] = make_uint2(v0.b, v1.b);
+      reinterpret_cast<uint2*>(dst + 2 * n_out)[k] = make_uint2(v0.c, v1.c);
+      reinterpret_cast<uint2*>(dst + 3 * n_out)[k] = make_uint2(v0.d, v1.d);
+      if (leaves) {
+        fri_leaf_store(leaves, 2 * k, v0, m31 != 0);
+        fri_leaf_store(leaves, 2 * k + 1, v1, m31 != 0);
+      }
+    }
+    return;
+  }
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n_out; i += (uint64_t)gridDim.x * blockDim.x) {
     uint32_t b = __ldg(lt0 + ((i >> 1) ^ 1));
     uint32_t yinv = ((i ^ (i >> 1)) & 1) ? m31_neg(b) : b;
@@ -1582,7 +1635,8 @@ class WideFibProver {
       uint8_t* leaves = tail0 > 0 ? fri[0].tree.layer(fri[0].log_size) : nullptr;
       if (lift <= 4) return set_err(err, err_len, STWO_B200_EARG, "lifting domain too small");
       const Src4 q4{{d_quot, d_quot + (1ull << lift), d_quot + (2ull << lift), d_quot + (3ull << lift)}};
-      fold_circle_first_dev_kernel<<<grid1d(1ull << (lift - 1), 256), 256, 0, s>>>(
+      // two outputs per thread (the vector path; the scalar one strides over the rest)
+      fold_circle_first_dev_kernel<<<grid1d(1ull << (lift - 2), 256), 256, 0, s>>>(
           q4, lift, d_alphas, d_itw, 1ull << tree_log, dst, leaves, m31 ? 1 : 0);
       STWO_CHECK_LAUNCH();
     }
@@ -1594,7 +1648,8 @@ class WideFibProver {
       uint32_t* nxt = (li + 1 < fri.size()) ? fri[li + 1].coords : d_last;
       uint8_t* leaves = li + 1 < tail0 ? fri[li + 1].tree.layer(fri[li + 1].log_size) : nullptr;
       uint32_t nlog = l.log_size - l.fold_step;
-      fold_line_dev_kernel<<<grid1d(1ull << nlog, 256), 256, 0, s>>>(l.coords, l.log_size, l.fold_step,
+      const uint64_t threads = l.fold_step == 1 && nlog >= 1 ? 1ull << (nlog - 1) : 1ull << nlog;  // pairs when fs = 1
+      fold_line_dev_kernel<<<grid1d(threads, 256), 256, 0, s>>>(l.coords, l.log_size, l.fold_step,
                                                                        d_alphas + li + 1, d_itw, 1ull << tree_log, nxt,
                                                                        leaves, m31 ? 1 : 0);
       STWO_CHECK_LAUNCH();
@@ -2383,14 +2438,14 @@ struct SeededFriProver {
       if ((rc = build_node_layers_impl(trees[0].layer(n), n, 0, m31, l0.data(), x, err, err_len))) return rc;
     }
     const Src4 src{{d_coords[0], d_coords[1], d_coords[2], d_coords[3]}};
-    fold_circle_first_dev_kernel<<<grid1d(1ull << (n - 1), 256), 256, 0, s>>>(
+    fold_circle_first_dev_kernel<<<grid1d(1ull << (n >= 2 ? n - 2 : 0), 256), 256, 0, s>>>(
         src, n, d_alphas, itw, 1ull << tree_log, line[0], trees[1].layer(n - 1), m31);
     STWO_CHECK_LAUNCH();
     for (uint32_t k = 1; k < n; k++) {
       const uint32_t L = n - k;  // log size of line[k-1]
       if ((rc = nodes_on_side(k, L))) return rc;
       uint8_t* next_leaves = k + 1 < n ? trees[k + 1].layer(L - 1) : nullptr;
-      fold_line_dev_kernel<<<grid1d(1ull << (L - 1), 256), 256, 0, s>>>(line[k - 1], L, 1, d_alphas + k, itw,
+      fold_line_dev_kernel<<<grid1d(1ull << (L >= 2 ? L - 2 : 0), 256), 256, 0, s>>>(line[k - 1], L, 1, d_alphas + k, itw,
                                                                          1ull << tree_log, line[k], next_leaves, m31);
       STWO_CHECK_LAUNCH();
     }
