@@ -657,9 +657,10 @@ def run_prove_reference(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
-# DRAM bytes of one trace evaluate (100 columns, 2^20 -> 2^21) measured by ncu:
-# strided pass 419.5 MB read + 791.1 MB written, contiguous pass 855.0 + 786.3 MB.
-EVALUATE_TRAFFIC_100x2e20 = (419.5 + 791.1 + 855.0 + 786.3) * 1e6
+# DRAM bytes of one trace evaluate (2^20 -> 2^21 per column) measured by ncu
+# on 40 columns (strided pass 167.8 MB read + 287.7 MB written, contiguous
+# pass 347.1 + 282.0 MB), scaled to the 100 columns of the proof.
+EVALUATE_TRAFFIC_100x2e20 = (167.8 + 287.7 + 347.1 + 282.0) * 1e6 * 100 / 40
 
 
 def run_prove_b200(args, world, rank, local):
@@ -820,7 +821,8 @@ def run_prove_b200(args, world, rank, local):
             # passes (fft_warp_strided_kernel<0>, fft_warp_contig_kernel<0>),
             # one ncu capture at this shape
             roof["traffic"] = EVALUATE_TRAFFIC_100x2e20
-            roof["traffic_source"] = "ncu capture (dram__bytes_read.sum + dram__bytes_write.sum) of the two evaluate passes at this shape"
+            roof["traffic_source"] = ("ncu capture (dram__bytes_read.sum + dram__bytes_write.sum) of the two "
+                                      "evaluate passes on 40 columns of 2^20, scaled to 100 columns")
             roof["note"] = ("bound by integer issue, not HBM: in that capture the ALU pipe is 57-70% busy and "
                             "56-69% of issue slots are active, at about 9-12 instructions per M31 butterfly")
     # The trace FFTs against the butterfly ceiling: the interpolation runs n
