@@ -22,9 +22,10 @@ Workloads (seeded synthetic M31 data, values uniform in [0, P)):
   fri_fold       the stand-alone FriOps folds at log 24 (fold_circle_into_line,
                  fold_line) against HBM: their profile target.
 
-The default line also carries, measured in the same run at N = 1, the uneven
-commit's per-column / batched / graph forms and the FRI-heavy commit with the
-stand-alone folds against HBM (skip with --no-extras).
+The default line also carries, measured in the same run at N = 1, the plain
+commit, the uneven commit's per-column / batched / graph forms, the FRI-heavy
+commit with the stand-alone folds against HBM, and a 24-request serving stream
+(skip with --no-extras).
 
 A step is one commit of the whole trace.  `value` is device-timed with inputs
 resident in HBM; `e2e` goes through the same public calls with the trace in
@@ -778,14 +779,18 @@ def run_prove_b200(args, world, rank, local):
     hbm_peak, peak_kind = load_peaks()
 
     # The rest of the metric, in the same run (N = 1 only; replica runs skip
-    # it): the uneven commit's forms and the FRI-heavy commit.
+    # it): the plain commit, the uneven commit's forms, the FRI-heavy commit
+    # and a short serving stream.
     extras = {}
     if world == 1 and args.extras:
         prover.close()
         a.close()
         b.close()
+        extras["commit_plain"] = extra_commit_plain(args, stream, world)
         extras["commit_uneven"] = extra_commit_uneven(args, stream, world, hbm_peak, probe_rate)
         extras["fri_heavy"] = extra_fri_heavy(args, stream, world, hbm_peak, probe_rate)
+        torch.cuda.synchronize()
+        extras["serving"] = measure_serving(24, 1, world, local, with_cpu=False)
 
     if rank != 0:
         return
@@ -1190,6 +1195,44 @@ def extra_commit_uneven(args, stream, world, hbm_peak, probe_rate):
     return out
 
 
+def extra_commit_plain(args, stream, world):
+    """32 columns of log 16, natural order, blowup 1: interpolate (bit
+    reversal in the first pass's loads), evaluate, lifted Blake2s tree."""
+    from stwo_b200 import B200Backend, DeviceBuffer, DeviceColumn, layer_to_host
+    from stwo_b200.backend import canonic_half_coset
+    spec = workload_spec("commit_plain")
+    logs, blowup = spec["logs"], spec["blowup"]
+    host_cols = make_columns(spec)
+    be = B200Backend(stream.cuda_stream)
+    L = max(logs) + blowup
+    init, lg = canonic_half_coset(L + 1)
+    tree = be.precompute_twiddles(init, lg)
+    inputs = [DeviceColumn.from_host(c, stream.cuda_stream) for c in host_cols]
+    coeffs = [DeviceColumn(c.size, stream.cuda_stream) for c in host_cols]
+    evals = [DeviceColumn(c.size << blowup, stream.cuda_stream) for c in host_cols]
+    layers = [DeviceBuffer(32 << k, stream.cuda_stream) for k in range(L + 1)]
+
+    def step():
+        be.interpolate_natural_into(inputs, coeffs, tree)
+        be.evaluate_polynomials_into(coeffs, blowup, tree, evals)
+        be.build_leaves_into(evals, L, layers[L])
+        be.build_nodes(layers)
+
+    for _ in range(3):
+        step()
+    steps = max(10, args.steps)
+    ms = max_over_ranks(time_region(stream, step, steps), world)
+    root = bytes(layer_to_host(layers[0])[0]).hex()
+    golden = load_digests().get("commit_plain_root")
+    cells = sum(c.size for c in host_cols)
+    for x in inputs + coeffs + evals + layers:
+        x.close()
+    return {"workload": "commit_plain: 32 columns of log 16, natural order, blowup 1, lifted Blake2s tree L=17",
+            "ms_per_step": ms, "committed_cells_per_s": cells / (ms * 1e-3), "root": root,
+            "bit_exact_root_vs_oracle": (root == golden) if golden else "no oracle digest",
+            "l2": "inputs smaller than L2 (8 MB trace; back-to-back steps, no flush): a latency figure"}
+
+
 def extra_fri_heavy(args, stream, world, hbm_peak, probe_rate):
     """FRI-heavy commit + decommit (log 24, 70 queries) and the stand-alone
     FriOps folds at log 24 against HBM."""
@@ -1444,12 +1487,22 @@ def run_stream(srv, reqs, inputs, arrivals):
 
 def run_serving_b200(args, world, rank, local):
     import torch
-    from oracle import ffi as oracle
     from stwo_b200 import ffi
-
     torch.cuda.set_device(local)
     ffi.init(local)
-    n_req = max(24, 8 * args.steps)
+    line = measure_serving(max(24, 8 * args.steps), args.warmup, world, local, with_cpu=True)
+    if rank != 0:
+        return
+    line.update({"steps": args.steps, "warmup": args.warmup})
+    print(json.dumps(line), flush=True)
+
+
+def measure_serving(n_req, warmup, world, local, with_cpu):
+    """One Poisson stream of n_req seeded requests through the batched server
+    and through serial proving on the same GPU (see the serving workload)."""
+    import torch
+    from oracle import ffi as oracle
+    from stwo_b200 import ffi
     reqs = serving_requests(n_req)
     inputs = [serving_inputs(ln, sd) for ln, _, sd in reqs]
     cells = sum(nc << ln for ln, nc, _ in reqs)
@@ -1458,7 +1511,7 @@ def run_serving_b200(args, world, rank, local):
     serial = ProveServer(SERVE_BUDGET, slots=1)
     # warm-up: the whole request list once through each server (resident
     # provers built up to the budget, kernels loaded, FRI graphs captured)
-    for _ in range(max(1, min(args.warmup, 2))):
+    for _ in range(max(1, min(warmup, 2))):
         run_stream(batched, reqs, inputs, [0.0] * n_req)
         run_stream(serial, reqs, inputs, [0.0] * n_req)
     # capacity: everything submitted at once, serial (1 slot) and batched
@@ -1493,19 +1546,10 @@ def run_serving_b200(args, world, rank, local):
 
     lat = [t["latency_ms"] for t in t_srv]
     lat_ser = [t["latency_ms"] for t in t_ser2]
-    if rank != 0:
-        return
-    # CPU baseline: the oracle proving the smallest request of the stream
     small = min(range(n_req), key=lambda i: reqs[i][1] << reqs[i][0])
-    ln, nc, _ = reqs[small]
-    a, b = inputs[small]
-    n_threads = oracle.set_threads(os.cpu_count() or 1)
-    t0 = time.perf_counter()
-    cpu_proof = oracle.prove_wide_fib(oracle.wide_fib_config(ln, nc), a, b)
-    cpu_s = time.perf_counter() - t0
     line = {
         "metric": METRIC, "value": cells / mk_srv * world, "unit": "proved trace cells/s",
-        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * mk_srv,
+        "n_gpus": world, "ms_per_step": 1000 * mk_srv,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32 (M31/QM31)",
         "data": "synthetic (seeded numpy PCG64)",
         "config": {"workload": "serving", "requests": n_req, "widths": "U{64..256}", "log_n_rows": "U{14..22}",
@@ -1526,12 +1570,20 @@ def run_serving_b200(args, world, rank, local):
                 "d2h_bytes_per_step": int(sum(len(p) for p in p_srv)), "ms_per_step": 1000 * mk_srv},
         "bit_exact_mix_vs_alone": exact_mix and exact_serial,
         "verifier_rejected": rejected,
-        "bit_exact_vs_oracle_sample": cpu_proof == p_srv[small],
-        "cpu_baseline": {"value": (nc << ln) / cpu_s, "unit": "proved trace cells/s", "cores": n_threads,
-                         "kind": "port", "sample": f"the stream's smallest request ({nc} x 2^{ln}) proved by the "
-                                                   "SimdBackend restatement (C++ oracle, OpenMP)"},
     }
-    print(json.dumps(line), flush=True)
+    if with_cpu:
+        # CPU baseline: the oracle proving the smallest request of the stream
+        ln, nc, _ = reqs[small]
+        a, b = inputs[small]
+        n_threads = oracle.set_threads(os.cpu_count() or 1)
+        t0 = time.perf_counter()
+        cpu_proof = oracle.prove_wide_fib(oracle.wide_fib_config(ln, nc), a, b)
+        cpu_s = time.perf_counter() - t0
+        line["bit_exact_vs_oracle_sample"] = cpu_proof == p_srv[small]
+        line["cpu_baseline"] = {"value": (nc << ln) / cpu_s, "unit": "proved trace cells/s", "cores": n_threads,
+                                "kind": "port", "sample": f"the stream's smallest request ({nc} x 2^{ln}) proved by "
+                                                          "the SimdBackend restatement (C++ oracle, OpenMP)"}
+    return line
 
 
 def main():
