@@ -894,6 +894,14 @@ __device__ __forceinline__ void fri_leaf_store(uint8_t* leaves, uint64_t i, cons
   g[1] = make_uint4(h[4], h[5], h[6], h[7]);
 }
 
+// Folds of more than 2^kFoldPairLog outputs take two outputs per thread (wide
+// loads; several waves of blocks either way); smaller ones, which are on the
+// latency-bound FRI chain, keep one output (and one leaf hash) per thread.
+constexpr uint32_t kFoldPairLog = 16;
+__host__ __device__ constexpr uint64_t fold_threads(uint32_t log_out) {
+  return log_out > kFoldPairLog ? 1ull << (log_out - 1) : 1ull << log_out;
+}
+
 // fold_line with alpha read from device memory (prover/backend/cpu/fri.rs:67-92).
 // When `leaves` is not null the fold also writes the leaf hashes of the next
 // layer's tree (its Merkle leaf layer), saving a launch and a re-read.
@@ -904,7 +912,7 @@ __global__ void fold_line_dev_kernel(const uint32_t* __restrict__ in, uint32_t l
   const uint64_t n_in = 1ull << log_m;
   const uint64_t n_out = n_in >> fold_step;
   qm31 a0 = *d_alpha;
-  if (fold_step == 1 && log_m >= 2 && reinterpret_cast<uintptr_t>(in) % 16 == 0 &&
+  if (fold_step == 1 && log_m - 1 > kFoldPairLog && reinterpret_cast<uintptr_t>(in) % 16 == 0 &&
       reinterpret_cast<uintptr_t>(out) % 8 == 0) {
     // two outputs per thread: one 16-byte load per input coordinate, one
     // 8-byte twiddle load and one 8-byte store per output coordinate
@@ -984,7 +992,7 @@ __global__ void fold_circle_first_dev_kernel(Src4 src, uint32_t log_n, const qm3
   const uint64_t n_in = 1ull << log_n, n_out = n_in >> 1;
   const uint32_t* lt0 = itw + (tw_len - (1ull << (log_n - 1)));
   qm31 alpha = *d_alpha;
-  bool vec = log_n >= 3 && reinterpret_cast<uintptr_t>(dst) % 8 == 0;
+  bool vec = log_n - 1 > kFoldPairLog && reinterpret_cast<uintptr_t>(dst) % 8 == 0;
   for (int c = 0; c < 4; c++) vec = vec && reinterpret_cast<uintptr_t>(src.c[c]) % 16 == 0;
   if (vec) {
     // two outputs per thread: one 16-byte load per source coordinate, one
@@ -1635,8 +1643,7 @@ class WideFibProver {
       uint8_t* leaves = tail0 > 0 ? fri[0].tree.layer(fri[0].log_size) : nullptr;
       if (lift <= 4) return set_err(err, err_len, STWO_B200_EARG, "lifting domain too small");
       const Src4 q4{{d_quot, d_quot + (1ull << lift), d_quot + (2ull << lift), d_quot + (3ull << lift)}};
-      // two outputs per thread (the vector path; the scalar one strides over the rest)
-      fold_circle_first_dev_kernel<<<grid1d(1ull << (lift - 2), 256), 256, 0, s>>>(
+      fold_circle_first_dev_kernel<<<grid1d(fold_threads(lift - 1), 256), 256, 0, s>>>(
           q4, lift, d_alphas, d_itw, 1ull << tree_log, dst, leaves, m31 ? 1 : 0);
       STWO_CHECK_LAUNCH();
     }
@@ -1648,7 +1655,7 @@ class WideFibProver {
       uint32_t* nxt = (li + 1 < fri.size()) ? fri[li + 1].coords : d_last;
       uint8_t* leaves = li + 1 < tail0 ? fri[li + 1].tree.layer(fri[li + 1].log_size) : nullptr;
       uint32_t nlog = l.log_size - l.fold_step;
-      const uint64_t threads = l.fold_step == 1 && nlog >= 1 ? 1ull << (nlog - 1) : 1ull << nlog;  // pairs when fs = 1
+      const uint64_t threads = l.fold_step == 1 ? fold_threads(nlog) : 1ull << nlog;
       fold_line_dev_kernel<<<grid1d(threads, 256), 256, 0, s>>>(l.coords, l.log_size, l.fold_step,
                                                                        d_alphas + li + 1, d_itw, 1ull << tree_log, nxt,
                                                                        leaves, m31 ? 1 : 0);
@@ -2438,14 +2445,14 @@ struct SeededFriProver {
       if ((rc = build_node_layers_impl(trees[0].layer(n), n, 0, m31, l0.data(), x, err, err_len))) return rc;
     }
     const Src4 src{{d_coords[0], d_coords[1], d_coords[2], d_coords[3]}};
-    fold_circle_first_dev_kernel<<<grid1d(1ull << (n >= 2 ? n - 2 : 0), 256), 256, 0, s>>>(
+    fold_circle_first_dev_kernel<<<grid1d(fold_threads(n - 1), 256), 256, 0, s>>>(
         src, n, d_alphas, itw, 1ull << tree_log, line[0], trees[1].layer(n - 1), m31);
     STWO_CHECK_LAUNCH();
     for (uint32_t k = 1; k < n; k++) {
       const uint32_t L = n - k;  // log size of line[k-1]
       if ((rc = nodes_on_side(k, L))) return rc;
       uint8_t* next_leaves = k + 1 < n ? trees[k + 1].layer(L - 1) : nullptr;
-      fold_line_dev_kernel<<<grid1d(1ull << (L >= 2 ? L - 2 : 0), 256), 256, 0, s>>>(line[k - 1], L, 1, d_alphas + k, itw,
+      fold_line_dev_kernel<<<grid1d(fold_threads(L - 1), 256), 256, 0, s>>>(line[k - 1], L, 1, d_alphas + k, itw,
                                                                          1ull << tree_log, line[k], next_leaves, m31);
       STWO_CHECK_LAUNCH();
     }
