@@ -44,6 +44,7 @@ struct FftPass {
   uint32_t cpb;        // columns per block: tiles of the same position share staged twiddles
   uint32_t n_cols;     // columns in this launch
   uint32_t natural = 0;  // the source is in natural order: the contiguous first pass gathers src[rev_N(i)]
+  uint32_t tile0 = 0;    // tile positions of this launch start here (a launch over part of a pass)
 };
 
 
@@ -174,7 +175,7 @@ __global__ void __launch_bounds__(NT, 1024 / NT) fft_pass_kernel(FftPass p, FftC
   const uint32_t n_tiles = CPB == 1 ? 1u : min((uint32_t)CPB, p.n_cols - col0);
   uint32_t* __restrict__ sm = smem;
   uint32_t* __restrict__ tws = smem + CPB * STRIDE;
-  const uint64_t tile = blockIdx.x;
+  const uint64_t tile = (uint64_t)p.tile0 + blockIdx.x;
   const uint32_t lo_bits = L0 - C;  // L0 >= C
   const uint64_t lo = tile & ((1ull << lo_bits) - 1);
   const uint64_t hi = tile >> lo_bits;
@@ -620,7 +621,7 @@ __global__ void __launch_bounds__(256, 4) fft_warp_contig_kernel(FftPass p, FftC
   uint32_t* tws = smem;
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   uint32_t* buf = smem + 1024 + warp * kTileWords;
-  const uint64_t hi = blockIdx.x;
+  const uint64_t hi = (uint64_t)p.tile0 + blockIdx.x;
   const uint64_t base = hi << 10;
   const uint32_t g0 = blockIdx.y * p.cpb;
   uint32_t c = g0 * kWarpCols + warp;
@@ -695,7 +696,7 @@ __global__ void __launch_bounds__(256, 4) fft_warp_strided_kernel(FftPass p, Fft
   uint32_t* tile = smem + 1024;  // 8 column regions of kColStride words
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint32_t L0 = p.layer0;
-  const uint64_t t = blockIdx.x;
+  const uint64_t t = (uint64_t)p.tile0 + blockIdx.x;
   const uint32_t lo_bits = L0 - 3;
   const uint64_t lo = t & ((1ull << lo_bits) - 1);
   const uint64_t hi = t >> lo_bits;
@@ -852,10 +853,15 @@ static int dispatch_tile(const FftPass& q, const FftCols& cols, dim3 grid, cudaS
   return set_err(err, err_len, STWO_B200_EARG, "unsupported FFT pass size T=%u", q.T);
 }
 
+// One pass over every tile position, or over tile positions
+// [tile0, tile0 + tile_cnt) when tile_cnt != 0.
 template <bool INV>
 static int launch_pass(const FftPass& p, const std::vector<const uint32_t*>& srcs, const std::vector<uint32_t*>& dsts,
-                       uint64_t total_log, cudaStream_t s, char* err, size_t err_len) {
-  uint64_t tiles = 1ull << (total_log - p.T - p.C);
+                       uint64_t total_log, cudaStream_t s, char* err, size_t err_len, uint64_t tile0 = 0,
+                       uint64_t tile_cnt = 0) {
+  const uint64_t all_tiles = 1ull << (total_log - p.T - p.C);
+  STWO_ARG_CHECK(tile0 + tile_cnt <= all_tiles && tile0 <= 0xffffffffull, "tile range out of the pass");
+  uint64_t tiles = tile_cnt ? tile_cnt : all_tiles;
   size_t E = (size_t)1 << (p.T + p.C);
   STWO_ARG_CHECK(p.C == 0 || p.C == 3, "unsupported FFT tile width");
   // Contiguous passes (small tiles, twiddles as large as the data) share one
@@ -873,6 +879,7 @@ static int launch_pass(const FftPass& p, const std::vector<const uint32_t*>& src
                 (reinterpret_cast<uintptr_t>(cols.dst[i]) % 16 == 0);
     }
     FftPass q = p;
+    q.tile0 = (uint32_t)tile0;
     q.vec_io = aligned && (p.C >= 2 || p.layer0 == 0) && E >= 4 && (p.src_mask & 3) == 3 &&
                (p.src_len == ~0ull || p.src_len % 4 == 0);
     q.cpb = cpb;
@@ -1048,6 +1055,50 @@ extern "C" int stwo_b200_interpolate_columns_natural(const uint32_t* const* d_na
                             as_stream(stream), err, err_len, true);
   return rc ? rc : ok(err, err_len);
 }
+
+namespace stwo_b200 {
+
+std::vector<uint32_t> fft_split(uint32_t log_n) { return split_for(log_n); }
+
+// Pass `pi` of the interpolation (the inverse transform) of same-size columns
+// of 2^log_n bit-reversed evaluations, in place, under the pass split
+// `split` (fft_split, fetched once by the caller so that both halves of a
+// split transform use the same plan).  For pi = 0 only the rows
+// [row_begin, row_end) are transformed: whole tiles of the first pass, whose
+// 2^split[0] rows are consecutive; the later passes take every row.
+int interpolate_pass(uint32_t* const* cols, uint32_t n_cols, uint32_t log_n, const std::vector<uint32_t>& split,
+                     uint32_t pi, uint64_t row_begin, uint64_t row_end, const uint32_t* d_itwiddles,
+                     uint32_t tree_log_size, cudaStream_t s, char* err, size_t err_len) {
+  STWO_ARG_CHECK(log_n >= 3 && log_n <= 30 && pi < split.size(), "interpolate pass out of range");
+  STWO_ARG_CHECK(d_itwiddles && log_n - 1 <= tree_log_size, "twiddle tree (log %u) too small for log size %u",
+                 tree_log_size, log_n);
+  uint32_t l0 = 0;
+  for (uint32_t k = 0; k < pi; k++) l0 += split[k];
+  FftPass p;
+  p.tree = d_itwiddles;
+  p.tree_len = 1ull << tree_log_size;
+  p.src_mask = ~0ull;
+  p.src_len = ~0ull;
+  p.log_domain = log_n;
+  p.layer0 = l0;
+  p.T = split[pi];
+  p.C = l0 == 0 ? 0u : 3u;
+  p.scale = (pi + 1 == split.size()) ? host_pow2_inv(log_n) : 1u;
+  std::vector<const uint32_t*> srcs(cols, cols + n_cols);
+  std::vector<uint32_t*> dsts(cols, cols + n_cols);
+  if (pi == 0) {
+    const uint64_t tile_rows = 1ull << p.T;
+    STWO_ARG_CHECK(row_begin % tile_rows == 0 && row_end % tile_rows == 0 && row_begin < row_end &&
+                       row_end <= (1ull << log_n),
+                   "rows [%llu, %llu) are not whole tiles of the first pass", (unsigned long long)row_begin,
+                   (unsigned long long)row_end);
+    return launch_pass<true>(p, srcs, dsts, log_n, s, err, err_len, row_begin / tile_rows,
+                             (row_end - row_begin) / tile_rows);
+  }
+  return launch_pass<true>(p, srcs, dsts, log_n, s, err, err_len);
+}
+
+}  // namespace stwo_b200
 
 extern "C" int stwo_b200_evaluate_polynomials(const uint32_t* const* d_coeffs, const uint32_t* log_sizes,
                                               uint32_t n_cols, uint32_t log_blowup, uint32_t* const* d_evals,

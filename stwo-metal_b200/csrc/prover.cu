@@ -18,6 +18,7 @@
 #include "blake2s.cuh"
 #include "channel.hpp"
 #include "common.cuh"
+#include "fft.hpp"
 #include "field.cuh"
 #include "pcs.hpp"
 #include "rowops.cuh"
@@ -1792,6 +1793,18 @@ int WideFibProver::prove_body(const uint32_t* d_a, const uint32_t* d_b, ProofOut
   }
 
   // ---- tree 1: trace ----
+  std::vector<uint32_t*> coeff_ptrs(N), eval_ptrs(N);
+  std::vector<uint32_t> logs_n(N, log_n), logs_1(N, L1);
+  for (uint32_t c = 0; c < N; c++) {
+    coeff_ptrs[c] = d_coeffs + (uint64_t)c * rows;
+    eval_ptrs[c] = d_evals + ((uint64_t)c << L1);
+  }
+  // With host inputs and a split interpolation, the first pass runs chunk by
+  // chunk as each chunk's trace rows are generated (its tiles are
+  // consecutive rows), under the copies of the later chunks.
+  const std::vector<uint32_t> ifft_split = fft_split(log_n);
+  const bool chunked_ifft = h_src_a && ifft_split.size() >= 2 && ((rows / kHostChunks) >> ifft_split[0]) >= 1 &&
+                            (rows / kHostChunks) % (1ull << ifft_split[0]) == 0;
   phase(kTraceGen);
   if (h_src_a) {
     // Host inputs: chunk k's copies (copy stream, ordered after the caller's
@@ -1808,21 +1821,24 @@ int WideFibProver::prove_body(const uint32_t* d_a, const uint32_t* d_b, ProofOut
       STWO_CUDA_TRY(cudaStreamWaitEvent(s, ev_chunk[k], 0));
       wide_fib_trace_kernel<<<grid1d(chunk, 256), 256, 0, s>>>(d_a + off, d_b + off, d_coeffs + off, N, chunk, rows);
       STWO_CHECK_LAUNCH();
+      if (chunked_ifft && (rc = interpolate_pass(coeff_ptrs.data(), N, log_n, ifft_split, 0, off, off + chunk, d_itw,
+                                                 tree_log, s, err, err_len)))
+        return rc;
     }
   } else {
     wide_fib_trace_kernel<<<grid1d(rows, 256), 256, 0, s>>>(d_a, d_b, d_coeffs, N, rows, rows);
     STWO_CHECK_LAUNCH();
   }
-  std::vector<uint32_t*> coeff_ptrs(N), eval_ptrs(N);
-  std::vector<uint32_t> logs_n(N, log_n), logs_1(N, L1);
-  for (uint32_t c = 0; c < N; c++) {
-    coeff_ptrs[c] = d_coeffs + (uint64_t)c * rows;
-    eval_ptrs[c] = d_evals + ((uint64_t)c << L1);
-  }
   phase(kTraceInterpolate);
-  if ((rc = stwo_b200_interpolate_columns(coeff_ptrs.data(), logs_n.data(), nullptr, N, d_itw, tree_log, s, err,
-                                          err_len)))
+  if (chunked_ifft) {
+    for (uint32_t pi = 1; pi < ifft_split.size(); pi++)
+      if ((rc = interpolate_pass(coeff_ptrs.data(), N, log_n, ifft_split, pi, 0, rows, d_itw, tree_log, s, err,
+                                 err_len)))
+        return rc;
+  } else if ((rc = stwo_b200_interpolate_columns(coeff_ptrs.data(), logs_n.data(), nullptr, N, d_itw, tree_log, s,
+                                                 err, err_len))) {
     return rc;
+  }
   phase(kTraceEvaluate);
   if ((rc = stwo_b200_evaluate_polynomials(const_cast<const uint32_t* const*>(coeff_ptrs.data()), logs_n.data(), N,
                                            blowup, eval_ptrs.data(), d_tw, tree_log, s, err, err_len)))

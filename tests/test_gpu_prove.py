@@ -79,12 +79,15 @@ def test_phase_timing_does_not_change_proofs(oracle):
 
 
 @pytest.mark.parametrize("pinned", [False, True])
-def test_prove_from_host_columns(oracle, pinned):
+@pytest.mark.parametrize("log_n", [12, 16])
+def test_prove_from_host_columns(oracle, pinned, log_n):
     # host inputs (pageable numpy, or page-locked memory from the library):
-    # copied chunk by chunk by the prover, the same proof bytes
+    # copied chunk by chunk by the prover, the same proof bytes.  At log 16
+    # the interpolation is split in passes and its first pass runs chunk by
+    # chunk as the trace rows are generated.
     import ctypes as C
     from stwo_b200 import ffi
-    log_n, cols = 12, 24
+    cols = 24
     a, b = oracle.wide_fib_inputs(log_n, 55)
     ref = oracle.prove_wide_fib(oracle.wide_fib_config(log_n, cols), a, b)
     prover = WideFibProver(wide_fib_config(log_n, cols))
