@@ -452,31 +452,26 @@ static void index_point(uint64_t idx, uint32_t& x, uint32_t& y) {
   }
 }
 
-// ---- warp-per-column 1024-point passes (T = 10) ----
-// A warp owns one column of a 1024-row tile: 32 values per lane.  Layers
-// 0..4 (row bits 0..4) run with the tile held lane-major (v[j] = row
-// lane*32 + j); layers 5..9 with it held row-major (v[j] = row j*32 + lane).
-// The two layouts exchange through a warp-private 32 x 33 shared-memory
-// region (conflict-free both ways), so a warp needs no block barrier once the
-// block's twiddles are staged.  Butterflies, twiddle indices (row >> (lam+1)
-// of tree layer layer0 + lam) and layer order are those of fft_stage.
-constexpr int kWarpCols = 8;                  // warps (columns) per block
-// Column region of the strided pass: row r at (r >> 5) * kTileStride + (r & 31)
-// (the staged-tile layout of the contiguous pass), regions kColStride words
-// apart.  kColStride = 4 (mod 32) keeps the 4-word scatter and gather of the
-// staging conflict-free; the 16-byte aligned lines let the lane-major side
-// of a column move as 8 x 16 bytes per lane.
-constexpr uint32_t kColStride = 32 * 36 + 4;
-__device__ __forceinline__ uint32_t colpos(uint32_t r) { return (r >> 5) * 36 + (r & 31); }
+// ---- 1024-point passes (T = 10) with 32 values per thread ----
+// A thread holds 32 words of one tile column.  Layers 0..4 (row bits 0..4)
+// run with them held lane-major (v[j] = row 32 b + j for the thread's 32-row
+// block b); layers 5..9 with them held row-major (v[j] = row 32 j + b).  The
+// contiguous pass gives a warp one column (b = lane) and exchanges the two
+// layouts through a warp-private staged tile, so a warp needs no block
+// barrier once the block's twiddles are staged; the strided pass spreads the
+// 8 columns of its tile over the lanes and exchanges through the block.
+// Butterflies, twiddle indices (row >> (lam+1) of tree layer layer0 + lam)
+// and layer order are those of fft_stage.
+constexpr int kWarpCols = 8;                  // warps (columns) per block of the contiguous pass
 
-// Layers 0..4 on v[j] = row lane*32 + j.
+// Layers 0..4 on v[j] = row 32 b + j.
 template <bool INV>
-__device__ __forceinline__ void warp_phase_lo(uint32_t (&v)[32], const uint32_t* __restrict__ tws, uint32_t lane) {
+__device__ __forceinline__ void warp_phase_lo(uint32_t (&v)[32], const uint32_t* __restrict__ tws, uint32_t b) {
 #pragma unroll
   for (int kk = 0; kk < 5; kk++) {
     const int lam = INV ? kk : 4 - kk;
-    // row >> (lam + 1) = (lane << (4 - lam)) + (j >> (lam + 1))
-    const uint32_t* tl = tws + (1024u - (1024u >> lam)) + (lane << (4 - lam));
+    // row >> (lam + 1) = (b << (4 - lam)) + (j >> (lam + 1))
+    const uint32_t* tl = tws + (1024u - (1024u >> lam)) + (b << (4 - lam));
     uint32_t t[16];
 #pragma unroll
     for (int m = 0; m < (1 << (4 - lam)); m++) t[m] = tl[m];
@@ -491,8 +486,8 @@ __device__ __forceinline__ void warp_phase_lo(uint32_t (&v)[32], const uint32_t*
   }
 }
 
-// Layers 5..9 on v[j] = row j*32 + lane: row >> (lam + 1) = j >> (lam - 4),
-// the same twiddle for every lane.
+// Layers 5..9 on v[j] = row 32 j + b: row >> (lam + 1) = j >> (lam - 4),
+// the same twiddle for every thread.
 template <bool INV>
 __device__ __forceinline__ void warp_phase_hi(uint32_t (&v)[32], const uint32_t* __restrict__ tws) {
 #pragma unroll
@@ -687,118 +682,90 @@ __global__ void __launch_bounds__(256, 4) fft_warp_contig_kernel(FftPass p, FftC
   }
 }
 
-// Strided pass (C = 3, layer0 >= 3): the block stages a 1024 x 8 tile of one
-// column; warp w transforms tile column w.
-template <bool INV>
+// Strided pass (C = 3, layer0 >= 3): a block transforms the 8 adjacent
+// columns of one tile position, 1024 rows x 8 words (each row one 32-byte
+// sector).  Thread (warp w, lane l) works on tile column c = l & 7 with
+// m = 4 w + (l >> 3):
+//   lane-major: rows 32 m + j (j = 0..31), layers 0..4 of the tile;
+//   row-major:  rows 32 j + m, layers 5..9.
+// In either layout the 8 lanes of a quarter-warp read or write one whole row
+// (a full sector) per instruction, so global memory is read and written
+// straight from registers; the one change of layout between the two halves
+// goes through shared memory.  Word (r, c) of the exchange tile sits at
+// (r + (r >> 5)) * 8 + c: both layouts then touch 32 distinct banks per
+// instruction.
+constexpr uint32_t kXchWords = (1024 + 32) * 8;
+__device__ __forceinline__ uint32_t xch_pos(uint32_t r, uint32_t c) { return (r + (r >> 5)) * 8 + c; }
+
+// A power-of-two source mask that covers every row and column bit of the
+// tile (the duplicated coefficients of a blowup evaluation) only changes the
+// tile base.
+__host__ __device__ __forceinline__ bool strided_mask_on_base(uint64_t mask, uint64_t len, uint32_t L0) {
+  return (mask == ~0ull && len == ~0ull) ||
+         (mask != ~0ull && ((mask + 1) & mask) == 0 && mask + 1 >= (1ull << (L0 + 10)) && len > mask);
+}
+
+// L0T != 0 fixes layer0 at compile time (the row stride 2^L0T words): the
+// 32 loads and stores of a thread then address one base register with
+// immediate offsets (up to 31 x 2^(L0T+5) words, within the 24-bit signed
+// offset of global accesses for L0T <= 11).  Those instances take only
+// sources whose mask acts on the tile base (checked by the launcher);
+// L0T = 0 takes any layer0 and mask.
+template <bool INV, int L0T>
 __global__ void __launch_bounds__(256, 4) fft_warp_strided_kernel(FftPass p, FftCols cols) {
   extern __shared__ __align__(16) uint32_t smem[];
   uint32_t* tws = smem;
-  uint32_t* tile = smem + 1024;  // 8 column regions of kColStride words
-  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const uint32_t L0 = p.layer0;
+  uint32_t* xch = smem + 1024;
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t c = lane & 7, m = (threadIdx.x >> 5) * 4 + (lane >> 3);
+  const uint32_t L0 = L0T ? (uint32_t)L0T : p.layer0;
   const uint64_t t = (uint64_t)p.tile0 + blockIdx.x;
   const uint32_t lo_bits = L0 - 3;
   const uint64_t lo = t & ((1ull << lo_bits) - 1);
   const uint64_t hi = t >> lo_bits;
   const uint64_t base = (hi << (L0 + 10)) | (lo << 3);
   const uint32_t* __restrict__ src = cols.src[blockIdx.y];
-  uint32_t* __restrict__ dst = cols.dst[blockIdx.y];
-  stage_tws10(p, hi, tws);
-  // A power-of-two source mask that covers every row and column bit of the
-  // tile (the duplicated coefficients of a blowup evaluation) only changes
-  // the tile base.
-  const bool mask_on_base = (p.src_mask == ~0ull && p.src_len == ~0ull) ||
-                            (p.src_mask != ~0ull && ((p.src_mask + 1) & p.src_mask) == 0 &&
-                             p.src_mask + 1 >= (1ull << (L0 + 10)) && p.src_len > p.src_mask);
-  if (p.vec_io && mask_on_base) {
-    // all 8 loads in flight before the first shared-memory store
-    const uint32_t* __restrict__ sb = src + (base & p.src_mask);
-    uint4 w[8];
+  // Rows held in the layout the pass starts from: lane-major for the
+  // inverse transform, row-major for the forward one.
+  const uint32_t r0 = INV ? 32 * m : m, rs = INV ? 1 : 32;
+  uint32_t v[32];
+  if (L0T != 0 || strided_mask_on_base(p.src_mask, p.src_len, L0)) {
+    const uint32_t* __restrict__ sp = src + (base & p.src_mask) + c + ((uint64_t)r0 << L0);
 #pragma unroll
-    for (int q = 0; q < 8; q++) {
-      const uint32_t e = threadIdx.x * 4 + 1024u * q;
-      w[q] = __ldg(reinterpret_cast<const uint4*>(sb + ((size_t)(e >> 3) << L0) + (e & 7)));
-    }
-#pragma unroll
-    for (int q = 0; q < 8; q++) {
-      const uint32_t e = threadIdx.x * 4 + 1024u * q;
-      const uint32_t row = e >> 3, c0 = e & 7;
-      const uint32_t r = colpos(row);
-      tile[c0 * kColStride + r] = w[q].x;
-      tile[(c0 + 1) * kColStride + r] = w[q].y;
-      tile[(c0 + 2) * kColStride + r] = w[q].z;
-      tile[(c0 + 3) * kColStride + r] = w[q].w;
-    }
-  } else if (p.vec_io) {
-#pragma unroll 4
-    for (uint32_t e = threadIdx.x * 4; e < 8192; e += 1024) {
-      const uint32_t row = e >> 3, c0 = e & 7;
-      const uint64_t gi = (base + ((uint64_t)row << L0) + c0) & p.src_mask;
-      const uint4 w = gi < p.src_len ? __ldg(reinterpret_cast<const uint4*>(src + gi)) : make_uint4(0, 0, 0, 0);
-      const uint32_t r = colpos(row);
-      tile[c0 * kColStride + r] = w.x;
-      tile[(c0 + 1) * kColStride + r] = w.y;
-      tile[(c0 + 2) * kColStride + r] = w.z;
-      tile[(c0 + 3) * kColStride + r] = w.w;
-    }
+    for (int j = 0; j < 32; j++) v[j] = __ldg(sp + ((uint64_t)(rs * j) << L0));
   } else {
-    for (uint32_t e = threadIdx.x; e < 8192; e += 256) {
-      const uint32_t row = e >> 3, c0 = e & 7;
-      const uint64_t gi = (base + ((uint64_t)row << L0) + c0) & p.src_mask;
-      tile[c0 * kColStride + colpos(row)] = gi < p.src_len ? __ldg(src + gi) : 0u;
+#pragma unroll
+    for (int j = 0; j < 32; j++) {
+      const uint64_t gi = (base + ((uint64_t)(r0 + rs * j) << L0) + c) & p.src_mask;
+      v[j] = gi < p.src_len ? __ldg(src + gi) : 0u;
     }
   }
+  stage_tws10(p, hi, tws);
   __syncthreads();
-  // Each warp's column stays in its region: lane-major accesses (a lane's
-  // own line, 8 x 16 bytes) and row-major ones (word 36 j + lane); the
-  // __syncwarp separates writes and reads of other lanes' lines.
-  uint32_t* cw = tile + warp * kColStride;
-  uint32_t v[32];
   if (INV) {
-    tile_to_lane_major(cw, lane, v);
-    warp_phase_lo<true>(v, tws, lane);
-    lane_major_to_tile(cw, lane, v);
-    __syncwarp();
+    warp_phase_lo<true>(v, tws, m);
 #pragma unroll
-    for (int j = 0; j < 32; j++) v[j] = cw[j * kTileStride + lane];
+    for (int j = 0; j < 32; j++) xch[xch_pos(32 * m + j, c)] = v[j];
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < 32; j++) v[j] = xch[xch_pos(32 * j + m, c)];
     warp_phase_hi<true>(v, tws);
-#pragma unroll
-    for (int j = 0; j < 32; j++) cw[j * kTileStride + lane] = v[j];
   } else {
-#pragma unroll
-    for (int j = 0; j < 32; j++) v[j] = cw[j * kTileStride + lane];
     warp_phase_hi<false>(v, tws);
 #pragma unroll
-    for (int j = 0; j < 32; j++) cw[j * kTileStride + lane] = v[j];
-    __syncwarp();
-    tile_to_lane_major(cw, lane, v);
-    warp_phase_lo<false>(v, tws, lane);
-    lane_major_to_tile(cw, lane, v);
+    for (int j = 0; j < 32; j++) xch[xch_pos(32 * j + m, c)] = v[j];
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < 32; j++) v[j] = xch[xch_pos(32 * m + j, c)];
+    warp_phase_lo<false>(v, tws, m);
   }
-  __syncthreads();
+  // Stores in the layout the pass ends in: row-major for the inverse
+  // transform, lane-major for the forward one.
   const uint32_t scale = p.scale;
-  if (p.vec_io) {
-#pragma unroll 4
-    for (uint32_t e = threadIdx.x * 4; e < 8192; e += 1024) {
-      const uint32_t row = e >> 3, c0 = e & 7;
-      const uint32_t r = colpos(row);
-      uint4 w = make_uint4(tile[c0 * kColStride + r], tile[(c0 + 1) * kColStride + r],
-                           tile[(c0 + 2) * kColStride + r], tile[(c0 + 3) * kColStride + r]);
-      if (scale != 1u) {
-        w.x = m31_mul(w.x, scale);
-        w.y = m31_mul(w.y, scale);
-        w.z = m31_mul(w.z, scale);
-        w.w = m31_mul(w.w, scale);
-      }
-      *reinterpret_cast<uint4*>(dst + base + ((uint64_t)row << L0) + c0) = w;
-    }
-  } else {
-    for (uint32_t e = threadIdx.x; e < 8192; e += 256) {
-      const uint32_t row = e >> 3, c0 = e & 7;
-      const uint32_t v1 = tile[c0 * kColStride + colpos(row)];
-      dst[base + ((uint64_t)row << L0) + c0] = scale != 1u ? m31_mul(v1, scale) : v1;
-    }
-  }
+  uint32_t* __restrict__ dp = cols.dst[blockIdx.y] + base + c + ((uint64_t)(INV ? m : 32 * m) << L0);
+#pragma unroll
+  for (int j = 0; j < 32; j++)
+    dp[(uint64_t)((INV ? 32 : 1) * j) << L0] = scale != 1u ? m31_mul(v[j], scale) : v[j];
 }
 
 template <bool INV>
@@ -816,11 +783,20 @@ static int launch_warp_pass(const FftPass& q, const FftCols& cols, uint64_t tile
     dim3 grid((unsigned)tiles, (unsigned)((groups + qq.cpb - 1) / qq.cpb));
     fft_warp_contig_kernel<INV><<<grid, 32 * kWarpCols, smem, s>>>(qq, cols);
   } else {
-    constexpr size_t smem = (1024 + 8 * kColStride) * sizeof(uint32_t);
-    static std::atomic<uint32_t> attr{0};
-    STWO_CUDA_TRY(ensure_smem_limit(fft_warp_strided_kernel<INV>, (int)smem, attr));
+    constexpr size_t smem = (1024 + kXchWords) * sizeof(uint32_t);
+    static std::atomic<uint32_t> attr10{0}, attr11{0}, attr{0};
+    const bool fixed = (q.layer0 == 10 || q.layer0 == 11) && strided_mask_on_base(q.src_mask, q.src_len, q.layer0);
     dim3 grid((unsigned)tiles, (unsigned)nc);
-    fft_warp_strided_kernel<INV><<<grid, 256, smem, s>>>(q, cols);
+    if (fixed && q.layer0 == 10) {
+      STWO_CUDA_TRY(ensure_smem_limit(fft_warp_strided_kernel<INV, 10>, (int)smem, attr10));
+      fft_warp_strided_kernel<INV, 10><<<grid, 256, smem, s>>>(q, cols);
+    } else if (fixed) {
+      STWO_CUDA_TRY(ensure_smem_limit(fft_warp_strided_kernel<INV, 11>, (int)smem, attr11));
+      fft_warp_strided_kernel<INV, 11><<<grid, 256, smem, s>>>(q, cols);
+    } else {
+      STWO_CUDA_TRY(ensure_smem_limit(fft_warp_strided_kernel<INV, 0>, (int)smem, attr));
+      fft_warp_strided_kernel<INV, 0><<<grid, 256, smem, s>>>(q, cols);
+    }
   }
   STWO_CHECK_LAUNCH();
   return STWO_B200_OK;
