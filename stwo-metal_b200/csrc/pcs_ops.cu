@@ -428,7 +428,7 @@ extern "C" int stwo_b200_batch_eval_at_point(const uint32_t* const* d_coeffs, ui
     return ok(err, err_len);
   }
   const spoint z{qm31_from_words(point), qm31_from_words(point + 4)};
-  const uint32_t lg = log_size, h = lg / 2;
+  const uint32_t lg = log_size, h = poly_eval_lo_bits(lg);
   const uint32_t n_chunk_polys = std::min<uint32_t>(n_polys, kMaxPolys);
   const size_t n_w = (1ull << h) + (1ull << (lg - h));
   const size_t words = n_w + (size_t)n_chunk_polys * poly_eval_chunks(lg) + n_polys;

@@ -199,17 +199,104 @@ __global__ void __launch_bounds__(256) oods_reduce_kernel(const qm31* __restrict
   if (threadIdx.x == 0) out[p] = red[0];
 }
 
+// OODS sampling of polynomials whose index splits as bucket b (the bits above
+// kEvalLoBits) and position e < 1024: sum_j c_j w_j = sum_b w_hi[b] sum_e
+// c_(1024 b + e) w_lo[e].  Each warp takes one unit (a polynomial and
+// kEvalUnitBuckets consecutive buckets) and keeps the next bucket's 16-byte
+// loads in flight while it multiplies the current one; a lane reads 4
+// consecutive coefficients per load.  The block stages w_lo once,
+// component-major, so the 4 weights of a lane's coefficients are one
+// conflict-free 16-byte shared load per component.  Per bucket a lane
+// reduces its sum, multiplies it by w_hi[b] and adds it to its unit total;
+// the warp reduces the totals once per unit into
+// partial[p * units_per_poly + unit].  The 4 wide multiply-adds per
+// coefficient bound it (about 80 us of the multiply-add pipe for 108 x 2^20
+// coefficients), above the HBM time of the reads.
+constexpr uint32_t kEvalLoBits = 10;
+constexpr uint32_t kEvalUnitBuckets = 8;
+__global__ void __launch_bounds__(256, 2) poly_eval_bucket_kernel(PolyTable t, uint32_t n_polys, uint32_t units_per_poly,
+                                                                  const qm31* __restrict__ w_lo,
+                                                                  const qm31* __restrict__ w_hi,
+                                                                  qm31* __restrict__ partial) {
+  __shared__ uint4 wc[4][256];  // wc[k][q]: component k of w_lo[4q .. 4q+3]
+  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t unit = blockIdx.x * 8 + warp;
+  const bool active = unit < n_polys * units_per_poly;
+  const uint32_t p = active ? unit / units_per_poly : 0, u = unit - p * units_per_poly;
+  const uint32_t b0 = u * kEvalUnitBuckets;
+  const uint32_t* __restrict__ col = t.p[p] + ((size_t)b0 << kEvalLoBits) + 4 * lane;
+  uint4 cur[8], nxt[8];
+  if (active) {
+#pragma unroll
+    for (int k = 0; k < 8; k++) cur[k] = ldg4(col + 128 * k);
+  }
+  {
+    const qm31 a = w_lo[4 * threadIdx.x], b = w_lo[4 * threadIdx.x + 1], c = w_lo[4 * threadIdx.x + 2],
+               d = w_lo[4 * threadIdx.x + 3];
+    wc[0][threadIdx.x] = make_uint4(a.a, b.a, c.a, d.a);
+    wc[1][threadIdx.x] = make_uint4(a.b, b.b, c.b, d.b);
+    wc[2][threadIdx.x] = make_uint4(a.c, b.c, c.c, d.c);
+    wc[3][threadIdx.x] = make_uint4(a.d, b.d, c.d, d.d);
+  }
+  __syncthreads();
+  if (!active) return;  // no block barrier follows
+  qm31 tot = qm31_zero();
+#pragma unroll 1
+  for (uint32_t bi = 0; bi < kEvalUnitBuckets; bi++) {
+    if (bi + 1 < kEvalUnitBuckets) {
+#pragma unroll
+      for (int k = 0; k < 8; k++) nxt[k] = ldg4(col + ((size_t)(bi + 1) << kEvalLoBits) + 128 * k);
+    }
+    acc4 s{0, 0, 0, 0};
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      const uint32_t q = 32 * k + lane;
+      const uint4 x = cur[k];
+      const uint4 wa = wc[0][q], wb = wc[1][q], wcc = wc[2][q], wd = wc[3][q];
+      s.a += (uint64_t)wa.x * x.x + (uint64_t)wa.y * x.y + (uint64_t)wa.z * x.z + (uint64_t)wa.w * x.w;
+      s.b += (uint64_t)wb.x * x.x + (uint64_t)wb.y * x.y + (uint64_t)wb.z * x.z + (uint64_t)wb.w * x.w;
+      s.c += (uint64_t)wcc.x * x.x + (uint64_t)wcc.y * x.y + (uint64_t)wcc.z * x.z + (uint64_t)wcc.w * x.w;
+      s.d += (uint64_t)wd.x * x.x + (uint64_t)wd.y * x.y + (uint64_t)wd.z * x.z + (uint64_t)wd.w * x.w;
+      acc4_fold(s);
+    }
+    tot = qm31_add(tot, qm31_mul(acc4_reduce(s), w_hi[b0 + bi]));
+#pragma unroll
+    for (int k = 0; k < 8; k++) cur[k] = nxt[k];
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const qm31 v = {__shfl_xor_sync(0xffffffffu, tot.a, o), __shfl_xor_sync(0xffffffffu, tot.b, o),
+                    __shfl_xor_sync(0xffffffffu, tot.c, o), __shfl_xor_sync(0xffffffffu, tot.d, o)};
+    tot = qm31_add(tot, v);
+  }
+  if (lane == 0) partial[unit] = tot;
+}
+
 uint32_t poly_eval_chunks(uint32_t lg) { return lg > 10 ? 1u << (lg - 10) : 1u; }  // kOodsChunk indices each
+// kEvalLoBits wherever the bucketed form applies (at least kEvalUnitBuckets
+// buckets per polynomial and a w_hi table of at most 2^14 entries).
+uint32_t poly_eval_lo_bits(uint32_t lg) { return lg >= 13 && lg <= 24 ? kEvalLoBits : lg / 2; }
 
 int launch_poly_eval(const uint32_t* const* polys, uint32_t n_polys, uint32_t lg, const qm31* d_w_lo,
                      const qm31* d_w_hi, qm31* d_partial, qm31* d_out, cudaStream_t s, char* err, size_t err_len) {
   STWO_ARG_CHECK(n_polys >= 1 && n_polys <= (uint32_t)kMaxPolys && lg <= 30, "poly eval: bad shape");
   PolyTable pt;
   for (uint32_t c = 0; c < n_polys; c++) pt.p[c] = polys[c];
+  const uint32_t h = poly_eval_lo_bits(lg);
+  if (h == kEvalLoBits) {
+    // 2^(lg - h) >= kEvalUnitBuckets buckets of 1024 indices per polynomial
+    const uint32_t units_per_poly = (1u << (lg - h)) / kEvalUnitBuckets;
+    const uint32_t units = n_polys * units_per_poly;
+    poly_eval_bucket_kernel<<<(units + 7) / 8, 256, 0, s>>>(pt, n_polys, units_per_poly, d_w_lo, d_w_hi, d_partial);
+    STWO_CHECK_LAUNCH();
+    oods_reduce_kernel<<<n_polys, 256, 0, s>>>(d_partial, units_per_poly, d_out);
+    STWO_CHECK_LAUNCH();
+    return STWO_B200_OK;
+  }
   const uint32_t chunks = poly_eval_chunks(lg);
   // about 4 waves of 148 SMs x 6 resident blocks, at least 8 polynomials (one per warp) per group
   const uint32_t groups = std::max(1u, std::min({8u, (4u * 148u * 6u + chunks - 1) / chunks, n_polys / 8u}));
-  oods_eval_kernel<<<dim3(chunks, groups), 256, 0, s>>>(pt, n_polys, lg, lg / 2, d_w_lo, d_w_hi, d_partial);
+  oods_eval_kernel<<<dim3(chunks, groups), 256, 0, s>>>(pt, n_polys, lg, h, d_w_lo, d_w_hi, d_partial);
   STWO_CHECK_LAUNCH();
   oods_reduce_kernel<<<n_polys, 256, 0, s>>>(d_partial, chunks, d_out);
   STWO_CHECK_LAUNCH();
@@ -815,7 +902,7 @@ __global__ void eval_weights_kernel(spoint z, uint32_t lg, uint32_t h, qm31* __r
 
 int launch_eval_weights(const spoint& z, uint32_t lg, qm31* d_w_lo, qm31* d_w_hi, cudaStream_t s, char* err,
                         size_t err_len) {
-  eval_weights_kernel<<<1, 1024, 0, s>>>(z, lg, lg / 2, d_w_lo, d_w_hi);
+  eval_weights_kernel<<<1, 1024, 0, s>>>(z, lg, poly_eval_lo_bits(lg), d_w_lo, d_w_hi);
   STWO_CHECK_LAUNCH();
   return STWO_B200_OK;
 }
@@ -1906,7 +1993,7 @@ int WideFibProver::prove_body(const uint32_t* d_a, const uint32_t* d_b, ProofOut
     // (log_n coefficients each) are sampled at the OODS point itself.
     STWO_ARG_CHECK(L1 == lift && eval_log - 1 == log_n, "sampling assumes one column size");
     STWO_ARG_CHECK(log_n <= 31, "log size too large for the fold factors");
-    const uint32_t lg = log_n, h = lg / 2;
+    const uint32_t lg = log_n, h = poly_eval_lo_bits(lg);
     size_t n_w = (1u << h) + (1u << (lg - h));
     phase(kOodsSampling);
     fs_oods_kernel<<<1, 1024, 0, s>>>(d_chan, t2.layer(0), lg, h, d_small, d_small + (1u << h), d_fs);

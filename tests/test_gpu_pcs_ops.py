@@ -123,11 +123,14 @@ def test_generate_secure_powers(be, oracle, n):
     assert (be.generate_secure_powers(felt, n) == oracle.generate_secure_powers(felt, n)).all()
 
 
-@pytest.mark.parametrize("log_n", [0, 1, 2, 5, 8, 9, 10, 11, 16, 20])
+# 13..24 run the bucketed form (1024-index buckets, 8 per warp), the others
+# the chunked one.
+@pytest.mark.parametrize("log_n", [0, 1, 2, 5, 8, 9, 10, 11, 12, 13, 16, 20, 21, 24])
 def test_eval_at_point(be, oracle, log_n):
     rng = np.random.default_rng(6000 + log_n)
     polys = [rng.integers(0, P, 1 << log_n, dtype=np.uint32) for _ in range(3)]
     polys[1][0] = P
+    polys[0][rng.integers(0, 1 << log_n, 1 + (1 << log_n) // 64)] = P  # words equal to P count as 0
     point = rpoint(rng)
     dev = [DeviceColumn.from_host(c) for c in polys]
     got = be.batch_eval_at_point(dev, point)
@@ -137,9 +140,10 @@ def test_eval_at_point(be, oracle, log_n):
     assert (be.eval_at_point(dev[2], point) == oracle.eval_at_secure_point(polys[2], point)).all()
 
 
-def test_batch_eval_at_point_many_polys(be, oracle):
-    rng = np.random.default_rng(6100)
-    polys = [rng.integers(0, P, 1 << 6, dtype=np.uint32) for _ in range(1030)]  # two launches
+@pytest.mark.parametrize("log_n", [6, 14])
+def test_batch_eval_at_point_many_polys(be, oracle, log_n):
+    rng = np.random.default_rng(6100 + log_n)
+    polys = [rng.integers(0, P, 1 << log_n, dtype=np.uint32) for _ in range(1030)]  # two launches
     point = rpoint(rng)
     got = be.batch_eval_at_point([DeviceColumn.from_host(c) for c in polys], point)
     for k in (0, 511, 1023, 1024, 1029):
