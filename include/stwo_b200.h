@@ -131,6 +131,22 @@ int stwo_b200_evaluate_polynomials(const uint32_t* const* d_coeffs, const uint32
                                    uint32_t log_blowup, uint32_t* const* d_evals, const uint32_t* d_twiddles,
                                    uint32_t tree_log_size, void* stream, char* err, size_t err_len);
 
+/* stwo_b200_interpolate_columns followed by stwo_b200_evaluate_polynomials
+ * for n_cols columns of one log size, as CommitmentTreeProver::new runs them
+ * for a trace (crates/stwo/src/prover/pcs/mod.rs:707-781): reads d_src[i]
+ * (bit-reversed evaluations on CanonicCoset(log_size); d_src NULL: d_coeffs
+ * holds them and is transformed in place), writes the coefficients to
+ * d_coeffs[i] and their evaluations on CanonicCoset(log_size + log_blowup)
+ * to d_evals[i].  Same words as the two calls; the interpolation's last pass
+ * and the evaluation's first run as one kernel where the pass plan allows
+ * (log sizes 20 and 21 by default, blowup 1 or 2).  No single reference
+ * counterpart: the reference runs ntt_b2n_column then evaluate_columns
+ * (raw.rs:472-479, 90-97). */
+int stwo_b200_interpolate_evaluate_columns(const uint32_t* const* d_src, uint32_t* const* d_coeffs,
+                                           uint32_t* const* d_evals, uint32_t n_cols, uint32_t log_size,
+                                           uint32_t log_blowup, const uint32_t* d_itwiddles, const uint32_t* d_twiddles,
+                                           uint32_t tree_log_size, void* stream, char* err, size_t err_len);
+
 /* ------------------------------------------------------ MerkleOpsLifted -- */
 /* MerkleOpsLifted<Blake2sMerkleHasherGeneric<m31_output>>::build_leaves
  * (prover/vcs_lifted/ops.rs:14-15; spec prover/backend/cpu/merkle_lifted.rs:

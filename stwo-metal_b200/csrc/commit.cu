@@ -84,8 +84,8 @@ struct Committer {
       g++;
       if (flags & STWO_B200_COMMIT_PER_COLUMN) {
         for (uint32_t i : kv.second)
-          if ((rc = interpolate_evaluate(d_evals, coeffs, ldes, {i}, err, err_len))) return rc;
-      } else if ((rc = interpolate_evaluate(d_evals, coeffs, ldes, kv.second, err, err_len))) {
+          if ((rc = transform(d_evals, coeffs, ldes, {i}, err, err_len))) return rc;
+      } else if ((rc = transform(d_evals, coeffs, ldes, kv.second, err, err_len))) {
         return rc;
       }
     }
@@ -99,22 +99,50 @@ struct Committer {
     return rc;
   }
 
-  int interpolate_evaluate(const uint32_t* const* evals, uint32_t* const* coeffs, uint32_t* const* ldes,
-                           const std::vector<uint32_t>& cols, char* err, size_t err_len) {
-    std::vector<const uint32_t*> e;
-    std::vector<uint32_t*> c, d;
-    std::vector<uint32_t> lg;
+  // interpolate + evaluate of the columns `cols`: one
+  // stwo_b200_interpolate_evaluate_columns call per log size (the
+  // interpolation's last pass and the evaluation's first share a kernel where
+  // the pass plan allows); the columns below log 3 in one batched pair of
+  // calls.
+  int transform(const uint32_t* const* evals, uint32_t* const* coeffs, uint32_t* const* ldes,
+                const std::vector<uint32_t>& cols, char* err, size_t err_len) {
+    std::map<uint32_t, std::vector<uint32_t>> by_size;
+    std::vector<const uint32_t*> se;
+    std::vector<uint32_t*> sc, sd;
+    std::vector<uint32_t> slg;
     for (uint32_t i : cols) {
-      e.push_back(evals[i]);
-      c.push_back(coeffs[i]);
-      d.push_back(ldes[i]);
-      lg.push_back(logs[i]);
+      if (logs[i] >= 3) {
+        by_size[logs[i]].push_back(i);
+      } else {
+        se.push_back(evals[i]);
+        sc.push_back(coeffs[i]);
+        sd.push_back(ldes[i]);
+        slg.push_back(logs[i]);
+      }
     }
-    const uint32_t n = (uint32_t)cols.size();
-    int rc = stwo_b200_interpolate_columns_into(e.data(), c.data(), lg.data(), nullptr, n, itw, tree_log, s, err,
-                                                err_len);
-    if (rc) return rc;
-    return stwo_b200_evaluate_polynomials(c.data(), lg.data(), n, blowup, d.data(), tw, tree_log, s, err, err_len);
+    int rc;
+    if (!se.empty()) {
+      const uint32_t n = (uint32_t)se.size();
+      if ((rc = stwo_b200_interpolate_columns_into(se.data(), sc.data(), slg.data(), nullptr, n, itw, tree_log, s, err,
+                                                   err_len)))
+        return rc;
+      if ((rc = stwo_b200_evaluate_polynomials(sc.data(), slg.data(), n, blowup, sd.data(), tw, tree_log, s, err,
+                                               err_len)))
+        return rc;
+    }
+    for (const auto& kv : by_size) {
+      std::vector<const uint32_t*> e;
+      std::vector<uint32_t*> c, d;
+      for (uint32_t i : kv.second) {
+        e.push_back(evals[i]);
+        c.push_back(coeffs[i]);
+        d.push_back(ldes[i]);
+      }
+      if ((rc = stwo_b200_interpolate_evaluate_columns(e.data(), c.data(), d.data(), (uint32_t)e.size(), kv.first,
+                                                       blowup, itw, tw, tree_log, s, err, err_len)))
+        return rc;
+    }
+    return STWO_B200_OK;
   }
 
   int enqueue(const uint32_t* const* evals, uint32_t* const* coeffs, uint32_t* const* ldes, uint8_t* const* layers,
@@ -123,11 +151,11 @@ struct Committer {
     int rc;
     if (flags & STWO_B200_COMMIT_PER_COLUMN) {
       for (uint32_t i = 0; i < n; i++)
-        if ((rc = interpolate_evaluate(evals, coeffs, ldes, {i}, err, err_len))) return rc;
+        if ((rc = transform(evals, coeffs, ldes, {i}, err, err_len))) return rc;
     } else {
       std::vector<uint32_t> all(n);
       for (uint32_t i = 0; i < n; i++) all[i] = i;
-      if ((rc = interpolate_evaluate(evals, coeffs, ldes, all, err, err_len))) return rc;
+      if ((rc = transform(evals, coeffs, ldes, all, err, err_len))) return rc;
     }
     std::vector<uint32_t> lde_logs(n);
     for (uint32_t i = 0; i < n; i++) lde_logs[i] = logs[i] + blowup;
@@ -329,10 +357,10 @@ extern "C" int stwo_b200_committer_autotune(stwo_b200_committer* h, const uint32
     float best_ms = 1e30f;
     for (const auto& cand : candidate_splits(n)) {
       if ((rc = stwo_b200_fft_set_plan(n, cand.data(), (uint32_t)cand.size(), err, err_len))) break;
-      if ((rc = c.interpolate_evaluate(d_evals, d_coeffs, d_ldes, kv.second, err, err_len))) break;  // warm-up
+      if ((rc = c.transform(d_evals, d_coeffs, d_ldes, kv.second, err, err_len))) break;  // warm-up
       cudaEventRecord(a, c.s);
       for (uint32_t r = 0; r < reps && !rc; r++)
-        rc = c.interpolate_evaluate(d_evals, d_coeffs, d_ldes, kv.second, err, err_len);
+        rc = c.transform(d_evals, d_coeffs, d_ldes, kv.second, err, err_len);
       cudaEventRecord(b, c.s);
       if (rc) break;
       if (cudaEventSynchronize(b) != cudaSuccess) {

@@ -20,6 +20,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "fft.hpp"
 #include "field.cuh"
 #include "stream.cuh"
 
@@ -510,31 +511,38 @@ __device__ __forceinline__ void warp_phase_hi(uint32_t (&v)[32], const uint32_t*
 
 // Stages the 1023 twiddles of a 10-layer tile position (as fft_pass_kernel),
 // doubled for bfly2 / ibfly2: slot s of the table holds layer
-// lam = clz(1023 - s) - 22, entry s - (1024 - 2^(10 - lam)).  Each of the 256 threads loads its 4 slots
-// before storing any, so the block waits for one memory round trip instead
-// of one per layer.
+// lam = clz(1023 - s) - 22, entry s - (1024 - 2^(10 - lam)).  Thread t holds
+// slots t, t + 256 (lam 0), t + 512 (lam 1) and t + 768 (lam >= 2), and loads
+// all four before storing any, so the block waits for one memory round trip
+// instead of one per layer.  CIRCLE: layer0 is 0, whose twiddles come from
+// line layer 1 (circle_tw); otherwise layer0 >= 1.
+template <bool CIRCLE>
 __device__ __forceinline__ void stage_tws10(const FftPass& p, uint64_t hi, uint32_t* tws) {
+  const uint32_t* tail = p.tree + p.tree_len;  // tree layer L starts 2^(N - L) words before the end
+  const uint32_t N = p.log_domain, L0 = CIRCLE ? 0u : p.layer0, t = threadIdx.x;
   uint32_t val[4];
-#pragma unroll
-  for (int k = 0; k < 4; k++) {
-    const uint32_t s = threadIdx.x + 256u * k;
-    const uint32_t u = 1023u - s;
-    val[k] = 0;
-    if (u != 0) {
-      const uint32_t lam = __clz(u) - 22;
-      const uint64_t h = (hi << (9 - lam)) + (s - (1024u - (1024u >> lam)));
-      const uint32_t layer = p.layer0 + lam;
-      if (layer == 0)
-        val[k] = circle_tw(p.tree + (p.tree_len - (1ull << (p.log_domain - 1))), h);
-      else
-        val[k] = __ldg(p.tree + (p.tree_len - (1ull << (p.log_domain - layer))) + h);
-    }
+  const uint64_t h0 = (hi << 9) + t;
+  if (CIRCLE) {
+    const uint32_t* lt0 = tail - (1ull << (N - 1));
+    val[0] = circle_tw(lt0, h0);
+    val[1] = circle_tw(lt0, h0 + 256);
+  } else {
+    const uint32_t* l0 = tail - (1ull << (N - L0)) + h0;
+    val[0] = __ldg(l0);
+    val[1] = __ldg(l0 + 256);
   }
-#pragma unroll
-  for (int k = 0; k < 4; k++) {
-    const uint32_t s = threadIdx.x + 256u * k;
-    if (s < 1023u) tws[s] = val[k] << 1;
+  val[2] = __ldg(tail - (1ull << (N - L0 - 1)) + (hi << 8) + t);
+  const uint32_t u = 255u - t;  // 1023 - slot
+  val[3] = 0;
+  if (u != 0) {
+    const uint32_t lam = __clz(u) - 22;
+    const uint64_t h = (hi << (9 - lam)) + (768u + t - (1024u - (1024u >> lam)));
+    val[3] = __ldg(tail - (1ull << (N - L0 - lam)) + h);
   }
+  tws[t] = val[0] << 1;
+  tws[t + 256] = val[1] << 1;
+  tws[t + 512] = val[2] << 1;
+  if (u != 0) tws[t + 768] = val[3] << 1;
 }
 
 // Staged column tile of the contiguous pass: word e of the 1024 at
@@ -627,7 +635,7 @@ __global__ void __launch_bounds__(256, 4) fft_warp_contig_kernel(FftPass p, FftC
     else
       tile_prefetch(cols.src[c] + base, buf, lane);
   }
-  stage_tws10(p, hi, tws);
+  stage_tws10<true>(p, hi, tws);
   __syncthreads();
   const uint32_t scale = p.scale;
   for (uint32_t g = 0; g < p.cpb; g++, c += kWarpCols) {
@@ -740,7 +748,7 @@ __global__ void __launch_bounds__(256, 4) fft_warp_strided_kernel(FftPass p, Fft
       v[j] = gi < p.src_len ? __ldg(src + gi) : 0u;
     }
   }
-  stage_tws10(p, hi, tws);
+  stage_tws10<false>(p, hi, tws);
   __syncthreads();
   if (INV) {
     warp_phase_lo<true>(v, tws, m);
@@ -766,6 +774,80 @@ __global__ void __launch_bounds__(256, 4) fft_warp_strided_kernel(FftPass p, Fft
 #pragma unroll
   for (int j = 0; j < 32; j++)
     dp[(uint64_t)((INV ? 32 : 1) * j) << L0] = scale != 1u ? m31_mul(v[j], scale) : v[j];
+}
+
+// The last pass of an interpolation fused with the first pass of the
+// evaluation on the 2^b times larger domain that follows it (interpolate,
+// then evaluate_into with the coefficients duplicated onto the 2^b
+// subdomains, prover/backend/simd/circle.rs:138-166,413-440).  Both are
+// 10-layer strided passes over the same tiles: layers L0..L0+9 of the 2^(L0+10)
+// interpolation (one tile position hi = 0) and of the 2^(L0+10+b) evaluation
+// (tile positions hi < 2^b, all reading the same coefficient tile).  A block
+// loads its tile of the interpolation's intermediate (lane-major), finishes
+// the inverse layers, stores the coefficients in place (row-major) and then,
+// for each hi, runs the forward layers from them and stores that tile of the
+// evaluation (lane-major).  hi = 0 starts from the coefficients in registers;
+// the later ones re-read the thread's own stores through L2.  Thread layout,
+// exchange tile and twiddle tables are those of fft_warp_strided_kernel; the
+// forward tables of all 2^b positions are staged with the inverse one.
+struct FftColsIE {
+  uint32_t* coef[kFftMaxCols];  // interpolation intermediate in, coefficients out
+  uint32_t* eval[kFftMaxCols];  // evaluation (2^b times longer) out
+};
+template <int L0T>
+__global__ void __launch_bounds__(256, 4) fft_warp_inv_fwd_kernel(FftPass pi, FftPass pf, FftColsIE cols,
+                                                                 uint32_t n_hi) {
+  extern __shared__ __align__(16) uint32_t smem[];
+  uint32_t* twi = smem;
+  uint32_t* xch = smem + 1024;
+  uint32_t* twf = xch + kXchWords;  // n_hi tables of 1024
+  constexpr uint32_t L0 = L0T;
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t c = lane & 7, m = (threadIdx.x >> 5) * 4 + (lane >> 3);
+  const uint64_t base = ((uint64_t)blockIdx.x << 3) + c;
+  uint32_t* __restrict__ coef = cols.coef[blockIdx.y] + base;
+  uint32_t* __restrict__ ev = cols.eval[blockIdx.y] + base;
+  uint32_t v[32];
+  {
+    const uint32_t* __restrict__ sp = coef + ((uint64_t)(32 * m) << L0);
+#pragma unroll
+    for (int j = 0; j < 32; j++) v[j] = __ldg(sp + ((uint64_t)j << L0));
+  }
+  stage_tws10<false>(pi, 0, twi);
+  for (uint32_t h = 0; h < n_hi; h++) stage_tws10<false>(pf, h, twf + 1024 * h);
+  __syncthreads();
+  warp_phase_lo<true>(v, twi, m);
+#pragma unroll
+  for (int j = 0; j < 32; j++) xch[xch_pos(32 * m + j, c)] = v[j];
+  __syncthreads();
+#pragma unroll
+  for (int j = 0; j < 32; j++) v[j] = xch[xch_pos(32 * j + m, c)];
+  warp_phase_hi<true>(v, twi);
+  uint32_t* __restrict__ cp = coef + ((uint64_t)m << L0);
+  const uint32_t scale = pi.scale;
+#pragma unroll
+  for (int j = 0; j < 32; j++) {
+    v[j] = m31_mul(v[j], scale);
+    cp[(uint64_t)(32 * j) << L0] = v[j];
+  }
+  for (uint32_t h = 0; h < n_hi; h++) {
+    if (h > 0) {
+#pragma unroll
+      for (int j = 0; j < 32; j++) v[j] = __ldcg(cp + ((uint64_t)(32 * j) << L0));
+    }
+    const uint32_t* tw = twf + 1024 * h;
+    __syncthreads();  // every thread has read its words of the previous exchange
+    warp_phase_hi<false>(v, tw);
+#pragma unroll
+    for (int j = 0; j < 32; j++) xch[xch_pos(32 * j + m, c)] = v[j];
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < 32; j++) v[j] = xch[xch_pos(32 * m + j, c)];
+    warp_phase_lo<false>(v, tw, m);
+    uint32_t* __restrict__ dp = ev + ((uint64_t)h << (L0 + 10)) + ((uint64_t)(32 * m) << L0);
+#pragma unroll
+    for (int j = 0; j < 32; j++) dp[(uint64_t)j << L0] = v[j];
+  }
 }
 
 template <bool INV>
@@ -1044,7 +1126,7 @@ std::vector<uint32_t> fft_split(uint32_t log_n) { return split_for(log_n); }
 // 2^split[0] rows are consecutive; the later passes take every row.
 int interpolate_pass(uint32_t* const* cols, uint32_t n_cols, uint32_t log_n, const std::vector<uint32_t>& split,
                      uint32_t pi, uint64_t row_begin, uint64_t row_end, const uint32_t* d_itwiddles,
-                     uint32_t tree_log_size, cudaStream_t s, char* err, size_t err_len) {
+                     uint32_t tree_log_size, cudaStream_t s, char* err, size_t err_len, const uint32_t* const* src) {
   STWO_ARG_CHECK(log_n >= 3 && log_n <= 30 && pi < split.size(), "interpolate pass out of range");
   STWO_ARG_CHECK(d_itwiddles && log_n - 1 <= tree_log_size, "twiddle tree (log %u) too small for log size %u",
                  tree_log_size, log_n);
@@ -1062,6 +1144,7 @@ int interpolate_pass(uint32_t* const* cols, uint32_t n_cols, uint32_t log_n, con
   p.scale = (pi + 1 == split.size()) ? host_pow2_inv(log_n) : 1u;
   std::vector<const uint32_t*> srcs(cols, cols + n_cols);
   std::vector<uint32_t*> dsts(cols, cols + n_cols);
+  if (pi == 0 && src) srcs.assign(src, src + n_cols);
   if (pi == 0) {
     const uint64_t tile_rows = 1ull << p.T;
     STWO_ARG_CHECK(row_begin % tile_rows == 0 && row_end % tile_rows == 0 && row_begin < row_end &&
@@ -1072,6 +1155,92 @@ int interpolate_pass(uint32_t* const* cols, uint32_t n_cols, uint32_t log_n, con
                              (row_end - row_begin) / tile_rows);
   }
   return launch_pass<true>(p, srcs, dsts, log_n, s, err, err_len);
+}
+
+int interpolate_evaluate(uint32_t* const* coeffs, uint32_t* const* evals, uint32_t n_cols, uint32_t log_n,
+                         uint32_t log_blowup, const std::vector<uint32_t>& split, uint32_t first_pass,
+                         const uint32_t* d_itwiddles, const uint32_t* d_twiddles, uint32_t tree_log_size,
+                         cudaStream_t s, char* err, size_t err_len, const uint32_t* const* src0) {
+  const uint32_t np = (uint32_t)split.size();
+  const uint32_t N = log_n + log_blowup;
+  STWO_ARG_CHECK(log_n >= 3 && N <= 30 && first_pass < np && split == split_for(log_n),
+                 "interpolate_evaluate: log size %u, blowup %u, pass %u", log_n, log_blowup, first_pass);
+  STWO_ARG_CHECK(d_twiddles && N - 1 <= tree_log_size, "twiddle tree (log %u) too small for log size %u",
+                 tree_log_size, N);
+  const uint32_t L0 = log_n - split.back();
+  const bool fused = np >= 2 && split.back() == 10 && (L0 == 10 || L0 == 11) && log_blowup >= 1 && log_blowup <= 2;
+  const uint32_t* const* src = first_pass == 0 ? src0 : nullptr;
+  if (!fused) {
+    for (uint32_t pi = first_pass; pi < np; pi++) {
+      int rc = interpolate_pass(coeffs, n_cols, log_n, split, pi, 0, 1ull << log_n, d_itwiddles, tree_log_size, s,
+                                err, err_len, src);
+      if (rc) return rc;
+    }
+    std::vector<uint32_t> logs(n_cols, log_n);
+    return stwo_b200_evaluate_polynomials(const_cast<const uint32_t* const*>(coeffs), logs.data(), n_cols,
+                                          log_blowup, evals, d_twiddles, tree_log_size, s, err, err_len);
+  }
+  for (uint32_t pi = first_pass; pi + 1 < np; pi++) {
+    int rc = interpolate_pass(coeffs, n_cols, log_n, split, pi, 0, 1ull << log_n, d_itwiddles, tree_log_size, s, err,
+                              err_len, src);
+    if (rc) return rc;
+  }
+  FftPass pi;
+  pi.tree = d_itwiddles;
+  pi.tree_len = 1ull << tree_log_size;
+  pi.src_mask = ~0ull;
+  pi.src_len = ~0ull;
+  pi.log_domain = log_n;
+  pi.layer0 = L0;
+  pi.T = 10;
+  pi.C = 3;
+  pi.scale = host_pow2_inv(log_n);
+  FftPass pf = pi;
+  pf.tree = d_twiddles;
+  pf.log_domain = N;
+  pf.scale = 1u;
+  const uint32_t n_hi = 1u << log_blowup;
+  const size_t smem = (1024 + kXchWords + 1024 * n_hi) * sizeof(uint32_t);
+  // the limit is set once per device, for the largest table set (blowup 2)
+  constexpr size_t smem_max = (1024 + kXchWords + 1024 * 4) * sizeof(uint32_t);
+  static std::atomic<uint32_t> attr10{0}, attr11{0};
+  STWO_CUDA_TRY(L0 == 10 ? ensure_smem_limit(fft_warp_inv_fwd_kernel<10>, (int)smem_max, attr10)
+                         : ensure_smem_limit(fft_warp_inv_fwd_kernel<11>, (int)smem_max, attr11));
+  for (uint32_t c0 = 0; c0 < n_cols; c0 += kFftMaxCols) {
+    const uint32_t nc = std::min<uint32_t>(kFftMaxCols, n_cols - c0);
+    FftColsIE cols;
+    for (uint32_t i = 0; i < nc; i++) {
+      STWO_ARG_CHECK(coeffs[c0 + i] && evals[c0 + i], "null column %u", c0 + i);
+      cols.coef[i] = coeffs[c0 + i];
+      cols.eval[i] = evals[c0 + i];
+    }
+    const dim3 grid(1u << (L0 - 3), nc);
+    if (L0 == 10)
+      fft_warp_inv_fwd_kernel<10><<<grid, 256, smem, s>>>(pi, pf, cols, n_hi);
+    else
+      fft_warp_inv_fwd_kernel<11><<<grid, 256, smem, s>>>(pi, pf, cols, n_hi);
+    STWO_CHECK_LAUNCH();
+  }
+  // The remaining evaluation passes, in place, top layers first (as
+  // stwo_b200_evaluate_polynomials).
+  const std::vector<PassPlan> plan = plan_passes(log_n);
+  std::vector<const uint32_t*> srcs(evals, evals + n_cols);
+  std::vector<uint32_t*> dsts(evals, evals + n_cols);
+  for (size_t k = plan.size() - 1; k-- > 0;) {
+    FftPass p;
+    p.tree = d_twiddles;
+    p.tree_len = 1ull << tree_log_size;
+    p.log_domain = N;
+    p.layer0 = plan[k].layer0;
+    p.T = plan[k].T;
+    p.C = plan[k].C;
+    p.scale = 1u;
+    p.src_mask = ~0ull;
+    p.src_len = ~0ull;
+    int rc = launch_pass<false>(p, srcs, dsts, N, s, err, err_len);
+    if (rc) return rc;
+  }
+  return STWO_B200_OK;
 }
 
 }  // namespace stwo_b200
@@ -1157,6 +1326,39 @@ extern "C" int stwo_b200_evaluate_polynomials(const uint32_t* const* d_coeffs, c
     STWO_CHECK_LAUNCH();
   }
   return ok(err, err_len);
+}
+
+// interpolate_columns + evaluate_polynomials of one column size, as the
+// commitment of a trace runs them (prover/pcs/mod.rs:707-781); the
+// interpolation's last pass and the evaluation's first share a kernel where
+// interpolate_evaluate allows it.
+extern "C" int stwo_b200_interpolate_evaluate_columns(const uint32_t* const* d_src, uint32_t* const* d_coeffs,
+                                                      uint32_t* const* d_evals, uint32_t n_cols, uint32_t log_size,
+                                                      uint32_t log_blowup, const uint32_t* d_itwiddles,
+                                                      const uint32_t* d_twiddles, uint32_t tree_log_size,
+                                                      void* stream, char* err, size_t err_len) {
+  cudaStream_t s = as_stream(stream);
+  STWO_ARG_CHECK(n_cols == 0 || (d_coeffs && d_evals), "null column arrays");
+  STWO_ARG_CHECK(log_size <= 30 && log_size + log_blowup <= 30, "log size %u + blowup %u too large", log_size,
+                 log_blowup);
+  if (n_cols == 0) return ok(err, err_len);
+  std::vector<uint32_t> logs(n_cols, log_size);
+  int rc;
+  if (log_size < 3) {
+    rc = d_src ? interpolate_impl(d_src, d_coeffs, logs.data(), nullptr, n_cols, d_itwiddles, tree_log_size, s, err,
+                                  err_len)
+               : interpolate_impl(d_coeffs, d_coeffs, logs.data(), nullptr, n_cols, d_itwiddles, tree_log_size, s,
+                                  err, err_len);
+    if (rc == 0)
+      rc = stwo_b200_evaluate_polynomials(const_cast<const uint32_t* const*>(d_coeffs), logs.data(), n_cols,
+                                          log_blowup, d_evals, d_twiddles, tree_log_size, stream, err, err_len);
+  } else {
+    STWO_ARG_CHECK(d_itwiddles && log_size - 1 <= tree_log_size, "twiddle tree (log %u) too small for log size %u",
+                   tree_log_size, log_size);
+    rc = interpolate_evaluate(d_coeffs, d_evals, n_cols, log_size, log_blowup, split_for(log_size), 0, d_itwiddles,
+                              d_twiddles, tree_log_size, s, err, err_len, d_src);
+  }
+  return rc ? rc : ok(err, err_len);
 }
 
 extern "C" int stwo_b200_fft_set_plan(uint32_t log_size, const uint32_t* pass_layers, uint32_t n_passes, char* err,

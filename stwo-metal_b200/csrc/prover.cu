@@ -1916,19 +1916,18 @@ int WideFibProver::prove_body(const uint32_t* d_a, const uint32_t* d_b, ProofOut
     wide_fib_trace_kernel<<<grid1d(rows, 256), 256, 0, s>>>(d_a, d_b, d_coeffs, N, rows, rows);
     STWO_CHECK_LAUNCH();
   }
+  // Interpolation passes before the last (the first one already ran per
+  // chunk when chunked); the last one runs with the evaluation, fused with its
+  // first pass where the split allows (interpolate_evaluate).
+  const uint32_t n_ifft = (uint32_t)ifft_split.size();
   phase(kTraceInterpolate);
-  if (chunked_ifft) {
-    for (uint32_t pi = 1; pi < ifft_split.size(); pi++)
-      if ((rc = interpolate_pass(coeff_ptrs.data(), N, log_n, ifft_split, pi, 0, rows, d_itw, tree_log, s, err,
-                                 err_len)))
-        return rc;
-  } else if ((rc = stwo_b200_interpolate_columns(coeff_ptrs.data(), logs_n.data(), nullptr, N, d_itw, tree_log, s,
-                                                 err, err_len))) {
-    return rc;
-  }
+  for (uint32_t pi = chunked_ifft ? 1 : 0; pi + 1 < n_ifft; pi++)
+    if ((rc = interpolate_pass(coeff_ptrs.data(), N, log_n, ifft_split, pi, 0, rows, d_itw, tree_log, s, err,
+                               err_len)))
+      return rc;
   phase(kTraceEvaluate);
-  if ((rc = stwo_b200_evaluate_polynomials(const_cast<const uint32_t* const*>(coeff_ptrs.data()), logs_n.data(), N,
-                                           blowup, eval_ptrs.data(), d_tw, tree_log, s, err, err_len)))
+  if ((rc = interpolate_evaluate(coeff_ptrs.data(), eval_ptrs.data(), N, log_n, blowup, ifft_split, n_ifft - 1, d_itw,
+                                 d_tw, tree_log, s, err, err_len)))
     return rc;
   phase(kTraceMerkle);
   if ((rc = commit_columns(eval_ptrs.data(), logs_1, t1, err, err_len))) return rc;

@@ -200,6 +200,17 @@ class B200Backend:
                  C.c_uint32(tree.log_size), self.stream)
         return outs
 
+    def interpolate_evaluate_into(self, srcs, coeffs, log_blowup: int, tree: TwiddleTree, outs):
+        """interpolate_columns + evaluate_polynomials of same-size columns in one
+        call: srcs (evaluations, or None to transform coeffs in place) ->
+        coeffs -> outs on the 2^log_blowup times larger domain."""
+        log_size = coeffs[0].log_size if coeffs else 0
+        ffi.call("stwo_b200_interpolate_evaluate_columns", _ptr_array(srcs) if srcs is not None else None,
+                 _ptr_array(coeffs), _ptr_array(outs), C.c_uint32(len(coeffs)), C.c_uint32(log_size),
+                 C.c_uint32(log_blowup), C.c_void_p(tree.itwiddles.ptr), C.c_void_p(tree.twiddles.ptr),
+                 C.c_uint32(tree.log_size), self.stream)
+        return outs
+
     # ---- PolyOps::evaluate_polynomials ---------------------------------------
     def evaluate_polynomials(self, coeffs, log_blowup: int, tree: TwiddleTree):
         outs = [DeviceColumn(c.length << log_blowup, self.stream) for c in coeffs]

@@ -144,6 +144,29 @@ def test_uneven_batch_roundtrip(be, oracle, big_tree):
         assert (e.to_host() == oracle.evaluate(co, l + 2, tw)).all()
 
 
+@pytest.mark.parametrize("log_n,log_blowup", [(1, 1), (3, 1), (8, 2), (16, 1), (20, 0), (20, 1), (20, 2), (21, 1),
+                                               (21, 2)])
+@pytest.mark.parametrize("in_place", [False, True])
+def test_interpolate_evaluate(be, oracle, big_tree, log_n, log_blowup, in_place):
+    # interpolate_columns + evaluate_polynomials in one call: at logs 20 and 21
+    # with a blowup the interpolation's last pass and the evaluation's first
+    # are one kernel.  Words equal to P included.
+    tree, tw, itw = big_tree
+    r = rng(3000 + log_n)
+    vals = [rand_col(r, log_n) for _ in range(3)]
+    vals[1][::5] = P
+    srcs = [DeviceColumn.from_host(v) for v in vals]
+    coeffs = srcs if in_place else [DeviceColumn(1 << log_n) for _ in vals]
+    outs = [DeviceColumn(1 << (log_n + log_blowup)) for _ in vals]
+    be.interpolate_evaluate_into(None if in_place else srcs, coeffs, log_blowup, tree, outs)
+    for k, v in enumerate(vals):
+        co = oracle.interpolate(v, itw)
+        assert (coeffs[k].to_host() == co).all(), k
+        assert (outs[k].to_host() == oracle.evaluate(co, log_n + log_blowup, tw)).all(), k
+        if not in_place:
+            assert (srcs[k].to_host() == v).all()
+
+
 def test_p_valued_inputs(be, oracle, big_tree):
     # Words equal to P (the redundant zero) propagate exactly like SimdBackend.
     tree, tw, itw = big_tree

@@ -20,6 +20,11 @@ CASES = [
     (12, 32, 1, 3, 1, 16, True),
     (14, 100, 1, 1, 0, 3, False),
     (16, 64, 1, 1, 0, 3, False),
+    # the interpolation's last pass fused with the evaluation's first
+    # (layers 10..19 at log 20, 11..20 at log 21; blowup 1 and 2)
+    (20, 8, 1, 1, 0, 3, False),
+    (20, 4, 2, 1, 0, 3, False),
+    (21, 4, 1, 1, 0, 3, False),
 ]
 
 
@@ -79,15 +84,16 @@ def test_phase_timing_does_not_change_proofs(oracle):
 
 
 @pytest.mark.parametrize("pinned", [False, True])
-@pytest.mark.parametrize("log_n", [12, 16])
+@pytest.mark.parametrize("log_n", [12, 16, 20])
 def test_prove_from_host_columns(oracle, pinned, log_n):
     # host inputs (pageable numpy, or page-locked memory from the library):
-    # copied chunk by chunk by the prover, the same proof bytes.  At log 16
+    # copied chunk by chunk by the prover, the same proof bytes.  From log 16
     # the interpolation is split in passes and its first pass runs chunk by
-    # chunk as the trace rows are generated.
+    # chunk as the trace rows are generated; at log 20 its last pass runs
+    # fused with the evaluation.
     import ctypes as C
     from stwo_b200 import ffi
-    cols = 24
+    cols = 24 if log_n < 20 else 6
     a, b = oracle.wide_fib_inputs(log_n, 55)
     ref = oracle.prove_wide_fib(oracle.wide_fib_config(log_n, cols), a, b)
     prover = WideFibProver(wide_fib_config(log_n, cols))
