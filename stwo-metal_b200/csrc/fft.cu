@@ -572,6 +572,18 @@ __device__ __forceinline__ void tile_wait() {
   asm volatile("cp.async.wait_group 0;\n" ::: "memory");
   __syncwarp();
 }
+// Bulk store of one staged-tile line (32 words, written by this thread) to
+// 128 bytes of global memory; the fence makes the thread's shared-memory
+// writes visible to the bulk copy.
+__device__ __forceinline__ void line_bulk_store(uint32_t* gdst, const uint32_t* line) {
+  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], 128;\n" ::"l"(gdst), "r"(smem_addr(line))
+               : "memory");
+  asm volatile("cp.async.bulk.commit_group;\n" ::: "memory");
+}
+// This thread's bulk stores have read their shared-memory source / are done.
+__device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory"); }
 // Tile position hi of a natural-order column of 2^log_n words (log_n >= 10)
 // staged in bit-reversed order, which fuses ColumnOps::bit_reverse_column
 // (prover/backend/simd/bit_reverse.rs:21-33) into the first pass: word e of
@@ -611,13 +623,20 @@ __device__ __forceinline__ void lane_major_to_tile(uint32_t* buf, uint32_t lane,
 
 // Contiguous pass (layer0 = 0, C = 0): warp w transforms 1024 consecutive
 // words of column g * kWarpCols + w for p.cpb column groups g of one tile
-// position, whose twiddles the block stages once.  Each warp streams its
-// tiles through its own staged tile with cp.async: the next tile's copy is
-// issued as soon as the transpose has freed the buffer, so it lands during
-// the second half of the butterflies and the stores.  No block barrier after
-// the staging.  Needs 16-byte aligned columns and no source masking.  With
-// p.natural (inverse transforms, source distinct from destination) the tiles
-// are gathered from a natural-order source instead.
+// position, whose twiddles the block stages once.  No block barrier after
+// the staging.  Needs 16-byte aligned columns and no source masking.
+//   Inverse: each warp streams its tiles through its own staged tile with
+// cp.async (the next tile's copy is issued as soon as the transpose has
+// freed the buffer, so it lands during the second half of the butterflies
+// and the stores), runs layers 0..4 lane-major, 5..9 row-major and stores
+// row-major (128 contiguous bytes per instruction).  With p.natural (source
+// distinct from destination) the tiles are gathered from a natural-order
+// source instead.
+//   Forward: each warp loads its tile row-major straight from global memory
+// (128 contiguous bytes per instruction), runs layers 9..5, turns the tile
+// lane-major through its staged tile, runs layers 4..0 and writes the lane's
+// 32 consecutive words back into its own line of the staged tile, from
+// where one 128-byte bulk copy per lane stores it.
 template <bool INV>
 __global__ void __launch_bounds__(256, 4) fft_warp_contig_kernel(FftPass p, FftCols cols) {
   extern __shared__ __align__(16) uint32_t smem[];
@@ -629,7 +648,7 @@ __global__ void __launch_bounds__(256, 4) fft_warp_contig_kernel(FftPass p, FftC
   const uint32_t g0 = blockIdx.y * p.cpb;
   uint32_t c = g0 * kWarpCols + warp;
   const bool natural = p.natural != 0;
-  if (c < p.n_cols) {
+  if (INV && c < p.n_cols) {
     if (natural)
       tile_gather_natural(cols.src[c], p.log_domain, hi, buf, lane);
     else
@@ -639,13 +658,13 @@ __global__ void __launch_bounds__(256, 4) fft_warp_contig_kernel(FftPass p, FftC
   __syncthreads();
   const uint32_t scale = p.scale;
   for (uint32_t g = 0; g < p.cpb; g++, c += kWarpCols) {
-    if (c >= p.n_cols) return;  // no block barrier follows
-    const uint32_t cn = c + kWarpCols;
-    const bool more = g + 1 < p.cpb && cn < p.n_cols;
+    if (c >= p.n_cols) break;  // no block barrier follows
     uint32_t* __restrict__ dst = cols.dst[c];
     uint32_t v[32];
-    tile_wait();
     if (INV) {
+      const uint32_t cn = c + kWarpCols;
+      const bool more = g + 1 < p.cpb && cn < p.n_cols;
+      tile_wait();
       tile_to_lane_major(buf, lane, v);
       warp_phase_lo<true>(v, tws, lane);
       lane_major_to_tile(buf, lane, v);
@@ -663,31 +682,26 @@ __global__ void __launch_bounds__(256, 4) fft_warp_contig_kernel(FftPass p, FftC
 #pragma unroll
       for (int j = 0; j < 32; j++) dst[base + j * 32 + lane] = scale != 1u ? m31_mul(v[j], scale) : v[j];
     } else {
+      const uint32_t* __restrict__ sp = cols.src[c] + base + lane;
 #pragma unroll
-      for (int j = 0; j < 32; j++) v[j] = buf[j * kTileStride + lane];
+      for (int j = 0; j < 32; j++) v[j] = __ldg(sp + 32 * j);
       warp_phase_hi<false>(v, tws);
+      bulk_wait_read();  // the previous tile's bulk stores have read this warp's lines
       __syncwarp();
 #pragma unroll
       for (int j = 0; j < 32; j++) buf[j * kTileStride + lane] = v[j];
       __syncwarp();
       tile_to_lane_major(buf, lane, v);
-      __syncwarp();
-      if (more) tile_prefetch(cols.src[cn] + base, buf, lane);
       warp_phase_lo<false>(v, tws, lane);
-      uint4* d4 = reinterpret_cast<uint4*>(dst + base + lane * 32);
+      if (scale != 1u) {
 #pragma unroll
-      for (int q = 0; q < 8; q++) {
-        uint4 w = make_uint4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
-        if (scale != 1u) {
-          w.x = m31_mul(w.x, scale);
-          w.y = m31_mul(w.y, scale);
-          w.z = m31_mul(w.z, scale);
-          w.w = m31_mul(w.w, scale);
-        }
-        d4[q] = w;
+        for (int j = 0; j < 32; j++) v[j] = m31_mul(v[j], scale);
       }
+      lane_major_to_tile(buf, lane, v);  // the lane's own line, read just above
+      line_bulk_store(dst + base + 32 * lane, buf + lane * kTileStride);
     }
   }
+  if (!INV) bulk_wait_all();
 }
 
 // Strided pass (C = 3, layer0 >= 3): a block transforms the 8 adjacent
