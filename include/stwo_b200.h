@@ -139,7 +139,8 @@ int stwo_b200_evaluate_polynomials(const uint32_t* const* d_coeffs, const uint32
  * d_coeffs[i] and their evaluations on CanonicCoset(log_size + log_blowup)
  * to d_evals[i].  Same words as the two calls; the interpolation's last pass
  * and the evaluation's first run as one kernel where the pass plan allows
- * (log sizes 20 and 21 by default, blowup 1 or 2).  No single reference
+ * (a last pass of 10 layers starting at layer 10, 11 or 12: log sizes 20
+ * and 21 by default; blowup 1 or 2).  No single reference
  * counterpart: the reference runs ntt_b2n_column then evaluate_columns
  * (raw.rs:472-479, 90-97). */
 int stwo_b200_interpolate_evaluate_columns(const uint32_t* const* d_src, uint32_t* const* d_coeffs,

@@ -729,8 +729,8 @@ __host__ __device__ __forceinline__ bool strided_mask_on_base(uint64_t mask, uin
 
 // L0T != 0 fixes layer0 at compile time (the row stride 2^L0T words): the
 // 32 loads and stores of a thread then address one base register with
-// immediate offsets (up to 31 x 2^(L0T+5) words, within the 24-bit signed
-// offset of global accesses for L0T <= 11).  Those instances take only
+// immediate offsets (up to 31 x 2^(L0T+5) words: within the 24-bit signed
+// offset of global accesses for L0T <= 11, half of them for L0T = 12).  Those instances take only
 // sources whose mask acts on the tile base (checked by the launcher);
 // L0T = 0 takes any layer0 and mask.
 template <bool INV, int L0T>
@@ -881,14 +881,18 @@ static int launch_warp_pass(const FftPass& q, const FftCols& cols, uint64_t tile
   } else {
     constexpr size_t smem = (1024 + kXchWords) * sizeof(uint32_t);
     static std::atomic<uint32_t> attr10{0}, attr11{0}, attr{0};
-    const bool fixed = (q.layer0 == 10 || q.layer0 == 11) && strided_mask_on_base(q.src_mask, q.src_len, q.layer0);
+    static std::atomic<uint32_t> attr12{0};
+    const bool fixed = q.layer0 >= 10 && q.layer0 <= 12 && strided_mask_on_base(q.src_mask, q.src_len, q.layer0);
     dim3 grid((unsigned)tiles, (unsigned)nc);
     if (fixed && q.layer0 == 10) {
       STWO_CUDA_TRY(ensure_smem_limit(fft_warp_strided_kernel<INV, 10>, (int)smem, attr10));
       fft_warp_strided_kernel<INV, 10><<<grid, 256, smem, s>>>(q, cols);
-    } else if (fixed) {
+    } else if (fixed && q.layer0 == 11) {
       STWO_CUDA_TRY(ensure_smem_limit(fft_warp_strided_kernel<INV, 11>, (int)smem, attr11));
       fft_warp_strided_kernel<INV, 11><<<grid, 256, smem, s>>>(q, cols);
+    } else if (fixed) {
+      STWO_CUDA_TRY(ensure_smem_limit(fft_warp_strided_kernel<INV, 12>, (int)smem, attr12));
+      fft_warp_strided_kernel<INV, 12><<<grid, 256, smem, s>>>(q, cols);
     } else {
       STWO_CUDA_TRY(ensure_smem_limit(fft_warp_strided_kernel<INV, 0>, (int)smem, attr));
       fft_warp_strided_kernel<INV, 0><<<grid, 256, smem, s>>>(q, cols);
@@ -1182,7 +1186,7 @@ int interpolate_evaluate(uint32_t* const* coeffs, uint32_t* const* evals, uint32
   STWO_ARG_CHECK(d_twiddles && N - 1 <= tree_log_size, "twiddle tree (log %u) too small for log size %u",
                  tree_log_size, N);
   const uint32_t L0 = log_n - split.back();
-  const bool fused = np >= 2 && split.back() == 10 && (L0 == 10 || L0 == 11) && log_blowup >= 1 && log_blowup <= 2;
+  const bool fused = np >= 2 && split.back() == 10 && L0 >= 10 && L0 <= 12 && log_blowup >= 1 && log_blowup <= 2;
   const uint32_t* const* src = first_pass == 0 ? src0 : nullptr;
   if (!fused) {
     for (uint32_t pi = first_pass; pi < np; pi++) {
@@ -1217,9 +1221,10 @@ int interpolate_evaluate(uint32_t* const* coeffs, uint32_t* const* evals, uint32
   const size_t smem = (1024 + kXchWords + 1024 * n_hi) * sizeof(uint32_t);
   // the limit is set once per device, for the largest table set (blowup 2)
   constexpr size_t smem_max = (1024 + kXchWords + 1024 * 4) * sizeof(uint32_t);
-  static std::atomic<uint32_t> attr10{0}, attr11{0};
-  STWO_CUDA_TRY(L0 == 10 ? ensure_smem_limit(fft_warp_inv_fwd_kernel<10>, (int)smem_max, attr10)
-                         : ensure_smem_limit(fft_warp_inv_fwd_kernel<11>, (int)smem_max, attr11));
+  static std::atomic<uint32_t> attr10{0}, attr11{0}, attr12{0};
+  STWO_CUDA_TRY(L0 == 10   ? ensure_smem_limit(fft_warp_inv_fwd_kernel<10>, (int)smem_max, attr10)
+                : L0 == 11 ? ensure_smem_limit(fft_warp_inv_fwd_kernel<11>, (int)smem_max, attr11)
+                           : ensure_smem_limit(fft_warp_inv_fwd_kernel<12>, (int)smem_max, attr12));
   for (uint32_t c0 = 0; c0 < n_cols; c0 += kFftMaxCols) {
     const uint32_t nc = std::min<uint32_t>(kFftMaxCols, n_cols - c0);
     FftColsIE cols;
@@ -1231,8 +1236,10 @@ int interpolate_evaluate(uint32_t* const* coeffs, uint32_t* const* evals, uint32
     const dim3 grid(1u << (L0 - 3), nc);
     if (L0 == 10)
       fft_warp_inv_fwd_kernel<10><<<grid, 256, smem, s>>>(pi, pf, cols, n_hi);
-    else
+    else if (L0 == 11)
       fft_warp_inv_fwd_kernel<11><<<grid, 256, smem, s>>>(pi, pf, cols, n_hi);
+    else
+      fft_warp_inv_fwd_kernel<12><<<grid, 256, smem, s>>>(pi, pf, cols, n_hi);
     STWO_CHECK_LAUNCH();
   }
   // The remaining evaluation passes, in place, top layers first (as

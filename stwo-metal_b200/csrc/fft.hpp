@@ -24,8 +24,8 @@ int interpolate_pass(uint32_t* const* cols, uint32_t n_cols, uint32_t log_n, con
 // their evaluation onto the 2^log_blowup times larger domain into `evals`
 // (stwo_b200_interpolate_columns then stwo_b200_evaluate_polynomials, same
 // words).  Where the split ends in a 10-layer strided pass over layers
-// 10..19 or 11..20 and the blowup is 1 or 2, that pass and the evaluation's
-// first run as one kernel.  With first_pass 0 and src0 given, the first
+// 10..19, 11..20 or 12..21 and the blowup is 1 or 2, that pass and the
+// evaluation's first run as one kernel.  With first_pass 0 and src0 given, the first
 // pass reads src0 (out of place).
 int interpolate_evaluate(uint32_t* const* coeffs, uint32_t* const* evals, uint32_t n_cols, uint32_t log_n,
                          uint32_t log_blowup, const std::vector<uint32_t>& split, uint32_t first_pass,

@@ -167,6 +167,35 @@ def test_interpolate_evaluate(be, oracle, big_tree, log_n, log_blowup, in_place)
             assert (srcs[k].to_host() == v).all()
 
 
+@pytest.mark.parametrize("log_blowup", [1, 2])
+def test_interpolate_evaluate_layer12_plan(be, oracle, big_tree, log_blowup):
+    # Log 22 under the split [12, 10] (the uneven commit's autotuned plan):
+    # the 10-layer strided passes start at layer 12, fused in the one call and
+    # separate in the two trait calls.
+    from stwo_b200 import fft_get_plan, fft_set_plan
+    tree, tw, itw = big_tree
+    old = fft_get_plan(22)
+    fft_set_plan(22, [12, 10])
+    try:
+        r = rng(3100 + log_blowup)
+        vals = [rand_col(r, 22) for _ in range(2)]
+        vals[0][::7] = P
+        srcs = [DeviceColumn.from_host(v) for v in vals]
+        coeffs = [DeviceColumn(1 << 22) for _ in vals]
+        outs = [DeviceColumn(1 << (22 + log_blowup)) for _ in vals]
+        be.interpolate_evaluate_into(srcs, coeffs, log_blowup, tree, outs)
+        c2 = [DeviceColumn(1 << 22) for _ in vals]
+        be.interpolate_columns_into(srcs, c2, tree)
+        o2 = be.evaluate_polynomials(c2, log_blowup, tree)
+        for k, v in enumerate(vals):
+            co = oracle.interpolate(v, itw)
+            ev = oracle.evaluate(co, 22 + log_blowup, tw)
+            assert (coeffs[k].to_host() == co).all() and (c2[k].to_host() == co).all(), k
+            assert (outs[k].to_host() == ev).all() and (o2[k].to_host() == ev).all(), k
+    finally:
+        fft_set_plan(22, old)
+
+
 def test_p_valued_inputs(be, oracle, big_tree):
     # Words equal to P (the redundant zero) propagate exactly like SimdBackend.
     tree, tw, itw = big_tree
