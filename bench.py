@@ -659,10 +659,11 @@ def run_prove_reference(args, world, rank):
 
 
 # DRAM bytes (read + written) of one trace interpolate + evaluate (2^20 ->
-# 2^21 per column; fft_warp_contig_kernel<1>, fft_warp_inv_fwd_kernel<10>,
-# fft_warp_contig_kernel<0>) measured by ncu on 40 columns, scaled to the 100
-# columns of the proof.
-TRACE_FFT_TRAFFIC_100x2e20 = None
+# 2^21 per column) measured by ncu on 40 columns -- fft_warp_contig_kernel<1>
+# 172.0 + 120.7 MB, fft_warp_inv_fwd_kernel<10> 167.8 + 451.7 MB,
+# fft_warp_contig_kernel<0> 347.7 + 275.4 MB -- scaled to the 100 columns of
+# the proof.
+TRACE_FFT_TRAFFIC_100x2e20 = (172.0 + 120.7 + 167.8 + 451.7 + 347.7 + 275.4) * 1e6 * 100 / 40
 
 
 def run_prove_b200(args, world, rank, local):
