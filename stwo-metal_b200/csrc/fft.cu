@@ -864,6 +864,217 @@ __global__ void __launch_bounds__(256, 4) fft_warp_inv_fwd_kernel(FftPass pi, Ff
   }
 }
 
+// ---- contiguous passes of 11 and 12 layers (T = 10 + K) ----
+// A group of 2^K warps owns one 2^T-row column tile, 32 values per thread,
+// in three layouts (q: the warp's 1024-row quarter of the tile, l: lane):
+//   lane-major (layers 0..4):    rows 1024 q + 32 l + j           (v[j]);
+//   row-major  (layers 5..9):    rows 1024 q + 32 j + l           (v[j]);
+//   top        (layers 10..T-1): rows 1024 k + 32 (q I + i) + l   (v[k I + i]),
+//                                k < 2^K, i < I = 32 >> K.
+// Each addresses the group's staged tile (row r at (r >> 5) * kTileStride +
+// (r & 31)) without bank conflicts.  Lane-major <-> row-major stays inside a
+// warp (its own quarter, as in the 10-layer pass); row-major <-> top crosses
+// the group's warps through a named barrier of the group.  The inverse pass
+// streams its quarter in with cp.async and stores the top layout (128
+// contiguous bytes per instruction); the forward pass loads the top layout
+// straight from global memory and stores each lane's line with a bulk copy.
+
+// Layers 5..9 of a 2^T-row tile on v[j] = row 1024 q + 32 j + l:
+// row >> (lam + 1) = (q << (9 - lam)) + (j >> (lam - 4)).
+template <bool INV, int T>
+__device__ __forceinline__ void group_phase_hi(uint32_t (&v)[32], const uint32_t* __restrict__ tws, uint32_t q) {
+#pragma unroll
+  for (int kk = 0; kk < 5; kk++) {
+    const int k = INV ? kk : 4 - kk;  // bit of j, layer 5 + k
+    const uint32_t* tl = tws + ((1u << T) - (1u << (T - 5 - k))) + (q << (4 - k));
+    uint32_t t[16];
+#pragma unroll
+    for (int m = 0; m < (1 << (4 - k)); m++) t[m] = tl[m];
+#pragma unroll
+    for (int j = 0; j < 32; j++) {
+      if (j & (1 << k)) continue;
+      if (INV)
+        ibfly2(v[j], v[j | (1 << k)], t[j >> (k + 1)]);
+      else
+        bfly2(v[j], v[j | (1 << k)], t[j >> (k + 1)]);
+    }
+  }
+}
+// Layers 0..4 on v[j] = row 32 b + j of a 2^T-row tile.
+template <bool INV, int T>
+__device__ __forceinline__ void group_phase_lo(uint32_t (&v)[32], const uint32_t* __restrict__ tws, uint32_t b) {
+#pragma unroll
+  for (int kk = 0; kk < 5; kk++) {
+    const int lam = INV ? kk : 4 - kk;
+    const uint32_t* tl = tws + ((1u << T) - (1u << (T - lam))) + (b << (4 - lam));
+    uint32_t t[16];
+#pragma unroll
+    for (int m = 0; m < (1 << (4 - lam)); m++) t[m] = tl[m];
+#pragma unroll
+    for (int j = 0; j < 32; j++) {
+      if (j & (1 << lam)) continue;
+      if (INV)
+        ibfly2(v[j], v[j | (1 << lam)], t[j >> (lam + 1)]);
+      else
+        bfly2(v[j], v[j | (1 << lam)], t[j >> (lam + 1)]);
+    }
+  }
+}
+// Layers 10..T-1 on the top layout: layer 10 + kk pairs k and k | 2^kk, with
+// row >> (11 + kk) = k >> (kk + 1).
+template <bool INV, int K>
+__device__ __forceinline__ void group_phase_top(uint32_t (&v)[32], const uint32_t* __restrict__ tws) {
+  constexpr int T = 10 + K, I = 32 >> K;
+#pragma unroll
+  for (int k0 = 0; k0 < K; k0++) {
+    const int kk = INV ? k0 : K - 1 - k0;
+    const uint32_t* tl = tws + ((1u << T) - (1u << (T - 10 - kk)));
+#pragma unroll
+    for (int k = 0; k < (1 << K); k++) {
+      if (k & (1 << kk)) continue;
+      const uint32_t t = tl[k >> (kk + 1)];
+#pragma unroll
+      for (int i = 0; i < I; i++) {
+        if (INV)
+          ibfly2(v[k * I + i], v[(k | (1 << kk)) * I + i], t);
+        else
+          bfly2(v[k * I + i], v[(k | (1 << kk)) * I + i], t);
+      }
+    }
+  }
+}
+// The 2^T - 1 twiddles of a contiguous T-layer tile position (layer0 = 0),
+// doubled, in the slot order of stage_tws10: layer lam at 2^T - 2^(T - lam),
+// 2^(T-1-lam) entries; layer 0 (the circle layer) from line layer 1.
+template <int T>
+__device__ __forceinline__ void stage_tws_contig(const FftPass& p, uint64_t hi, uint32_t* tws) {
+  const uint32_t* tail = p.tree + p.tree_len;
+  const uint32_t N = p.log_domain, t = threadIdx.x;
+  {
+    constexpr uint32_t R = (1u << (T - 1)) / 256;
+    const uint32_t* lt0 = tail - (1ull << (N - 1));
+    uint32_t val[R];
+#pragma unroll
+    for (uint32_t r = 0; r < R; r++) val[r] = circle_tw(lt0, (hi << (T - 1)) + t + 256 * r);
+#pragma unroll
+    for (uint32_t r = 0; r < R; r++) tws[t + 256 * r] = val[r] << 1;
+  }
+#pragma unroll
+  for (int lam = 1; lam < T; lam++) {
+    const uint32_t cnt = 1u << (T - 1 - lam), off = (1u << T) - (1u << (T - lam));
+    const uint32_t* l = tail - (1ull << (N - lam)) + (hi << (T - 1 - lam));
+#pragma unroll
+    for (uint32_t e = 0; e < cnt; e += 256)
+      if (e + t < cnt) tws[off + e + t] = __ldg(l + e + t) << 1;
+  }
+}
+// Named barrier 1 + grp of the n_threads threads of group grp (< 4; barrier 0
+// is the block's).  Immediate ids, so that a block holds 5 barriers.
+__device__ __forceinline__ void group_barrier(uint32_t grp, uint32_t n_threads) {
+  switch (grp) {
+    case 0: asm volatile("bar.sync 1, %0;\n" ::"r"(n_threads) : "memory"); break;
+    case 1: asm volatile("bar.sync 2, %0;\n" ::"r"(n_threads) : "memory"); break;
+    case 2: asm volatile("bar.sync 3, %0;\n" ::"r"(n_threads) : "memory"); break;
+    default: asm volatile("bar.sync 4, %0;\n" ::"r"(n_threads) : "memory"); break;
+  }
+}
+
+template <bool INV, int K>
+__global__ void __launch_bounds__(256, 4) fft_group_contig_kernel(FftPass p, FftCols cols) {
+  constexpr int T = 10 + K;
+  constexpr uint32_t W = 1u << K, G = 8u / W, I = 32u >> K;
+  constexpr uint32_t kLines = 1u << (T - 5);
+  extern __shared__ __align__(16) uint32_t smem[];
+  uint32_t* tws = smem;
+  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t grp = warp / W, q = warp % W;
+  uint32_t* buf = smem + (1u << T) + grp * kLines * kTileStride;
+  uint32_t* qb = buf + 32 * q * kTileStride;  // the warp's quarter: 32 lines
+  const uint64_t hi = (uint64_t)p.tile0 + blockIdx.x;
+  const uint64_t base = hi << T;
+  const uint32_t c = blockIdx.y * G + grp;
+  const bool active = c < p.n_cols;
+  uint32_t v[32];
+  if (active) {
+    if (INV) {
+      tile_prefetch(cols.src[c] + base + 1024 * q, qb, lane);
+    } else {
+      const uint32_t* __restrict__ sp = cols.src[c] + base + 32 * (q * I) + lane;
+#pragma unroll
+      for (uint32_t k = 0; k < W; k++)
+#pragma unroll
+        for (uint32_t i = 0; i < I; i++) v[k * I + i] = __ldg(sp + 1024 * k + 32 * i);
+    }
+  }
+  stage_tws_contig<T>(p, hi, tws);
+  __syncthreads();
+  if (!active) return;  // whole groups only: the barriers below are per group
+  const uint32_t n_bar = 32 * W;
+  const uint32_t scale = p.scale;
+  if (INV) {
+    tile_wait();
+    tile_to_lane_major(qb, lane, v);
+    group_phase_lo<true, T>(v, tws, 32 * q + lane);
+    lane_major_to_tile(qb, lane, v);
+    __syncwarp();
+#pragma unroll
+    for (int j = 0; j < 32; j++) v[j] = qb[j * kTileStride + lane];
+    group_phase_hi<true, T>(v, tws, q);
+#pragma unroll
+    for (int j = 0; j < 32; j++) qb[j * kTileStride + lane] = v[j];
+    group_barrier(grp, n_bar);
+#pragma unroll
+    for (uint32_t k = 0; k < W; k++)
+#pragma unroll
+      for (uint32_t i = 0; i < I; i++) v[k * I + i] = buf[(32 * k + q * I + i) * kTileStride + lane];
+    group_phase_top<true, K>(v, tws);
+    uint32_t* __restrict__ dp = cols.dst[c] + base + 32 * (q * I) + lane;
+#pragma unroll
+    for (uint32_t k = 0; k < W; k++)
+#pragma unroll
+      for (uint32_t i = 0; i < I; i++) {
+        const uint32_t x = v[k * I + i];
+        dp[1024 * k + 32 * i] = scale != 1u ? m31_mul(x, scale) : x;
+      }
+  } else {
+    group_phase_top<false, K>(v, tws);
+#pragma unroll
+    for (uint32_t k = 0; k < W; k++)
+#pragma unroll
+      for (uint32_t i = 0; i < I; i++) buf[(32 * k + q * I + i) * kTileStride + lane] = v[k * I + i];
+    group_barrier(grp, n_bar);
+#pragma unroll
+    for (int j = 0; j < 32; j++) v[j] = qb[j * kTileStride + lane];
+    group_phase_hi<false, T>(v, tws, q);
+#pragma unroll
+    for (int j = 0; j < 32; j++) qb[j * kTileStride + lane] = v[j];
+    __syncwarp();
+    tile_to_lane_major(qb, lane, v);
+    group_phase_lo<false, T>(v, tws, 32 * q + lane);
+    if (scale != 1u) {
+#pragma unroll
+      for (int j = 0; j < 32; j++) v[j] = m31_mul(v[j], scale);
+    }
+    lane_major_to_tile(qb, lane, v);  // the lane's own line, read just above
+    line_bulk_store(cols.dst[c] + base + 1024 * q + 32 * lane, qb + lane * kTileStride);
+    bulk_wait_all();
+  }
+}
+
+template <bool INV, int K>
+static int launch_group_contig(const FftPass& q, const FftCols& cols, uint64_t tiles, size_t nc, cudaStream_t s,
+                               char* err, size_t err_len) {
+  constexpr int T = 10 + K;
+  constexpr uint32_t G = 8u >> K;
+  constexpr size_t smem = ((1u << T) + G * (1u << (T - 5)) * kTileStride) * sizeof(uint32_t);
+  static std::atomic<uint32_t> attr{0};
+  STWO_CUDA_TRY(ensure_smem_limit(fft_group_contig_kernel<INV, K>, (int)smem, attr));
+  dim3 grid((unsigned)tiles, (unsigned)((nc + G - 1) / G));
+  fft_group_contig_kernel<INV, K><<<grid, 256, smem, s>>>(q, cols);
+  STWO_CHECK_LAUNCH();
+  return STWO_B200_OK;
+}
+
 template <bool INV>
 static int launch_warp_pass(const FftPass& q, const FftCols& cols, uint64_t tiles, size_t nc, cudaStream_t s,
                             char* err, size_t err_len) {
@@ -965,10 +1176,15 @@ static int launch_pass(const FftPass& p, const std::vector<const uint32_t*>& src
     const bool warp_contig = p.T == 10 && p.C == 0 && p.layer0 == 0 && aligned && p.src_mask == ~0ull &&
                              p.src_len == ~0ull;
     const bool warp_strided = p.T == 10 && p.C == 3 && p.layer0 >= 3;
+    const bool group_contig = (p.T == 11 || p.T == 12) && p.C == 0 && p.layer0 == 0 && aligned && !p.natural &&
+                              p.src_mask == ~0ull && p.src_len == ~0ull;
     STWO_ARG_CHECK(!p.natural || (INV && p.C == 0 && p.layer0 == 0 && p.src_mask == ~0ull && p.src_len == ~0ull),
                    "natural-order source needs an unmasked first inverse pass");
     if (warp_contig || warp_strided)
       rc = launch_warp_pass<INV>(q, cols, tiles, nc, s, err, err_len);
+    else if (group_contig)
+      rc = p.T == 11 ? launch_group_contig<INV, 1>(q, cols, tiles, nc, s, err, err_len)
+                     : launch_group_contig<INV, 2>(q, cols, tiles, nc, s, err, err_len);
     else if (p.C == 3)
       rc = dispatch_tile<INV, 3, 1>(q, cols, grid, s, err, err_len);
     else if (cpb == 4)
