@@ -1381,12 +1381,16 @@ struct GatherPlan {
 
 // Witness node (layer log, index) list of a lifted Merkle decommitment in
 // proof order (prover/vcs_lifted/prover.rs:114-185).
-static std::vector<std::pair<uint32_t, size_t>> witness_nodes(std::vector<size_t> queries, uint32_t L) {
+// The level lists live in two per-thread buffers that keep their capacity
+// between calls: a proof runs this for about two dozen trees of ~20 levels.
+static std::vector<std::pair<uint32_t, size_t>> witness_nodes(const std::vector<size_t>& queries, uint32_t L) {
   std::vector<std::pair<uint32_t, size_t>> out;
-  queries.erase(std::unique(queries.begin(), queries.end()), queries.end());
-  std::vector<size_t> prev = queries;
+  out.reserve(queries.size() * L);
+  thread_local std::vector<size_t> prev, cur;
+  prev.assign(queries.begin(), queries.end());
+  prev.erase(std::unique(prev.begin(), prev.end()), prev.end());
   for (uint32_t layer_log = L; layer_log-- > 0;) {
-    std::vector<size_t> cur;
+    cur.clear();
     for (size_t i = 0; i < prev.size();) {
       size_t first = prev[i];
       bool pair = (i + 1 < prev.size()) && ((first ^ 1) == prev[i + 1]);
@@ -1394,17 +1398,28 @@ static std::vector<std::pair<uint32_t, size_t>> witness_nodes(std::vector<size_t
       cur.push_back(first >> 1);
       i += pair ? 2 : 1;
     }
-    prev = cur;
+    prev.swap(cur);
   }
   return out;
 }
 
+// Little-endian proof encoding: integers are appended as their in-memory
+// bytes, which on this (little-endian) host are the little-endian bytes.
+static_assert(__BYTE_ORDER__ == __ORDER_LITTLE_ENDIAN__, "the proof encoding copies little-endian integers");
 struct ProofOut {
   std::vector<uint8_t> bytes;
-  void u32(uint32_t v) { for (int i = 0; i < 4; i++) bytes.push_back((v >> (8 * i)) & 0xFF); }
-  void u64(uint64_t v) { for (int i = 0; i < 8; i++) bytes.push_back((v >> (8 * i)) & 0xFF); }
-  void q(const qm31& x) { u32(x.a); u32(x.b); u32(x.c); u32(x.d); }
-  void h(const uint8_t* p) { bytes.insert(bytes.end(), p, p + 32); }
+  void raw(const void* p, size_t n) {
+    const size_t at = bytes.size();
+    bytes.resize(at + n);
+    std::memcpy(bytes.data() + at, p, n);
+  }
+  void u32(uint32_t v) { raw(&v, 4); }
+  void u64(uint64_t v) { raw(&v, 8); }
+  void q(const qm31& x) {
+    const uint32_t w[4] = {x.a, x.b, x.c, x.d};
+    raw(w, 16);
+  }
+  void h(const uint8_t* p) { raw(p, 32); }
 };
 
 // Phases timed with CUDA events when timing is enabled
@@ -1492,6 +1507,7 @@ class WideFibProver {
   uint64_t* d_gather_addr = nullptr;
   uint32_t* d_gather_out = nullptr;
   size_t gather_cap = 0;
+  size_t last_proof_bytes = 1u << 16;  // capacity reserved for the next proof's bytes
   qm31* d_oods_partial = nullptr;  // OODS partial sums (polynomials x chunks)
   qm31* h_pinned = nullptr;       // staging for small uploads / downloads
   DevChannel* h_chan = nullptr;   // staging of the device channel state (own region: the
@@ -2214,13 +2230,31 @@ int WideFibProver::prove_body(const uint32_t* d_a, const uint32_t* d_b, ProofOut
     Hash32 pre = dev_ch.pow_prefixed(cfg.pow_bits);
     Digest8 d;
     std::memcpy(d.w, pre.data(), 32);
-    bool found = false;
+    bool found = false, replayed = false;
     for (uint32_t hi = 0; !found; hi++) {
       for (uint32_t base = 0; base < (1u << 20) && !found; base += 1u << 16) {
         STWO_CUDA_TRY(cudaMemsetAsync(d_found, 0xFF, 4, s));
         if ((rc = launch_grind(d.w, hi, base, 1u << 16, cfg.pow_bits, m31, d_found, s, err, err_len))) return rc;
         uint32_t* hf = reinterpret_cast<uint32_t*>(h_pinned) + (h_pinned_bytes / 4 - 1);
         STWO_CUDA_TRY(cudaMemcpyAsync(hf, d_found, 4, cudaMemcpyDeviceToHost, s));
+        if (!replayed) {
+          // host replay of the FRI transcript while the first grind batch
+          // runs: every device alpha and the channel state at the end of the
+          // commit
+          replayed = true;
+          for (size_t i = 0; i < fri_roots.size(); i++) {
+            ch.mix_root(fri_roots[i]);
+            if (!qm31_eq(ch.draw_secure_felt(), dev_alphas[i])) {
+              cudaStreamSynchronize(s);
+              return set_err(err, err_len, STWO_B200_ESTATE, "device and host channels diverged at FRI layer %zu",
+                             i);
+            }
+          }
+          if (std::memcmp(ch.digest().data(), fri_end_digest, 32) != 0 || ch.n_draws() != fri_end_draws) {
+            cudaStreamSynchronize(s);
+            return set_err(err, err_len, STWO_B200_ESTATE, "device and host channel states differ after FRI");
+          }
+        }
         STWO_CUDA_TRY(cudaStreamSynchronize(s));
         if (*hf != 0xFFFFFFFFu) {
           nonce = ((uint64_t)hi << 32) | *hf;
@@ -2248,6 +2282,7 @@ int WideFibProver::prove_body(const uint32_t* d_a, const uint32_t* d_b, ProofOut
   // ---- decommitments: one gather of every needed word ----
   phase(kDecommit);
   GatherPlan g;
+  g.addrs.reserve(std::max<size_t>(gather_cap, 4096));
   struct FriDecommit {
     std::vector<size_t> positions;       // subset positions
     std::vector<bool> is_query;
@@ -2331,19 +2366,6 @@ int WideFibProver::prove_body(const uint32_t* d_a, const uint32_t* d_b, ProofOut
     }
     gather_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(d_gather_addr, (uint32_t)n, d_gather_out);
     STWO_CHECK_LAUNCH();
-    // host replay of the FRI transcript while the gather runs: every device
-    // alpha and the channel state at the end of the commit
-    for (size_t i = 0; i < fri_roots.size(); i++) {
-      ch.mix_root(fri_roots[i]);
-      if (!qm31_eq(ch.draw_secure_felt(), dev_alphas[i])) {
-        cudaStreamSynchronize(s);
-        return set_err(err, err_len, STWO_B200_ESTATE, "device and host channels diverged at FRI layer %zu", i);
-      }
-    }
-    if (std::memcmp(ch.digest().data(), fri_end_digest, 32) != 0 || ch.n_draws() != fri_end_draws) {
-      cudaStreamSynchronize(s);
-      return set_err(err, err_len, STWO_B200_ESTATE, "device and host channel states differ after FRI");
-    }
     size_t wchunk = h_pinned_bytes / 4;
     for (size_t off = 0; off < n; off += wchunk) {
       size_t m = std::min(wchunk, n - off);
@@ -2355,6 +2377,7 @@ int WideFibProver::prove_body(const uint32_t* d_a, const uint32_t* d_b, ProofOut
     // core/pcs/quotients.rs:27-35 and core/fri.rs:361-395) ----
     auto hash_at = [&](size_t slot, ProofOut& o) { o.h(reinterpret_cast<const uint8_t*>(words.data() + slot)); };
     const char magic[8] = {'S', 'T', 'W', 'O', 'P', 'R', 'F', '1'};
+    if (out.bytes.capacity() < last_proof_bytes) out.bytes.reserve(last_proof_bytes);
     out.bytes.assign(magic, magic + 8);
     out.u32(cfg.pow_bits);
     out.u32(cfg.log_blowup);
@@ -2428,6 +2451,7 @@ int WideFibProver::prove_body(const uint32_t* d_a, const uint32_t* d_b, ProofOut
     out.u64(lp.size());
     for (auto& x : lp) out.q(x);
   }
+  last_proof_bytes = std::max(last_proof_bytes, out.bytes.size());
   finish_timing();
   return 0;
 }
