@@ -616,6 +616,7 @@ __global__ void __launch_bounds__(kStreamBlock) quotient_tma_kernel(QuotientPara
 struct Digest8 {
   uint32_t w[8];
 };
+constexpr uint32_t kGrindBatch = 1u << 16;  // nonces per grind launch of the prover
 __global__ void grind_kernel(Digest8 pre, uint32_t hi, uint32_t low_base, uint32_t bits, int m31,
                              uint32_t* __restrict__ found) {
   uint32_t low = low_base + blockIdx.x * blockDim.x + threadIdx.x;
@@ -742,6 +743,98 @@ __device__ void dev_chan_mix_staged(DevChannel* ch, const uint32_t* s_words, uin
   dev_finalize(h, ch->m31 != 0);
   for (int k = 0; k < 8; k++) ch->digest[k] = h[k];
   ch->n_draws = 0;
+}
+
+// The end of the FRI commit on the device channel (prover/fri.rs:274-291,
+// pcs/mod.rs:140-142), so that the first proof-of-work batch runs without a
+// host round trip: the last layer's 2^last_log evaluations (4 coordinate
+// columns) -> coefficients as LineEvaluation::interpolate computes them
+// (bit reversal, the line IFFT with the inverse x-coordinates xi, in the
+// order the host walks them, times 1/n, bit reversal into coefficient
+// order); the first 2^bound_log are mixed into a copy of the channel, and
+// pow[0..8) receives H(POW_PREFIX, [0; 12], digest, n_bits)
+// (core/channel/blake2s.rs:124-132); pow[8] = 1 when a higher coefficient is
+// nonzero.  The channel itself is left at its end-of-commit state, which the
+// host downloads to replay the transcript.  One thread.
+constexpr uint32_t kFinishMaxLast = 64;
+__global__ void fri_finish_kernel(const DevChannel* __restrict__ ch, const uint32_t* __restrict__ last,
+                                  uint32_t last_log, uint32_t bound_log, const uint32_t* __restrict__ xi,
+                                  uint32_t n_inv, uint32_t pow_bits, uint32_t* __restrict__ pow) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const uint32_t n = 1u << last_log;
+  qm31 v[kFinishMaxLast];
+  for (uint32_t i = 0; i < n; i++) {
+    const uint32_t j = last_log ? __brev(i) >> (32 - last_log) : 0u;
+    v[j] = {last[i], last[n + i], last[2 * n + i], last[3 * n + i]};
+  }
+  uint32_t off = 0;
+  for (uint32_t lg = last_log; lg >= 1; lg--) {
+    const uint32_t sz = 1u << lg;
+    for (uint32_t c0 = 0; c0 < n; c0 += sz)
+      for (uint32_t i = 0; i < sz / 2; i++) {
+        const qm31 l = v[c0 + i], r = v[c0 + i + sz / 2];
+        v[c0 + i] = qm31_add(l, r);
+        v[c0 + i + sz / 2] = qm31_mul_m31(qm31_sub(l, r), xi[off + i]);
+      }
+    off += sz / 2;
+  }
+  for (uint32_t i = 0; i < n; i++) v[i] = qm31_mul_m31(v[i], n_inv);
+  for (uint32_t i = 0; i < n; i++) {
+    const uint32_t j = last_log ? __brev(i) >> (32 - last_log) : 0u;
+    if (j > i) {
+      const qm31 t = v[i];
+      v[i] = v[j];
+      v[j] = t;
+    }
+  }
+  uint32_t bad = 0;
+  for (uint32_t i = 1u << bound_log; i < n; i++) bad |= !qm31_eq(v[i], qm31_zero());
+  // mix_felts on a copy of the digest: digest || a, b, c, d of each coefficient
+  const uint32_t nb = 1u << bound_log, total = 8 + 4 * nb, blocks = (total + 15) / 16;
+  auto word = [&](uint32_t w) -> uint32_t {
+    if (w < 8) return ch->digest[w];
+    if (w >= total) return 0u;
+    const qm31 x = v[(w - 8) >> 2];
+    const uint32_t k = (w - 8) & 3;
+    return k == 0 ? x.a : k == 1 ? x.b : k == 2 ? x.c : x.d;
+  };
+  uint32_t h[8], m[16];
+  blake2s_init(h);
+  for (uint32_t bk = 0; bk < blocks; bk++) {
+    for (int k = 0; k < 16; k++) m[k] = word(bk * 16 + k);
+    const bool fin = bk + 1 == blocks;
+    blake2s_compress_lat(h, m, fin ? 4 * total : 64 * (bk + 1), fin);
+  }
+  dev_finalize(h, ch->m31 != 0);
+  m[0] = 0x12345678u;
+  m[1] = m[2] = m[3] = 0;
+  for (int k = 0; k < 8; k++) m[4 + k] = h[k];
+  m[12] = pow_bits;
+  m[13] = m[14] = m[15] = 0;
+  uint32_t p[8];
+  blake2s_init(p);
+  blake2s_compress_lat(p, m, 52, true);
+  dev_finalize(p, ch->m31 != 0);
+  for (int k = 0; k < 8; k++) pow[k] = p[k];
+  pow[8] = bad;
+}
+// grind_kernel with the prefixed digest read from device memory.
+__global__ void grind_dev_kernel(const uint32_t* __restrict__ pre, uint32_t hi, uint32_t low_base, uint32_t bits,
+                                 int m31, uint32_t* __restrict__ found) {
+  uint32_t low = low_base + blockIdx.x * blockDim.x + threadIdx.x;
+  uint32_t m[16];
+#pragma unroll
+  for (int k = 0; k < 8; k++) m[k] = __ldg(pre + k);
+  m[8] = low;
+  m[9] = hi;
+#pragma unroll
+  for (int k = 10; k < 16; k++) m[k] = 0;
+  uint32_t h[8];
+  blake2s_init(h);
+  blake2s_compress(h, m, 40, true);
+  uint32_t w0 = m31 ? m31_reduce_u32(h[0]) : h[0];
+  uint32_t tz = w0 == 0 ? 32u : (uint32_t)__ffs(w0) - 1;
+  if (tz >= bits) atomicMin(found, low);
 }
 
 // The channel state in registers, for the one-CTA kernels that run several
@@ -1380,12 +1473,12 @@ struct GatherPlan {
 };
 
 // Witness node (layer log, index) list of a lifted Merkle decommitment in
-// proof order (prover/vcs_lifted/prover.rs:114-185).
-// The level lists live in two per-thread buffers that keep their capacity
-// between calls: a proof runs this for about two dozen trees of ~20 levels.
-static std::vector<std::pair<uint32_t, size_t>> witness_nodes(const std::vector<size_t>& queries, uint32_t L) {
-  std::vector<std::pair<uint32_t, size_t>> out;
-  out.reserve(queries.size() * L);
+// proof order (prover/vcs_lifted/prover.rs:114-185), into `out`.  The level
+// lists live in two per-thread buffers that keep their capacity between
+// calls: a proof runs this for about two dozen trees of ~20 levels.
+static void witness_nodes_into(const std::vector<size_t>& queries, uint32_t L,
+                               std::vector<std::pair<uint32_t, size_t>>& out) {
+  out.clear();
   thread_local std::vector<size_t> prev, cur;
   prev.assign(queries.begin(), queries.end());
   prev.erase(std::unique(prev.begin(), prev.end()), prev.end());
@@ -1400,8 +1493,29 @@ static std::vector<std::pair<uint32_t, size_t>> witness_nodes(const std::vector<
     }
     prev.swap(cur);
   }
+}
+
+static std::vector<std::pair<uint32_t, size_t>> witness_nodes(const std::vector<size_t>& queries, uint32_t L) {
+  std::vector<std::pair<uint32_t, size_t>> out;
+  witness_nodes_into(queries, L, out);
   return out;
 }
+
+// Decommitment plans of one proof: an FRI layer (positions of the folded
+// subsets, their value and witness-node slots in the gather) and a trace
+// tree (queried values column-major, witness nodes).
+struct FriDecommit {
+  std::vector<size_t> positions;  // subset positions
+  std::vector<uint8_t> is_query;
+  std::vector<size_t> value_slot;  // 4 words per position
+  std::vector<std::pair<uint32_t, size_t>> nodes;
+  std::vector<size_t> node_slot;
+};
+struct TreeDecommit {
+  std::vector<size_t> value_slot;  // column-major: col * n_q + qi
+  std::vector<std::pair<uint32_t, size_t>> nodes;
+  std::vector<size_t> node_slot;
+};
 
 // Little-endian proof encoding: integers are appended as their in-memory
 // bytes, which on this (little-endian) host are the little-endian bytes.
@@ -1497,6 +1611,13 @@ class WideFibProver {
   uint32_t* d_quot = nullptr;     // 4 x 2^lift
   std::vector<FriLayerBuf> fri;   // inner layers
   uint32_t* d_last = nullptr;     // 4 x 2^last_log
+  // Device finish of the FRI commit (fri_finish_kernel) for last layers of up
+  // to kFinishMaxLast values: its proof-of-work prefix and flag, and the
+  // inverse x-coordinates of the last layer's line IFFT.
+  bool dev_finish = false;
+  uint32_t* d_pow = nullptr;
+  uint32_t* d_last_xi = nullptr;
+  uint32_t last_n_inv = 0;
   qm31* d_small = nullptr;        // powers / weights / partials / alpha powers
   uint32_t* d_denom = nullptr;
   FsOut* d_fs = nullptr;         // values drawn by the device Fiat-Shamir steps
@@ -1508,6 +1629,12 @@ class WideFibProver {
   uint32_t* d_gather_out = nullptr;
   size_t gather_cap = 0;
   size_t last_proof_bytes = 1u << 16;  // capacity reserved for the next proof's bytes
+  // host decommitment plan, reused from proof to proof
+  GatherPlan gplan;
+  std::vector<FriDecommit> fri_dec_buf;
+  TreeDecommit td_buf[2];
+  std::vector<size_t> lq_buf, nq_buf, tq_buf;
+  std::vector<uint32_t> words_buf;
   qm31* d_oods_partial = nullptr;  // OODS partial sums (polynomials x chunks)
   qm31* h_pinned = nullptr;       // staging for small uploads / downloads
   DevChannel* h_chan = nullptr;   // staging of the device channel state (own region: the
@@ -1652,6 +1779,9 @@ class WideFibProver {
       if ((rc = alloc((void**)&l.tree.base, MerkleTree::bytes_for(l.log_size), err, err_len))) return rc;
     }
     if ((rc = alloc((void**)&d_last, 16ull << last_log, err, err_len))) return rc;
+    dev_finish = (1u << last_log) <= kFinishMaxLast;
+    if ((rc = alloc((void**)&d_pow, 64, err, err_len))) return rc;
+    if ((rc = alloc((void**)&d_last_xi, 4u << last_log, err, err_len))) return rc;
     size_t small_q = std::max<size_t>(4096, 2 * (1u << 12) + (size_t)kMaxPolys * 1024);
     if ((rc = alloc((void**)&d_small, small_q * sizeof(qm31), err, err_len))) return rc;
     // OODS partial sums: one per (polynomial, 1024-index chunk)
@@ -1690,6 +1820,24 @@ class WideFibProver {
         dn[bitrev32(j, log_expand)] = m31_inv(x);
       }
       STWO_CUDA_TRY(cudaMemcpyAsync(d_denom, dn, 4ull << log_expand, cudaMemcpyHostToDevice, s));
+    }
+    if (dev_finish) {
+      // The inverse x-coordinates of the last layer's line IFFT, in the order
+      // the host interpolation after the FRI commit walks them (line domain:
+      // the half coset of CanonicCoset(lift) doubled down to last_log).
+      const uint32_t last_log = c.log_last_layer_degree_bound + blowup;
+      uint32_t* xi = reinterpret_cast<uint32_t*>(h_pinned) + 4096;
+      uint64_t dinit = (1ull << (31 - (lift + 1))) << (lift - 1 - last_log);
+      uint64_t dstep = 1ull << (31 - last_log);
+      uint32_t off = 0;
+      for (uint32_t lg = last_log; lg >= 1; lg--) {
+        for (uint64_t i = 0; i < (1ull << (lg - 1)); i++) xi[off + i] = m31_inv(index_to_cpoint(dinit + dstep * i).x);
+        off += 1u << (lg - 1);
+        dinit = (dinit * 2) & ((1ull << 31) - 1);
+        dstep = (dstep * 2) & ((1ull << 31) - 1);
+      }
+      last_n_inv = m31_inv(m31_reduce_u32(1u << last_log));
+      if (off) STWO_CUDA_TRY(cudaMemcpyAsync(d_last_xi, xi, 4ull * off, cudaMemcpyHostToDevice, s));
     }
     STWO_CUDA_TRY(cudaStreamSynchronize(s));
     return 0;
@@ -2075,6 +2223,18 @@ int WideFibProver::prove_body(const uint32_t* d_a, const uint32_t* d_b, ProofOut
   STWO_CUDA_TRY(cudaMemcpyAsync(h_tx + tx_flag_off, d_found + kStreamErrWord, 4, cudaMemcpyDeviceToHost, s));
   STWO_CUDA_TRY(cudaEventRecord(ev_tx, s));
   if ((rc = run_fri(err, err_len))) return rc;
+  if (dev_finish) {
+    // the last layer, the proof-of-work prefix and the first grind batch,
+    // queued behind the FRI commit; the host checks the prefix against its
+    // own and continues the search from the second batch when this one
+    // finds no nonce
+    fri_finish_kernel<<<1, 32, 0, s>>>(d_chan, d_last, last_log, cfg.log_last_layer_degree_bound, d_last_xi,
+                                       last_n_inv, cfg.pow_bits, d_pow);
+    STWO_CHECK_LAUNCH();
+    STWO_CUDA_TRY(cudaMemsetAsync(d_found, 0xFF, 4, s));
+    grind_dev_kernel<<<kGrindBatch / 256, 256, 0, s>>>(d_pow, 0, 0, cfg.pow_bits, m31, d_found);
+    STWO_CHECK_LAUNCH();
+  }
   Hash32 root1, root2;
   std::vector<qm31> sampled(np);
   {
@@ -2144,7 +2304,7 @@ int WideFibProver::prove_body(const uint32_t* d_a, const uint32_t* d_b, ProofOut
   const uint64_t n_last = 1ull << last_log;
   HostChannel dev_ch(m31);
   const uint8_t* hp = reinterpret_cast<const uint8_t*>(h_pinned);
-  size_t alpha_off = 0, chan_off = 0, flag_off = 0, last_off = 0;
+  size_t alpha_off = 0, chan_off = 0, flag_off = 0, last_off = 0, pow_off = 0;
   uint32_t fri_end_digest[8];
   uint32_t fri_end_draws = 0;
   std::vector<qm31> dev_alphas;
@@ -2166,6 +2326,12 @@ int WideFibProver::prove_body(const uint32_t* d_a, const uint32_t* d_b, ProofOut
     flag_off = off;
     STWO_CUDA_TRY(cudaMemcpyAsync(hpw + off, d_found + kStreamErrWord, 4, cudaMemcpyDeviceToHost, s));
     off += 16;
+    if (dev_finish) {
+      pow_off = off;
+      STWO_CUDA_TRY(cudaMemcpyAsync(hpw + off, d_pow, 36, cudaMemcpyDeviceToHost, s));
+      STWO_CUDA_TRY(cudaMemcpyAsync(hpw + off + 48, d_found, 4, cudaMemcpyDeviceToHost, s));
+      off += 64;
+    }
     last_off = off;
     STWO_ARG_CHECK(off + 16 * n_last <= h_pinned_bytes, "pinned staging too small for the last layer");
     STWO_CUDA_TRY(cudaMemcpyAsync(hpw + off, d_last, 16 * n_last, cudaMemcpyDeviceToHost, s));
@@ -2226,35 +2392,51 @@ int WideFibProver::prove_body(const uint32_t* d_a, const uint32_t* d_b, ProofOut
   // ---- proof of work (pcs/mod.rs:140-142) ----
   uint64_t nonce = 0;
   phase(kGrind);
+  // Host replay of the FRI transcript: every device alpha and the channel
+  // state at the end of the commit.  It runs while the first host-launched
+  // grind batch runs or, when the device's batch found the nonce, while the
+  // decommit gather runs.
+  bool replayed = false;
+  auto replay_fri = [&]() -> int {
+    replayed = true;
+    for (size_t i = 0; i < fri_roots.size(); i++) {
+      ch.mix_root(fri_roots[i]);
+      if (!qm31_eq(ch.draw_secure_felt(), dev_alphas[i])) {
+        cudaStreamSynchronize(s);
+        return set_err(err, err_len, STWO_B200_ESTATE, "device and host channels diverged at FRI layer %zu", i);
+      }
+    }
+    if (std::memcmp(ch.digest().data(), fri_end_digest, 32) != 0 || ch.n_draws() != fri_end_draws) {
+      cudaStreamSynchronize(s);
+      return set_err(err, err_len, STWO_B200_ESTATE, "device and host channel states differ after FRI");
+    }
+    return 0;
+  };
   {
     Hash32 pre = dev_ch.pow_prefixed(cfg.pow_bits);
     Digest8 d;
     std::memcpy(d.w, pre.data(), 32);
-    bool found = false, replayed = false;
+    bool found = false;
+    uint32_t base0 = 0;
+    if (dev_finish) {
+      // the device's prefix and first batch (fri_finish_kernel, grind_dev_kernel)
+      const uint32_t* pw = reinterpret_cast<const uint32_t*>(hp + pow_off);
+      if (std::memcmp(pw, pre.data(), 32) != 0)
+        return set_err(err, err_len, STWO_B200_ESTATE, "device and host channels diverged at the proof of work");
+      if (pw[12] != 0xFFFFFFFFu) {
+        nonce = pw[12];
+        found = true;
+      } else {
+        base0 = kGrindBatch;
+      }
+    }
     for (uint32_t hi = 0; !found; hi++) {
-      for (uint32_t base = 0; base < (1u << 20) && !found; base += 1u << 16) {
+      for (uint32_t base = hi == 0 ? base0 : 0; base < (1u << 20) && !found; base += kGrindBatch) {
         STWO_CUDA_TRY(cudaMemsetAsync(d_found, 0xFF, 4, s));
-        if ((rc = launch_grind(d.w, hi, base, 1u << 16, cfg.pow_bits, m31, d_found, s, err, err_len))) return rc;
+        if ((rc = launch_grind(d.w, hi, base, kGrindBatch, cfg.pow_bits, m31, d_found, s, err, err_len))) return rc;
         uint32_t* hf = reinterpret_cast<uint32_t*>(h_pinned) + (h_pinned_bytes / 4 - 1);
         STWO_CUDA_TRY(cudaMemcpyAsync(hf, d_found, 4, cudaMemcpyDeviceToHost, s));
-        if (!replayed) {
-          // host replay of the FRI transcript while the first grind batch
-          // runs: every device alpha and the channel state at the end of the
-          // commit
-          replayed = true;
-          for (size_t i = 0; i < fri_roots.size(); i++) {
-            ch.mix_root(fri_roots[i]);
-            if (!qm31_eq(ch.draw_secure_felt(), dev_alphas[i])) {
-              cudaStreamSynchronize(s);
-              return set_err(err, err_len, STWO_B200_ESTATE, "device and host channels diverged at FRI layer %zu",
-                             i);
-            }
-          }
-          if (std::memcmp(ch.digest().data(), fri_end_digest, 32) != 0 || ch.n_draws() != fri_end_draws) {
-            cudaStreamSynchronize(s);
-            return set_err(err, err_len, STWO_B200_ESTATE, "device and host channel states differ after FRI");
-          }
-        }
+        if (!replayed && (rc = replay_fri())) return rc;
         STWO_CUDA_TRY(cudaStreamSynchronize(s));
         if (*hf != 0xFFFFFFFFu) {
           nonce = ((uint64_t)hi << 32) | *hf;
@@ -2281,18 +2463,16 @@ int WideFibProver::prove_body(const uint32_t* d_a, const uint32_t* d_b, ProofOut
 
   // ---- decommitments: one gather of every needed word ----
   phase(kDecommit);
-  GatherPlan g;
-  g.addrs.reserve(std::max<size_t>(gather_cap, 4096));
-  struct FriDecommit {
-    std::vector<size_t> positions;       // subset positions
-    std::vector<bool> is_query;
-    std::vector<size_t> value_slot;      // 4 words per position
-    std::vector<std::pair<uint32_t, size_t>> nodes;
-    std::vector<size_t> node_slot;
-  };
-  auto plan_fri = [&](const uint32_t* coords, uint32_t log_size, const MerkleTree& tree,
+  // The plan's vectors are prover members, cleared here: they keep their
+  // capacity from one proof to the next.
+  GatherPlan& g = gplan;
+  g.addrs.clear();
+  auto plan_fri = [&](FriDecommit& d, const uint32_t* coords, uint32_t log_size, const MerkleTree& tree,
                       const std::vector<size_t>& q, uint32_t fold_step) {
-    FriDecommit d;
+    d.positions.clear();
+    d.is_query.clear();
+    d.value_slot.clear();
+    d.node_slot.clear();
     for (size_t i = 0; i < q.size();) {
       size_t j = i;
       while (j < q.size() && (q[j] >> fold_step) == (q[i] >> fold_step)) j++;
@@ -2302,58 +2482,59 @@ int WideFibProver::prove_body(const uint32_t* d_a, const uint32_t* d_b, ProofOut
         bool isq = k < j && q[k] == pos;
         if (isq) k++;
         d.positions.push_back(pos);
-        d.is_query.push_back(isq);
+        d.is_query.push_back(isq ? 1 : 0);
         size_t slot = g.add_word(coords + pos);
         for (int c = 1; c < 4; c++) g.add_word(coords + ((uint64_t)c << log_size) + pos);
         d.value_slot.push_back(slot);
       }
       i = j;
     }
-    d.nodes = witness_nodes(d.positions, tree.L);
+    witness_nodes_into(d.positions, tree.L, d.nodes);
     for (auto& nd : d.nodes) d.node_slot.push_back(g.add_hash(tree.layer(nd.first) + nd.second * 32));
-    return d;
   };
-  std::vector<FriDecommit> fri_dec;
-  fri_dec.push_back(plan_fri(d_quot, lift, tq, queries, 1));
+  std::vector<FriDecommit>& fri_dec = fri_dec_buf;
+  fri_dec.resize(fri.size() + 1);
+  plan_fri(fri_dec[0], d_quot, lift, tq, queries, 1);
   {
-    std::vector<size_t> lq;
+    std::vector<size_t>& lq = lq_buf;
+    std::vector<size_t>& nq = nq_buf;
+    lq.clear();
     for (size_t q : queries)
       if (lq.empty() || lq.back() != (q >> 1)) lq.push_back(q >> 1);
-    for (auto& l : fri) {
-      fri_dec.push_back(plan_fri(l.coords, l.log_size, l.tree, lq, l.fold_step));
-      std::vector<size_t> nq;
+    for (size_t li = 0; li < fri.size(); li++) {
+      const auto& l = fri[li];
+      plan_fri(fri_dec[li + 1], l.coords, l.log_size, l.tree, lq, l.fold_step);
+      nq.clear();
       for (size_t q : lq)
         if (nq.empty() || nq.back() != (q >> l.fold_step)) nq.push_back(q >> l.fold_step);
-      lq = nq;
+      lq.swap(nq);
     }
   }
   // trees 1 and 2 at the lifting size: queried values and witness nodes
-  struct TreeDecommit {
-    std::vector<size_t> value_slot;  // column-major: col * n_q + qi
-    std::vector<std::pair<uint32_t, size_t>> nodes;
-    std::vector<size_t> node_slot;
-  };
-  auto plan_tree = [&](const std::vector<uint32_t*>& cols, uint32_t log_size, const MerkleTree& tree) {
-    TreeDecommit d;
+  auto plan_tree = [&](TreeDecommit& d, const std::vector<uint32_t*>& cols, uint32_t log_size,
+                       const MerkleTree& tree) {
+    d.value_slot.clear();
+    d.node_slot.clear();
     // prepare_query_positions_for_tree (core/pcs/utils.rs:195-213) and the
     // lifted read index (prover/vcs_lifted/prover.rs:83-109)
-    std::vector<size_t> tq;
-    for (size_t p : queries) tq.push_back(((p >> (lift - tree.L + 1)) << 1) + (p & 1));
+    std::vector<size_t>& tqs = tq_buf;
+    tqs.clear();
+    for (size_t p : queries) tqs.push_back(((p >> (lift - tree.L + 1)) << 1) + (p & 1));
+    const size_t shift = tree.L - log_size;
     for (size_t c = 0; c < cols.size(); c++)
-      for (size_t p : tq) {
-        size_t shift = tree.L - log_size;
-        d.value_slot.push_back(g.add_word(cols[c] + (((p >> (shift + 1)) << 1) + (p & 1))));
-      }
-    d.nodes = witness_nodes(tq, tree.L);
+      for (size_t p : tqs) d.value_slot.push_back(g.add_word(cols[c] + (((p >> (shift + 1)) << 1) + (p & 1))));
+    witness_nodes_into(tqs, tree.L, d.nodes);
     for (auto& nd : d.nodes) d.node_slot.push_back(g.add_hash(tree.layer(nd.first) + nd.second * 32));
-    return d;
   };
-  TreeDecommit td1 = plan_tree(eval_ptrs, L1, t1);
-  TreeDecommit td2 = plan_tree(lde, L2, t2);
+  TreeDecommit& td1 = td_buf[0];
+  TreeDecommit& td2 = td_buf[1];
+  plan_tree(td1, eval_ptrs, L1, t1);
+  plan_tree(td2, lde, L2, t2);
   if ((rc = ensure_gather(g.addrs.size(), err, err_len))) return rc;
   {
     size_t n = g.addrs.size();
-    std::vector<uint32_t> words(n);
+    std::vector<uint32_t>& words = words_buf;
+    words.resize(n);
     // upload addresses through the pinned staging buffer in chunks
     size_t chunk = h_pinned_bytes / 8;
     for (size_t off = 0; off < n; off += chunk) {
@@ -2366,6 +2547,7 @@ int WideFibProver::prove_body(const uint32_t* d_a, const uint32_t* d_b, ProofOut
     }
     gather_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(d_gather_addr, (uint32_t)n, d_gather_out);
     STWO_CHECK_LAUNCH();
+    if (!replayed && (rc = replay_fri())) return rc;
     size_t wchunk = h_pinned_bytes / 4;
     for (size_t off = 0; off < n; off += wchunk) {
       size_t m = std::min(wchunk, n - off);

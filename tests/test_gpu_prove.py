@@ -44,6 +44,22 @@ def test_wide_fib_proof_bytes_match_oracle(oracle, log_n, cols, blowup, step, la
     assert oracle.verify_wide_fib(got, log_n, cols, m31) is None
 
 
+@pytest.mark.parametrize("pow_bits,last", [(0, 0), (20, 0), (10, 5), (10, 6)])
+def test_proof_of_work_and_last_layer_forms(oracle, pow_bits, last):
+    # The last-layer interpolation, the proof-of-work prefix and the first
+    # grind batch (2^16 nonces) run on the device for last layers of up to 64
+    # values.  At 20 bits that batch misses with probability ~0.94 and the
+    # host continues the search; a last layer of 2^7 values stays on the host.
+    log_n, cols = 10, 8
+    a, b = oracle.wide_fib_inputs(log_n, 500 + pow_bits + last)
+    ocfg = oracle.wide_fib_config(log_n, cols, pow_bits=pow_bits, log_last_layer_degree_bound=last)
+    ref = oracle.prove_wide_fib(ocfg, a, b)
+    prover = WideFibProver(wide_fib_config(log_n, cols, pow_bits=pow_bits, log_last_layer_degree_bound=last))
+    got = prover.prove(DeviceColumn.from_host(a), DeviceColumn.from_host(b))
+    assert got == ref
+    assert prover.prove(DeviceColumn.from_host(a), DeviceColumn.from_host(b)) == ref
+
+
 def test_prover_reuse_is_deterministic(oracle):
     # Resident buffers are reused across proofs: a second proof of other
     # inputs, then the first inputs again, reproduce the oracle bytes.
