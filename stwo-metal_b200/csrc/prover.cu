@@ -931,21 +931,26 @@ __global__ void fs_composition_kernel(DevChannel* ch, const uint8_t* root, uint3
 
 // Weight tables of oods_eval_kernel from the fold factors f[0..lg) (shared
 // memory, written before a block barrier): w_lo[t] = prod over set bits b of t
-// of f[b] (t < 2^h), w_hi[t] = prod over set bits b of t of f[h + b].
+// of f[b] (t < 2^h), w_hi[t] = prod over set bits b of t of f[h + b].  Built by
+// doubling, one product per entry: entries [2^b, 2^(b+1)) are entries
+// [0, 2^b) times f[b], a block barrier per bit.  The products are canonical
+// field values, so the order of the factors does not change the words.  All
+// threads of the block call it.
 __device__ void build_eval_weights(const qm31* f, uint32_t lg, uint32_t h, qm31* __restrict__ w_lo,
                                    qm31* __restrict__ w_hi) {
   const uint32_t hi_bits = lg - h;
-  for (uint32_t t = threadIdx.x; t < (1u << h); t += blockDim.x) {
-    qm31 w = qm31_one();
-    for (uint32_t b = 0; b < h; b++)
-      if ((t >> b) & 1) w = qm31_mul(w, f[b]);
-    w_lo[t] = w;
+  if (threadIdx.x == 0) {
+    w_lo[0] = qm31_one();
+    w_hi[0] = qm31_one();
   }
-  for (uint32_t t = threadIdx.x; t < (1u << hi_bits); t += blockDim.x) {
-    qm31 w = qm31_one();
-    for (uint32_t b = 0; b < hi_bits; b++)
-      if ((t >> b) & 1) w = qm31_mul(w, f[h + b]);
-    w_hi[t] = w;
+  __syncthreads();
+  const uint32_t rounds = h > hi_bits ? h : hi_bits;
+  for (uint32_t b = 0; b < rounds; b++) {
+    for (uint32_t t = threadIdx.x; t < (1u << b); t += blockDim.x) {
+      if (b < h) w_lo[(1u << b) + t] = qm31_mul(w_lo[t], f[b]);
+      if (b < hi_bits) w_hi[(1u << b) + t] = qm31_mul(w_hi[t], f[h + b]);
+    }
+    __syncthreads();
   }
 }
 
