@@ -167,6 +167,23 @@ def test_interpolate_evaluate(be, oracle, big_tree, log_n, log_blowup, in_place)
             assert (srcs[k].to_host() == v).all()
 
 
+def test_interpolate_evaluate_many_columns(be, oracle, big_tree):
+    # 260 columns of log 20 in one call: the fused kernel launches per 256
+    # columns; columns on both sides of the boundary against the oracle.
+    tree, tw, itw = big_tree
+    r = rng(3200)
+    base = [rand_col(r, 20) for _ in range(4)]
+    picks = {0: 0, 255: 1, 256: 2, 259: 3}
+    srcs = [DeviceColumn.from_host(base[picks.get(k, k % 4)]) for k in range(260)]
+    coeffs = [DeviceColumn(1 << 20) for _ in range(260)]
+    outs = [DeviceColumn(1 << 21) for _ in range(260)]
+    be.interpolate_evaluate_into(srcs, coeffs, 1, tree, outs)
+    for k, b in picks.items():
+        co = oracle.interpolate(base[b], itw)
+        assert (coeffs[k].to_host() == co).all(), k
+        assert (outs[k].to_host() == oracle.evaluate(co, 21, tw)).all(), k
+
+
 @pytest.mark.parametrize("log_blowup", [1, 2])
 def test_interpolate_evaluate_layer12_plan(be, oracle, big_tree, log_blowup):
     # Log 22 under the split [12, 10] (the uneven commit's autotuned plan):
