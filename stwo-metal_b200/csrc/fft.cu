@@ -399,9 +399,14 @@ static bool plan_is_valid(uint32_t n, const uint32_t* t, uint32_t k) {
   return sum == n && (k == 1 || t[0] >= 3);
 }
 
-// Default: passes of <= 12 layers, two up to 23 layers, three above.
+// Default: passes of <= 12 layers, two up to 23 layers, three above.  From
+// 16 to 19 layers the first pass takes 10 (the 10-layer warp kernel), and at
+// 22 the split is [12, 10] (a 12-layer warp-group pass, then a 10-layer warp
+// pass), the splits the autotuner picks for them.
 static std::vector<uint32_t> default_split(uint32_t n) {
   if (n <= 12) return {n};
+  if (n >= 16 && n <= 19) return {10, n - 10};
+  if (n == 22) return {12, 10};
   uint32_t parts = n <= 23 ? 2 : 3;
   std::vector<uint32_t> t;
   uint32_t rest = n;
