@@ -167,6 +167,31 @@ def test_interpolate_evaluate(be, oracle, big_tree, log_n, log_blowup, in_place)
             assert (srcs[k].to_host() == v).all()
 
 
+@pytest.mark.parametrize("log_n,plan", [(13, [3, 10]), (15, [5, 10]), (16, [6, 10])])
+def test_strided_pass_runtime_layer_offset(be, oracle, big_tree, log_n, plan):
+    # Splits ending in a 10-layer pass that starts at layer 3..9: the strided
+    # warp kernel with the layer offset read at run time (the autotuner can
+    # pick these), for the interpolation and for blowup-1 and -2 evaluations.
+    from stwo_b200 import fft_get_plan, fft_set_plan
+    tree, tw, itw = big_tree
+    old = fft_get_plan(log_n)
+    fft_set_plan(log_n, plan)
+    try:
+        r = rng(3300 + log_n)
+        vals = [rand_col(r, log_n) for _ in range(3)]
+        vals[2][::9] = P
+        cols = [DeviceColumn.from_host(v) for v in vals]
+        be.interpolate_columns(cols, tree)
+        for blowup in (1, 2):
+            evs = be.evaluate_polynomials(cols, blowup, tree)
+            for k, v in enumerate(vals):
+                co = oracle.interpolate(v, itw)
+                assert (cols[k].to_host() == co).all(), k
+                assert (evs[k].to_host() == oracle.evaluate(co, log_n + blowup, tw)).all(), (k, blowup)
+    finally:
+        fft_set_plan(log_n, old)
+
+
 def test_interpolate_evaluate_many_columns(be, oracle, big_tree):
     # 260 columns of log 20 in one call: the fused kernel launches per 256
     # columns; columns on both sides of the boundary against the oracle.
