@@ -65,6 +65,15 @@ def load_peaks():
 
 
 # ------------------------------------------------------------ workloads ----
+def lifted_leaf_compressions(lde_logs, L):
+    """Blake2s compressions of the lifted leaves as the staged leaf kernel
+    runs them: 16-column group g of the columns sorted by size at the size of
+    its largest column, the last group at the lifting size L."""
+    logs = sorted(lde_logs)
+    n_groups = (len(logs) + 15) // 16
+    return sum(1 << (L if g + 1 == n_groups else logs[min(16 * g + 15, len(logs) - 1)]) for g in range(n_groups))
+
+
 def workload_spec(name: str):
     if name == "commit_uneven":
         r = np.random.default_rng(3)
@@ -332,7 +341,6 @@ def run_b200(args, spec, world, rank, local):
     evals_sorted = [evals[i] for i in order]
     cells = sum(c.size for c in host_cols)
     eval_cells = cells << blowup
-    n_leaf_blocks = (len(logs) + 15) // 16
     torch.cuda.synchronize()
 
     # Committer forms (commit_uneven): per-column launches, batched launches,
@@ -364,7 +372,7 @@ def run_b200(args, spec, world, rank, local):
         rec(evs, 1)
         be.evaluate_polynomials_into(coeffs, blowup, tree, evals)
         rec(evs, 2)
-        be.build_leaves_into(evals_sorted, L, layers[L])
+        be.build_leaves_layers(evals_sorted, L, layers)
         rec(evs, 3)
         be.build_nodes(layers)
         rec(evs, 4)
@@ -525,7 +533,7 @@ def run_b200(args, spec, world, rank, local):
         "nodes": 32 * (1 << L) + 32 * ((1 << L) - 1),
     }
     dominant = max(("ifft", "rfft", "leaves", "nodes"), key=lambda p: phase_ms[p])
-    compressions = (1 << L) * n_leaf_blocks
+    compressions = lifted_leaf_compressions([x + blowup for x in logs], L)
     if dominant == "leaves":
         achieved = compressions / (phase_ms["leaves"] * 1e-3) / 1e9
         roof = {"bound": "int32", "kernel": "lifted_leaves_kernel", "achieved": achieved,
@@ -1174,7 +1182,7 @@ def extra_commit_uneven(args, stream, world, hbm_peak, probe_rate):
             marks[1].record(stream)
             be.evaluate_polynomials_into(coeffs, blowup, tree, evals)
             marks[2].record(stream)
-            be.build_leaves_into(evals_sorted, L, layers[L])
+            be.build_leaves_layers(evals_sorted, L, layers)
             marks[3].record(stream)
             be.build_nodes(layers)
             marks[4].record(stream)
@@ -1184,7 +1192,7 @@ def extra_commit_uneven(args, stream, world, hbm_peak, probe_rate):
     root = bytes(layer_to_host(layers[0])[0]).hex()
     golden = load_digests().get("commit_uneven_root")
     alg = {"ifft": 8 * cells, "rfft": 4 * cells + 4 * eval_cells}
-    compressions = (1 << L) * ((len(logs) + 15) // 16)
+    compressions = lifted_leaf_compressions([x + blowup for x in logs], L)
     out = {
         "workload": "commit_uneven: 512 columns, log sizes U{12..22} seed 3, blowup 2, lifted Blake2s tree L=24",
         "committed_cells": cells,
@@ -1226,7 +1234,7 @@ def extra_commit_plain(args, stream, world):
     def step():
         be.interpolate_natural_into(inputs, coeffs, tree)
         be.evaluate_polynomials_into(coeffs, blowup, tree, evals)
-        be.build_leaves_into(evals, L, layers[L])
+        be.build_leaves_layers(evals, L, layers)
         be.build_nodes(layers)
 
     for _ in range(3):

@@ -153,6 +153,11 @@ int stwo_b200_interpolate_evaluate_columns(const uint32_t* const* d_src, uint32_
  * (prover/vcs_lifted/ops.rs:14-15; spec prover/backend/cpu/merkle_lifted.rs:
  * 44-78).  Columns must already be sorted by non-decreasing log size.
  * Writes 2^lifting_log_size 32-byte leaves (1 leaf when n_cols == 0).
+ * Columns of more than one size hash in stages, as SimdBackend does
+ * (backend/simd/blake2s_lifted.rs:42-160); the chaining values between
+ * stages take a stream-ordered temporary of 32 * 2^lifting_log_size bytes
+ * (build_leaves_layers below takes the tree's layers instead), and one more
+ * of that size when more than 1024 columns hash at the lifting size.
  * Replaces commit_on_first_layer_lifted (raw.rs:176-183). */
 int stwo_b200_merkle_build_leaves(const uint32_t* const* d_cols, const uint32_t* log_sizes, uint32_t n_cols,
                                   uint32_t lifting_log_size, int m31_output, uint8_t* d_leaves, void* stream,
@@ -175,6 +180,16 @@ int stwo_b200_merkle_build_layers(const uint32_t* const* d_cols, const uint32_t*
  * (the second half of build_merkle_layers, prover/vcs_lifted/ops.rs:39-43). */
 int stwo_b200_merkle_build_nodes(uint8_t* const* d_layers, uint32_t lifting_log_size, int m31_output,
                                  void* stream, char* err, size_t err_len);
+
+/* The first half of build_merkle_layers (prover/vcs_lifted/ops.rs:37-38):
+ * build_leaves of columns already sorted by non-decreasing log size into
+ * d_layers[lifting_log_size], with d_layers[k] (k < lifting_log_size, 2^k
+ * hashes each) as the chaining values between the hashing stages, so that
+ * nothing is allocated unless more than 1024 columns hash at the lifting
+ * size.  build_nodes overwrites d_layers[k < lifting_log_size] afterwards. */
+int stwo_b200_merkle_build_leaves_layers(const uint32_t* const* d_cols, const uint32_t* log_sizes, uint32_t n_cols,
+                                         uint32_t lifting_log_size, int m31_output, uint8_t* const* d_layers,
+                                         void* stream, char* err, size_t err_len);
 
 /* Throughput probe (no reference counterpart): `blocks` x 256 threads each
  * chain `iters` Blake2s compressions in registers.  compressions / elapsed

@@ -43,20 +43,33 @@ __device__ __forceinline__ uint32_t lift_index(uint32_t i, uint32_t r) {
   return r == 0 ? i : (((i >> (r + 1)) << 1) + (i & 1));
 }
 
-// Leaves for columns [c_begin, c_end) of `t`; `state` (nullable) carries the
-// chaining value between launches when a tree has more than kLeafMaxCols
-// columns; only the last launch finalizes.
-__global__ void __launch_bounds__(256) lifted_leaves_kernel(LeafCols t, uint32_t n_cols, uint32_t L, int m31,
+// One stage of the lifted leaves.  The leaf hash absorbs the sorted columns
+// 16 per compression, and the chaining value after a compression depends
+// only on columns of log size <= that compression's largest, so it is a
+// function of lift(i, L - that log size): it is computed once per index of
+// that size and lifted (lift(lift(i, a), b) = lift(i, a + b)), as SimdBackend
+// does (backend/simd/blake2s_lifted.rs:42-160).  A stage runs the
+// compressions of the columns in `t` (all of log size <= S, t.shift[c] =
+// S - log_c) for the 2^S indices of size S.  It starts from the initial state
+// (prev == nullptr) or from the chaining values of size 2^(S - prev_r) in
+// `prev` (8 planes of 2^(S - prev_r) words), read at lift(i, prev_r); it
+// leaves its chaining values in `next` (8 planes of 2^S words; may be `prev`
+// when prev_r == 0, each thread reading its own entries first) or, in the
+// last stage, the finalized leaf hashes in `out`.
+__global__ void __launch_bounds__(256) lifted_leaves_kernel(LeafCols t, uint32_t n_cols, uint32_t S, int m31,
                                                            uint32_t bytes_before, uint32_t total_bytes,
-                                                           uint32_t* state, int is_first, int is_last, uint8_t* out) {
-  const uint32_t n = 1u << L;  // L <= 30
+                                                           const uint32_t* prev, uint32_t prev_r, uint32_t* next,
+                                                           int is_last, uint8_t* out) {
+  const uint32_t n = 1u << S;  // S <= 30
+  const uint32_t n_prev = n >> prev_r;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     uint32_t h[8];
-    if (is_first) {
+    if (prev == nullptr) {
       blake2s_init(h);
     } else {
+      const uint32_t j = lift_index(i, prev_r);
 #pragma unroll
-      for (int k = 0; k < 8; k++) h[k] = state[(uint64_t)k * n + i];
+      for (int k = 0; k < 8; k++) h[k] = prev[(uint64_t)k * n_prev + j];
     }
     uint32_t m[16];
     uint32_t done = bytes_before;
@@ -93,7 +106,7 @@ __global__ void __launch_bounds__(256) lifted_leaves_kernel(LeafCols t, uint32_t
       store_hash(out, i, h, m31 != 0);
     } else {
 #pragma unroll
-      for (int k = 0; k < 8; k++) state[(uint64_t)k * n + i] = h[k];
+      for (int k = 0; k < 8; k++) next[(uint64_t)k * n + i] = h[k];
     }
   }
 }
@@ -293,12 +306,21 @@ static unsigned grid_for(uint64_t n, unsigned threads) {
   return (unsigned)std::min<uint64_t>(std::max<uint64_t>(b, 1), 148ull * 64);
 }
 
+// Leaves of the lifted tree in stages.  Compression group g (columns
+// [16g, 16g + 16) of the sorted list) runs at the size of its largest column,
+// the last group at L (it writes the leaves); consecutive groups of one size
+// form a stage, one launch per up to kLeafMaxCols columns.  The chaining
+// values between stages of size S < L go to layer_ws[S] when the caller
+// passes the tree's layer buffers (2^S hashes of 32 bytes each, rebuilt by
+// the node layers afterwards), else to a temporary buffer that packs size S
+// at byte offset 32 * 2^S.
 int build_leaves_impl(const uint32_t* const* d_cols, const uint32_t* log_sizes, uint32_t n_cols, uint32_t L,
-                      int m31, uint8_t* d_leaves, cudaStream_t s, char* err, size_t err_len) {
+                      int m31, uint8_t* d_leaves, uint8_t* const* layer_ws, cudaStream_t s, char* err,
+                      size_t err_len) {
   STWO_ARG_CHECK(d_leaves != nullptr, "null leaves");
   if (n_cols == 0) {
     LeafCols t{};
-    lifted_leaves_kernel<<<1, 32, 0, s>>>(t, 0, 0, m31, 0, 0, nullptr, 1, 1, d_leaves);
+    lifted_leaves_kernel<<<1, 32, 0, s>>>(t, 0, 0, m31, 0, 0, nullptr, 0, nullptr, 1, d_leaves);
     STWO_CHECK_LAUNCH();
     return STWO_B200_OK;
   }
@@ -308,30 +330,66 @@ int build_leaves_impl(const uint32_t* const* d_cols, const uint32_t* log_sizes, 
     STWO_ARG_CHECK(log_sizes[c] <= L, "column log size %u exceeds lifting log size %u", log_sizes[c], L);
     STWO_ARG_CHECK(c == 0 || log_sizes[c - 1] <= log_sizes[c], "columns must be sorted by length");
   }
-  uint64_t n = 1ull << L;
-  uint32_t total_bytes = 4u * n_cols;
-  uint32_t* state = nullptr;
-  const uint32_t chunks = (n_cols + kLeafMaxCols - 1) / kLeafMaxCols;
-  if (chunks > 1) STWO_CUDA_TRY(cudaMallocAsync(&state, n * 32, s));
-  for (uint32_t ch = 0; ch < chunks; ch++) {
+  const uint32_t n_groups = (n_cols + 15) / 16;
+  auto group_size = [&](uint32_t g) {
+    return g + 1 == n_groups ? L : log_sizes[std::min<uint32_t>(16 * g + 15, n_cols - 1)];
+  };
+  struct Launch {
+    uint32_t g0, g1, S;
+  };
+  std::vector<Launch> launches;
+  for (uint32_t g = 0; g < n_groups;) {
+    uint32_t e = g + 1;
+    while (e < n_groups && e - g < kLeafMaxCols / 16 && group_size(e) == group_size(g)) e++;
+    launches.push_back({g, e, group_size(g)});
+    g = e;
+  }
+  // temporary state: sizes below L packed (when the caller gave no layer
+  // buffers), and one buffer of size L for a last stage of > kLeafMaxCols
+  // columns
+  bool need_small = false, need_top = false;
+  for (size_t k = 0; k + 1 < launches.size(); k++) {
+    if (launches[k].S < L)
+      need_small |= layer_ws == nullptr;
+    else
+      need_top = true;
+  }
+  const uint64_t top_bytes = 32ull << L;
+  uint8_t* ws = nullptr;
+  const uint64_t ws_bytes = (need_small ? top_bytes : 0) + (need_top ? top_bytes : 0);
+  if (ws_bytes) STWO_CUDA_TRY(cudaMallocAsync(&ws, ws_bytes, s));
+  auto state_of = [&](uint32_t S) -> uint32_t* {
+    if (S == L) return reinterpret_cast<uint32_t*>(ws + (need_small ? top_bytes : 0));
+    if (layer_ws) return reinterpret_cast<uint32_t*>(layer_ws[S]);
+    return reinterpret_cast<uint32_t*>(ws + (32ull << S));
+  };
+  const uint32_t total_bytes = 4u * n_cols;
+  const uint32_t* prev = nullptr;
+  uint32_t prev_S = 0;
+  for (size_t k = 0; k < launches.size(); k++) {
+    const Launch& ln = launches[k];
+    const bool last = k + 1 == launches.size();
+    const uint32_t c0 = 16 * ln.g0, c1 = std::min<uint32_t>(16 * ln.g1, n_cols);
+    const uint32_t nc = c1 - c0;
     LeafCols t;
-    uint32_t c0 = ch * kLeafMaxCols;
-    uint32_t nc = std::min<uint32_t>(kLeafMaxCols, n_cols - c0);
-    for (uint32_t k = 0; k < nc; k++) {
-      t.col[k] = d_cols[c0 + k];
-      t.shift[k] = (uint8_t)(L - log_sizes[c0 + k]);
+    for (uint32_t c = 0; c < nc; c++) {
+      t.col[c] = d_cols[c0 + c];
+      t.shift[c] = (uint8_t)(ln.S - log_sizes[c0 + c]);
     }
     for (uint32_t g = 0; g < kLeafMaxCols / 16; g++) {
       const uint32_t k0 = 16 * g;
       bool uniform = k0 < nc;
-      for (uint32_t k = k0 + 1; uniform && k < std::min<uint32_t>(k0 + 16, nc); k++) uniform = t.shift[k] == t.shift[k0];
+      for (uint32_t c = k0 + 1; uniform && c < std::min<uint32_t>(k0 + 16, nc); c++) uniform = t.shift[c] == t.shift[k0];
       t.group_shift[g] = uniform ? t.shift[k0] : kMixedShift;
     }
-    lifted_leaves_kernel<<<grid_for(n, 256), 256, 0, s>>>(t, nc, L, m31, 4u * c0, total_bytes, state, ch == 0,
-                                                          ch + 1 == chunks, d_leaves);
+    uint32_t* next = last ? nullptr : state_of(ln.S);
+    lifted_leaves_kernel<<<grid_for(1ull << ln.S, 256), 256, 0, s>>>(t, nc, ln.S, m31, 4u * c0, total_bytes, prev,
+                                                                     ln.S - prev_S, next, last, d_leaves);
     STWO_CHECK_LAUNCH();
+    prev = next;
+    prev_S = ln.S;
   }
-  if (state) STWO_CUDA_TRY(cudaFreeAsync(state, s));
+  if (ws) STWO_CUDA_TRY(cudaFreeAsync(ws, s));
   return STWO_B200_OK;
 }
 
@@ -381,8 +439,8 @@ using namespace stwo_b200;
 extern "C" int stwo_b200_merkle_build_leaves(const uint32_t* const* d_cols, const uint32_t* log_sizes,
                                              uint32_t n_cols, uint32_t lifting_log_size, int m31_output,
                                              uint8_t* d_leaves, void* stream, char* err, size_t err_len) {
-  int rc = build_leaves_impl(d_cols, log_sizes, n_cols, lifting_log_size, m31_output, d_leaves, as_stream(stream),
-                             err, err_len);
+  int rc = build_leaves_impl(d_cols, log_sizes, n_cols, lifting_log_size, m31_output, d_leaves, nullptr,
+                             as_stream(stream), err, err_len);
   return rc ? rc : ok(err, err_len);
 }
 
@@ -403,7 +461,7 @@ extern "C" int stwo_b200_merkle_build_layers(const uint32_t* const* d_cols, cons
   STWO_ARG_CHECK(d_layers != nullptr, "null layers");
   if (n_cols == 0) {
     STWO_ARG_CHECK(lifting_log_size == 0, "empty commitment needs lifting_log_size 0");
-    int rc = build_leaves_impl(nullptr, nullptr, 0, 0, m31_output, d_layers[0], s, err, err_len);
+    int rc = build_leaves_impl(nullptr, nullptr, 0, 0, m31_output, d_layers[0], nullptr, s, err, err_len);
     return rc ? rc : ok(err, err_len);
   }
   // prover/vcs_lifted/ops.rs:37 stable sort by length.
@@ -417,7 +475,7 @@ extern "C" int stwo_b200_merkle_build_layers(const uint32_t* const* d_cols, cons
     logs[i] = log_sizes[order[i]];
   }
   const uint32_t L = lifting_log_size;
-  int rc = build_leaves_impl(cols.data(), logs.data(), n_cols, L, m31_output, d_layers[L], s, err, err_len);
+  int rc = build_leaves_impl(cols.data(), logs.data(), n_cols, L, m31_output, d_layers[L], d_layers, s, err, err_len);
   if (rc) return rc;
   rc = build_node_layers_impl(d_layers[L], L, 0, m31_output, d_layers, s, err, err_len);
   return rc ? rc : ok(err, err_len);
@@ -429,6 +487,17 @@ extern "C" int stwo_b200_merkle_build_nodes(uint8_t* const* d_layers, uint32_t l
   STWO_ARG_CHECK(lifting_log_size <= 31, "bad lifting log size");
   int rc = build_node_layers_impl(d_layers[lifting_log_size], lifting_log_size, 0, m31_output, d_layers,
                                   as_stream(stream), err, err_len);
+  return rc ? rc : ok(err, err_len);
+}
+
+extern "C" int stwo_b200_merkle_build_leaves_layers(const uint32_t* const* d_cols, const uint32_t* log_sizes,
+                                                    uint32_t n_cols, uint32_t lifting_log_size, int m31_output,
+                                                    uint8_t* const* d_layers, void* stream, char* err,
+                                                    size_t err_len) {
+  STWO_ARG_CHECK(d_layers != nullptr, "null layers");
+  STWO_ARG_CHECK(lifting_log_size <= 30, "lifting log size %u too large", lifting_log_size);
+  int rc = build_leaves_impl(d_cols, log_sizes, n_cols, lifting_log_size, m31_output, d_layers[lifting_log_size],
+                             d_layers, as_stream(stream), err, err_len);
   return rc ? rc : ok(err, err_len);
 }
 

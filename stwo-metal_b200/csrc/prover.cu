@@ -27,7 +27,8 @@
 namespace stwo_b200 {
 
 int build_leaves_impl(const uint32_t* const* d_cols, const uint32_t* log_sizes, uint32_t n_cols, uint32_t L,
-                      int m31, uint8_t* d_leaves, cudaStream_t s, char* err, size_t err_len);
+                      int m31, uint8_t* d_leaves, uint8_t* const* layer_ws, cudaStream_t s, char* err,
+                      size_t err_len);
 int build_node_layers_impl(const uint8_t* in, uint32_t in_log, uint32_t stop_log, int m31,
                            uint8_t* const* outs_by_log, cudaStream_t s, char* err, size_t err_len);
 
@@ -1887,8 +1888,8 @@ class WideFibProver {
       std::vector<uint32_t*> q4(4);
       for (int k = 0; k < 4; k++) q4[k] = d_quot + ((uint64_t)k << lift);
       phase(kFriMerkle);
-      if ((rc = build_leaves_impl(q4.data(), std::vector<uint32_t>(4, lift).data(), 4, lift, m31, tq.layer(lift), s,
-                                  err, err_len)))
+      if ((rc = build_leaves_impl(q4.data(), std::vector<uint32_t>(4, lift).data(), 4, lift, m31, tq.layer(lift),
+                                  nullptr, s, err, err_len)))
         return rc;
       if ((rc = fri_tree_top(tq, lift, d_alphas, err, err_len))) return rc;
     }
@@ -2753,7 +2754,7 @@ struct SeededFriProver {
       cudaStream_t x = side[0];
       STWO_CUDA_TRY(cudaEventRecord(ev_fork[0], s));
       STWO_CUDA_TRY(cudaStreamWaitEvent(x, ev_fork[0], 0));
-      if ((rc = build_leaves_impl(d_coords, lg, 4, n, m31, trees[0].layer(n), x, err, err_len))) return rc;
+      if ((rc = build_leaves_impl(d_coords, lg, 4, n, m31, trees[0].layer(n), nullptr, x, err, err_len))) return rc;
       auto l0 = layer_ptrs(trees[0]);
       if ((rc = build_node_layers_impl(trees[0].layer(n), n, 0, m31, l0.data(), x, err, err_len))) return rc;
     }

@@ -243,6 +243,15 @@ class B200Backend:
                  _ptr_array(layers), self.stream)
         return layers
 
+    def build_leaves_layers(self, cols, lifting_log_size: int, layers, m31_output: bool = False):
+        """Leaves of columns sorted by length into layers[L]; layers[k < L]
+        hold the chaining values between the hashing stages until
+        build_nodes overwrites them."""
+        ffi.call("stwo_b200_merkle_build_leaves_layers", _ptr_array(cols), _u32_array([c.log_size for c in cols]),
+                 C.c_uint32(len(cols)), C.c_uint32(lifting_log_size), C.c_int(int(m31_output)),
+                 _ptr_array(layers), self.stream)
+        return layers[lifting_log_size]
+
     def build_leaves_into(self, cols, lifting_log_size: int, out: DeviceBuffer, m31_output: bool = False):
         ffi.call("stwo_b200_merkle_build_leaves", _ptr_array(cols), _u32_array([c.log_size for c in cols]),
                  C.c_uint32(len(cols)), C.c_uint32(lifting_log_size), C.c_int(int(m31_output)), C.c_void_p(out.ptr),

@@ -295,6 +295,33 @@ def test_merkle_many_columns_chunked(be, oracle):
     assert (layer_to_host(layers[7]) == ref[7]).all()
 
 
+STAGED_LEAF_CASES = [
+    # (log sizes, lifting log size): the leaves run in stages, one per run of
+    # 16-column compression groups of one largest log size, the chaining
+    # values lifted between stages
+    (sorted(int(x) for x in np.random.default_rng(7).integers(1, 13, 200)), 12),  # mixed groups, many stages
+    (sorted(int(x) for x in np.random.default_rng(8).integers(1, 11, 90)), 13),   # last group alone at L > max
+    ([3] * 1200 + [6] * 40, 6),   # 75 groups of one size: two launches, the second in place
+    ([5] * 1100, 5),              # 69 groups at L: the first launch leaves its chaining values for the second
+    ([1] * 16 + [2] * 16 + [9], 9),  # one group per stage, the last one partial
+]
+
+
+@pytest.mark.parametrize("logs,L", STAGED_LEAF_CASES)
+@pytest.mark.parametrize("m31", [False, True])
+def test_lifted_leaves_stages(be, oracle, logs, L, m31):
+    r = rng(len(logs) + L)
+    vals = [rand_col(r, l) for l in logs]
+    cols = [DeviceColumn.from_host(v) for v in vals]
+    ref = oracle.merkle_build_layers(vals, L, m31)
+    # with the tree's layer buffers as the stages' chaining values
+    layers = be.build_merkle_layers(cols, L, m31)
+    for k in range(L + 1):
+        assert (layer_to_host(layers[k]) == ref[k]).all(), k
+    # leaves alone: the chaining values packed in a temporary buffer
+    assert (layer_to_host(be.build_leaves(cols, L, m31)) == ref[L]).all()
+
+
 def test_build_leaves_and_next_layer(be, oracle):
     r = rng(5)
     vals = [rand_col(r, l) for l in [3, 5, 5, 8]]
