@@ -163,14 +163,16 @@ def eval_at_point_m31(coeffs, x: int, y: int) -> int:
     return int(out.value)
 
 
-def merkle_build_layers(cols, lifting_log_size: int, m31: bool = False):
-    """Lifted Merkle layers, root first; each layer a (2^k, 32) uint8 array."""
+def merkle_build_layers(cols, lifting_log_size: int, m31: bool = False, staged: bool = False):
+    """Lifted Merkle layers, root first; each layer a (2^k, 32) uint8 array.
+    staged: the leaves in SimdBackend's staged form (the same hashes, fewer
+    compressions for columns of different sizes)."""
     arrs = [_u32(c) for c in cols]
     logs = _u32([int(a.size).bit_length() - 1 for a in arrs])
     L = lifting_log_size
     out = np.zeros(((1 << (L + 1)) - 1) * 32, np.uint8)
     _check(lib().oracle_merkle_build_layers(_ptrs(arrs) if arrs else None, _p(logs), C.c_uint32(len(arrs)),
-                                            C.c_uint32(L), C.c_int(int(m31)), _p8(out)))
+                                            C.c_uint32(L), C.c_int(int(m31)), C.c_int(int(staged)), _p8(out)))
     layers, off = [], 0
     for k in range(L + 1):
         layers.append(out[off * 32:(off + (1 << k)) * 32].reshape(1 << k, 32))

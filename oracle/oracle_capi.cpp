@@ -114,12 +114,13 @@ int oracle_eval_at_point_m31(const uint32_t* coeffs, uint32_t log_n, uint32_t x,
 }
 
 // Lifted Merkle: layers root first, concatenated (layer k has 2^k hashes).
+// staged != 0: the leaves in SimdBackend's staged form (same hashes).
 int oracle_merkle_build_layers(const uint32_t* const* cols, const uint32_t* log_sizes, uint32_t n_cols, uint32_t L,
-                               int m31, uint8_t* layers_out) {
+                               int m31, int staged, uint8_t* layers_out) {
   return guard([&] {
     std::vector<const uint32_t*> c(cols, cols + n_cols);
     std::vector<uint32_t> l(log_sizes, log_sizes + n_cols);
-    auto layers = build_merkle_layers(c, l, L, m31 != 0);
+    auto layers = build_merkle_layers(c, l, L, m31 != 0, staged != 0);
     size_t off = 0;
     for (auto& layer : layers) {
       std::memcpy(layers_out + off, layer.data(), layer.size() * 32);

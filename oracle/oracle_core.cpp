@@ -238,6 +238,57 @@ std::vector<Hash> build_leaves(const std::vector<const uint32_t*>& cols, const s
   return out;
 }
 
+// SimdBackend's form of the same leaves (prover/backend/simd/blake2s_lifted.rs
+// :42-160): message block b (columns [16b, 16b + 16) of the sorted list) is
+// compressed at the size of its largest column, 2^S chaining values, each
+// starting from the previous block's value at lift_index(i, S - S_prev)
+// (lift_index(lift_index(i, a), b) == lift_index(i, a + b)); the last block
+// runs at L with the final flag.  Fewer compressions than build_leaves when
+// the columns differ in size; the same hashes.
+std::vector<Hash> build_leaves_staged(const std::vector<const uint32_t*>& cols, const std::vector<uint32_t>& log_sizes,
+                                      uint32_t L, bool m31) {
+  if (cols.empty()) return {blake2s_hash(nullptr, 0, m31)};
+  for (size_t c = 0; c + 1 < cols.size(); c++)
+    if (log_sizes[c] > log_sizes[c + 1]) throw std::runtime_error("columns must be sorted by length");
+  if (log_sizes[0] < 1) throw std::runtime_error("A column must be of length >= 2.");
+  if (log_sizes.back() > L) throw std::runtime_error("lifting_log_size below max column size");
+  using State = std::array<uint32_t, 8>;
+  const size_t n_cols = cols.size(), n_blocks = (n_cols + 15) / 16;
+  State init;
+  {
+    Blake2s b;
+    std::memcpy(init.data(), b.h, 32);
+  }
+  std::vector<State> prev, next;
+  uint32_t prev_log = 0;
+  for (size_t blk = 0; blk < n_blocks; blk++) {
+    const bool last = blk + 1 == n_blocks;
+    const uint32_t S = last ? L : log_sizes[std::min(16 * blk + 15, n_cols - 1)];
+    const uint64_t t = last ? 4 * (uint64_t)n_cols : 64 * (uint64_t)(blk + 1);
+    next.assign((size_t)1 << S, State{});
+#pragma omp parallel for schedule(static)
+    for (long long i = 0; i < (long long)next.size(); i++) {
+      State h = blk == 0 ? init : prev[lift_index((uint64_t)i, S - prev_log)];
+      uint32_t m[16];
+      for (size_t k = 0; k < 16; k++) {
+        const size_t c = 16 * blk + k;
+        m[k] = c < n_cols ? cols[c][lift_index((uint64_t)i, S - log_sizes[c])] : 0u;
+      }
+      Blake2s::compress(h.data(), m, t, last);
+      next[i] = h;
+    }
+    std::swap(prev, next);
+    prev_log = S;
+  }
+  std::vector<Hash> out(prev.size());
+#pragma omp parallel for schedule(static)
+  for (long long i = 0; i < (long long)out.size(); i++) {
+    std::memcpy(out[i].data(), prev[i].data(), 32);
+    if (m31) out[i] = reduce_to_m31(out[i]);
+  }
+  return out;
+}
+
 std::vector<Hash> build_next_layer(const std::vector<Hash>& prev, bool m31) {
   size_t n = prev.size() / 2;
   std::vector<Hash> out(n);
@@ -254,7 +305,7 @@ std::vector<Hash> build_next_layer(const std::vector<Hash>& prev, bool m31) {
 // prover/vcs_lifted/ops.rs:29-45 build_merkle_layers: stable sort by length,
 // leaves, then lifting_log_size node layers; returned root first.
 std::vector<std::vector<Hash>> build_merkle_layers(std::vector<const uint32_t*> cols, std::vector<uint32_t> log_sizes,
-                                                   uint32_t L, bool m31) {
+                                                   uint32_t L, bool m31, bool staged) {
   if (cols.empty()) return {build_leaves({}, {}, L, m31)};
   std::vector<size_t> order(cols.size());
   for (size_t i = 0; i < order.size(); i++) order[i] = i;
@@ -263,7 +314,7 @@ std::vector<std::vector<Hash>> build_merkle_layers(std::vector<const uint32_t*> 
   std::vector<uint32_t> sl;
   for (size_t i : order) { sc.push_back(cols[i]); sl.push_back(log_sizes[i]); }
   std::vector<std::vector<Hash>> layers;
-  layers.push_back(build_leaves(sc, sl, L, m31));
+  layers.push_back(staged ? build_leaves_staged(sc, sl, L, m31) : build_leaves(sc, sl, L, m31));
   for (uint32_t i = 0; i < L; i++) layers.push_back(build_next_layer(layers.back(), m31));
   std::reverse(layers.begin(), layers.end());
   return layers;

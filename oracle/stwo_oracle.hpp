@@ -317,9 +317,12 @@ uint32_t eval_at_point_m31(const uint32_t* coeffs, uint32_t log_n, CPoint p);
 
 std::vector<Hash> build_leaves(const std::vector<const uint32_t*>& cols, const std::vector<uint32_t>& log_sizes,
                                uint32_t L, bool m31);
+std::vector<Hash> build_leaves_staged(const std::vector<const uint32_t*>& cols, const std::vector<uint32_t>& log_sizes,
+                                      uint32_t L, bool m31);
 std::vector<Hash> build_next_layer(const std::vector<Hash>& prev, bool m31);
+// staged: the leaves in SimdBackend's staged form (build_leaves_staged)
 std::vector<std::vector<Hash>> build_merkle_layers(std::vector<const uint32_t*> cols, std::vector<uint32_t> log_sizes,
-                                                   uint32_t L, bool m31);
+                                                   uint32_t L, bool m31, bool staged = false);
 std::vector<Hash> commit_on_layer(uint32_t log_size, const Hash* prev, const std::vector<const uint32_t*>& cols,
                                   bool m31);
 

@@ -182,6 +182,24 @@ def test_lifted_leaves_streaming_definition(oracle):
         assert bytes(layers[-1][i]) == hashlib.blake2s(data).digest()
 
 
+@pytest.mark.parametrize("logs,L,m31", [
+    ([5, 3, 5, 1, 4, 3] + [4] * 17, 6, False),
+    ([2] * 16 + [3] * 16, 3, True),                       # whole blocks, the last at L
+    ([1] * 5 + [2] * 40 + [6] * 3 + [7] * 20, 9, False),  # last block alone at L > max
+    ([4], 4, True),
+])
+def test_lifted_leaves_staged_form(oracle, logs, L, m31):
+    # simd/blake2s_lifted.rs:42-160: message blocks hashed at the size of
+    # their largest column, chaining values lifted block to block; the same
+    # leaves as the per-leaf byte stream of cpu/merkle_lifted.rs:44-78.
+    rng = np.random.default_rng(len(logs) + L)
+    cols = [rng.integers(0, P, 1 << l, dtype=np.uint32) for l in logs]
+    direct = oracle.merkle_build_layers(cols, L, m31)
+    staged = oracle.merkle_build_layers(cols, L, m31, staged=True)
+    for k in range(L + 1):
+        assert (direct[k] == staged[k]).all(), k
+
+
 def test_lifted_equals_mixed_degree_on_lifted_input(oracle):
     # prover/vcs_lifted/prover.rs:307-336
     LOG, LIFT = 3, 9
