@@ -997,73 +997,84 @@ __global__ void __launch_bounds__(256, 4) fft_group_contig_kernel(FftPass p, Fft
   uint32_t* qb = buf + 32 * q * kTileStride;  // the warp's quarter: 32 lines
   const uint64_t hi = (uint64_t)p.tile0 + blockIdx.x;
   const uint64_t base = hi << T;
-  const uint32_t c = blockIdx.y * G + grp;
-  const bool active = c < p.n_cols;
+  // group grp transforms columns (blockIdx.y * cpb + g) * G + grp, g < cpb,
+  // of this tile position with the twiddles staged once
+  uint32_t c = blockIdx.y * p.cpb * G + grp;
   uint32_t v[32];
-  if (active) {
+  auto load_top = [&](uint32_t col) {
+    const uint32_t* __restrict__ sp = cols.src[col] + base + 32 * (q * I) + lane;
+#pragma unroll
+    for (uint32_t k = 0; k < W; k++)
+#pragma unroll
+      for (uint32_t i = 0; i < I; i++) v[k * I + i] = __ldg(sp + 1024 * k + 32 * i);
+  };
+  if (INV && c < p.n_cols) tile_prefetch(cols.src[c] + base + 1024 * q, qb, lane);
+  stage_tws_contig<T>(p, hi, tws);
+  __syncthreads();
+  const uint32_t n_bar = 32 * W;
+  const uint32_t scale = p.scale;
+  // c is uniform over a group: whole groups leave, the barriers below are per group
+  for (uint32_t g = 0; g < p.cpb && c < p.n_cols; g++, c += G) {
+    const uint32_t cn = c + G;
+    const bool more = g + 1 < p.cpb && cn < p.n_cols;
     if (INV) {
-      tile_prefetch(cols.src[c] + base + 1024 * q, qb, lane);
-    } else {
-      const uint32_t* __restrict__ sp = cols.src[c] + base + 32 * (q * I) + lane;
+      tile_wait();
+      tile_to_lane_major(qb, lane, v);
+      group_phase_lo<true, T>(v, tws, 32 * q + lane);
+      lane_major_to_tile(qb, lane, v);
+      __syncwarp();
+#pragma unroll
+      for (int j = 0; j < 32; j++) v[j] = qb[j * kTileStride + lane];
+      group_phase_hi<true, T>(v, tws, q);
+#pragma unroll
+      for (int j = 0; j < 32; j++) qb[j * kTileStride + lane] = v[j];
+      group_barrier(grp, n_bar);
 #pragma unroll
       for (uint32_t k = 0; k < W; k++)
 #pragma unroll
-        for (uint32_t i = 0; i < I; i++) v[k * I + i] = __ldg(sp + 1024 * k + 32 * i);
-    }
-  }
-  stage_tws_contig<T>(p, hi, tws);
-  __syncthreads();
-  if (!active) return;  // whole groups only: the barriers below are per group
-  const uint32_t n_bar = 32 * W;
-  const uint32_t scale = p.scale;
-  if (INV) {
-    tile_wait();
-    tile_to_lane_major(qb, lane, v);
-    group_phase_lo<true, T>(v, tws, 32 * q + lane);
-    lane_major_to_tile(qb, lane, v);
-    __syncwarp();
-#pragma unroll
-    for (int j = 0; j < 32; j++) v[j] = qb[j * kTileStride + lane];
-    group_phase_hi<true, T>(v, tws, q);
-#pragma unroll
-    for (int j = 0; j < 32; j++) qb[j * kTileStride + lane] = v[j];
-    group_barrier(grp, n_bar);
-#pragma unroll
-    for (uint32_t k = 0; k < W; k++)
-#pragma unroll
-      for (uint32_t i = 0; i < I; i++) v[k * I + i] = buf[(32 * k + q * I + i) * kTileStride + lane];
-    group_phase_top<true, K>(v, tws);
-    uint32_t* __restrict__ dp = cols.dst[c] + base + 32 * (q * I) + lane;
-#pragma unroll
-    for (uint32_t k = 0; k < W; k++)
-#pragma unroll
-      for (uint32_t i = 0; i < I; i++) {
-        const uint32_t x = v[k * I + i];
-        dp[1024 * k + 32 * i] = scale != 1u ? m31_mul(x, scale) : x;
+        for (uint32_t i = 0; i < I; i++) v[k * I + i] = buf[(32 * k + q * I + i) * kTileStride + lane];
+      if (more) {
+        group_barrier(grp, n_bar);  // every warp has read its top rows out of the quarters
+        tile_prefetch(cols.src[cn] + base + 1024 * q, qb, lane);
       }
-  } else {
-    group_phase_top<false, K>(v, tws);
+      group_phase_top<true, K>(v, tws);
+      uint32_t* __restrict__ dp = cols.dst[c] + base + 32 * (q * I) + lane;
 #pragma unroll
-    for (uint32_t k = 0; k < W; k++)
+      for (uint32_t k = 0; k < W; k++)
 #pragma unroll
-      for (uint32_t i = 0; i < I; i++) buf[(32 * k + q * I + i) * kTileStride + lane] = v[k * I + i];
-    group_barrier(grp, n_bar);
+        for (uint32_t i = 0; i < I; i++) {
+          const uint32_t x = v[k * I + i];
+          dp[1024 * k + 32 * i] = scale != 1u ? m31_mul(x, scale) : x;
+        }
+    } else {
+      load_top(c);
+      group_phase_top<false, K>(v, tws);
+      if (g > 0) {
+        bulk_wait_read();  // this warp's bulk stores of the previous column have read its lines
+        group_barrier(grp, n_bar);
+      }
 #pragma unroll
-    for (int j = 0; j < 32; j++) v[j] = qb[j * kTileStride + lane];
-    group_phase_hi<false, T>(v, tws, q);
+      for (uint32_t k = 0; k < W; k++)
 #pragma unroll
-    for (int j = 0; j < 32; j++) qb[j * kTileStride + lane] = v[j];
-    __syncwarp();
-    tile_to_lane_major(qb, lane, v);
-    group_phase_lo<false, T>(v, tws, 32 * q + lane);
-    if (scale != 1u) {
+        for (uint32_t i = 0; i < I; i++) buf[(32 * k + q * I + i) * kTileStride + lane] = v[k * I + i];
+      group_barrier(grp, n_bar);
 #pragma unroll
-      for (int j = 0; j < 32; j++) v[j] = m31_mul(v[j], scale);
+      for (int j = 0; j < 32; j++) v[j] = qb[j * kTileStride + lane];
+      group_phase_hi<false, T>(v, tws, q);
+#pragma unroll
+      for (int j = 0; j < 32; j++) qb[j * kTileStride + lane] = v[j];
+      __syncwarp();
+      tile_to_lane_major(qb, lane, v);
+      group_phase_lo<false, T>(v, tws, 32 * q + lane);
+      if (scale != 1u) {
+#pragma unroll
+        for (int j = 0; j < 32; j++) v[j] = m31_mul(v[j], scale);
+      }
+      lane_major_to_tile(qb, lane, v);  // the lane's own line, read just above
+      line_bulk_store(cols.dst[c] + base + 1024 * q + 32 * lane, qb + lane * kTileStride);
     }
-    lane_major_to_tile(qb, lane, v);  // the lane's own line, read just above
-    line_bulk_store(cols.dst[c] + base + 1024 * q + 32 * lane, qb + lane * kTileStride);
-    bulk_wait_all();
   }
+  if (!INV) bulk_wait_all();
 }
 
 template <bool INV, int K>
@@ -1074,8 +1085,13 @@ static int launch_group_contig(const FftPass& q, const FftCols& cols, uint64_t t
   constexpr size_t smem = ((1u << T) + G * (1u << (T - 5)) * kTileStride) * sizeof(uint32_t);
   static std::atomic<uint32_t> attr{0};
   STWO_CUDA_TRY(ensure_smem_limit(fft_group_contig_kernel<INV, K>, (int)smem, attr));
-  dim3 grid((unsigned)tiles, (unsigned)((nc + G - 1) / G));
-  fft_group_contig_kernel<INV, K><<<grid, 256, smem, s>>>(q, cols);
+  // up to 4 columns per group: fewer twiddle stagings while the grid still
+  // has several waves of blocks
+  const uint32_t groups = (uint32_t)((nc + G - 1) / G);
+  FftPass qq = q;
+  qq.cpb = std::max<uint32_t>(1, std::min<uint32_t>(4, (uint32_t)((tiles * groups) / (148 * 4 * 6))));
+  dim3 grid((unsigned)tiles, (unsigned)((groups + qq.cpb - 1) / qq.cpb));
+  fft_group_contig_kernel<INV, K><<<grid, 256, smem, s>>>(qq, cols);
   STWO_CHECK_LAUNCH();
   return STWO_B200_OK;
 }

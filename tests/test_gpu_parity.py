@@ -209,6 +209,35 @@ def test_interpolate_evaluate_many_columns(be, oracle, big_tree):
         assert (outs[k].to_host() == oracle.evaluate(co, 21, tw)).all(), k
 
 
+@pytest.mark.parametrize("log_n,plan,n_cols", [(22, [12, 10], 15), (21, [11, 10], 27)])
+def test_group_passes_loop_over_columns(be, oracle, big_tree, log_n, plan, n_cols):
+    # Enough columns that the 11- and 12-layer contiguous passes give each
+    # warp group several columns of one tile position (the interpolation's
+    # first pass and the blowup-2 evaluation's last), with a ragged last
+    # group; three distinct columns repeated, checked at every position.
+    from stwo_b200 import fft_get_plan, fft_set_plan
+    tree, tw, itw = big_tree
+    old = fft_get_plan(log_n)
+    fft_set_plan(log_n, plan)
+    try:
+        r = rng(3300 + log_n)
+        base = [rand_col(r, log_n) for _ in range(3)]
+        base[1][::5] = P
+        srcs = [DeviceColumn.from_host(base[k % 3]) for k in range(n_cols)]
+        coeffs = [DeviceColumn(1 << log_n) for _ in range(n_cols)]
+        outs = [DeviceColumn(1 << (log_n + 2)) for _ in range(n_cols)]
+        be.interpolate_evaluate_into(srcs, coeffs, 2, tree, outs)
+        ref = []
+        for b in base:
+            co = oracle.interpolate(b, itw)
+            ref.append((co, oracle.evaluate(co, log_n + 2, tw)))
+        for k in range(n_cols):
+            assert (coeffs[k].to_host() == ref[k % 3][0]).all(), k
+            assert (outs[k].to_host() == ref[k % 3][1]).all(), k
+    finally:
+        fft_set_plan(log_n, old)
+
+
 @pytest.mark.parametrize("log_blowup", [1, 2])
 def test_interpolate_evaluate_layer12_plan(be, oracle, big_tree, log_blowup):
     # Log 22 under the split [12, 10] (the uneven commit's autotuned plan):
