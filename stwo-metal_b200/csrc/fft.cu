@@ -1085,11 +1085,11 @@ static int launch_group_contig(const FftPass& q, const FftCols& cols, uint64_t t
   constexpr size_t smem = ((1u << T) + G * (1u << (T - 5)) * kTileStride) * sizeof(uint32_t);
   static std::atomic<uint32_t> attr{0};
   STWO_CUDA_TRY(ensure_smem_limit(fft_group_contig_kernel<INV, K>, (int)smem, attr));
-  // up to 4 columns per group: fewer twiddle stagings while the grid still
-  // has several waves of blocks
+  // up to 16 columns per group: fewer twiddle stagings while the grid still
+  // has six waves of blocks
   const uint32_t groups = (uint32_t)((nc + G - 1) / G);
   FftPass qq = q;
-  qq.cpb = std::max<uint32_t>(1, std::min<uint32_t>(4, (uint32_t)((tiles * groups) / (148 * 4 * 6))));
+  qq.cpb = std::max<uint32_t>(1, std::min<uint32_t>(16, (uint32_t)((tiles * groups) / (148 * 4 * 6))));
   dim3 grid((unsigned)tiles, (unsigned)((groups + qq.cpb - 1) / qq.cpb));
   fft_group_contig_kernel<INV, K><<<grid, 256, smem, s>>>(qq, cols);
   STWO_CHECK_LAUNCH();
@@ -1103,11 +1103,11 @@ static int launch_warp_pass(const FftPass& q, const FftCols& cols, uint64_t tile
     constexpr size_t smem = (1024 + kWarpCols * kTileWords) * sizeof(uint32_t);
     static std::atomic<uint32_t> attr{0};
     STWO_CUDA_TRY(ensure_smem_limit(fft_warp_contig_kernel<INV>, (int)smem, attr));
-    // up to 4 column groups per block: fewer twiddle stagings while the grid
-    // still has several waves of blocks
+    // up to 16 column groups per block: fewer twiddle stagings while the grid
+    // still has six waves of blocks
     const uint32_t groups = (uint32_t)((nc + kWarpCols - 1) / kWarpCols);
     FftPass qq = q;
-    qq.cpb = std::max<uint32_t>(1, std::min<uint32_t>(4, (uint32_t)((tiles * groups) / (148 * 4 * 6))));
+    qq.cpb = std::max<uint32_t>(1, std::min<uint32_t>(16, (uint32_t)((tiles * groups) / (148 * 4 * 6))));
     dim3 grid((unsigned)tiles, (unsigned)((groups + qq.cpb - 1) / qq.cpb));
     fft_warp_contig_kernel<INV><<<grid, 32 * kWarpCols, smem, s>>>(qq, cols);
   } else {
