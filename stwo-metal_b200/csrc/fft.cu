@@ -809,6 +809,7 @@ __global__ void __launch_bounds__(256, 4) fft_warp_strided_kernel(FftPass p, Fft
 // the later ones re-read the thread's own stores through L2.  Thread layout,
 // exchange tile and twiddle tables are those of fft_warp_strided_kernel; the
 // forward tables of all 2^b positions are staged with the inverse one.
+// Launched at b = 1 (interpolate_evaluate).
 struct FftColsIE {
   uint32_t* coef[kFftMaxCols];  // interpolation intermediate in, coefficients out
   uint32_t* eval[kFftMaxCols];  // evaluation (2^b times longer) out
@@ -1423,7 +1424,9 @@ int interpolate_evaluate(uint32_t* const* coeffs, uint32_t* const* evals, uint32
   STWO_ARG_CHECK(d_twiddles && N - 1 <= tree_log_size, "twiddle tree (log %u) too small for log size %u",
                  tree_log_size, N);
   const uint32_t L0 = log_n - split.back();
-  const bool fused = np >= 2 && split.back() == 10 && L0 >= 10 && L0 <= 12 && log_blowup >= 1 && log_blowup <= 2;
+  // Blowup 1 only: at blowup 2 the fused kernel (four forward tables, three
+  // halves re-read through L2) measured 3-4% slower than the two passes.
+  const bool fused = np >= 2 && split.back() == 10 && L0 >= 10 && L0 <= 12 && log_blowup == 1;
   const uint32_t* const* src = first_pass == 0 ? src0 : nullptr;
   if (!fused) {
     for (uint32_t pi = first_pass; pi < np; pi++) {
@@ -1456,12 +1459,10 @@ int interpolate_evaluate(uint32_t* const* coeffs, uint32_t* const* evals, uint32
   pf.scale = 1u;
   const uint32_t n_hi = 1u << log_blowup;
   const size_t smem = (1024 + kXchWords + 1024 * n_hi) * sizeof(uint32_t);
-  // the limit is set once per device, for the largest table set (blowup 2)
-  constexpr size_t smem_max = (1024 + kXchWords + 1024 * 4) * sizeof(uint32_t);
   static std::atomic<uint32_t> attr10{0}, attr11{0}, attr12{0};
-  STWO_CUDA_TRY(L0 == 10   ? ensure_smem_limit(fft_warp_inv_fwd_kernel<10>, (int)smem_max, attr10)
-                : L0 == 11 ? ensure_smem_limit(fft_warp_inv_fwd_kernel<11>, (int)smem_max, attr11)
-                           : ensure_smem_limit(fft_warp_inv_fwd_kernel<12>, (int)smem_max, attr12));
+  STWO_CUDA_TRY(L0 == 10   ? ensure_smem_limit(fft_warp_inv_fwd_kernel<10>, (int)smem, attr10)
+                : L0 == 11 ? ensure_smem_limit(fft_warp_inv_fwd_kernel<11>, (int)smem, attr11)
+                           : ensure_smem_limit(fft_warp_inv_fwd_kernel<12>, (int)smem, attr12));
   for (uint32_t c0 = 0; c0 < n_cols; c0 += kFftMaxCols) {
     const uint32_t nc = std::min<uint32_t>(kFftMaxCols, n_cols - c0);
     FftColsIE cols;

@@ -149,8 +149,8 @@ def test_uneven_batch_roundtrip(be, oracle, big_tree):
 @pytest.mark.parametrize("in_place", [False, True])
 def test_interpolate_evaluate(be, oracle, big_tree, log_n, log_blowup, in_place):
     # interpolate_columns + evaluate_polynomials in one call: at logs 20 and 21
-    # with a blowup the interpolation's last pass and the evaluation's first
-    # are one kernel.  Words equal to P included.
+    # with blowup 1 the interpolation's last pass and the evaluation's first
+    # are one kernel (separate passes at blowup 2).  Words equal to P included.
     tree, tw, itw = big_tree
     r = rng(3000 + log_n)
     vals = [rand_col(r, log_n) for _ in range(3)]
@@ -241,8 +241,8 @@ def test_group_passes_loop_over_columns(be, oracle, big_tree, log_n, plan, n_col
 @pytest.mark.parametrize("log_blowup", [1, 2])
 def test_interpolate_evaluate_layer12_plan(be, oracle, big_tree, log_blowup):
     # Log 22 under the split [12, 10] (the uneven commit's autotuned plan):
-    # the 10-layer strided passes start at layer 12, fused in the one call and
-    # separate in the two trait calls.
+    # the 10-layer strided passes start at layer 12, fused in the one call at
+    # blowup 1 and separate in the two trait calls (and at blowup 2).
     from stwo_b200 import fft_get_plan, fft_set_plan
     tree, tw, itw = big_tree
     old = fft_get_plan(22)

@@ -21,7 +21,8 @@ CASES = [
     (14, 100, 1, 1, 0, 3, False),
     (16, 64, 1, 1, 0, 3, False),
     # the interpolation's last pass fused with the evaluation's first
-    # (layers 10..19 at log 20, 11..20 at log 21; blowup 1 and 2)
+    # (layers 10..19 at log 20, 11..20 at log 21; blowup 1), and the two
+    # separate passes at blowup 2
     (20, 8, 1, 1, 0, 3, False),
     (20, 4, 2, 1, 0, 3, False),
     (21, 4, 1, 1, 0, 3, False),
