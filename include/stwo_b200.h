@@ -247,9 +247,10 @@ int stwo_b200_decompose(const uint32_t* const* d_in4, uint32_t log_size, uint32_
  * (18,960 bytes) is a fixed device array that every GPU loading the library
  * keeps until exit.  Inputs up to 2^30 elements per coordinate; larger sizes
  * are rejected.  The first call on a device looks up the array's device
- * address and caches it per device (make it before any stream capture; a
- * cudaDeviceReset between calls is not supported).  Calls share the array:
- * calls that overlap on the GPU race.  Synchronises `stream`. */
+ * address and caches it per device (a cudaDeviceReset between calls is not
+ * supported).  Calls share the array: calls that overlap on the GPU race.
+ * Like stwo_b200_decompose, the call synchronises `stream` before it
+ * returns, to hand lambda to the host. */
 int stwo_b200_decompose_noalloc(const uint32_t* const* d_in4, uint32_t log_size, uint32_t* const* d_out4,
                                 uint32_t* lambda_out, void* stream, char* err, size_t err_len);
 

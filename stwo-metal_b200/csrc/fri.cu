@@ -340,9 +340,9 @@ extern "C" int stwo_b200_decompose(const uint32_t* const* d_in4, uint32_t log_si
 // host code the symbol's name is a host-side stand-in, not a device address,
 // so the address is fetched once per device with cudaGetSymbolAddress (with
 // that device current) and cached; the first call on a device does that
-// set-up, so make it before any stream capture.  The cache is keyed by device
-// ordinal: a cudaDeviceReset between calls (which recreates the device's
-// context and may move the array) is not supported.  All calls on a device share
+// set-up.  The cache is keyed by device ordinal: a cudaDeviceReset between
+// calls (which recreates the device's context and may move the array) is not
+// supported.  All calls on a device share
 // the array and it keeps the last call's contents: each call overwrites every
 // word it reads, and calls that overlap on the GPU (different streams, or
 // host threads without ordering) race on it.
