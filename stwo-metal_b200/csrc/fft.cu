@@ -727,9 +727,12 @@ __device__ __forceinline__ uint32_t xch_pos(uint32_t r, uint32_t c) { return (r 
 // A power-of-two source mask that covers every row and column bit of the
 // tile (the duplicated coefficients of a blowup evaluation) only changes the
 // tile base.
-__host__ __device__ __forceinline__ bool strided_mask_on_base(uint64_t mask, uint64_t len, uint32_t L0) {
+__host__ __device__ __forceinline__ bool strided_mask_on_span(uint64_t mask, uint64_t len, uint32_t span_log) {
   return (mask == ~0ull && len == ~0ull) ||
-         (mask != ~0ull && ((mask + 1) & mask) == 0 && mask + 1 >= (1ull << (L0 + 10)) && len > mask);
+         (mask != ~0ull && ((mask + 1) & mask) == 0 && mask + 1 >= (1ull << span_log) && len > mask);
+}
+__host__ __device__ __forceinline__ bool strided_mask_on_base(uint64_t mask, uint64_t len, uint32_t L0) {
+  return strided_mask_on_span(mask, len, L0 + 10);
 }
 
 // L0T != 0 fixes layer0 at compile time (the row stride 2^L0T words): the
@@ -793,6 +796,132 @@ __global__ void __launch_bounds__(256, 4) fft_warp_strided_kernel(FftPass p, Fft
 #pragma unroll
   for (int j = 0; j < 32; j++)
     dp[(uint64_t)((INV ? 32 : 1) * j) << L0] = scale != 1u ? m31_mul(v[j], scale) : v[j];
+}
+
+// Strided passes of T = 6..9 layers (layer0 = L0, L0 + T >= 13) on the
+// thread layout of fft_warp_strided_kernel.  A block again covers 8 adjacent
+// columns x 1024 tile rows, but tile row r = r_hi 2^T + r_lo is row r_lo of
+// the pass (stride 2^L0 words) in the 8-column group r_hi above the first
+// (offset 8 r_hi words): 2^(10-T) tiles of the pass side by side.  Layers
+// 0..4 run lane-major and layers 5..T-1 row-major, as in the 10-layer pass.
+// A layer's twiddles depend on r_lo and the tile position, not on r_hi, so
+// the block stages each layer's table replicated over r_hi and the lookups
+// index r >> (lam + 1) unchanged.  Tile position: global words
+// (hi << (L0 + T)) | (lo << (13 - T)), lo < 2^(L0 + T - 13).  Sources whose
+// mask acts on the tile base only (checked by the launcher).
+template <int T>
+__device__ __forceinline__ uint64_t short_row_off(uint32_t r, uint32_t L0) {
+  return ((uint64_t)(r & ((1u << T) - 1)) << L0) + ((uint64_t)(r >> T) << 3);
+}
+// Layers 5..T-1 on v[j] = row 32 j + b (see warp_phase_hi).
+template <bool INV, int T>
+__device__ __forceinline__ void warp_phase_hi_short(uint32_t (&v)[32], const uint32_t* __restrict__ tws) {
+  constexpr int NK = T - 5;
+#pragma unroll
+  for (int kk = 0; kk < NK; kk++) {
+    const int k = INV ? kk : NK - 1 - kk;  // bit of j
+    const uint32_t* tl = tws + (1024u - (1024u >> (5 + k)));
+    uint32_t t[16];
+#pragma unroll
+    for (int m = 0; m < (1 << (4 - k)); m++) t[m] = tl[m];
+#pragma unroll
+    for (int j = 0; j < 32; j++) {
+      if (j & (1 << k)) continue;
+      if (INV)
+        ibfly2(v[j], v[j | (1 << k)], t[j >> (k + 1)]);
+      else
+        bfly2(v[j], v[j | (1 << k)], t[j >> (k + 1)]);
+    }
+  }
+}
+// The tables of layers 0..T-1 in the slots of stage_tws10 (layer lam at
+// 1024 - 2^(10 - lam), 2^(9 - lam) entries), entry e holding twiddle
+// (hi << (T - 1 - lam)) + (e mod 2^(T - 1 - lam)) of tree layer L0 + lam,
+// doubled.  All loads before any store.
+template <int T>
+__device__ __forceinline__ void stage_tws_short(const FftPass& p, uint32_t L0, uint64_t hi, uint32_t* tws) {
+  const uint32_t* tail = p.tree + p.tree_len;
+  const uint32_t N = p.log_domain, t = threadIdx.x;
+  uint32_t val[4];
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    const uint32_t sl = t + 256u * k;
+    const uint32_t lam = sl < 1023u ? __clz(1023u - sl) - 22 : 10u;
+    val[k] = 0;
+    if (lam < (uint32_t)T) {
+      const uint32_t e = sl - (1024u - (1024u >> lam));
+      const uint64_t idx = (hi << (T - 1 - lam)) + (e & ((1u << (T - 1 - lam)) - 1));
+      val[k] = __ldg(tail - (1ull << (N - L0 - lam)) + idx);
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    const uint32_t sl = t + 256u * k;
+    if (sl < 1023u && __clz(1023u - sl) - 22 < (uint32_t)T) tws[sl] = val[k] << 1;
+  }
+}
+template <bool INV, int T, int L0T>
+__global__ void __launch_bounds__(256, 4) fft_warp_strided_short_kernel(FftPass p, FftCols cols) {
+  extern __shared__ __align__(16) uint32_t smem[];
+  uint32_t* tws = smem;
+  uint32_t* xch = smem + 1024;
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t c = lane & 7, m = (threadIdx.x >> 5) * 4 + (lane >> 3);
+  const uint32_t L0 = L0T ? (uint32_t)L0T : p.layer0;
+  const uint64_t t = blockIdx.x;
+  const uint32_t lo_bits = L0 + T - 13;
+  const uint64_t lo = t & ((1ull << lo_bits) - 1);
+  const uint64_t hi = t >> lo_bits;
+  const uint64_t base = (hi << (L0 + T)) | (lo << (13 - T));
+  // Rows held in the layout the pass starts from: lane-major (32 m + j) for
+  // the inverse transform, row-major (32 j + m) for the forward one.  With
+  // T >= 5, row 32 m + j lies at short_row_off(32 m) + (j << L0), and row
+  // 32 j + m at (m << L0) + short_row_off(32 j).
+  uint32_t v[32];
+  {
+    const uint32_t* __restrict__ sp = cols.src[blockIdx.y] + (base & p.src_mask) + c;
+    if (INV) {
+      sp += short_row_off<T>(32 * m, L0);
+#pragma unroll
+      for (int j = 0; j < 32; j++) v[j] = __ldg(sp + ((uint64_t)j << L0));
+    } else {
+      sp += (uint64_t)m << L0;
+#pragma unroll
+      for (int j = 0; j < 32; j++) v[j] = __ldg(sp + short_row_off<T>(32 * j, L0));
+    }
+  }
+  stage_tws_short<T>(p, L0, hi, tws);
+  __syncthreads();
+  if (INV) {
+    warp_phase_lo<true>(v, tws, m);
+#pragma unroll
+    for (int j = 0; j < 32; j++) xch[xch_pos(32 * m + j, c)] = v[j];
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < 32; j++) v[j] = xch[xch_pos(32 * j + m, c)];
+    warp_phase_hi_short<true, T>(v, tws);
+  } else {
+    warp_phase_hi_short<false, T>(v, tws);
+#pragma unroll
+    for (int j = 0; j < 32; j++) xch[xch_pos(32 * j + m, c)] = v[j];
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < 32; j++) v[j] = xch[xch_pos(32 * m + j, c)];
+    warp_phase_lo<false>(v, tws, m);
+  }
+  // Stores in the layout the pass ends in: row-major for the inverse
+  // transform, lane-major for the forward one.
+  const uint32_t scale = p.scale;
+  uint32_t* __restrict__ dp = cols.dst[blockIdx.y] + base + c;
+  if (INV) {
+    dp += (uint64_t)m << L0;
+#pragma unroll
+    for (int j = 0; j < 32; j++) dp[short_row_off<T>(32 * j, L0)] = scale != 1u ? m31_mul(v[j], scale) : v[j];
+  } else {
+    dp += short_row_off<T>(32 * m, L0);
+#pragma unroll
+    for (int j = 0; j < 32; j++) dp[(uint64_t)j << L0] = scale != 1u ? m31_mul(v[j], scale) : v[j];
+  }
 }
 
 // The last pass of an interpolation fused with the first pass of the
@@ -1135,6 +1264,39 @@ static int launch_warp_pass(const FftPass& q, const FftCols& cols, uint64_t tile
   return STWO_B200_OK;
 }
 
+template <bool INV, int T>
+static int launch_strided_short_t(const FftPass& q, const FftCols& cols, uint64_t blocks, size_t nc, cudaStream_t s,
+                                  char* err, size_t err_len) {
+  constexpr size_t smem = (1024 + kXchWords) * sizeof(uint32_t);
+  static std::atomic<uint32_t> attr10{0}, attr11{0}, attr{0};
+  dim3 grid((unsigned)blocks, (unsigned)nc);
+  if (q.layer0 == 10) {
+    STWO_CUDA_TRY(ensure_smem_limit(fft_warp_strided_short_kernel<INV, T, 10>, (int)smem, attr10));
+    fft_warp_strided_short_kernel<INV, T, 10><<<grid, 256, smem, s>>>(q, cols);
+  } else if (q.layer0 == 11) {
+    STWO_CUDA_TRY(ensure_smem_limit(fft_warp_strided_short_kernel<INV, T, 11>, (int)smem, attr11));
+    fft_warp_strided_short_kernel<INV, T, 11><<<grid, 256, smem, s>>>(q, cols);
+  } else {
+    STWO_CUDA_TRY(ensure_smem_limit(fft_warp_strided_short_kernel<INV, T, 0>, (int)smem, attr));
+    fft_warp_strided_short_kernel<INV, T, 0><<<grid, 256, smem, s>>>(q, cols);
+  }
+  STWO_CHECK_LAUNCH();
+  return STWO_B200_OK;
+}
+
+// A whole strided pass of 6..9 layers: 2^(10 - T) of its tiles per block.
+template <bool INV>
+static int launch_strided_short(const FftPass& q, const FftCols& cols, uint64_t tiles, size_t nc, cudaStream_t s,
+                                char* err, size_t err_len) {
+  const uint64_t blocks = tiles >> (10 - q.T);
+  switch (q.T) {
+    case 6: return launch_strided_short_t<INV, 6>(q, cols, blocks, nc, s, err, err_len);
+    case 7: return launch_strided_short_t<INV, 7>(q, cols, blocks, nc, s, err, err_len);
+    case 8: return launch_strided_short_t<INV, 8>(q, cols, blocks, nc, s, err, err_len);
+    default: return launch_strided_short_t<INV, 9>(q, cols, blocks, nc, s, err, err_len);
+  }
+}
+
 template <bool INV, int T, int C, int CPB>
 static int launch_tile(const FftPass& q, const FftCols& cols, dim3 grid, cudaStream_t s, char* err, size_t err_len) {
   constexpr int NT = fft_threads(T, C, CPB);
@@ -1198,12 +1360,17 @@ static int launch_pass(const FftPass& p, const std::vector<const uint32_t*>& src
     const bool warp_contig = p.T == 10 && p.C == 0 && p.layer0 == 0 && aligned && p.src_mask == ~0ull &&
                              p.src_len == ~0ull;
     const bool warp_strided = p.T == 10 && p.C == 3 && p.layer0 >= 3;
+    // whole passes only: its blocks cover 2^(10 - T) tiles each
+    const bool warp_short = p.C == 3 && p.T >= 6 && p.T <= 9 && p.layer0 + p.T >= 13 && tile_cnt == 0 &&
+                            tile0 == 0 && strided_mask_on_span(p.src_mask, p.src_len, p.layer0 + p.T);
     const bool group_contig = (p.T == 11 || p.T == 12) && p.C == 0 && p.layer0 == 0 && aligned && !p.natural &&
                               p.src_mask == ~0ull && p.src_len == ~0ull;
     STWO_ARG_CHECK(!p.natural || (INV && p.C == 0 && p.layer0 == 0 && p.src_mask == ~0ull && p.src_len == ~0ull),
                    "natural-order source needs an unmasked first inverse pass");
     if (warp_contig || warp_strided)
       rc = launch_warp_pass<INV>(q, cols, tiles, nc, s, err, err_len);
+    else if (warp_short)
+      rc = launch_strided_short<INV>(q, cols, tiles, nc, s, err, err_len);
     else if (group_contig)
       rc = p.T == 11 ? launch_group_contig<INV, 1>(q, cols, tiles, nc, s, err, err_len)
                      : launch_group_contig<INV, 2>(q, cols, tiles, nc, s, err, err_len);

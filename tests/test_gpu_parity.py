@@ -209,6 +209,34 @@ def test_interpolate_evaluate_many_columns(be, oracle, big_tree):
         assert (outs[k].to_host() == oracle.evaluate(co, 21, tw)).all(), k
 
 
+@pytest.mark.parametrize("log_n,plan", [(16, [10, 6]), (17, [10, 7]), (18, [10, 8]), (19, [10, 9]), (19, [11, 8]),
+                                        (15, [7, 8]), (13, [7, 6]), (14, [5, 9])])
+def test_short_strided_passes(be, oracle, big_tree, log_n, plan):
+    # Second passes of 6..9 layers: the warp kernel that puts 2^(10 - T) tiles
+    # of the pass side by side in one block (layer offsets 10 and 11 fixed at
+    # compile time, others read at run time), for the interpolation and for
+    # evaluations at blowups 0..2 (the duplicated coefficients masked).
+    from stwo_b200 import fft_get_plan, fft_set_plan
+    tree, tw, itw = big_tree
+    old = fft_get_plan(log_n)
+    fft_set_plan(log_n, plan)
+    try:
+        r = rng(3400 + log_n + plan[0])
+        vals = [rand_col(r, log_n) for _ in range(3)]
+        vals[1][::3] = P
+        cols = [DeviceColumn.from_host(v) for v in vals]
+        be.interpolate_columns(cols, tree)
+        for blowup in (0, 1, 2):
+            evs = be.evaluate_polynomials(cols, blowup, tree)
+            for k, v in enumerate(vals):
+                co = oracle.interpolate(v, itw)
+                if blowup == 0:
+                    assert (cols[k].to_host() == co).all(), k
+                assert (evs[k].to_host() == oracle.evaluate(co, log_n + blowup, tw)).all(), (k, blowup)
+    finally:
+        fft_set_plan(log_n, old)
+
+
 @pytest.mark.parametrize("log_n,plan,n_cols", [(22, [12, 10], 15), (21, [11, 10], 27)])
 def test_group_passes_loop_over_columns(be, oracle, big_tree, log_n, plan, n_cols):
     # Enough columns that the 11- and 12-layer contiguous passes give each
