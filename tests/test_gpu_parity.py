@@ -377,6 +377,13 @@ def test_lifted_leaves_stages(be, oracle, logs, L, m31):
         assert (layer_to_host(layers[k]) == ref[k]).all(), k
     # leaves alone: the chaining values packed in a temporary buffer
     assert (layer_to_host(be.build_leaves(cols, L, m31)) == ref[L]).all()
+    # leaves into caller-owned layers (build_leaves_layers), then the nodes
+    from stwo_b200 import DeviceBuffer
+    own = [DeviceBuffer(32 << k) for k in range(L + 1)]
+    assert (layer_to_host(be.build_leaves_layers(cols, L, own, m31)) == ref[L]).all()
+    be.build_nodes(own, m31)
+    for k in range(L + 1):
+        assert (layer_to_host(own[k]) == ref[k]).all(), k
 
 
 def test_build_leaves_and_next_layer(be, oracle):
