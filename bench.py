@@ -621,7 +621,8 @@ def prove_config_json(spec, world):
             "channel": "Blake2sMerkleChannel", "inputs": "col0/col1 uniform [0, 2^31-1) per row, seed 2",
             "l2": prove_l2_note(spec),
             "twiddles": "resident on the device from prover creation (outside the timed region; the "
-                        "reference harness precomputes them inside every sample)",
+                        "reference harness precomputes them inside every sample; their device time is the "
+                        "line's twiddle_precompute_ms)",
             "e2e_inputs": "the two seed columns (2 x 2^log_n_rows words) are copied per proof; the other "
                           "columns are generated on the device, as the Wide-Fibonacci trace is defined",
             "parallelism": f"replicas x{world}"}
@@ -672,6 +673,33 @@ def run_prove_reference(args, world, rank):
 # fft_warp_contig_kernel<0> 347.7 + 275.4 MB -- scaled to the 100 columns of
 # the proof.
 TRACE_FFT_TRAFFIC_100x2e20 = (172.0 + 120.7 + 167.8 + 451.7 + 347.7 + 275.4) * 1e6 * 100 / 40
+
+
+def twiddle_precompute_ms(log_size, stream, reps=5):
+    """Device time of PolyOps::precompute_twiddles for CanonicCoset(log_size)
+    .half_coset into preallocated buffers (CUDA events, after one warm-up)."""
+    import ctypes
+    import torch
+    from stwo_b200 import B200Backend, DeviceColumn, ffi
+    from stwo_b200.backend import canonic_half_coset
+    be = B200Backend(stream.cuda_stream)
+    init, lg = canonic_half_coset(log_size)
+    tw, itw = DeviceColumn(1 << lg, stream.cuda_stream), DeviceColumn(1 << lg, stream.cuda_stream)
+
+    def run():
+        ffi.call("stwo_b200_precompute_twiddles", ctypes.c_uint64(init), ctypes.c_uint32(lg), ctypes.c_void_p(tw.ptr),
+                 ctypes.c_void_p(itw.ptr), be.stream)
+
+    run()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        a.record(stream)
+        for _ in range(reps):
+            run()
+        b.record(stream)
+    torch.cuda.synchronize()
+    return a.elapsed_time(b) / reps
 
 
 def run_prove_b200(args, world, rank, local):
@@ -867,6 +895,10 @@ def run_prove_b200(args, world, rank, local):
         if ph.get(k, 0) > 0:
             rate = amt / (ph[k] * 1e-3)
             phase_frac[k] = rate / (hbm_peak * 1e9) if kd == "hbm" else rate / probe_rate
+    # The prover computes its twiddle tree (CanonicCoset(log_n + blowup + 1)
+    # .half_coset) once at creation and keeps it resident, outside the timed
+    # proofs; its device time is reported beside them.
+    tw_ms = twiddle_precompute_ms(spec["log_n"] + spec["log_blowup"] + 1, stream)
     # the CPU baseline (and the byte comparison with it) is measured at N = 1 only
     cpu_s, cpu_proof, cpu_threads = cpu_prove(spec, a_host, b_host) if world == 1 else (None, None, None)
     srt = sorted(step_ms)
@@ -895,6 +927,7 @@ def run_prove_b200(args, world, rank, local):
         "fft_issue_roofline": fft_issue,
         "phase_ms": phase_ms,
         "phase_roofline_frac": phase_frac,
+        "twiddle_precompute_ms": tw_ms,
         "blake2s_probe_compressions_per_s": probe_rate,
         "butterfly_probe_per_s": bfly_rate,
         "proof_bytes": len(proof),
