@@ -386,6 +386,21 @@ def test_lifted_leaves_stages(be, oracle, logs, L, m31):
         assert (layer_to_host(own[k]) == ref[k]).all(), k
 
 
+def test_lifted_leaves_reject_bad_columns(be):
+    # build_leaves and build_leaves_layers take columns already sorted by
+    # length, none larger than the lifting size
+    from stwo_b200 import DeviceBuffer
+    from stwo_b200.ffi import B200Error
+    r = rng(11)
+    cols = [DeviceColumn.from_host(rand_col(r, l)) for l in (5, 3)]
+    with pytest.raises(B200Error, match="sorted"):
+        be.build_leaves(cols, 6)
+    with pytest.raises(B200Error, match="exceeds"):
+        be.build_leaves(cols[::-1], 4)
+    with pytest.raises(B200Error, match="sorted"):
+        be.build_leaves_layers(cols, 6, [DeviceBuffer(32 << k) for k in range(7)])
+
+
 def test_build_leaves_and_next_layer(be, oracle):
     r = rng(5)
     vals = [rand_col(r, l) for l in [3, 5, 5, 8]]
