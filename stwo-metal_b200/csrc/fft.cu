@@ -514,6 +514,30 @@ __device__ __forceinline__ void warp_phase_hi(uint32_t (&v)[32], const uint32_t*
   }
 }
 
+// Layers 5..T-1 on v[j] = row 32 j + b (see warp_phase_hi), T = 6..10.  Below
+// 10 layers each butterfly reads its twiddle from shared memory directly.
+template <bool INV, int T>
+__device__ __forceinline__ void warp_phase_hi_short(uint32_t (&v)[32], const uint32_t* __restrict__ tws) {
+  if constexpr (T == 10) {
+    warp_phase_hi<INV>(v, tws);
+    return;
+  }
+  constexpr int NK = T - 5;
+#pragma unroll
+  for (int kk = 0; kk < NK; kk++) {
+    const int k = INV ? kk : NK - 1 - kk;  // bit of j
+    const uint32_t* tl = tws + (1024u - (1024u >> (5 + k)));
+#pragma unroll
+    for (int j = 0; j < 32; j++) {
+      if (j & (1 << k)) continue;
+      const uint32_t t = tl[j >> (k + 1)];
+      if (INV)
+        ibfly2(v[j], v[j | (1 << k)], t);
+      else
+        bfly2(v[j], v[j | (1 << k)], t);
+    }
+  }
+}
 // Stages the 1023 twiddles of a 10-layer tile position (as fft_pass_kernel),
 // doubled for bfly2 / ibfly2: slot s of the table holds layer
 // lam = clz(1023 - s) - 22, entry s - (1024 - 2^(10 - lam)).  Thread t holds
@@ -642,7 +666,11 @@ __device__ __forceinline__ void lane_major_to_tile(uint32_t* buf, uint32_t lane,
 // lane-major through its staged tile, runs layers 4..0 and writes the lane's
 // 32 consecutive words back into its own line of the staged tile, from
 // where one 128-byte bulk copy per lane stores it.
-template <bool INV>
+//   T < 10 (6..9): a pass of T layers.  The 1024 words are 2^(10-T) tiles of
+// the pass side by side; layer lam < T pairs the same words and takes the
+// same twiddle (word >> (lam + 1) of the layer) as in the 10-layer pass, so
+// the kernel runs only the row-major layers 5..T-1.
+template <bool INV, int T>
 __global__ void __launch_bounds__(256, 4) fft_warp_contig_kernel(FftPass p, FftCols cols) {
   extern __shared__ __align__(16) uint32_t smem[];
   uint32_t* tws = smem;
@@ -683,14 +711,14 @@ __global__ void __launch_bounds__(256, 4) fft_warp_contig_kernel(FftPass p, FftC
         else
           tile_prefetch(cols.src[cn] + base, buf, lane);
       }
-      warp_phase_hi<true>(v, tws);
+      warp_phase_hi_short<true, T>(v, tws);
 #pragma unroll
       for (int j = 0; j < 32; j++) dst[base + j * 32 + lane] = scale != 1u ? m31_mul(v[j], scale) : v[j];
     } else {
       const uint32_t* __restrict__ sp = cols.src[c] + base + lane;
 #pragma unroll
       for (int j = 0; j < 32; j++) v[j] = __ldg(sp + 32 * j);
-      warp_phase_hi<false>(v, tws);
+      warp_phase_hi_short<false, T>(v, tws);
       bulk_wait_read();  // the previous tile's bulk stores have read this warp's lines
       __syncwarp();
 #pragma unroll
@@ -812,27 +840,6 @@ __global__ void __launch_bounds__(256, 4) fft_warp_strided_kernel(FftPass p, Fft
 template <int T>
 __device__ __forceinline__ uint64_t short_row_off(uint32_t r, uint32_t L0) {
   return ((uint64_t)(r & ((1u << T) - 1)) << L0) + ((uint64_t)(r >> T) << 3);
-}
-// Layers 5..T-1 on v[j] = row 32 j + b (see warp_phase_hi).
-template <bool INV, int T>
-__device__ __forceinline__ void warp_phase_hi_short(uint32_t (&v)[32], const uint32_t* __restrict__ tws) {
-  constexpr int NK = T - 5;
-#pragma unroll
-  for (int kk = 0; kk < NK; kk++) {
-    const int k = INV ? kk : NK - 1 - kk;  // bit of j
-    const uint32_t* tl = tws + (1024u - (1024u >> (5 + k)));
-    uint32_t t[16];
-#pragma unroll
-    for (int m = 0; m < (1 << (4 - k)); m++) t[m] = tl[m];
-#pragma unroll
-    for (int j = 0; j < 32; j++) {
-      if (j & (1 << k)) continue;
-      if (INV)
-        ibfly2(v[j], v[j | (1 << k)], t[j >> (k + 1)]);
-      else
-        bfly2(v[j], v[j | (1 << k)], t[j >> (k + 1)]);
-    }
-  }
 }
 // The tables of layers 0..T-1 in the slots of stage_tws10 (layer lam at
 // 1024 - 2^(10 - lam), 2^(9 - lam) entries), entry e holding twiddle
@@ -1226,20 +1233,35 @@ static int launch_group_contig(const FftPass& q, const FftCols& cols, uint64_t t
   return STWO_B200_OK;
 }
 
+// A contiguous pass of T = 6..10 layers over `chunks` 1024-word chunks.
+template <bool INV, int T>
+static int launch_warp_contig(const FftPass& q, const FftCols& cols, uint64_t chunks, size_t nc, cudaStream_t s,
+                              char* err, size_t err_len) {
+  constexpr size_t smem = (1024 + kWarpCols * kTileWords) * sizeof(uint32_t);
+  static std::atomic<uint32_t> attr{0};
+  STWO_CUDA_TRY(ensure_smem_limit(fft_warp_contig_kernel<INV, T>, (int)smem, attr));
+  // up to 16 column groups per block: fewer twiddle stagings while the grid
+  // still has six waves of blocks
+  const uint32_t groups = (uint32_t)((nc + kWarpCols - 1) / kWarpCols);
+  FftPass qq = q;
+  qq.cpb = std::max<uint32_t>(1, std::min<uint32_t>(16, (uint32_t)((chunks * groups) / (148 * 4 * 6))));
+  dim3 grid((unsigned)chunks, (unsigned)((groups + qq.cpb - 1) / qq.cpb));
+  fft_warp_contig_kernel<INV, T><<<grid, 32 * kWarpCols, smem, s>>>(qq, cols);
+  STWO_CHECK_LAUNCH();
+  return STWO_B200_OK;
+}
+
 template <bool INV>
 static int launch_warp_pass(const FftPass& q, const FftCols& cols, uint64_t tiles, size_t nc, cudaStream_t s,
                             char* err, size_t err_len) {
   if (q.C == 0) {
-    constexpr size_t smem = (1024 + kWarpCols * kTileWords) * sizeof(uint32_t);
-    static std::atomic<uint32_t> attr{0};
-    STWO_CUDA_TRY(ensure_smem_limit(fft_warp_contig_kernel<INV>, (int)smem, attr));
-    // up to 16 column groups per block: fewer twiddle stagings while the grid
-    // still has six waves of blocks
-    const uint32_t groups = (uint32_t)((nc + kWarpCols - 1) / kWarpCols);
-    FftPass qq = q;
-    qq.cpb = std::max<uint32_t>(1, std::min<uint32_t>(16, (uint32_t)((tiles * groups) / (148 * 4 * 6))));
-    dim3 grid((unsigned)tiles, (unsigned)((groups + qq.cpb - 1) / qq.cpb));
-    fft_warp_contig_kernel<INV><<<grid, 32 * kWarpCols, smem, s>>>(qq, cols);
+    switch (q.T) {
+      case 6: return launch_warp_contig<INV, 6>(q, cols, tiles >> 4, nc, s, err, err_len);
+      case 7: return launch_warp_contig<INV, 7>(q, cols, tiles >> 3, nc, s, err, err_len);
+      case 8: return launch_warp_contig<INV, 8>(q, cols, tiles >> 2, nc, s, err, err_len);
+      case 9: return launch_warp_contig<INV, 9>(q, cols, tiles >> 1, nc, s, err, err_len);
+      default: return launch_warp_contig<INV, 10>(q, cols, tiles, nc, s, err, err_len);
+    }
   } else {
     constexpr size_t smem = (1024 + kXchWords) * sizeof(uint32_t);
     static std::atomic<uint32_t> attr10{0}, attr11{0}, attr{0};
@@ -1357,8 +1379,11 @@ static int launch_pass(const FftPass& p, const std::vector<const uint32_t*>& src
     q.n_cols = (uint32_t)nc;
     dim3 grid((unsigned)tiles, (unsigned)((nc + cpb - 1) / cpb));
     int rc;
-    const bool warp_contig = p.T == 10 && p.C == 0 && p.layer0 == 0 && aligned && p.src_mask == ~0ull &&
-                             p.src_len == ~0ull;
+    // 6..9 layers: whole passes over domains of at least 1024 words (a block
+    // covers 2^(10 - T) tiles)
+    const bool warp_contig = p.C == 0 && p.layer0 == 0 && aligned && p.src_mask == ~0ull && p.src_len == ~0ull &&
+                             (p.T == 10 || (p.T >= 6 && p.T < 10 && total_log >= 10 && p.log_domain >= 10 &&
+                                            tile_cnt == 0 && tile0 == 0));
     const bool warp_strided = p.T == 10 && p.C == 3 && p.layer0 >= 3;
     // whole passes only: its blocks cover 2^(10 - T) tiles each
     const bool warp_short = p.C == 3 && p.T >= 6 && p.T <= 9 && p.layer0 + p.T >= 13 && tile_cnt == 0 &&

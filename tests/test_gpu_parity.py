@@ -209,6 +209,36 @@ def test_interpolate_evaluate_many_columns(be, oracle, big_tree):
         assert (outs[k].to_host() == oracle.evaluate(co, 21, tw)).all(), k
 
 
+@pytest.mark.parametrize("log_n,plan", [(13, [7, 6]), (14, [6, 8]), (15, [9, 6]), (16, [6, 10]), (12, [8, 4]),
+                                        (11, [9, 2]), (10, [6, 4])])
+def test_short_contiguous_passes(be, oracle, big_tree, log_n, plan):
+    # First (inverse) / last (forward) passes of 6..9 layers on the contiguous
+    # warp kernel, 2^(10 - T) tiles per 1024-word warp tile, for natural- and
+    # bit-reversed-order interpolation and evaluations at blowups 0..2.
+    from stwo_b200 import fft_get_plan, fft_set_plan
+    tree, tw, itw = big_tree
+    old = fft_get_plan(log_n)
+    fft_set_plan(log_n, plan)
+    try:
+        r = rng(3500 + log_n + plan[0])
+        vals = [rand_col(r, log_n) for _ in range(9)]
+        vals[2][::3] = P
+        cols = [DeviceColumn.from_host(v) for v in vals]
+        nat = [DeviceColumn(1 << log_n) for _ in vals]
+        be.interpolate_natural_into([DeviceColumn.from_host(oracle.bit_reverse(v)) for v in vals], nat, tree)
+        be.interpolate_columns(cols, tree)
+        for blowup in (0, 1, 2):
+            evs = be.evaluate_polynomials(cols, blowup, tree)
+            for k, v in enumerate(vals):
+                co = oracle.interpolate(v, itw)
+                if blowup == 0:
+                    assert (cols[k].to_host() == co).all(), k
+                    assert (nat[k].to_host() == co).all(), k
+                assert (evs[k].to_host() == oracle.evaluate(co, log_n + blowup, tw)).all(), (k, blowup)
+    finally:
+        fft_set_plan(log_n, old)
+
+
 @pytest.mark.parametrize("log_n,plan", [(16, [10, 6]), (17, [10, 7]), (18, [10, 8]), (19, [10, 9]), (19, [11, 8]),
                                         (15, [7, 8]), (13, [7, 6]), (14, [5, 9])])
 def test_short_strided_passes(be, oracle, big_tree, log_n, plan):
