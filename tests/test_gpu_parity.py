@@ -209,6 +209,49 @@ def test_interpolate_evaluate_many_columns(be, oracle, big_tree):
         assert (outs[k].to_host() == oracle.evaluate(co, 21, tw)).all(), k
 
 
+def candidate_splits(n):
+    """The pass splits the committer's autotuner times for an n-layer FFT
+    (every one of them can end up in the plan table)."""
+    c = [[n]] if n <= 12 else []
+    c += [[a, n - a] for a in range(3, min(12, n - 1) + 1) if 1 <= n - a <= 12]
+    if n >= 15:
+        for a in range(max(3, n // 3 - 1), min(12, n // 3 + 1) + 1):
+            for b in range(max(1, (n - a) // 2 - 1), min(12, (n - a) // 2 + 1) + 1):
+                if 1 <= n - a - b <= 12:
+                    c.append([a, b, n - a - b])
+    return c
+
+
+@pytest.mark.parametrize("log_n", [13, 14, 16])
+def test_every_candidate_split(be, oracle, big_tree, log_n):
+    # Whatever split the autotuner keeps, each pass shape it implies (warp,
+    # group or tile kernels, contiguous and strided, every layer offset) gives
+    # the oracle's coefficients and blowup-1 and -2 evaluations; 9 columns
+    # leave a partial column group.
+    from stwo_b200 import fft_get_plan, fft_set_plan
+    tree, tw, itw = big_tree
+    r = rng(3600 + log_n)
+    vals = [rand_col(r, log_n) for _ in range(9)]
+    vals[4][::7] = P
+    co = [oracle.interpolate(v, itw) for v in vals]
+    ev = {b: [oracle.evaluate(c, log_n + b, tw) for c in co] for b in (1, 2)}
+    old = fft_get_plan(log_n)
+    try:
+        for plan in candidate_splits(log_n):
+            fft_set_plan(log_n, plan)
+            cols = [DeviceColumn.from_host(v) for v in vals]
+            for b in (1, 2):
+                outs = [DeviceColumn(1 << (log_n + b)) for _ in vals]
+                be.interpolate_evaluate_into(cols if b == 1 else None, [DeviceColumn(1 << log_n) for _ in vals]
+                                             if b == 1 else cols, b, tree, outs)
+                for k in range(len(vals)):
+                    assert (outs[k].to_host() == ev[b][k]).all(), (plan, b, k)
+            for k in range(len(vals)):
+                assert (cols[k].to_host() == co[k]).all(), (plan, k)
+    finally:
+        fft_set_plan(log_n, old)
+
+
 @pytest.mark.parametrize("log_n,plan", [(13, [7, 6]), (14, [6, 8]), (15, [9, 6]), (16, [6, 10]), (12, [8, 4]),
                                         (11, [9, 2]), (10, [6, 4])])
 def test_short_contiguous_passes(be, oracle, big_tree, log_n, plan):
