@@ -222,17 +222,17 @@ def candidate_splits(n):
     return c
 
 
-@pytest.mark.parametrize("log_n", [13, 14, 16])
-def test_every_candidate_split(be, oracle, big_tree, log_n):
+@pytest.mark.parametrize("log_n,n_cols", [(13, 9), (14, 9), (16, 9), (19, 5), (22, 3)])
+def test_every_candidate_split(be, oracle, big_tree, log_n, n_cols):
     # Whatever split the autotuner keeps, each pass shape it implies (warp,
     # group or tile kernels, contiguous and strided, every layer offset) gives
     # the oracle's coefficients and blowup-1 and -2 evaluations; 9 columns
-    # leave a partial column group.
+    # leave a partial column group (fewer columns at logs 19 and 22).
     from stwo_b200 import fft_get_plan, fft_set_plan
     tree, tw, itw = big_tree
     r = rng(3600 + log_n)
-    vals = [rand_col(r, log_n) for _ in range(9)]
-    vals[4][::7] = P
+    vals = [rand_col(r, log_n) for _ in range(n_cols)]
+    vals[n_cols // 2][::7] = P
     co = [oracle.interpolate(v, itw) for v in vals]
     ev = {b: [oracle.evaluate(c, log_n + b, tw) for c in co] for b in (1, 2)}
     old = fft_get_plan(log_n)
