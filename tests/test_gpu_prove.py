@@ -61,6 +61,25 @@ def test_proof_of_work_and_last_layer_forms(oracle, pow_bits, last):
     assert prover.prove(DeviceColumn.from_host(a), DeviceColumn.from_host(b)) == ref
 
 
+@pytest.mark.parametrize("plan", [[6, 10], [8, 8], [7, 9], [4, 6, 6]])
+def test_proof_under_other_pass_splits(oracle, plan):
+    # The prover's transforms follow the process-wide plan table: the log-16
+    # trace transforms under splits other than the default [10, 6] --
+    # contiguous 6..8-layer warp passes, strided passes at layer offsets 6..8,
+    # three passes -- give the oracle's proof bytes.
+    from stwo_b200 import fft_get_plan, fft_set_plan
+    log_n, cols = 16, 8
+    a, b = oracle.wide_fib_inputs(log_n, 900 + sum(plan))
+    ref = oracle.prove_wide_fib(oracle.wide_fib_config(log_n, cols), a, b)
+    old = fft_get_plan(log_n)
+    fft_set_plan(log_n, plan)
+    try:
+        prover = WideFibProver(wide_fib_config(log_n, cols))
+        assert prover.prove(DeviceColumn.from_host(a), DeviceColumn.from_host(b)) == ref
+    finally:
+        fft_set_plan(log_n, old)
+
+
 def test_prover_reuse_is_deterministic(oracle):
     # Resident buffers are reused across proofs: a second proof of other
     # inputs, then the first inputs again, reproduce the oracle bytes.
